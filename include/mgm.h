@@ -1,0 +1,210 @@
+/*
+ * mgm.h -- C ABI of the B200 (sm_100a) meshless RBF-FD multigrid hot path.
+ *
+ * Plain C types only (no torch, no C++), so any host language that can call C
+ * can bind it (ctypes, cgo, JNI, N-API).  Every entry point returns an int
+ * status (MGM_OK or an MGM_ERR_* code) unless it returns a handle; the text of
+ * the last failure in the calling thread is available from mgm_last_error().
+ *
+ * Layout conventions at the boundary (host memory):
+ *   - node arrays: length n, in the level's node order;
+ *   - stencil arrays (cloud indices and operator weights): row-major [n][k],
+ *     i.e. the reference's jagged `int**` / `double**` rows laid end to end;
+ *   - boundary tags: one byte per node, non-zero = boundary.
+ *
+ * Each declaration cites the reference function it replaces
+ * (Multigrid_meshless, path within that project : line).
+ */
+#ifndef MGM_H
+#define MGM_H
+
+#if defined(__GNUC__)
+#define MGM_API __attribute__((visibility("default")))
+#else
+#define MGM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MGM_OK 0
+#define MGM_ERR_CUDA 1      /* a CUDA call failed (message holds the CUDA error) */
+#define MGM_ERR_ARG 2       /* invalid argument or input (e.g. disconnected stencil graph) */
+#define MGM_ERR_DIVERGED 3  /* NaN/Inf or growth in a residual */
+#define MGM_ERR_TIMEOUT 4   /* a bounded device-side wait ran out */
+#define MGM_ERR_NOMEM 5     /* device allocation failed */
+#define MGM_ERR_STATE 6     /* call made in the wrong state (e.g. before set-up) */
+
+/* ------------------------------------------------------------------ */
+/* Diagnostics                                                         */
+/* ------------------------------------------------------------------ */
+MGM_API const char *mgm_last_error(void);
+/* Number of kernels this library has launched in the calling process. */
+MGM_API long long mgm_kernel_launches(void);
+MGM_API int mgm_version(void);
+
+/* ------------------------------------------------------------------ */
+/* Stateless set-up operations: host arrays in, host arrays out.       */
+/* Each call uploads its inputs, runs its kernels and downloads the    */
+/* result (the reference's own call shape).                            */
+/* ------------------------------------------------------------------ */
+
+/* find_cloud_index (header_files/kdtree_functions.h:113-151).
+ * Nodes i >= nb: the k nearest nodes (self first).  Nodes i < nb: cloud[i][0]
+ * = i followed by the k-1 nearest nodes whose btag is 0.  Distances are the
+ * reference's sqrt(((dx*dx)+dy*dy)+dz*dz) (kdtree_functions.h:28-35, 84);
+ * exactly equal distances are ordered by lower node index. */
+MGM_API int mgm_knn_cloud(int n, int nb, int dim, const double *x, const double *y, const double *z,
+                  const unsigned char *btag, int k, int *cloud);
+
+/* find_nearest_point (header_files/kdtree_functions.h:153-175) with
+ * num_cloud_points = 1: for each node of set 1, the nearest node of set 2. */
+MGM_API int mgm_nearest_points(int n1, const double *x1, const double *y1, const double *z1,
+                       int n2, const double *x2, const double *y2, const double *z2, int dim, int *nearest);
+
+/* rcm_reordering_with_boundarynodes (header_files/mesh_functions.h:774-872):
+ * FIFO breadth-first order from node 0 over cloud slots 1..k-1.  queue1[i] =
+ * old index of new node i.  Returns MGM_ERR_ARG if the stencil graph is
+ * disconnected (the reference leaves the tail of its queue uninitialised). */
+MGM_API int mgm_bfs_order(int n, int k, const int *cloud, int *queue1);
+
+/* The permutation step of rcm_reordering_with_boundarynodes
+ * (mesh_functions.h:821-855), in place: coordinates, normals, boundary tags
+ * and cloud rows gathered through queue1, cloud entries renumbered. */
+MGM_API int mgm_apply_order(int n, int k, const int *queue1, double *x, double *y, double *z,
+                    double *nx, double *ny, double *nz, unsigned char *btag, int *cloud);
+
+/* correct_normal_directions (header_files/mesh_functions.h:478-527), in place. */
+MGM_API int mgm_correct_normals(int n, int k, const double *x, const double *y, const double *z,
+                        const unsigned char *btag, const int *cloud, double *nx, double *ny, double *nz);
+
+/* calculate_avg_dx (header_files/mesh_functions.h:895-910). */
+MGM_API int mgm_avg_dx(int n, int k, int dim, const double *x, const double *y, const double *z,
+               const unsigned char *btag, const int *cloud, double *d_avg);
+
+/* create_derivative_matrices (header_files/rbf.h:401-421) including
+ * create_laplacian_for_Poisson (rbf.h:382-399).  Outputs [n][k]; Dz is only
+ * written when dim == 3 (may be NULL otherwise). */
+MGM_API int mgm_derivative_weights(int n, int k, int dim, int phs, int poly_degree,
+                           const double *x, const double *y, const double *z,
+                           const double *nx, const double *ny, const double *nz,
+                           const unsigned char *btag, const int *cloud,
+                           double *Dx, double *Dy, double *Dz, double *lap, double *lapP);
+
+/* create_restriction_matrix / create_prolongation_matrix
+ * (header_files/mesh_functions.h:533-600, 602-670): RBF interpolation weights
+ * [nt][ks] from the source level's cloud around src_pt[i] to target node i.
+ * Rows i < rows_from stay zero (the reference starts at num_boundary_nodes,
+ * :563, :633); with only_interior != 0, rows with a boundary tag stay zero
+ * instead and every other row is filled. */
+MGM_API int mgm_transfer_weights(int nt, const double *tx, const double *ty, const double *tz,
+                         const unsigned char *tbtag, const int *src_pt, int rows_from, int only_interior,
+                         int ns, int ks, int dim, int phs, int poly_degree_src,
+                         const double *sx, const double *sy, const double *sz, const int *scloud, double *W);
+
+/* multiply_sparse_matrix_vector_gpu (header_files/mat_lib.h:80-89):
+ * out[i] = sum_j D[i][j] * f[cloud[i][j]], j ascending, no fused multiply-add
+ * (bit-identical to the reference's C build). */
+MGM_API int mgm_spmv(int n, int k, const double *D, const int *cloud, const double *f, double *out);
+
+/* ------------------------------------------------------------------ */
+/* Device-resident solver context (copyin_*_to_gpu + the time loop)    */
+/* ------------------------------------------------------------------ */
+typedef struct mgm_ctx mgm_ctx;
+
+/* Creates a context on the current CUDA device.  dim 2 or 3, phs the
+ * polyharmonic exponent (parameters.phs_degree, structures.h:19). */
+MGM_API mgm_ctx *mgm_create(int dim, int phs_degree, int num_levels);
+MGM_API void mgm_destroy(mgm_ctx *ctx);
+
+/* Raw level input (the state read_PointStructure leaves, mesh_functions.h:172-476):
+ * boundary nodes first (indices < nb), no corner nodes. */
+MGM_API int mgm_set_level(mgm_ctx *ctx, int lev, int n, int nb, const double *x, const double *y, const double *z,
+                  const double *nx, const double *ny, const double *nz, const unsigned char *btag,
+                  int poly_degree, int k);
+
+#define MGM_SETUP_REFERENCE_TRANSFER 1 /* also build the reference's transfer rows (rows >= nb only) */
+/* Runs, on the GPU, read_complete_mesh_data's pipeline after the reader
+ * (mesh_functions.h:914-928: kNN clouds, breadth-first reorder, normals,
+ * average spacing, nearest points, restriction/prolongation weights) and
+ * create_derivative_matrices on every level (rbf.h:401-421), then packs the
+ * ELL operators and prepares the Poisson solver (coarsest-level inverse,
+ * smoother bounds).  flags: MGM_SETUP_*. */
+MGM_API int mgm_setup(mgm_ctx *ctx, int flags);
+
+MGM_API int mgm_level_size(mgm_ctx *ctx, int lev, int *n, int *nb, int *k, int *num_poly_terms);
+MGM_API int mgm_level_d_avg(mgm_ctx *ctx, int lev, double *d_avg);
+
+/* Downloads a level after set-up (arrays sized by mgm_level_size; [n][k] row-major).
+ * Any pointer may be NULL to skip it.  Dz only in 3D. */
+MGM_API int mgm_get_geometry(mgm_ctx *ctx, int lev, double *x, double *y, double *z, double *nx, double *ny, double *nz,
+                     unsigned char *btag, int *cloud);
+MGM_API int mgm_get_operators(mgm_ctx *ctx, int lev, double *Dx, double *Dy, double *Dz, double *lap, double *lapP);
+/* restriction_points / prolongation_points and the reference-semantics
+ * restr_mat ([n][k of level lev-1]) / prol_mat ([n][k of level lev+1]). */
+MGM_API int mgm_get_transfer(mgm_ctx *ctx, int lev, int *rpts, int *ppts, double *restr, double *prol);
+
+/* Flow parameters (read_flow_parameters, mesh_functions.h:37-100: rho = 1,
+ * mu = rho/Re, nu = mu/rho).  dt <= 0 computes calculate_dt
+ * (general_functions.h:34-41) from level 0's average spacing. */
+MGM_API int mgm_set_flow(mgm_ctx *ctx, double Re, double courant, float omega, int num_relax, int num_vcycles, double dt);
+MGM_API int mgm_get_dt(mgm_ctx *ctx, double *dt);
+
+/* Level-0 fields.  which: MGM_FIELD_*.  Host arrays of length n(level). */
+#define MGM_FIELD_U 0
+#define MGM_FIELD_V 1
+#define MGM_FIELD_W 2
+#define MGM_FIELD_P 3
+#define MGM_FIELD_U_NEW 4
+#define MGM_FIELD_V_NEW 5
+#define MGM_FIELD_W_NEW 6
+#define MGM_FIELD_RES 10
+#define MGM_FIELD_SOURCE 11
+#define MGM_FIELD_DPDN 12
+MGM_API int mgm_set_field(mgm_ctx *ctx, int lev, int which, const double *values);
+MGM_API int mgm_get_field(mgm_ctx *ctx, int lev, int which, double *values);
+
+/* Boundary/initial conditions on level 0: MGM_BC_LID (init/init_LDC.c:16-44)
+ * or MGM_BC_TAYLOR_COUETTE (init/init_TC.c:17-54).  Fields are zeroed first. */
+#define MGM_BC_LID 0
+#define MGM_BC_TAYLOR_COUETTE 1
+MGM_API int mgm_apply_bc(mgm_ctx *ctx, int kind);
+
+/* Poisson solve modes */
+#define MGM_MODE_REFERENCE 0   /* multigrid_Poisson_solver semantics, fixed num_vcycles (Jacobi-order sweeps) */
+#define MGM_MODE_FP64 1        /* convergent V-cycle preconditioned FGMRES, all FP64 */
+#define MGM_MODE_FP32_IR 2     /* same, V-cycle in FP32 inside the FP64 FGMRES refinement */
+
+/* fractional_step_explicit (header_files/fractional_step_solver.h:47-71):
+ * momentum, divergence, boundary dp/dn, Poisson solve (mode), velocity
+ * correction; *steady_err receives sqrt(sum |du|^2 / n).  For the solve modes
+ * other than MGM_MODE_REFERENCE the Poisson solve runs to the relative
+ * residual set by mgm_set_solver. */
+MGM_API int mgm_step(mgm_ctx *ctx, int mode, double *steady_err);
+
+/* Solver controls for MGM_MODE_FP64 / MGM_MODE_FP32_IR. */
+MGM_API int mgm_set_solver(mgm_ctx *ctx, double rel_tol, int max_iters, int cheb_degree, double cheb_ratio);
+/* Statistics of the last Poisson solve: outer iterations (V-cycles) and the
+ * true relative residual ||b - A p|| / ||b|| over rows != 0 (FP64). */
+MGM_API int mgm_last_solve(mgm_ctx *ctx, int *iters, double *rel_res);
+
+/* The fractional step's parts, on the device state
+ * (fractional_step_solver.h:73-275).  mass_res may be NULL. */
+MGM_API int mgm_intermediate_velocity(mgm_ctx *ctx);
+MGM_API int mgm_mass_residual(mgm_ctx *ctx);
+MGM_API int mgm_poisson(mgm_ctx *ctx, int mode);
+MGM_API int mgm_update_velocity(mgm_ctx *ctx, double *mass_res);
+
+/* Poisson solve of A p = b on level 0 (A = lap_Poison with row 0 replaced by
+ * p[0] = 0), b given on the host (b[0] and boundary rows as given), p used as
+ * the initial guess and returned.  The pinned row's rhs is forced to 0. */
+MGM_API int mgm_solve_poisson(mgm_ctx *ctx, int mode, const double *b, double *p, int *iters, double *rel_res);
+
+/* Synchronises the context's stream. */
+MGM_API int mgm_sync(mgm_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,101 @@
+"""ctypes binding of libmgm.so (the C ABI declared in include/mgm.h).
+
+The library is loaded from this package directory.  There is no CPU
+fallback: if the shared library is missing or no CUDA device is present,
+calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmgm.so")
+
+dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+vp = C.c_void_p
+
+# status codes (include/mgm.h)
+MGM_OK, MGM_ERR_CUDA, MGM_ERR_ARG, MGM_ERR_DIVERGED, MGM_ERR_TIMEOUT, MGM_ERR_NOMEM, MGM_ERR_STATE = range(7)
+MODE_REFERENCE, MODE_FP64, MODE_FP32_IR = 0, 1, 2
+BC_LID, BC_TAYLOR_COUETTE = 0, 1
+SETUP_REFERENCE_TRANSFER = 1
+FIELD = {"u": 0, "v": 1, "w": 2, "p": 3, "u_new": 4, "v_new": 5, "w_new": 6, "res": 10, "source": 11, "dpdn": 12}
+
+# every exported entry point and its argument types (restype int unless noted)
+SIGNATURES = {
+    "mgm_last_error": ([], C.c_char_p),
+    "mgm_kernel_launches": ([], C.c_longlong),
+    "mgm_version": ([], C.c_int),
+    "mgm_knn_cloud": ([C.c_int, C.c_int, C.c_int, dp, dp, dp, u8p, C.c_int, ip], C.c_int),
+    "mgm_nearest_points": ([C.c_int, dp, dp, dp, C.c_int, dp, dp, dp, C.c_int, ip], C.c_int),
+    "mgm_bfs_order": ([C.c_int, C.c_int, ip, ip], C.c_int),
+    "mgm_apply_order": ([C.c_int, C.c_int, ip, dp, dp, dp, dp, dp, dp, u8p, ip], C.c_int),
+    "mgm_correct_normals": ([C.c_int, C.c_int, dp, dp, dp, u8p, ip, dp, dp, dp], C.c_int),
+    "mgm_avg_dx": ([C.c_int, C.c_int, C.c_int, dp, dp, dp, u8p, ip, C.POINTER(C.c_double)], C.c_int),
+    "mgm_derivative_weights": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, dp, dp, u8p, ip,
+                                dp, dp, vp, dp, dp], C.c_int),
+    "mgm_transfer_weights": ([C.c_int, dp, dp, dp, u8p, ip, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                              C.c_int, dp, dp, dp, ip, dp], C.c_int),
+    "mgm_spmv": ([C.c_int, C.c_int, dp, ip, dp, dp], C.c_int),
+    "mgm_create": ([C.c_int, C.c_int, C.c_int], vp),
+    "mgm_destroy": ([vp], None),
+    "mgm_set_level": ([vp, C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, dp, dp, u8p, C.c_int, C.c_int], C.c_int),
+    "mgm_setup": ([vp, C.c_int], C.c_int),
+    "mgm_level_size": ([vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                        C.POINTER(C.c_int)], C.c_int),
+    "mgm_level_d_avg": ([vp, C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "mgm_get_geometry": ([vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
+    "mgm_get_operators": ([vp, C.c_int, vp, vp, vp, vp, vp], C.c_int),
+    "mgm_get_transfer": ([vp, C.c_int, vp, vp, vp, vp], C.c_int),
+    "mgm_set_flow": ([vp, C.c_double, C.c_double, C.c_float, C.c_int, C.c_int, C.c_double], C.c_int),
+    "mgm_get_dt": ([vp, C.POINTER(C.c_double)], C.c_int),
+    "mgm_set_field": ([vp, C.c_int, C.c_int, dp], C.c_int),
+    "mgm_get_field": ([vp, C.c_int, C.c_int, dp], C.c_int),
+    "mgm_apply_bc": ([vp, C.c_int], C.c_int),
+    "mgm_step": ([vp, C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "mgm_set_solver": ([vp, C.c_double, C.c_int, C.c_int, C.c_double], C.c_int),
+    "mgm_last_solve": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
+    "mgm_intermediate_velocity": ([vp], C.c_int),
+    "mgm_mass_residual": ([vp], C.c_int),
+    "mgm_poisson": ([vp, C.c_int], C.c_int),
+    "mgm_update_velocity": ([vp, C.POINTER(C.c_double)], C.c_int),
+    "mgm_solve_poisson": ([vp, C.c_int, dp, dp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
+    "mgm_sync": ([vp], C.c_int),
+}
+
+_LIB = None
+
+
+class MgmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[mgm status {code}] {msg}")
+        self.code = code
+
+
+def load(path: str = LIB_PATH):
+    """Loads libmgm.so (once).  Raises if it is missing: there is no fallback."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: build it with `python -m multigrid_meshless_b200.build`")
+        lib = C.CDLL(path)
+        for name, (args, res) in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.argtypes = args
+            f.restype = res
+        _LIB = lib
+    return _LIB
+
+
+def check(status: int):
+    if status != MGM_OK:
+        raise MgmError(status, load().mgm_last_error().decode(errors="replace"))
+
+
+def ptr(a):
+    return None if a is None else a.ctypes.data

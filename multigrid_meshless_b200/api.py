@@ -1,0 +1,253 @@
+"""Python mirror of the reference's call surface, on top of the C ABI.
+
+Function names follow the reference (Multigrid_meshless header_files/*.h):
+
+  find_cloud_index            kdtree_functions.h:113-151   -> knn_cloud()
+  find_nearest_point          kdtree_functions.h:153-175   -> nearest_points()
+  rcm_reordering_with_boundarynodes  mesh_functions.h:774-872 -> bfs_order(), apply_order()
+  correct_normal_directions   mesh_functions.h:478-527     -> correct_normals()
+  calculate_avg_dx            mesh_functions.h:895-910     -> avg_dx()
+  create_derivative_matrices  rbf.h:401-421                -> derivative_weights()
+  create_{restriction,prolongation}_matrix  mesh_functions.h:533-670 -> transfer_weights()
+  multiply_sparse_matrix_vector_gpu  mat_lib.h:80-89       -> spmv()
+  fractional_step_explicit    fractional_step_solver.h:47-71 -> Multigrid.step()
+
+Arrays at this boundary use the reference's layout: node vectors of length n
+and stencil rows [n][k].  Every call runs on the GPU through libmgm.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, load, ptr
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _u8(a):
+    return np.ascontiguousarray(a, dtype=np.uint8)
+
+
+def knn_cloud(x, y, z, btag, nb, k, dim):
+    L = load()
+    n = len(x)
+    out = np.zeros((n, k), np.int32)
+    check(L.mgm_knn_cloud(n, nb, dim, _f(x), _f(y), _f(z), _u8(btag), k, out))
+    return out
+
+
+def nearest_points(x1, y1, z1, x2, y2, z2, dim):
+    L = load()
+    out = np.zeros(len(x1), np.int32)
+    check(L.mgm_nearest_points(len(x1), _f(x1), _f(y1), _f(z1), len(x2), _f(x2), _f(y2), _f(z2), dim, out))
+    return out
+
+
+def bfs_order(cloud):
+    L = load()
+    cloud = _i(cloud)
+    n, k = cloud.shape
+    q = np.zeros(n, np.int32)
+    check(L.mgm_bfs_order(n, k, cloud, q))
+    return q
+
+
+def apply_order(queue1, x, y, z, nx, ny, nz, btag, cloud):
+    """Returns permuted copies (x, y, z, nx, ny, nz, btag, cloud)."""
+    L = load()
+    arrs = [_f(a).copy() for a in (x, y, z, nx, ny, nz)]
+    bt = _u8(btag).copy()
+    cl = _i(cloud).copy()
+    n, k = cl.shape
+    check(L.mgm_apply_order(n, k, _i(queue1), *arrs, bt, cl))
+    return (*arrs, bt, cl)
+
+
+def correct_normals(x, y, z, btag, cloud, nx, ny, nz):
+    L = load()
+    cl = _i(cloud)
+    n, k = cl.shape
+    nx, ny, nz = _f(nx).copy(), _f(ny).copy(), _f(nz).copy()
+    check(L.mgm_correct_normals(n, k, _f(x), _f(y), _f(z), _u8(btag), cl, nx, ny, nz))
+    return nx, ny, nz
+
+
+def avg_dx(x, y, z, btag, cloud, dim):
+    L = load()
+    cl = _i(cloud)
+    n, k = cl.shape
+    d = C.c_double(0)
+    check(L.mgm_avg_dx(n, k, dim, _f(x), _f(y), _f(z), _u8(btag), cl, C.byref(d)))
+    return d.value
+
+
+def derivative_weights(x, y, z, nx, ny, nz, btag, cloud, dim, phs, poly_degree):
+    """Returns dict Dx, Dy, (Dz), lap, lapP, each [n][k]."""
+    L = load()
+    cl = _i(cloud)
+    n, k = cl.shape
+    out = {nm: np.zeros((n, k)) for nm in ("Dx", "Dy", "lap", "lapP")}
+    Dz = np.zeros((n, k)) if dim == 3 else None
+    check(L.mgm_derivative_weights(n, k, dim, phs, poly_degree, _f(x), _f(y), _f(z), _f(nx), _f(ny), _f(nz),
+                                   _u8(btag), cl, out["Dx"], out["Dy"], ptr(Dz), out["lap"], out["lapP"]))
+    if Dz is not None:
+        out["Dz"] = Dz
+    return out
+
+
+def transfer_weights(tx, ty, tz, tbtag, src_pt, rows_from, only_interior, sx, sy, sz, scloud, dim, phs, poly_src):
+    L = load()
+    scl = _i(scloud)
+    ns, ks = scl.shape
+    nt = len(tx)
+    W = np.zeros((nt, ks))
+    check(L.mgm_transfer_weights(nt, _f(tx), _f(ty), _f(tz), _u8(tbtag), _i(src_pt), rows_from, only_interior,
+                                 ns, ks, dim, phs, poly_src, _f(sx), _f(sy), _f(sz), scl, W))
+    return W
+
+
+def spmv(D, cloud, f):
+    L = load()
+    D = _f(D)
+    n, k = D.shape
+    out = np.zeros(n)
+    check(L.mgm_spmv(n, k, D, _i(cloud), _f(f), out))
+    return out
+
+
+def kernel_launches() -> int:
+    return int(load().mgm_kernel_launches())
+
+
+class Multigrid:
+    """A device-resident multigrid hierarchy (the reference's PointStructure
+    array after read_complete_mesh_data + create_derivative_matrices, and its
+    FieldVariables after copyin_*_to_gpu)."""
+
+    def __init__(self, clouds, ks, polys, phs=3, reference_transfer=False):
+        self.L = load()
+        self.nl = len(clouds)
+        self.dim = clouds[0].dim
+        h = self.L.mgm_create(self.dim, phs, self.nl)
+        if not h:
+            raise _lib.MgmError(-1, self.L.mgm_last_error().decode())
+        self.h = h
+        for l, c in enumerate(clouds):
+            check(self.L.mgm_set_level(h, l, c.n, c.nb, _f(c.x), _f(c.y), _f(c.z), _f(c.nx), _f(c.ny), _f(c.nz),
+                                       _u8(c.btag), polys[l], ks[l]))
+        check(self.L.mgm_setup(h, _lib.SETUP_REFERENCE_TRANSFER if reference_transfer else 0))
+        self.sizes = []
+        for l in range(self.nl):
+            n, nb, k, npl = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+            check(self.L.mgm_level_size(h, l, C.byref(n), C.byref(nb), C.byref(k), C.byref(npl)))
+            self.sizes.append((n.value, nb.value, k.value, npl.value))
+        self.reference_transfer = reference_transfer
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mgm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def n(self, l=0):
+        return self.sizes[l][0]
+
+    def geometry(self, l):
+        n, nb, k, _ = self.sizes[l]
+        a = {nm: np.zeros(n) for nm in ("x", "y", "z", "nx", "ny", "nz")}
+        a["btag"] = np.zeros(n, np.uint8)
+        a["cloud"] = np.zeros((n, k), np.int32)
+        check(self.L.mgm_get_geometry(self.h, l, *(ptr(a[nm]) for nm in ("x", "y", "z", "nx", "ny", "nz", "btag",
+                                                                            "cloud"))))
+        d = C.c_double()
+        check(self.L.mgm_level_d_avg(self.h, l, C.byref(d)))
+        a["d_avg"] = d.value
+        return a
+
+    def operators(self, l):
+        n, nb, k, _ = self.sizes[l]
+        out = {nm: np.zeros((n, k)) for nm in ("Dx", "Dy", "lap", "lapP")}
+        Dz = np.zeros((n, k)) if self.dim == 3 else None
+        check(self.L.mgm_get_operators(self.h, l, ptr(out["Dx"]), ptr(out["Dy"]), ptr(Dz), ptr(out["lap"]),
+                                       ptr(out["lapP"])))
+        if Dz is not None:
+            out["Dz"] = Dz
+        return out
+
+    def transfer(self, l):
+        n = self.sizes[l][0]
+        rp = np.zeros(n, np.int32)
+        pp = np.zeros(n, np.int32)
+        restr = np.zeros((n, self.sizes[l - 1][2])) if (l > 0 and self.reference_transfer) else None
+        prol = np.zeros((n, self.sizes[l + 1][2])) if (l < self.nl - 1 and self.reference_transfer) else None
+        check(self.L.mgm_get_transfer(self.h, l, ptr(rp), ptr(pp), ptr(restr), ptr(prol)))
+        return {"rpts": rp, "ppts": pp, "restr": restr, "prol": prol}
+
+    def set_flow(self, Re, courant, omega=1.0, num_relax=3, num_vcycles=10, dt=0.0):
+        check(self.L.mgm_set_flow(self.h, Re, courant, omega, num_relax, num_vcycles, dt))
+        d = C.c_double()
+        check(self.L.mgm_get_dt(self.h, C.byref(d)))
+        self.dt = d.value
+        return self.dt
+
+    def set_solver(self, rel_tol=1e-8, max_iters=60, cheb_degree=3, cheb_ratio=6.0):
+        check(self.L.mgm_set_solver(self.h, rel_tol, max_iters, cheb_degree, cheb_ratio))
+
+    def apply_bc(self, kind=_lib.BC_LID):
+        check(self.L.mgm_apply_bc(self.h, kind))
+
+    def set_field(self, name, values, l=0):
+        check(self.L.mgm_set_field(self.h, l, _lib.FIELD[name], _f(values)))
+
+    def get_field(self, name, l=0):
+        out = np.zeros(self.sizes[l][0])
+        check(self.L.mgm_get_field(self.h, l, _lib.FIELD[name], out))
+        return out
+
+    def step(self, mode=_lib.MODE_FP64):
+        e = C.c_double()
+        check(self.L.mgm_step(self.h, mode, C.byref(e)))
+        return e.value
+
+    def intermediate_velocity(self):
+        check(self.L.mgm_intermediate_velocity(self.h))
+
+    def mass_residual(self):
+        check(self.L.mgm_mass_residual(self.h))
+
+    def poisson(self, mode):
+        check(self.L.mgm_poisson(self.h, mode))
+
+    def update_velocity(self, with_mass=False):
+        m = C.c_double()
+        check(self.L.mgm_update_velocity(self.h, C.byref(m) if with_mass else None))
+        return m.value
+
+    def last_solve(self):
+        it, rr = C.c_int(), C.c_double()
+        check(self.L.mgm_last_solve(self.h, C.byref(it), C.byref(rr)))
+        return it.value, rr.value
+
+    def solve_poisson(self, b, p0=None, mode=_lib.MODE_FP64):
+        n = self.sizes[0][0]
+        p = np.zeros(n) if p0 is None else _f(p0).copy()
+        it, rr = C.c_int(), C.c_double()
+        check(self.L.mgm_solve_poisson(self.h, mode, _f(b), p, C.byref(it), C.byref(rr)))
+        return p, it.value, rr.value
+
+    def sync(self):
+        check(self.L.mgm_sync(self.h))

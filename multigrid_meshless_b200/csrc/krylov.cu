@@ -1,0 +1,307 @@
+// krylov.cu -- FP64 vector kernels of the flexible GMRES outer iteration and
+// the dense Gauss-Jordan (partial pivoting) used once at set-up for the
+// coarsest-level inverse.
+#include "krylov.cuh"
+
+namespace mgm {
+
+template <int BS>
+__device__ __forceinline__ double bsum(double v, double *sm)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = threadIdx.x < BS / 32 ? sm[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;
+}
+
+// r = b - A x  (A: pinned FP64 operator, ELL), and per-block |r|^2, |b|^2 partials
+__global__ void __launch_bounds__(256) k_resid64(int n, int k, const int *__restrict__ idx, const double *__restrict__ A,
+                                                 const double *__restrict__ b, const double *__restrict__ x,
+                                                 double *__restrict__ r, double *__restrict__ part)
+{
+    __shared__ double sm[32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double rr = 0, bb = 0;
+    if (i < n) {
+        double s = 0.0;
+        for (int j = 0; j < k; j++) {
+            const long o = (long)j * n + i;
+            s = fma(A[o], x[idx[o]], s);
+        }
+        const double ri = b[i] - s;
+        r[i] = ri;
+        rr = ri * ri;
+        bb = b[i] * b[i];
+    }
+    rr = bsum<256>(rr, sm);
+    bb = bsum<256>(bb, sm);
+    if (threadIdx.x == 0) { part[2 * blockIdx.x] = rr; part[2 * blockIdx.x + 1] = bb; }
+}
+
+// w = A z  (z in precision T)
+template <class T>
+__global__ void __launch_bounds__(256) k_apply64(int n, int k, const int *__restrict__ idx, const double *__restrict__ A,
+                                                 const T *__restrict__ z, double *__restrict__ w)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    for (int j = 0; j < k; j++) {
+        const long o = (long)j * n + i;
+        s = fma(A[o], (double)z[idx[o]], s);
+    }
+    w[i] = s;
+}
+
+// partial dot products h_c = V_c . w for c < cnt; part[c * nblk + blk]
+__global__ void __launch_bounds__(256) k_multidot(int n, int cnt, const double *__restrict__ V, long ldv,
+                                                  const double *__restrict__ w, double *__restrict__ part)
+{
+    __shared__ double sm[32];
+    for (int c = 0; c < cnt; c++) {
+        double s = 0.0;
+        const double *vc = V + c * ldv;
+        for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+            s = fma(vc[i], w[i], s);
+        s = bsum<256>(s, sm);
+        if (threadIdx.x == 0) part[(long)c * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+__global__ void k_reduce_parts(const double *__restrict__ part, int nblk, int cnt, double *__restrict__ out)
+{
+    __shared__ double sm[32];
+    for (int c = 0; c < cnt; c++) {
+        double s = 0.0;
+        for (int t = threadIdx.x; t < nblk; t += blockDim.x) s += part[(long)c * nblk + t];
+        s = bsum<256>(s, sm);
+        if (threadIdx.x == 0) out[c] = s;
+    }
+}
+
+// w -= sum_c h[c] V_c
+__global__ void __launch_bounds__(256) k_orth_update(int n, int cnt, const double *__restrict__ V, long ldv,
+                                                     const double *__restrict__ h, double *__restrict__ w)
+{
+    __shared__ double hs[kMaxKrylov + 1];
+    for (int c = threadIdx.x; c < cnt; c += blockDim.x) hs[c] = h[c];
+    __syncthreads();
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = w[i];
+    for (int c = 0; c < cnt; c++) s = fma(-hs[c], V[c * ldv + i], s);
+    w[i] = s;
+}
+
+// out = in * (1 / *nrm) where nrm holds |.|^2 or |.| (is_sq)
+__global__ void k_scale_by(int n, const double *__restrict__ in, double *__restrict__ out, const double *__restrict__ nrm,
+                           int is_sq)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double d = is_sq ? sqrt(*nrm) : *nrm;
+    out[i] = d > 0 ? in[i] / d : 0.0;
+}
+
+// x += sum_c y[c] Z_c  (Z in precision T)
+template <class T>
+__global__ void __launch_bounds__(256) k_combine(int n, int cnt, const T *__restrict__ Z, long ldz,
+                                                 const double *__restrict__ y, double *__restrict__ x)
+{
+    __shared__ double ys[kMaxKrylov + 1];
+    for (int c = threadIdx.x; c < cnt; c += blockDim.x) ys[c] = y[c];
+    __syncthreads();
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = x[i];
+    for (int c = 0; c < cnt; c++) s = fma(ys[c], (double)Z[c * ldz + i], s);
+    x[i] = s;
+}
+
+template <class T>
+__global__ void k_copy_convert(long n, const double *__restrict__ in, T *__restrict__ out)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (T)in[i];
+}
+
+template <class T>
+__global__ void k_copy_out(long n, const T *__restrict__ in, T *__restrict__ out)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[i];
+}
+
+void resid64(int n, int k, const int *idx, const double *A, const double *b, const double *x, double *r, double *part,
+             cudaStream_t s)
+{
+    k_resid64<<<blocks_for(n, 256), 256, 0, s>>>(n, k, idx, A, b, x, r, part);
+    MGM_LAUNCHED();
+}
+template <class T>
+void apply64(int n, int k, const int *idx, const double *A, const T *z, double *w, cudaStream_t s)
+{
+    k_apply64<T><<<blocks_for(n, 256), 256, 0, s>>>(n, k, idx, A, z, w);
+    MGM_LAUNCHED();
+}
+template void apply64<double>(int, int, const int *, const double *, const double *, double *, cudaStream_t);
+template void apply64<float>(int, int, const int *, const double *, const float *, double *, cudaStream_t);
+
+int dot_blocks(int n) { return std::max(1, std::min(blocks_for(n, 256), 148 * 4)); }
+
+void multidot(int n, int cnt, const double *V, long ldv, const double *w, double *part, double *out, cudaStream_t s)
+{
+    const int nb = dot_blocks(n);
+    k_multidot<<<nb, 256, 0, s>>>(n, cnt, V, ldv, w, part);
+    MGM_LAUNCHED();
+    k_reduce_parts<<<1, 256, 0, s>>>(part, nb, cnt, out);
+    MGM_LAUNCHED();
+}
+void reduce_parts(const double *part, int nblk, int cnt, double *out, cudaStream_t s)
+{
+    k_reduce_parts<<<1, 256, 0, s>>>(part, nblk, cnt, out);
+    MGM_LAUNCHED();
+}
+void orth_update(int n, int cnt, const double *V, long ldv, const double *h, double *w, cudaStream_t s)
+{
+    k_orth_update<<<blocks_for(n, 256), 256, 0, s>>>(n, cnt, V, ldv, h, w);
+    MGM_LAUNCHED();
+}
+void scale_by(int n, const double *in, double *out, const double *nrm, int is_sq, cudaStream_t s)
+{
+    k_scale_by<<<blocks_for(n, 256), 256, 0, s>>>(n, in, out, nrm, is_sq);
+    MGM_LAUNCHED();
+}
+template <class T>
+void combine(int n, int cnt, const T *Z, long ldz, const double *y, double *x, cudaStream_t s)
+{
+    k_combine<T><<<blocks_for(n, 256), 256, 0, s>>>(n, cnt, Z, ldz, y, x);
+    MGM_LAUNCHED();
+}
+template void combine<double>(int, int, const double *, long, const double *, double *, cudaStream_t);
+template void combine<float>(int, int, const float *, long, const double *, double *, cudaStream_t);
+template <class T>
+void copy_convert(long n, const double *in, T *out, cudaStream_t s)
+{
+    k_copy_convert<T><<<blocks_for(n, 256), 256, 0, s>>>(n, in, out);
+    MGM_LAUNCHED();
+}
+template void copy_convert<double>(long, const double *, double *, cudaStream_t);
+template void copy_convert<float>(long, const double *, float *, cudaStream_t);
+template <class T>
+void copy_out(long n, const T *in, T *out, cudaStream_t s)
+{
+    k_copy_out<T><<<blocks_for(n, 256), 256, 0, s>>>(n, in, out);
+    MGM_LAUNCHED();
+}
+template void copy_out<double>(long, const double *, double *, cudaStream_t);
+template void copy_out<float>(long, const float *, float *, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// dense Gauss-Jordan with partial pivoting on [M | I], one matrix, set-up only
+// ---------------------------------------------------------------------------
+__global__ void k_pivot_search(int n, const double *M, int col, int *piv_row, double *piv_val)
+{
+    __shared__ double bv[256];
+    __shared__ int bi[256];
+    double best = -1;
+    int br = col;
+    for (int r = col + threadIdx.x; r < n; r += blockDim.x) {
+        double v = fabs(M[(long)r * 2 * n + col]);
+        if (v > best) { best = v; br = r; }
+    }
+    bv[threadIdx.x] = best;
+    bi[threadIdx.x] = br;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) {
+            if (bv[threadIdx.x + off] > bv[threadIdx.x] ||
+                (bv[threadIdx.x + off] == bv[threadIdx.x] && bi[threadIdx.x + off] < bi[threadIdx.x])) {
+                bv[threadIdx.x] = bv[threadIdx.x + off];
+                bi[threadIdx.x] = bi[threadIdx.x + off];
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { *piv_row = bi[0]; *piv_val = M[(long)bi[0] * 2 * n + col]; }
+}
+
+__global__ void k_swap_scale(int n, double *M, int col, const int *piv_row, const double *piv_val)
+{
+    const int pr = *piv_row;
+    const double p = *piv_val;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < 2 * n; c += gridDim.x * blockDim.x) {
+        double a = M[(long)col * 2 * n + c], b = M[(long)pr * 2 * n + c];
+        if (pr != col) M[(long)pr * 2 * n + c] = a;
+        M[(long)col * 2 * n + c] = b / p;
+    }
+}
+
+__global__ void k_eliminate(int n, double *M, int col, double *colbuf)
+{
+    // colbuf holds column `col` of every row (taken before the update)
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)n * 2 * n) return;
+    const int r = (int)(t / (2 * n)), c = (int)(t % (2 * n));
+    if (r == col) return;
+    const double f = colbuf[r];
+    if (f != 0.0) M[t] -= f * M[(long)col * 2 * n + c];
+}
+
+__global__ void k_take_col(int n, const double *M, int col, double *colbuf)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n) colbuf[r] = M[(long)r * 2 * n + col];
+}
+
+__global__ void k_build_aug_dense(int n, int k, const int *idx, const double *A, double *M)
+{
+    // M = [A_dense | I], A from the ELL operator (duplicates in a row accumulate)
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double *row = M + (long)i * 2 * n;
+    for (int c = 0; c < 2 * n; c++) row[c] = (c == n + i) ? 1.0 : 0.0;
+    for (int j = 0; j < k; j++) {
+        const long o = (long)j * n + i;
+        row[idx[o]] += A[o];
+    }
+}
+
+__global__ void k_extract_inverse(int n, const double *M, double *inv64, float *inv32)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)n * n) return;
+    const int r = (int)(t / n), c = (int)(t % n);
+    const double v = M[(long)r * 2 * n + n + c];
+    inv64[t] = v;
+    inv32[t] = (float)v;
+}
+
+void dense_inverse(int n, int k, const int *idx, const double *A, double *inv64, float *inv32, cudaStream_t s)
+{
+    DBuf<double> M((size_t)n * 2 * n), colbuf(n);
+    DBuf<int> piv(1);
+    DBuf<double> pval(1);
+    k_build_aug_dense<<<blocks_for(n, 128), 128, 0, s>>>(n, k, idx, A, M.p);
+    MGM_LAUNCHED();
+    for (int c = 0; c < n; c++) {
+        k_pivot_search<<<1, 256, 0, s>>>(n, M.p, c, piv.p, pval.p);
+        MGM_LAUNCHED();
+        k_swap_scale<<<blocks_for(2 * n, 256), 256, 0, s>>>(n, M.p, c, piv.p, pval.p);
+        MGM_LAUNCHED();
+        k_take_col<<<blocks_for(n, 256), 256, 0, s>>>(n, M.p, c, colbuf.p);
+        MGM_LAUNCHED();
+        k_eliminate<<<blocks_for((long)n * 2 * n, 256), 256, 0, s>>>(n, M.p, c, colbuf.p);
+        MGM_LAUNCHED();
+    }
+    k_extract_inverse<<<blocks_for((long)n * n, 256), 256, 0, s>>>(n, M.p, inv64, inv32);
+    MGM_LAUNCHED();
+    MGM_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace mgm

@@ -1,0 +1,1034 @@
+// mgm_api.cu -- host runtime and C ABI (include/mgm.h).
+//
+// The context owns every device array of every level: the reference's
+// jagged host rows (structures.h:44-106) become, per level, SoA coordinates,
+// a uint8 boundary tag, and ELL operators column-major by stencil slot.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "../../include/mgm.h"
+#include "krylov.cuh"
+#include "stencil.cuh"
+
+namespace mgm {
+
+long long g_launches = 0;
+static thread_local std::string t_err;
+void set_error(int code, const std::string &msg)
+{
+    (void)code;
+    t_err = msg;
+}
+
+struct Level {
+    int n = 0, nb = 0, k = 0, poly = 0, np = 0;
+    double d_avg = 0;
+    DBuf<double> x, y, z, nx, ny, nz;
+    DBuf<uint8_t> btag;
+    DBuf<int> cloud;  // row-major [n][k] after the reorder
+    DBuf<int> idx;    // ELL [k][n]
+    DBuf<double> Dx, Dy, Dz, lap, lapP;  // ELL
+    DBuf<int> rpts, ppts;
+    // reference-semantics transfer rows (rows >= nb), ELL
+    DBuf<int> ref_r_idx, ref_p_idx;
+    DBuf<double> ref_restr, ref_prol;
+    // solver transfer: restriction into this level (interior rows), prolongation into this level (all rows)
+    DBuf<int> s_r_idx, s_p_idx;
+    DBuf<double> s_r_w64, s_p_w64;
+    DBuf<float> s_r_w32, s_p_w32;
+    // pinned operator
+    DBuf<double> A64, dinv64;
+    DBuf<float> A32, dinv32;
+    DBuf<int> bnd_list;
+    int nbl = 0;
+    double lmax = 2.0;
+    // reference-mode state
+    DBuf<double> p, ptmp, src, res;
+    // solver work vectors
+    DBuf<double> r64, e64, e64b, d64, q64;
+    DBuf<float> r32, e32, e32b, d32, q32;
+};
+
+}  // namespace mgm
+
+using namespace mgm;
+
+struct mgm_ctx {
+    int dim = 2, phs = 3, nl = 0;
+    int device = 0;
+    cudaStream_t s = nullptr;
+    std::vector<Level> L;
+    bool setup_done = false;
+    bool have_ref_transfer = false;
+    // flow
+    double Re = 100, courant = 0.5, dt = 0, nu = 0.01, rho = 1;
+    float omega = 1.0f;
+    int num_relax = 3, num_vcycles = 10;
+    // level-0 fields
+    DBuf<double> u, v, w, u_new, v_new, w_new, dpdn, partial, scal;
+    // solver controls and state
+    double tol = 1e-8;
+    int max_iters = 60, cheb_deg = 3;
+    double cheb_ratio = 6.0;
+    DBuf<double> cinv64;
+    DBuf<float> cinv32;
+    DBuf<double> V, Z64, wv, kpart, kscal, bvec;
+    DBuf<float> Z32;
+    int last_iters = 0;
+    double last_relres = 0;
+    double *h_pinned = nullptr;
+};
+
+// ---------------------------------------------------------------------------
+namespace {
+
+template <class F>
+int guard(F &&f)
+{
+    try {
+        f();
+        return MGM_OK;
+    } catch (const Error &e) {
+        t_err = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        t_err = "host allocation failed";
+        return MGM_ERR_NOMEM;
+    } catch (const std::exception &e) {
+        t_err = e.what();
+        return MGM_ERR_ARG;
+    }
+}
+
+cudaStream_t tmp_stream()
+{
+    static thread_local cudaStream_t s = nullptr;
+    if (!s) MGM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return s;
+}
+
+void check_ctx(mgm_ctx *c)
+{
+    MGM_REQUIRE(c != nullptr, "null context");
+    MGM_CUDA(cudaSetDevice(c->device));
+}
+
+__global__ void k_gather_idx(int n, int k, const int *__restrict__ pts, const int *__restrict__ src_cloud,
+                             int *__restrict__ out)
+{
+    // out[j][i] = src_cloud[pts[i]][j]
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)n * k) return;
+    const int j = (int)(t / n), i = (int)(t % n);
+    out[t] = src_cloud[(long)pts[i] * k + j];
+}
+
+__global__ void k_pin_operator(int n, int k, const double *__restrict__ lapP, double *__restrict__ A64,
+                               float *__restrict__ A32, double *__restrict__ d64, float *__restrict__ d32)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)n * k) return;
+    const int j = (int)(t / n), i = (int)(t % n);
+    double a = lapP[t];
+    if (i == 0) a = (j == 0) ? 1.0 : 0.0;  // pinned row p[0] = 0
+    A64[t] = a;
+    A32[t] = (float)a;
+    if (j == 0) { d64[i] = 1.0 / a; d32[i] = (float)(1.0 / a); }
+}
+
+__global__ void k_bc(int n, int kind, const double *x, const double *y, double *u, double *v, double *un, double *vn)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (kind == MGM_BC_LID) {
+        if (fabs(y[i] - 1.0) < 1e-9) { u[i] = 1.0; v[i] = 0.0; }
+    } else {
+        const double r = sqrt(x[i] * x[i] + y[i] * y[i]);
+        if (fabs(r - 0.5) < 1e-9) {
+            u[i] = -y[i] / r; v[i] = x[i] / r;
+            un[i] = u[i]; vn[i] = v[i];
+        }
+    }
+}
+
+__global__ void k_zero_pinned(double *b) { b[0] = 0.0; }
+
+void knn_clouds(Level &L, int dim, cudaStream_t s)
+{
+    const int n = L.n, k = L.k, nb = L.nb;
+    L.cloud.alloc((size_t)n * k);
+    GridIndex gall, gint;
+    grid_build(gall, n, L.x.p, L.y.p, L.z.p, nullptr, dim, s);
+    if (n > nb)
+        knn_query(gall, L.x.p, L.y.p, L.z.p, n - nb, L.x.p + nb, L.y.p + nb, L.z.p + nb, nullptr, k, 0,
+                  L.cloud.p + (size_t)nb * k, k, s);
+    if (nb > 0) {
+        grid_build(gint, n, L.x.p, L.y.p, L.z.p, L.btag.p, dim, s);
+        knn_query(gint, L.x.p, L.y.p, L.z.p, nb, L.x.p, L.y.p, L.z.p, nullptr, k, 1, L.cloud.p, k, s);
+    }
+    MGM_CUDA(cudaStreamSynchronize(s));
+}
+
+void nearest_of(const Level &T, const Level &S, int dim, DBuf<int> &out, cudaStream_t s)
+{
+    GridIndex g;
+    grid_build(g, S.n, S.x.p, S.y.p, S.z.p, nullptr, dim, s);
+    out.alloc(T.n);
+    knn_query(g, S.x.p, S.y.p, S.z.p, T.n, T.x.p, T.y.p, T.z.p, nullptr, 1, 0, out.p, 1, s);
+    MGM_CUDA(cudaStreamSynchronize(s));
+}
+
+// ELL transfer matrix from row-major weights (target rows [nt][ks]) with gather through src cloud
+void build_transfer(const Level &T, const Level &S, const DBuf<int> &pts, int rows_from, int only_interior, int dim,
+                    int phs, DBuf<int> &gidx, DBuf<double> &w64, DBuf<float> *w32, cudaStream_t s)
+{
+    const int nt = T.n, ks = S.k;
+    DBuf<double> rm((size_t)nt * ks);
+    Monomials mono = monomials(dim, S.poly);
+    transfer_weights(nt, T.x.p, T.y.p, T.z.p, T.btag.p, pts.p, rows_from, only_interior, ks, dim, phs, mono, S.x.p,
+                     S.y.p, S.z.p, S.cloud.p, rm.p, s);
+    w64.alloc((size_t)nt * ks);
+    transpose_rowmajor_to_ell_d(rm.p, w64.p, nt, ks, s);
+    gidx.alloc((size_t)nt * ks);
+    k_gather_idx<<<blocks_for((long)nt * ks, 256), 256, 0, s>>>(nt, ks, pts.p, S.cloud.p, gidx.p);
+    MGM_LAUNCHED();
+    if (w32) {
+        w32->alloc((size_t)nt * ks);
+        convert_d2f(w64.p, w32->p, (long)nt * ks, s);
+    }
+    MGM_CUDA(cudaStreamSynchronize(s));
+}
+
+template <class T>
+std::vector<SolveLevel<T>> solve_levels(mgm_ctx *c);
+
+template <>
+std::vector<SolveLevel<double>> solve_levels<double>(mgm_ctx *c)
+{
+    std::vector<SolveLevel<double>> out;
+    for (int l = 0; l < c->nl; l++) {
+        Level &L = c->L[l];
+        SolveLevel<double> S{};
+        S.n = L.n; S.k = L.k; S.nb_list = L.nbl;
+        S.idx = L.idx.p; S.A = L.A64.p; S.dinv = L.dinv64.p; S.btag = L.btag.p; S.bnd_list = L.bnd_list.p;
+        S.r = L.r64.p; S.e = L.e64.p; S.e2 = L.e64b.p; S.d = L.d64.p; S.q = L.q64.p;
+        S.kr = l > 0 ? c->L[l - 1].k : 0; S.r_idx = L.s_r_idx.p; S.r_w = L.s_r_w64.p;
+        S.kp = l < c->nl - 1 ? c->L[l + 1].k : 0; S.p_idx = L.s_p_idx.p; S.p_w = L.s_p_w64.p;
+        S.lmax = L.lmax;
+        out.push_back(S);
+    }
+    return out;
+}
+
+template <>
+std::vector<SolveLevel<float>> solve_levels<float>(mgm_ctx *c)
+{
+    std::vector<SolveLevel<float>> out;
+    for (int l = 0; l < c->nl; l++) {
+        Level &L = c->L[l];
+        SolveLevel<float> S{};
+        S.n = L.n; S.k = L.k; S.nb_list = L.nbl;
+        S.idx = L.idx.p; S.A = L.A32.p; S.dinv = L.dinv32.p; S.btag = L.btag.p; S.bnd_list = L.bnd_list.p;
+        S.r = L.r32.p; S.e = L.e32.p; S.e2 = L.e32b.p; S.d = L.d32.p; S.q = L.q32.p;
+        S.kr = l > 0 ? c->L[l - 1].k : 0; S.r_idx = L.s_r_idx.p; S.r_w = L.s_r_w32.p;
+        S.kp = l < c->nl - 1 ? c->L[l + 1].k : 0; S.p_idx = L.s_p_idx.p; S.p_w = L.s_p_w32.p;
+        S.lmax = L.lmax;
+        out.push_back(S);
+    }
+    return out;
+}
+
+StepArgs step_args(mgm_ctx *c)
+{
+    Level &L = c->L[0];
+    StepArgs a{};
+    a.n = L.n; a.k = L.k; a.idx = L.idx.p;
+    a.Dx = L.Dx.p; a.Dy = L.Dy.p; a.Dz = L.Dz.p; a.lap = L.lap.p;
+    a.btag = L.btag.p; a.nx = L.nx.p; a.ny = L.ny.p; a.nz = L.nz.p;
+    a.u = c->u.p; a.v = c->v.p; a.w = c->w.p; a.u_new = c->u_new.p; a.v_new = c->v_new.p; a.w_new = c->w_new.p;
+    a.p = L.p.p; a.source = L.src.p; a.dpdn = c->dpdn.p;
+    a.dt = c->dt; a.nu = c->nu; a.rho = c->rho;
+    return a;
+}
+
+std::vector<RefLevel> ref_levels(mgm_ctx *c)
+{
+    std::vector<RefLevel> out;
+    for (int l = 0; l < c->nl; l++) {
+        Level &L = c->L[l];
+        RefLevel R{};
+        R.n = L.n; R.k = L.k; R.idx = L.idx.p; R.lap = L.lap.p; R.lapP = L.lapP.p; R.btag = L.btag.p;
+        R.p = L.p.p; R.ptmp = L.ptmp.p; R.src = L.src.p; R.res = L.res.p;
+        R.r_idx = L.ref_r_idx.p; R.restr = L.ref_restr.p; R.p_idx = L.ref_p_idx.p; R.prol = L.ref_prol.p;
+        out.push_back(R);
+    }
+    return out;
+}
+
+// Flexible GMRES(m) in FP64 right-preconditioned by one V-cycle in precision T.
+// Solves A p = b (pinned level-0 operator); p is the initial guess.
+template <class T>
+void fgmres(mgm_ctx *c, const double *b, double *p)
+{
+    cudaStream_t s = c->s;
+    Level &L0 = c->L[0];
+    const int n = L0.n, k = L0.k;
+    const int m = std::min(c->max_iters, kMaxKrylov);
+    const long ld = n;
+    auto levels = solve_levels<T>(c);
+    CoarseSolve<T> cs;
+    cs.n = c->L[c->nl - 1].n;
+    if constexpr (sizeof(T) == 8) cs.inv = (const T *)c->cinv64.p; else cs.inv = (const T *)c->cinv32.p;
+    T *Z = sizeof(T) == 8 ? (T *)c->Z64.p : (T *)c->Z32.p;
+    double *V = c->V.p, *w = c->wv.p;
+    const int nbres = blocks_for(n, 256);
+    double *hp = c->h_pinned;  // pinned host scratch [2*kMaxKrylov+8]
+    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs_(m), sn_(m), g(m + 1);
+    int total_it = 0;
+    double bnorm = 0, relres = 1;
+    const int max_restarts = 4;
+    for (int restart = 0; restart <= max_restarts; restart++) {
+        // r0 = b - A p  -> V_0 (unnormalised), norms
+        resid64(n, k, L0.idx.p, L0.A64.p, b, p, V, c->kpart.p, s);
+        MGM_CUDA(cudaMemcpyAsync(hp, c->kpart.p, sizeof(double) * 2 * nbres, cudaMemcpyDeviceToHost, s));
+        MGM_CUDA(cudaStreamSynchronize(s));
+        double rr = 0, bb = 0;
+        for (int t = 0; t < nbres; t++) { rr += hp[2 * t]; bb += hp[2 * t + 1]; }
+        bnorm = sqrt(bb);
+        const double beta = sqrt(rr);
+        relres = bnorm > 0 ? beta / bnorm : 0.0;
+        if (!std::isfinite(relres)) throw Error{MGM_ERR_DIVERGED, "Poisson solve: non-finite residual"};
+        if (bnorm == 0 || relres < c->tol || total_it >= c->max_iters * (max_restarts + 1)) break;
+        hp[0] = beta;
+        MGM_CUDA(cudaMemcpyAsync(c->kscal.p, hp, sizeof(double), cudaMemcpyHostToDevice, s));
+        scale_by(n, V, V, c->kscal.p, 0, s);
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int j_done = 0;
+        for (int j = 0; j < m; j++) {
+            // z_j = M^-1 v_j
+            copy_convert<T>(n, V + j * ld, levels[0].r, s);
+            vcycle<T>(levels, cs, c->cheb_deg, c->cheb_ratio, s);
+            copy_out<T>(n, levels[0].e, Z + j * ld, s);
+            // w = A z_j, classical Gram-Schmidt with one re-orthogonalisation
+            apply64<T>(n, k, L0.idx.p, L0.A64.p, Z + j * ld, w, s);
+            multidot(n, j + 1, V, ld, w, c->kpart.p, c->kscal.p, s);
+            orth_update(n, j + 1, V, ld, c->kscal.p, w, s);
+            multidot(n, j + 1, V, ld, w, c->kpart.p, c->kscal.p + kMaxKrylov + 2, s);
+            orth_update(n, j + 1, V, ld, c->kscal.p + kMaxKrylov + 2, w, s);
+            multidot(n, 1, w, ld, w, c->kpart.p, c->kscal.p + 2 * kMaxKrylov + 4, s);
+            scale_by(n, w, V + (j + 1) * ld, c->kscal.p + 2 * kMaxKrylov + 4, 1, s);
+            MGM_CUDA(cudaMemcpyAsync(hp, c->kscal.p, sizeof(double) * (2 * kMaxKrylov + 5), cudaMemcpyDeviceToHost, s));
+            MGM_CUDA(cudaStreamSynchronize(s));
+            double *col = &H[(size_t)j * (m + 1)];
+            for (int i = 0; i <= j; i++) col[i] = hp[i] + hp[kMaxKrylov + 2 + i];
+            col[j + 1] = sqrt(std::max(hp[2 * kMaxKrylov + 4], 0.0));
+            for (int i = 0; i < j; i++) {
+                const double t0 = cs_[i] * col[i] + sn_[i] * col[i + 1];
+                col[i + 1] = -sn_[i] * col[i] + cs_[i] * col[i + 1];
+                col[i] = t0;
+            }
+            const double a = col[j], bb2 = col[j + 1];
+            const double rden = std::hypot(a, bb2);
+            cs_[j] = rden > 0 ? a / rden : 1.0;
+            sn_[j] = rden > 0 ? bb2 / rden : 0.0;
+            col[j] = rden;
+            col[j + 1] = 0;
+            g[j + 1] = -sn_[j] * g[j];
+            g[j] = cs_[j] * g[j];
+            total_it++;
+            j_done = j + 1;
+            const double est = fabs(g[j + 1]) / bnorm;
+            if (!std::isfinite(est)) throw Error{MGM_ERR_DIVERGED, "Poisson solve: non-finite Krylov residual"};
+            if (est < c->tol) break;
+        }
+        // y = H^-1 g (upper triangular), p += Z y
+        std::vector<double> y(j_done);
+        for (int i = j_done - 1; i >= 0; i--) {
+            double sacc = g[i];
+            for (int q = i + 1; q < j_done; q++) sacc -= H[(size_t)q * (m + 1) + i] * y[q];
+            y[i] = sacc / H[(size_t)i * (m + 1) + i];
+        }
+        for (int i = 0; i < j_done; i++) hp[i] = y[i];
+        MGM_CUDA(cudaMemcpyAsync(c->kscal.p, hp, sizeof(double) * j_done, cudaMemcpyHostToDevice, s));
+        combine<T>(n, j_done, Z, ld, c->kscal.p, p, s);
+    }
+    c->last_iters = total_it;
+    c->last_relres = relres;
+    if (!(relres < c->tol) && bnorm > 0)
+        throw Error{MGM_ERR_DIVERGED, "Poisson solve did not reach the tolerance (rel. residual " +
+                                          std::to_string(relres) + " after " + std::to_string(total_it) + " V-cycles)"};
+}
+
+void poisson(mgm_ctx *c, int mode)
+{
+    Level &L0 = c->L[0];
+    if (mode == MGM_MODE_REFERENCE) {
+        MGM_REQUIRE(c->have_ref_transfer || c->nl == 1, "reference mode needs mgm_setup(..., MGM_SETUP_REFERENCE_TRANSFER)");
+        auto R = ref_levels(c);
+        const double w1 = (double)c->omega, w2 = (double)(1 - c->omega);
+        ref_multigrid(R, w1, w2, c->num_relax, c->num_vcycles, c->s);
+        return;
+    }
+    // b = source with the pinned row's rhs 0 (boundary rows keep their (zero) source)
+    copy_out<double>(L0.n, L0.src.p, c->bvec.p, c->s);
+    k_zero_pinned<<<1, 1, 0, c->s>>>(c->bvec.p);
+    MGM_LAUNCHED();
+    if (mode == MGM_MODE_FP64) fgmres<double>(c, c->bvec.p, L0.p.p);
+    else if (mode == MGM_MODE_FP32_IR) fgmres<float>(c, c->bvec.p, L0.p.p);
+    else throw Error{MGM_ERR_ARG, "unknown Poisson mode"};
+}
+
+void alloc_solver_buffers(mgm_ctx *c)
+{
+    const int n = c->L[0].n;
+    const int m = std::min(c->max_iters, kMaxKrylov);
+    c->V.alloc((size_t)(m + 1) * n);
+    c->Z64.alloc((size_t)m * n);
+    c->Z32.alloc((size_t)m * n);
+    c->wv.alloc(n);
+    c->bvec.alloc(n);
+    c->kpart.alloc((size_t)std::max(2 * blocks_for(n, 256), (kMaxKrylov + 1) * dot_blocks(n)) + 16);
+    c->kscal.alloc(3 * kMaxKrylov + 16);
+    if (!c->h_pinned) MGM_CUDA(cudaMallocHost(&c->h_pinned, sizeof(double) * (3 * kMaxKrylov + 16 + 2 * 65536)));
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char *mgm_last_error(void) { return t_err.c_str(); }
+long long mgm_kernel_launches(void) { return g_launches; }
+int mgm_version(void) { return 1; }
+
+int mgm_knn_cloud(int n, int nb, int dim, const double *x, const double *y, const double *z, const unsigned char *btag,
+                  int k, int *cloud)
+{
+    return guard([&] {
+        MGM_REQUIRE(n > 0 && nb >= 0 && nb <= n && k >= 1 && k <= kMaxK && (dim == 2 || dim == 3), "mgm_knn_cloud: bad sizes");
+        MGM_REQUIRE(x && y && z && btag && cloud, "mgm_knn_cloud: null pointer");
+        int ninterior = 0;
+        for (int i = 0; i < n; i++) ninterior += btag[i] ? 0 : 1;
+        MGM_REQUIRE(n >= k && (nb == 0 || ninterior >= k - 1), "mgm_knn_cloud: fewer candidate nodes than the stencil size");
+        cudaStream_t s = tmp_stream();
+        Level L;
+        L.n = n; L.nb = nb; L.k = k;
+        L.x.upload(x, n, s); L.y.upload(y, n, s); L.z.upload(z, n, s);
+        L.btag.upload(btag, n, s);
+        knn_clouds(L, dim, s);
+        L.cloud.download(cloud, (size_t)n * k, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int mgm_nearest_points(int n1, const double *x1, const double *y1, const double *z1, int n2, const double *x2,
+                       const double *y2, const double *z2, int dim, int *nearest)
+{
+    return guard([&] {
+        MGM_REQUIRE(n1 >= 0 && n2 > 0, "mgm_nearest_points: bad sizes");
+        if (n1 == 0) return;
+        cudaStream_t s = tmp_stream();
+        Level A, B;
+        A.n = n1; B.n = n2;
+        A.x.upload(x1, n1, s); A.y.upload(y1, n1, s); A.z.upload(z1, n1, s);
+        B.x.upload(x2, n2, s); B.y.upload(y2, n2, s); B.z.upload(z2, n2, s);
+        DBuf<int> out;
+        nearest_of(A, B, dim, out, s);
+        out.download(nearest, n1, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int mgm_bfs_order(int n, int k, const int *cloud, int *queue1)
+{
+    return guard([&] {
+        MGM_REQUIRE(n > 0 && k >= 2, "mgm_bfs_order: bad sizes");
+        for (long t = 0; t < (long)n * k; t++) MGM_REQUIRE(cloud[t] >= 0 && cloud[t] < n, "mgm_bfs_order: cloud index out of range");
+        cudaStream_t s = tmp_stream();
+        DBuf<int> dc, dq(n);
+        dc.upload(cloud, (size_t)n * k, s);
+        int reached = bfs_order(n, k, dc.p, dq.p, s);
+        dq.download(queue1, n, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+        MGM_REQUIRE(reached == n, "mgm_bfs_order: stencil graph is disconnected (reached " + std::to_string(reached) +
+                                      " of " + std::to_string(n) + " nodes)");
+    });
+}
+
+int mgm_apply_order(int n, int k, const int *queue1, double *x, double *y, double *z, double *nx, double *ny, double *nz,
+                    unsigned char *btag, int *cloud)
+{
+    return guard([&] {
+        MGM_REQUIRE(n > 0 && k >= 1, "mgm_apply_order: bad sizes");
+        cudaStream_t s = tmp_stream();
+        DBuf<int> q, cl;
+        DBuf<double> a[6];
+        double *h[6] = {x, y, z, nx, ny, nz};
+        DBuf<uint8_t> bt;
+        q.upload(queue1, n, s);
+        for (int t = 0; t < 6; t++) a[t].upload(h[t], n, s);
+        bt.upload(btag, n, s);
+        cl.upload(cloud, (size_t)n * k, s);
+        apply_order(n, k, q.p, a[0].p, a[1].p, a[2].p, a[3].p, a[4].p, a[5].p, bt.p, cl.p, s);
+        for (int t = 0; t < 6; t++) a[t].download(h[t], n, s);
+        bt.download(btag, n, s);
+        cl.download(cloud, (size_t)n * k, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int mgm_correct_normals(int n, int k, const double *x, const double *y, const double *z, const unsigned char *btag,
+                        const int *cloud, double *nx, double *ny, double *nz)
+{
+    return guard([&] {
+        cudaStream_t s = tmp_stream();
+        DBuf<double> a[6];
+        const double *in[3] = {x, y, z};
+        double *io[3] = {nx, ny, nz};
+        for (int t = 0; t < 3; t++) a[t].upload(in[t], n, s);
+        for (int t = 0; t < 3; t++) a[3 + t].upload(io[t], n, s);
+        DBuf<uint8_t> bt;
+        DBuf<int> cl;
+        bt.upload(btag, n, s);
+        cl.upload(cloud, (size_t)n * k, s);
+        correct_normals(n, k, a[0].p, a[1].p, a[2].p, bt.p, cl.p, a[3].p, a[4].p, a[5].p, s);
+        for (int t = 0; t < 3; t++) a[3 + t].download(io[t], n, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int mgm_avg_dx(int n, int k, int dim, const double *x, const double *y, const double *z, const unsigned char *btag,
+               const int *cloud, double *d_avg)
+{
+    return guard([&] {
+        cudaStream_t s = tmp_stream();
+        DBuf<double> a[3], out(1);
+        const double *in[3] = {x, y, z};
+        for (int t = 0; t < 3; t++) a[t].upload(in[t], n, s);
+        DBuf<uint8_t> bt;
+        DBuf<int> cl;
+        bt.upload(btag, n, s);
+        cl.upload(cloud, (size_t)n * k, s);
+        avg_dx(n, k, dim, a[0].p, a[1].p, a[2].p, bt.p, cl.p, out.p, s);
+        out.download(d_avg, 1, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int mgm_derivative_weights(int n, int k, int dim, int phs, int poly_degree, const double *x, const double *y,
+                           const double *z, const double *nx, const double *ny, const double *nz,
+                           const unsigned char *btag, const int *cloud, double *Dx, double *Dy, double *Dz, double *lap,
+                           double *lapP)
+{
+    return guard([&] {
+        MGM_REQUIRE(n > 0 && k >= 2 && (dim == 2 || dim == 3), "mgm_derivative_weights: bad sizes");
+        MGM_REQUIRE(dim == 2 || Dz != nullptr, "mgm_derivative_weights: Dz required in 3D");
+        for (long t = 0; t < (long)n * k; t++) MGM_REQUIRE(cloud[t] >= 0 && cloud[t] < n, "mgm_derivative_weights: cloud index out of range");
+        cudaStream_t s = tmp_stream();
+        Monomials mono = monomials(dim, poly_degree);
+        DBuf<double> a[6];
+        const double *in[6] = {x, y, z, nx, ny, nz};
+        for (int t = 0; t < 6; t++) a[t].upload(in[t], n, s);
+        DBuf<uint8_t> bt;
+        DBuf<int> cl;
+        bt.upload(btag, n, s);
+        cl.upload(cloud, (size_t)n * k, s);
+        DBuf<double> o[5];
+        for (int t = 0; t < 5; t++) o[t].alloc((size_t)n * k);
+        derivative_weights(n, k, dim, phs, mono, a[0].p, a[1].p, a[2].p, a[3].p, a[4].p, a[5].p, bt.p, cl.p, o[0].p,
+                           o[1].p, dim == 3 ? o[2].p : nullptr, o[3].p, o[4].p, s);
+        double *h[5] = {Dx, Dy, Dz, lap, lapP};
+        for (int t = 0; t < 5; t++)
+            if (h[t] && (t != 2 || dim == 3)) o[t].download(h[t], (size_t)n * k, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int mgm_transfer_weights(int nt, const double *tx, const double *ty, const double *tz, const unsigned char *tbtag,
+                         const int *src_pt, int rows_from, int only_interior, int ns, int ks, int dim, int phs,
+                         int poly_degree_src, const double *sx, const double *sy, const double *sz, const int *scloud,
+                         double *W)
+{
+    return guard([&] {
+        MGM_REQUIRE(nt >= 0 && ns > 0 && ks >= 2, "mgm_transfer_weights: bad sizes");
+        for (int i = 0; i < nt; i++) MGM_REQUIRE(src_pt[i] >= 0 && src_pt[i] < ns, "mgm_transfer_weights: source point out of range");
+        for (long t = 0; t < (long)ns * ks; t++) MGM_REQUIRE(scloud[t] >= 0 && scloud[t] < ns, "mgm_transfer_weights: cloud index out of range");
+        if (nt == 0) return;
+        cudaStream_t s = tmp_stream();
+        Monomials mono = monomials(dim, poly_degree_src);
+        DBuf<double> t3[3], s3[3], out((size_t)nt * ks);
+        const double *ti[3] = {tx, ty, tz}, *si[3] = {sx, sy, sz};
+        for (int q = 0; q < 3; q++) { t3[q].upload(ti[q], nt, s); s3[q].upload(si[q], ns, s); }
+        DBuf<uint8_t> bt;
+        DBuf<int> sp, cl;
+        bt.upload(tbtag, nt, s);
+        sp.upload(src_pt, nt, s);
+        cl.upload(scloud, (size_t)ns * ks, s);
+        transfer_weights(nt, t3[0].p, t3[1].p, t3[2].p, bt.p, sp.p, rows_from, only_interior, ks, dim, phs, mono,
+                         s3[0].p, s3[1].p, s3[2].p, cl.p, out.p, s);
+        out.download(W, (size_t)nt * ks, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int mgm_spmv(int n, int k, const double *D, const int *cloud, const double *f, double *out)
+{
+    return guard([&] {
+        MGM_REQUIRE(n > 0 && k >= 1, "mgm_spmv: bad sizes");
+        for (long t = 0; t < (long)n * k; t++) MGM_REQUIRE(cloud[t] >= 0 && cloud[t] < n, "mgm_spmv: cloud index out of range");
+        cudaStream_t s = tmp_stream();
+        DBuf<double> rm, W((size_t)n * k), fv, o(n);
+        DBuf<int> cr, idx((size_t)n * k);
+        rm.upload(D, (size_t)n * k, s);
+        cr.upload(cloud, (size_t)n * k, s);
+        fv.upload(f, n, s);
+        transpose_rowmajor_to_ell_d(rm.p, W.p, n, k, s);
+        transpose_rowmajor_to_ell_i(cr.p, idx.p, n, k, s);
+        spmv_parity(n, k, W.p, idx.p, fv.p, o.p, s);
+        o.download(out, n, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+// ---------------------------------------------------------------------------
+mgm_ctx *mgm_create(int dim, int phs_degree, int num_levels)
+{
+    mgm_ctx *c = nullptr;
+    int st = guard([&] {
+        MGM_REQUIRE(dim == 2 || dim == 3, "mgm_create: dim must be 2 or 3");
+        MGM_REQUIRE(num_levels >= 1 && num_levels <= 16, "mgm_create: 1..16 levels");
+        MGM_REQUIRE(phs_degree >= 1 && phs_degree <= 11, "mgm_create: phs degree out of range");
+        int ndev = 0;
+        MGM_CUDA(cudaGetDeviceCount(&ndev));
+        MGM_REQUIRE(ndev > 0, "mgm_create: no CUDA device");
+        std::unique_ptr<mgm_ctx> cc(new mgm_ctx());
+        MGM_CUDA(cudaGetDevice(&cc->device));
+        cc->dim = dim; cc->phs = phs_degree; cc->nl = num_levels;
+        cc->L.resize(num_levels);
+        MGM_CUDA(cudaStreamCreateWithFlags(&cc->s, cudaStreamNonBlocking));
+        c = cc.release();
+    });
+    return st == MGM_OK ? c : nullptr;
+}
+
+void mgm_destroy(mgm_ctx *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->s) cudaStreamSynchronize(c->s);
+    if (c->h_pinned) cudaFreeHost(c->h_pinned);
+    c->L.clear();
+    if (c->s) cudaStreamDestroy(c->s);
+    delete c;
+}
+
+int mgm_set_level(mgm_ctx *c, int lev, int n, int nb, const double *x, const double *y, const double *z,
+                  const double *nx, const double *ny, const double *nz, const unsigned char *btag, int poly_degree, int k)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(lev >= 0 && lev < c->nl, "mgm_set_level: level out of range");
+        MGM_REQUIRE(n > 0 && nb >= 1 && nb <= n && k >= 2 && k <= kMaxK && poly_degree >= 0, "mgm_set_level: bad sizes");
+        MGM_REQUIRE(x && y && z && nx && ny && nz && btag, "mgm_set_level: null pointer");
+        for (int i = 0; i < n; i++)
+            MGM_REQUIRE(std::isfinite(x[i]) && std::isfinite(y[i]) && std::isfinite(z[i]), "mgm_set_level: non-finite coordinate");
+        int ninterior = 0;
+        for (int i = 0; i < n; i++) ninterior += btag[i] ? 0 : 1;
+        MGM_REQUIRE(ninterior >= k - 1 && n >= k, "mgm_set_level: fewer interior nodes than the stencil needs");
+        Monomials mono = monomials(c->dim, poly_degree);
+        MGM_REQUIRE(k + mono.np <= kMaxN, "mgm_set_level: k + num_poly_terms too large");
+        Level &L = c->L[lev];
+        L = Level();
+        L.n = n; L.nb = nb; L.k = k; L.poly = poly_degree; L.np = mono.np;
+        cudaStream_t s = c->s;
+        L.x.upload(x, n, s); L.y.upload(y, n, s); L.z.upload(z, n, s);
+        L.nx.upload(nx, n, s); L.ny.upload(ny, n, s); L.nz.upload(nz, n, s);
+        L.btag.upload(btag, n, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+        c->setup_done = false;
+    });
+}
+
+int mgm_setup(mgm_ctx *c, int flags)
+{
+    return guard([&] {
+        check_ctx(c);
+        cudaStream_t s = c->s;
+        for (int l = 0; l < c->nl; l++) MGM_REQUIRE(c->L[l].n > 0, "mgm_setup: level " + std::to_string(l) + " not set");
+        // read_complete_mesh_data (mesh_functions.h:914-928), per level after the reader
+        for (int l = 0; l < c->nl; l++) {
+            Level &L = c->L[l];
+            knn_clouds(L, c->dim, s);
+            DBuf<int> q1(L.n);
+            int reached = bfs_order(L.n, L.k, L.cloud.p, q1.p, s);
+            MGM_REQUIRE(reached == L.n, "mgm_setup: stencil graph of level " + std::to_string(l) + " is disconnected");
+            apply_order(L.n, L.k, q1.p, L.x.p, L.y.p, L.z.p, L.nx.p, L.ny.p, L.nz.p, L.btag.p, L.cloud.p, s);
+            correct_normals(L.n, L.k, L.x.p, L.y.p, L.z.p, L.btag.p, L.cloud.p, L.nx.p, L.ny.p, L.nz.p, s);
+            DBuf<double> d(1);
+            avg_dx(L.n, L.k, c->dim, L.x.p, L.y.p, L.z.p, L.btag.p, L.cloud.p, d.p, s);
+            d.download(&L.d_avg, 1, s);
+            L.idx.alloc((size_t)L.n * L.k);
+            transpose_rowmajor_to_ell_i(L.cloud.p, L.idx.p, L.n, L.k, s);
+        }
+        MGM_CUDA(cudaStreamSynchronize(s));
+        // create_prolongation_and_restriction_matrices (mesh_functions.h:874-893)
+        for (int l = 0; l < c->nl; l++) {
+            Level &L = c->L[l];
+            nearest_of(L, l < c->nl - 1 ? c->L[l + 1] : L, c->dim, L.ppts, s);
+            nearest_of(L, l > 0 ? c->L[l - 1] : L, c->dim, L.rpts, s);
+        }
+        c->have_ref_transfer = (flags & MGM_SETUP_REFERENCE_TRANSFER) != 0;
+        for (int l = 0; l < c->nl; l++) {
+            Level &L = c->L[l];
+            if (l < c->nl - 1) {
+                Level &C = c->L[l + 1];
+                if (c->have_ref_transfer)
+                    build_transfer(L, C, L.ppts, L.nb, 0, c->dim, c->phs, L.ref_p_idx, L.ref_prol, nullptr, s);
+                build_transfer(L, C, L.ppts, 0, 0, c->dim, c->phs, L.s_p_idx, L.s_p_w64, &L.s_p_w32, s);
+            }
+            if (l > 0) {
+                Level &F = c->L[l - 1];
+                if (c->have_ref_transfer)
+                    build_transfer(L, F, L.rpts, L.nb, 0, c->dim, c->phs, L.ref_r_idx, L.ref_restr, nullptr, s);
+                build_transfer(L, F, L.rpts, 0, 1, c->dim, c->phs, L.s_r_idx, L.s_r_w64, &L.s_r_w32, s);
+            }
+        }
+        // create_derivative_matrices (rbf.h:401-421) on every level
+        for (int l = 0; l < c->nl; l++) {
+            Level &L = c->L[l];
+            const size_t nk = (size_t)L.n * L.k;
+            DBuf<double> rm[5];
+            for (int t = 0; t < 5; t++) rm[t].alloc(nk);
+            Monomials mono = monomials(c->dim, L.poly);
+            derivative_weights(L.n, L.k, c->dim, c->phs, mono, L.x.p, L.y.p, L.z.p, L.nx.p, L.ny.p, L.nz.p, L.btag.p,
+                               L.cloud.p, rm[0].p, rm[1].p, c->dim == 3 ? rm[2].p : nullptr, rm[3].p, rm[4].p, s);
+            DBuf<double> *dst[5] = {&L.Dx, &L.Dy, &L.Dz, &L.lap, &L.lapP};
+            for (int t = 0; t < 5; t++) {
+                if (t == 2 && c->dim != 3) continue;
+                dst[t]->alloc(nk);
+                transpose_rowmajor_to_ell_d(rm[t].p, dst[t]->p, L.n, L.k, s);
+            }
+            // pinned solver operator, boundary row list, work vectors
+            L.A64.alloc(nk); L.A32.alloc(nk); L.dinv64.alloc(L.n); L.dinv32.alloc(L.n);
+            k_pin_operator<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.lapP.p, L.A64.p, L.A32.p, L.dinv64.p,
+                                                                   L.dinv32.p);
+            MGM_LAUNCHED();
+            std::vector<uint8_t> hb(L.n);
+            L.btag.download(hb.data(), L.n, s);
+            MGM_CUDA(cudaStreamSynchronize(s));
+            std::vector<int> bl;
+            for (int i = 0; i < L.n; i++) if (hb[i]) bl.push_back(i);
+            L.nbl = (int)bl.size();
+            L.bnd_list.upload(bl.data(), bl.size(), s);
+            for (DBuf<double> *b : {&L.p, &L.ptmp, &L.src, &L.res, &L.r64, &L.e64, &L.e64b, &L.d64, &L.q64}) { b->alloc(L.n); b->zero(s); }
+            for (DBuf<float> *b : {&L.r32, &L.e32, &L.e32b, &L.d32, &L.q32}) { b->alloc(L.n); b->zero(s); }
+        }
+        // smoother bounds and the coarsest-level inverse
+        for (int l = 0; l < c->nl - 1; l++) {
+            auto lv = solve_levels<double>(c);
+            estimate_lmax<double>(lv[l], s);
+            c->L[l].lmax = lv[l].lmax;
+        }
+        Level &Lc = c->L[c->nl - 1];
+        MGM_REQUIRE(Lc.n <= 8192, "mgm_setup: coarsest level too large for the dense solve (use more levels)");
+        c->cinv64.alloc((size_t)Lc.n * Lc.n);
+        c->cinv32.alloc((size_t)Lc.n * Lc.n);
+        dense_inverse(Lc.n, Lc.k, Lc.idx.p, Lc.A64.p, c->cinv64.p, c->cinv32.p, s);
+        // level-0 fields
+        const int n0 = c->L[0].n;
+        for (DBuf<double> *b : {&c->u, &c->v, &c->w, &c->u_new, &c->v_new, &c->w_new, &c->dpdn}) { b->alloc(n0); b->zero(s); }
+        c->partial.alloc(blocks_for(n0, 256) + 8);
+        c->scal.alloc(8);
+        alloc_solver_buffers(c);
+        MGM_CUDA(cudaStreamSynchronize(s));
+        c->setup_done = true;
+    });
+}
+
+int mgm_level_size(mgm_ctx *c, int lev, int *n, int *nb, int *k, int *np)
+{
+    return guard([&] {
+        MGM_REQUIRE(c && lev >= 0 && lev < c->nl, "mgm_level_size: bad level");
+        Level &L = c->L[lev];
+        if (n) *n = L.n;
+        if (nb) *nb = L.nb;
+        if (k) *k = L.k;
+        if (np) *np = L.np;
+    });
+}
+
+int mgm_level_d_avg(mgm_ctx *c, int lev, double *d)
+{
+    return guard([&] {
+        MGM_REQUIRE(c && lev >= 0 && lev < c->nl && c->setup_done, "mgm_level_d_avg: not set up");
+        *d = c->L[lev].d_avg;
+    });
+}
+
+int mgm_get_geometry(mgm_ctx *c, int lev, double *x, double *y, double *z, double *nx, double *ny, double *nz,
+                     unsigned char *btag, int *cloud)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(lev >= 0 && lev < c->nl && c->setup_done, "mgm_get_geometry: not set up");
+        Level &L = c->L[lev];
+        cudaStream_t s = c->s;
+        double *h[6] = {x, y, z, nx, ny, nz};
+        DBuf<double> *d[6] = {&L.x, &L.y, &L.z, &L.nx, &L.ny, &L.nz};
+        for (int t = 0; t < 6; t++) if (h[t]) d[t]->download(h[t], L.n, s);
+        if (btag) L.btag.download(btag, L.n, s);
+        if (cloud) L.cloud.download(cloud, (size_t)L.n * L.k, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int mgm_get_operators(mgm_ctx *c, int lev, double *Dx, double *Dy, double *Dz, double *lap, double *lapP)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(lev >= 0 && lev < c->nl && c->setup_done, "mgm_get_operators: not set up");
+        Level &L = c->L[lev];
+        cudaStream_t s = c->s;
+        const size_t nk = (size_t)L.n * L.k;
+        double *h[5] = {Dx, Dy, Dz, lap, lapP};
+        DBuf<double> *d[5] = {&L.Dx, &L.Dy, &L.Dz, &L.lap, &L.lapP};
+        DBuf<double> tmp(nk);
+        for (int t = 0; t < 5; t++) {
+            if (!h[t] || (t == 2 && c->dim != 3)) continue;
+            transpose_ell_to_rowmajor_d(d[t]->p, tmp.p, L.n, L.k, s);
+            tmp.download(h[t], nk, s);
+            MGM_CUDA(cudaStreamSynchronize(s));
+        }
+    });
+}
+
+int mgm_get_transfer(mgm_ctx *c, int lev, int *rpts, int *ppts, double *restr, double *prol)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(lev >= 0 && lev < c->nl && c->setup_done, "mgm_get_transfer: not set up");
+        Level &L = c->L[lev];
+        cudaStream_t s = c->s;
+        if (rpts) L.rpts.download(rpts, L.n, s);
+        if (ppts) L.ppts.download(ppts, L.n, s);
+        if (restr && lev > 0) {
+            MGM_REQUIRE(c->have_ref_transfer, "mgm_get_transfer: reference transfer rows were not built");
+            const int kf = c->L[lev - 1].k;
+            DBuf<double> tmp((size_t)L.n * kf);
+            transpose_ell_to_rowmajor_d(L.ref_restr.p, tmp.p, L.n, kf, s);
+            tmp.download(restr, (size_t)L.n * kf, s);
+            MGM_CUDA(cudaStreamSynchronize(s));
+        }
+        if (prol && lev < c->nl - 1) {
+            MGM_REQUIRE(c->have_ref_transfer, "mgm_get_transfer: reference transfer rows were not built");
+            const int kc = c->L[lev + 1].k;
+            DBuf<double> tmp((size_t)L.n * kc);
+            transpose_ell_to_rowmajor_d(L.ref_prol.p, tmp.p, L.n, kc, s);
+            tmp.download(prol, (size_t)L.n * kc, s);
+            MGM_CUDA(cudaStreamSynchronize(s));
+        }
+        MGM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int mgm_set_flow(mgm_ctx *c, double Re, double courant, float omega, int num_relax, int num_vcycles, double dt)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done, "mgm_set_flow: call mgm_setup first");
+        MGM_REQUIRE(Re > 0 && num_relax >= 0 && num_vcycles >= 0, "mgm_set_flow: bad parameters");
+        c->Re = Re; c->courant = courant; c->omega = omega; c->num_relax = num_relax; c->num_vcycles = num_vcycles;
+        c->rho = 1;
+        const double mu = c->rho / Re;
+        c->nu = mu / c->rho;
+        if (dt > 0) c->dt = dt;
+        else {
+            // calculate_dt (general_functions.h:34-41)
+            const double d = c->L[0].d_avg;
+            const double termd = 2 * c->nu / (d * d);
+            const double termc = 1 / d;
+            c->dt = 0.5 / (termd + termc) * courant;
+        }
+    });
+}
+
+int mgm_get_dt(mgm_ctx *c, double *dt)
+{
+    return guard([&] { MGM_REQUIRE(c, "null context"); *dt = c->dt; });
+}
+
+static DBuf<double> *field_buf(mgm_ctx *c, int lev, int which)
+{
+    Level &L = c->L[lev];
+    if (lev == 0) {
+        switch (which) {
+        case MGM_FIELD_U: return &c->u;
+        case MGM_FIELD_V: return &c->v;
+        case MGM_FIELD_W: return &c->w;
+        case MGM_FIELD_U_NEW: return &c->u_new;
+        case MGM_FIELD_V_NEW: return &c->v_new;
+        case MGM_FIELD_W_NEW: return &c->w_new;
+        case MGM_FIELD_DPDN: return &c->dpdn;
+        }
+    }
+    switch (which) {
+    case MGM_FIELD_P: return &L.p;
+    case MGM_FIELD_RES: return &L.res;
+    case MGM_FIELD_SOURCE: return &L.src;
+    }
+    throw Error{MGM_ERR_ARG, "unknown field id for this level"};
+}
+
+int mgm_set_field(mgm_ctx *c, int lev, int which, const double *values)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done && lev >= 0 && lev < c->nl, "mgm_set_field: not set up");
+        field_buf(c, lev, which)->upload(values, c->L[lev].n, c->s);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+    });
+}
+
+int mgm_get_field(mgm_ctx *c, int lev, int which, double *values)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done && lev >= 0 && lev < c->nl, "mgm_get_field: not set up");
+        field_buf(c, lev, which)->download(values, c->L[lev].n, c->s);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+    });
+}
+
+int mgm_apply_bc(mgm_ctx *c, int kind)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done, "mgm_apply_bc: call mgm_setup first");
+        MGM_REQUIRE(kind == MGM_BC_LID || kind == MGM_BC_TAYLOR_COUETTE, "mgm_apply_bc: unknown kind");
+        cudaStream_t s = c->s;
+        for (DBuf<double> *b : {&c->u, &c->v, &c->w, &c->u_new, &c->v_new, &c->w_new}) b->zero(s);
+        c->L[0].p.zero(s);
+        Level &L = c->L[0];
+        k_bc<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, kind, L.x.p, L.y.p, c->u.p, c->v.p, c->u_new.p, c->v_new.p);
+        MGM_LAUNCHED();
+        MGM_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int mgm_set_solver(mgm_ctx *c, double rel_tol, int max_iters, int cheb_degree, double cheb_ratio)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(rel_tol > 0 && max_iters >= 1 && max_iters <= kMaxKrylov && cheb_degree >= 1 && cheb_degree <= 16 &&
+                        cheb_ratio > 1, "mgm_set_solver: bad parameters");
+        c->tol = rel_tol; c->cheb_deg = cheb_degree; c->cheb_ratio = cheb_ratio;
+        if (max_iters != c->max_iters) {
+            c->max_iters = max_iters;
+            if (c->setup_done) alloc_solver_buffers(c);
+        }
+    });
+}
+
+int mgm_last_solve(mgm_ctx *c, int *iters, double *rel_res)
+{
+    return guard([&] {
+        MGM_REQUIRE(c, "null context");
+        if (iters) *iters = c->last_iters;
+        if (rel_res) *rel_res = c->last_relres;
+    });
+}
+
+int mgm_intermediate_velocity(mgm_ctx *c)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done && c->dt > 0, "mgm_intermediate_velocity: call mgm_setup and mgm_set_flow first");
+        launch_momentum(step_args(c), c->dim, c->s);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+    });
+}
+
+int mgm_mass_residual(mgm_ctx *c)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done && c->dt > 0, "mgm_mass_residual: not ready");
+        launch_divergence(step_args(c), c->dim, c->s);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+    });
+}
+
+int mgm_poisson(mgm_ctx *c, int mode)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done, "mgm_poisson: not ready");
+        poisson(c, mode);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+    });
+}
+
+int mgm_update_velocity(mgm_ctx *c, double *mass_res)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done && c->dt > 0, "mgm_update_velocity: not ready");
+        StepArgs a = step_args(c);
+        launch_correct(a, c->dim, c->partial.p, c->scal.p, c->s);
+        if (mass_res) {
+            launch_mass_diag(a, c->dim, c->partial.p, c->scal.p + 1, c->s);
+            c->scal.download(c->h_pinned, 2, c->s);
+            MGM_CUDA(cudaStreamSynchronize(c->s));
+            *mass_res = c->h_pinned[1];
+        }
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+    });
+}
+
+int mgm_step(mgm_ctx *c, int mode, double *steady_err)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done && c->dt > 0, "mgm_step: call mgm_setup and mgm_set_flow first");
+        StepArgs a = step_args(c);
+        launch_momentum(a, c->dim, c->s);
+        launch_divergence(a, c->dim, c->s);
+        poisson(c, mode);
+        launch_correct(a, c->dim, c->partial.p, c->scal.p, c->s);
+        c->scal.download(c->h_pinned, 1, c->s);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+        if (steady_err) *steady_err = c->h_pinned[0];
+    });
+}
+
+int mgm_solve_poisson(mgm_ctx *c, int mode, const double *b, double *p, int *iters, double *rel_res)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done, "mgm_solve_poisson: not ready");
+        MGM_REQUIRE(mode == MGM_MODE_FP64 || mode == MGM_MODE_FP32_IR, "mgm_solve_poisson: mode must be FP64 or FP32_IR");
+        Level &L0 = c->L[0];
+        L0.src.upload(b, L0.n, c->s);
+        L0.p.upload(p, L0.n, c->s);
+        poisson(c, mode);
+        L0.p.download(p, L0.n, c->s);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+        if (iters) *iters = c->last_iters;
+        if (rel_res) *rel_res = c->last_relres;
+    });
+}
+
+int mgm_sync(mgm_ctx *c)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+    });
+}
+
+}  // extern "C"

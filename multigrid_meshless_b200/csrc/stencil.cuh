@@ -1,0 +1,81 @@
+// stencil.cuh -- argument blocks of the stencil and solver kernels.
+#pragma once
+#include "mgm_internal.cuh"
+
+namespace mgm {
+
+// level-0 state of one fractional step (device pointers; operators ELL [k][n])
+struct StepArgs {
+    int n, k;
+    const int *idx;
+    const double *Dx, *Dy, *Dz, *lap;
+    const uint8_t *btag;
+    const double *nx, *ny, *nz;
+    double *u, *v, *w, *u_new, *v_new, *w_new;
+    double *p, *source, *dpdn;
+    double dt, nu, rho;
+};
+
+void launch_momentum(const StepArgs &a, int dim, cudaStream_t s);
+void launch_divergence(const StepArgs &a, int dim, cudaStream_t s);
+void launch_correct(const StepArgs &a, int dim, double *partial, double *d_err, cudaStream_t s);
+void launch_mass_diag(const StepArgs &a, int dim, double *partial, double *d_out, cudaStream_t s);
+
+// one level of the reference-semantics multigrid
+struct RefLevel {
+    int n, k;
+    const int *idx;
+    const double *lap, *lapP;
+    const uint8_t *btag;
+    double *p, *ptmp, *src, *res;
+    // restriction into this level: gather index into the finer level's res (ELL [k_fine][n])
+    const int *r_idx;
+    const double *restr;
+    // prolongation into this level from the coarser level (ELL [k_coarse][n])
+    const int *p_idx;
+    const double *prol;
+};
+
+void ref_relaxation(const RefLevel &L, double w1, double w2, int num_relax, cudaStream_t s);
+void ref_residual_interior(const RefLevel &L, cudaStream_t s);
+void ref_restrict(const RefLevel &F, const RefLevel &C, cudaStream_t s);
+void ref_prolongate(const RefLevel &F, const RefLevel &C, cudaStream_t s);
+void ref_multigrid(std::vector<RefLevel> &Ls, double w1, double w2, int num_relax, int num_vcycles, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// convergent solver (solver.cu)
+// ---------------------------------------------------------------------------
+// One level of the preconditioning V-cycle in precision T.
+template <class T>
+struct SolveLevel {
+    int n, k, nb_list;            // rows, stencil width, number of boundary rows
+    const int *idx;               // ELL [k][n]
+    const T *A;                   // lap_Poison, row 0 replaced by the pin (A[0][0] = 1, rest 0)
+    const T *dinv;                // 1 / diagonal
+    const uint8_t *btag;
+    const int *bnd_list;          // boundary rows (incl. the pinned row 0)
+    T *r, *e, *e2, *d, *q;        // rhs, correction (double-buffered), Chebyshev direction, residual
+    // restriction into this level (coarse row i <- fine interior residual), ELL [kf][n]
+    int kr;
+    const int *r_idx;
+    const T *r_w;
+    // prolongation from the coarser level into this level (all rows), ELL [kc][n]
+    int kp;
+    const int *p_idx;
+    const T *p_w;
+    double lmax;                  // spectral radius estimate of D^-1 A on interior rows
+};
+
+template <class T>
+struct CoarseSolve {
+    int n;
+    const T *inv;  // dense inverse of the pinned coarsest operator, row-major [n][n]
+};
+
+template <class T>
+void vcycle(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int cheb_degree, double cheb_ratio,
+            cudaStream_t s);
+template <class T>
+void estimate_lmax(SolveLevel<T> &L, cudaStream_t s);
+
+}  // namespace mgm

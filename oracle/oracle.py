@@ -1,0 +1,372 @@
+"""ctypes front-end of the CPU checkers (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference
+legs import this module.  It loads
+  * oracle/liboracle.so   -- the project's restatement of the reference hot path
+                            (mgm_oracle.c), and
+  * oracle/_ref/libref.so -- the reference's own C code compiled from its
+                            sources (ref_shim.c), when it has been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_ORC = {}
+_REF = None
+
+dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+
+
+def lib(crpow: bool = False):
+    """liboracle.so (libm pow, as the reference) or liboracle_crpow.so
+    (correctly rounded powers, as the CUDA path)."""
+    key = "crpow" if crpow else "libm"
+    if key not in _ORC:
+        path = os.path.join(HERE, "liboracle_crpow.so" if crpow else "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: run `make -C oracle`")
+        L = C.CDLL(path)
+        L.orc_knn_cloud.argtypes = [C.c_int, C.c_int, dp, dp, dp, u8p, C.c_int, C.c_int, ip]
+        L.orc_count_ties.argtypes = [C.c_int, C.c_int, dp, dp, dp, C.c_int, ip]
+        L.orc_count_ties.restype = C.c_long
+        L.orc_nearest.argtypes = [C.c_int, dp, dp, dp, C.c_int, dp, dp, dp, C.c_int, ip]
+        L.orc_bfs_order.argtypes = [C.c_int, C.c_int, ip, ip]
+        L.orc_bfs_order.restype = C.c_int
+        L.orc_apply_order.argtypes = [C.c_int, C.c_int, ip, dp, dp, dp, dp, dp, dp, u8p, ip]
+        L.orc_correct_normals.argtypes = [C.c_int, C.c_int, dp, dp, dp, u8p, ip, dp, dp, dp]
+        L.orc_avg_dx.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp, dp, u8p, ip]
+        L.orc_avg_dx.restype = C.c_double
+        L.orc_dt.argtypes = [C.c_double, C.c_double, C.c_double]
+        L.orc_dt.restype = C.c_double
+        L.orc_derivative_weights.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, dp, dp,
+                                             u8p, ip, dp, dp, dp, dp, dp]
+        L.orc_transfer_weights.argtypes = [C.c_int, dp, dp, dp, u8p, ip, C.c_int, C.c_int,
+                                           C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, dp, dp, dp, ip, dp]
+        L.orc_spmv.argtypes = [C.c_int, C.c_int, dp, ip, dp, dp]
+        L.orc_ctx_new.restype = C.c_void_p
+        L.orc_ctx_new.argtypes = [C.c_int, C.c_int]
+        L.orc_ctx_free.argtypes = [C.c_void_p]
+        L.orc_ctx_level.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, ip, u8p, dp, dp, dp, dp, dp, dp, dp, dp,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, dp, dp, dp]
+        L.orc_ctx_fields.argtypes = [C.c_void_p] + [dp] * 13
+        L.orc_ctx_params.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_float, C.c_int, C.c_int, C.c_int]
+        L.orc_multigrid.argtypes = [C.c_void_p]
+        L.orc_relaxation.argtypes = [C.c_void_p, C.c_int]
+        L.orc_step.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.orc_step.restype = C.c_double
+        for nm in ("orc_intermediate_velocity", "orc_mass_residual"):
+            getattr(L, nm).argtypes = [C.c_void_p]
+        L.orc_update_velocity.argtypes = [C.c_void_p]
+        L.orc_update_velocity.restype = C.c_double
+        _ORC[key] = L
+    return _ORC[key]
+
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libref.so"))
+
+
+def ref_lib():
+    global _REF
+    if _REF is None:
+        path = os.path.join(HERE, "_ref", "libref.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
+        L = C.CDLL(path)
+        L.ref_begin.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.ref_set_flow.argtypes = [C.c_double, C.c_double, C.c_float, C.c_int, C.c_int]
+        L.ref_set_level.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, dp, dp, u8p, C.c_int, C.c_int, C.c_double]
+        for nm in ("ref_clouds", "ref_rcm", "ref_normals", "ref_derivatives", "ref_relaxation", "ref_residuals",
+                   "ref_restrict", "ref_prolongate"):
+            getattr(L, nm).argtypes = [C.c_int]
+        L.ref_avg_dx.argtypes = [C.c_int]
+        L.ref_avg_dx.restype = C.c_double
+        L.ref_set_davg.argtypes = [C.c_int, C.c_double]
+        L.ref_num_poly_terms.argtypes = [C.c_int]
+        L.ref_get_geometry.argtypes = [C.c_int, dp, dp, dp, dp, dp, dp, u8p, ip]
+        L.ref_get_ops.argtypes = [C.c_int, dp, dp, dp, dp, dp]
+        L.ref_get_transfer.argtypes = [C.c_int, ip, ip, C.c_void_p, C.c_void_p]
+        L.ref_bc.argtypes = [C.c_int]
+        L.ref_dt.restype = C.c_double
+        L.ref_set_dt.argtypes = [C.c_double]
+        L.ref_field_get.argtypes = [C.c_int, C.c_int, dp]
+        L.ref_field_set.argtypes = [C.c_int, C.c_int, dp]
+        L.ref_step.restype = C.c_double
+        L.ref_spmv.argtypes = [C.c_int, C.c_int, dp, dp]
+        _REF = L
+    return _REF
+
+
+# field ids of ref_shim.c:field_ptr
+FIELD = {"u": 0, "v": 1, "w": 2, "p": 3, "u_new": 4, "v_new": 5, "w_new": 6, "u_old": 7, "v_old": 8,
+         "w_old": 9, "res": 10, "source": 11, "dpdn": 12, "dpdx": 13, "dpdy": 14, "dpdz": 15}
+
+
+@dataclass
+class Level:
+    """One level after the reference's set-up pipeline (arrays row-major [n][k])."""
+    n: int
+    nb: int
+    k: int
+    dim: int
+    poly: int
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    nx: np.ndarray
+    ny: np.ndarray
+    nz: np.ndarray
+    btag: np.ndarray
+    cloud: np.ndarray
+    d_avg: float = 0.0
+    Dx: np.ndarray | None = None
+    Dy: np.ndarray | None = None
+    Dz: np.ndarray | None = None
+    lap: np.ndarray | None = None
+    lapP: np.ndarray | None = None
+    rpts: np.ndarray | None = None
+    ppts: np.ndarray | None = None
+    restr: np.ndarray | None = None   # [n][k of finer level]
+    prol: np.ndarray | None = None    # [n][k of coarser level]
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def ref_pipeline(clouds, ks, polys, phs=3, with_weights=True, search_scale=0.3):
+    """Runs read_complete_mesh_data's steps (minus the file reader) and
+    create_derivative_matrices through the reference's own code."""
+    R = ref_lib()
+    nl = len(clouds)
+    dim = clouds[0].dim
+    R.ref_begin(dim, phs, nl)
+    for l, c in enumerate(clouds):
+        R.ref_set_level(l, c.n, c.nb, _f64(c.x), _f64(c.y), _f64(c.z), _f64(c.nx), _f64(c.ny), _f64(c.nz),
+                        np.ascontiguousarray(c.btag, np.uint8), polys[l], ks[l], search_scale * c.h)
+        R.ref_clouds(l)
+        R.ref_rcm(l)
+        R.ref_normals(l)
+        R.ref_avg_dx(l)
+    out = []
+    for l, c in enumerate(clouds):
+        n, k = c.n, ks[l]
+        a = {nm: np.zeros(n) for nm in ("x", "y", "z", "nx", "ny", "nz")}
+        bt = np.zeros(n, np.uint8)
+        cl = np.zeros(n * k, np.int32)
+        R.ref_get_geometry(l, a["x"], a["y"], a["z"], a["nx"], a["ny"], a["nz"], bt, cl)
+        d_avg = R.ref_avg_dx(l)
+        out.append(Level(n, c.nb, k, dim, polys[l], a["x"], a["y"], a["z"], a["nx"], a["ny"], a["nz"], bt,
+                         cl.reshape(n, k), d_avg))
+    if with_weights:
+        R.ref_rp()
+        for l in range(nl):
+            R.ref_derivatives(l)
+        for l, L in enumerate(out):
+            n, k = L.n, L.k
+            ops = [np.zeros(n * k) for _ in range(5)]
+            R.ref_get_ops(l, *ops)
+            L.Dx, L.Dy, L.Dz, L.lap, L.lapP = [o.reshape(n, k) for o in ops]
+            if dim != 3:
+                L.Dz = None
+            rp = np.zeros(n, np.int32); pp = np.zeros(n, np.int32)
+            restr = np.zeros(n * out[l - 1].k) if l > 0 else None
+            prol = np.zeros(n * out[l + 1].k) if l < nl - 1 else None
+            R.ref_get_transfer(l, rp, pp,
+                               restr.ctypes.data if restr is not None else None,
+                               prol.ctypes.data if prol is not None else None)
+            L.rpts, L.ppts = rp, pp
+            L.restr = restr.reshape(n, out[l - 1].k) if restr is not None else None
+            L.prol = prol.reshape(n, out[l + 1].k) if prol is not None else None
+    return out
+
+
+def orc_level_setup(c, k, crpow=False):
+    """kNN -> breadth-first reorder -> normals -> d_avg on one cloud (restatement)."""
+    O = lib(crpow)
+    n = c.n
+    x, y, z = _f64(c.x).copy(), _f64(c.y).copy(), _f64(c.z).copy()
+    nx, ny, nz = _f64(c.nx).copy(), _f64(c.ny).copy(), _f64(c.nz).copy()
+    bt = np.ascontiguousarray(c.btag, np.uint8).copy()
+    cl = np.zeros(n * k, np.int32)
+    O.orc_knn_cloud(n, c.nb, x, y, z, bt, k, c.dim, cl)
+    q1 = np.zeros(n, np.int32)
+    cnt = O.orc_bfs_order(n, k, cl, q1)
+    if cnt != n:
+        raise RuntimeError(f"stencil graph disconnected: reached {cnt} of {n} nodes")
+    O.orc_apply_order(n, k, q1, x, y, z, nx, ny, nz, bt, cl)
+    O.orc_correct_normals(n, k, x, y, z, bt, cl, nx, ny, nz)
+    d_avg = O.orc_avg_dx(n, k, c.dim, x, y, z, bt, cl)
+    return dict(x=x, y=y, z=z, nx=nx, ny=ny, nz=nz, btag=bt, cloud=cl.reshape(n, k), d_avg=d_avg, queue1=q1)
+
+
+def orc_pipeline(clouds, ks, polys, phs=3, with_weights=True, reference_rows=True, crpow=False):
+    """The restatement of ref_pipeline.  reference_rows=False builds the
+    transfer weights for every non-boundary row (convergent-solver variant)."""
+    O = lib(crpow)
+    dim = clouds[0].dim
+    nl = len(clouds)
+    out = []
+    for l, c in enumerate(clouds):
+        s = orc_level_setup(c, ks[l], crpow)
+        out.append(Level(c.n, c.nb, ks[l], dim, polys[l], s["x"], s["y"], s["z"], s["nx"], s["ny"], s["nz"],
+                         s["btag"], s["cloud"], s["d_avg"]))
+    # create_prolongation_and_restriction_matrices (mesh_functions.h:874-893)
+    for l, L in enumerate(out):
+        nxt = out[l + 1] if l < nl - 1 else L
+        prv = out[l - 1] if l > 0 else L
+        L.ppts = np.zeros(L.n, np.int32)
+        O.orc_nearest(L.n, L.x, L.y, L.z, nxt.n, nxt.x, nxt.y, nxt.z, dim, L.ppts)
+        L.rpts = np.zeros(L.n, np.int32)
+        O.orc_nearest(L.n, L.x, L.y, L.z, prv.n, prv.x, prv.y, prv.z, dim, L.rpts)
+    if not with_weights:
+        return out
+    for l, L in enumerate(out):
+        if l < nl - 1:
+            C_ = out[l + 1]
+            W = np.zeros(L.n * C_.k)
+            O.orc_transfer_weights(L.n, L.x, L.y, L.z, L.btag, L.ppts, L.nb, 0 if reference_rows else 1,
+                                   C_.n, C_.k, dim, phs, C_.poly, C_.x, C_.y, C_.z,
+                                   np.ascontiguousarray(C_.cloud.ravel()), W)
+            L.prol = W.reshape(L.n, C_.k)
+        if l > 0:
+            F = out[l - 1]
+            W = np.zeros(L.n * F.k)
+            O.orc_transfer_weights(L.n, L.x, L.y, L.z, L.btag, L.rpts, L.nb, 0 if reference_rows else 1,
+                                   F.n, F.k, dim, phs, F.poly, F.x, F.y, F.z,
+                                   np.ascontiguousarray(F.cloud.ravel()), W)
+            L.restr = W.reshape(L.n, F.k)
+        n, k = L.n, L.k
+        ops = [np.zeros(n * k) for _ in range(5)]
+        O.orc_derivative_weights(n, k, dim, phs, L.poly, L.x, L.y, L.z, L.nx, L.ny, L.nz, L.btag,
+                                 np.ascontiguousarray(L.cloud.ravel()), *ops)
+        L.Dx, L.Dy, L.Dz, L.lap, L.lapP = [o.reshape(n, k) for o in ops]
+        if dim != 3:
+            L.Dz = None
+    return out
+
+
+class OracleSolver:
+    """Reference-semantics fractional step on restated levels (mgm_oracle.c)."""
+
+    def __init__(self, levels, Re, courant, omega, num_relax, num_vcycles, jacobi=True, dt=None):
+        O = lib()
+        self.O = O
+        self.levels = levels
+        L0 = levels[0]
+        self.h = O.orc_ctx_new(len(levels), L0.dim)
+        self.keep = []
+        self.p, self.source, self.res = [], [], []
+        for l, L in enumerate(levels):
+            p = np.zeros(L.n); s = np.zeros(L.n); r = np.zeros(L.n)
+            self.p.append(p); self.source.append(s); self.res.append(r)
+            Dz = L.Dz if L.Dz is not None else np.zeros((L.n, L.k))
+            arrs = [np.ascontiguousarray(L.cloud.ravel(), np.int32), L.btag, L.nx, L.ny, L.nz,
+                    np.ascontiguousarray(L.Dx.ravel()), np.ascontiguousarray(L.Dy.ravel()),
+                    np.ascontiguousarray(Dz.ravel()), np.ascontiguousarray(L.lap.ravel()),
+                    np.ascontiguousarray(L.lapP.ravel())]
+            rp = np.ascontiguousarray(L.rpts, np.int32)
+            pp = np.ascontiguousarray(L.ppts, np.int32)
+            restr = np.ascontiguousarray(L.restr.ravel()) if L.restr is not None else None
+            prol = np.ascontiguousarray(L.prol.ravel()) if L.prol is not None else None
+            self.keep += arrs + [rp, pp, restr, prol]
+            O.orc_ctx_level(self.h, l, L.n, L.k, *arrs, rp.ctypes.data, pp.ctypes.data,
+                            restr.ctypes.data if restr is not None else None,
+                            prol.ctypes.data if prol is not None else None, p, s, r)
+        n = L0.n
+        self.f = {nm: np.zeros(n) for nm in ("u", "v", "w", "u_new", "v_new", "w_new", "u_old", "v_old", "w_old",
+                                             "dpdn", "dpdx", "dpdy", "dpdz")}
+        O.orc_ctx_fields(self.h, *[self.f[nm] for nm in ("u", "v", "w", "u_new", "v_new", "w_new", "u_old",
+                                                         "v_old", "w_old", "dpdn", "dpdx", "dpdy", "dpdz")])
+        if dt is None:
+            dt = O.orc_dt(L0.d_avg, Re, courant)
+        self.dt = dt
+        O.orc_ctx_params(self.h, dt, Re, omega, num_relax, num_vcycles, 1 if jacobi else 0)
+
+    def step(self):
+        mr = C.c_double(0)
+        e = self.O.orc_step(self.h, C.byref(mr))
+        return e, mr.value
+
+    def multigrid(self):
+        self.O.orc_multigrid(self.h)
+
+    def __del__(self):
+        try:
+            self.O.orc_ctx_free(self.h)
+        except Exception:
+            pass
+
+
+def lid_bc(L, f):
+    """init_LDC.c:16-44 on level 0: u = 1 where |y - 1| < 1e-9."""
+    f["u"][:] = 0; f["v"][:] = 0; f["w"][:] = 0
+    top = np.abs(L.y - 1.0) < 1e-9
+    f["u"][top] = 1.0
+
+
+def tc_bc(L, f):
+    """init_TC.c:17-54 on level 0: inner wall r = 0.5 rotating, u = -y/r, v = x/r."""
+    for nm in ("u", "v", "w", "u_new", "v_new", "w_new"):
+        f[nm][:] = 0
+    r = np.sqrt(L.x * L.x + L.y * L.y)
+    inner = np.abs(r - 0.5) < 1e-9
+    f["u"][inner] = -L.y[inner] / r[inner]
+    f["v"][inner] = L.x[inner] / r[inner]
+    f["u_new"][inner] = f["u"][inner]
+    f["v_new"][inner] = f["v"][inner]
+
+
+def pinned_operator(lapP, cloud):
+    """lap_Poison as a scipy CSR matrix with row 0 replaced by p[0] = 0 -- the
+    system the reference's multigrid aims at (it re-pins p to node 0 after every
+    sweep, fractional_step_solver.h:180-183)."""
+    import scipy.sparse as sp
+    n, k = lapP.shape
+    A = sp.csr_matrix((np.ascontiguousarray(lapP.ravel()).copy(), np.ascontiguousarray(cloud.ravel()).astype(np.int64),
+                       np.arange(0, n * k + 1, k)), shape=(n, n))
+    A = A.tolil()
+    A[0, :] = 0
+    A[0, 0] = 1.0
+    return A.tocsr()
+
+
+def pinned_poisson_direct(lapP, cloud, b):
+    """FP64 direct solve of the pinned system (the converged answer every
+    iterative mode is compared with).  b[0] is taken as 0."""
+    import scipy.sparse.linalg as spla
+    A = pinned_operator(lapP, cloud)
+    bb = np.array(b, dtype=np.float64)
+    bb[0] = 0.0
+    return spla.spsolve(A.tocsc(), bb)
+
+
+def rel_residual(lapP, cloud, b, p):
+    A = pinned_operator(lapP, cloud)
+    bb = np.array(b, dtype=np.float64)
+    bb[0] = 0.0
+    r = bb - A @ p
+    return float(np.linalg.norm(r) / np.linalg.norm(bb))
+
+
+def levels_from_device(mg):
+    """Oracle Level objects holding the operators a device hierarchy built
+    (so the restated step runs on bit-identical weights)."""
+    out = []
+    for l in range(mg.nl):
+        g = mg.geometry(l)
+        ops = mg.operators(l)
+        tr = mg.transfer(l)
+        n, nb, k, _ = mg.sizes[l]
+        L = Level(n, nb, k, mg.dim, 0, g["x"], g["y"], g["z"], g["nx"], g["ny"], g["nz"], g["btag"], g["cloud"],
+                  g["d_avg"], ops["Dx"], ops["Dy"], ops.get("Dz"), ops["lap"], ops["lapP"], tr["rpts"], tr["ppts"],
+                  tr["restr"], tr["prol"])
+        out.append(L)
+    return out

@@ -1,0 +1,118 @@
+"""The fractional step and the Poisson solves on the GPU, through the C ABI.
+
+* MGM_MODE_REFERENCE: the reference's fractional_step_explicit with its
+  multigrid_Poisson_solver, sweeps in data-parallel (Jacobi) order.  Compared
+  bit for bit with the oracle restatement run in the same sweep order on the
+  same (device-built) operators; the steady-state error is a reduction whose
+  summation order differs, compared to 1e-12 relative.
+* MGM_MODE_FP64 / MGM_MODE_FP32_IR: the pinned Poisson system solved to a
+  1e-8 relative residual; the pressure must match an FP64 direct solve to
+  1e-6 relative L2 (the parity bound for pressure and velocity).
+"""
+import numpy as np
+import pytest
+
+import multigrid_meshless_b200 as mgm
+from multigrid_meshless_b200 import api, clouds
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+P_TOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def cavity(require_gpu):
+    cl = clouds.cavity_hierarchy(48, 3, seed=21)
+    mg = api.Multigrid(cl, [20, 20, 20], [3, 3, 3], reference_transfer=True)
+    yield mg
+    mg.close()
+
+
+def test_reference_mode_step_bit_exact(cavity):
+    mg = cavity
+    levels = O.levels_from_device(mg)
+    dt = mg.set_flow(Re=100.0, courant=0.5, omega=1.2, num_relax=3, num_vcycles=2)
+    S = O.OracleSolver(levels, 100.0, 0.5, 1.2, 3, 2, jacobi=True)
+    assert S.dt == dt
+    mg.apply_bc(mgm.BC_LID)
+    O.lid_bc(levels[0], S.f)
+    assert np.array_equal(mg.get_field("u"), S.f["u"])
+    for s in range(3):
+        err = mg.step(mgm.MODE_REFERENCE)
+        err_o, _ = S.step()
+        for nm in ("u", "v", "u_new", "v_new"):
+            assert np.array_equal(mg.get_field(nm), S.f[nm]), f"step {s}: {nm}"
+        assert np.array_equal(mg.get_field("p"), S.p[0]), f"step {s}: p"
+        assert np.array_equal(mg.get_field("source"), S.source[0]), f"step {s}: source"
+        for l in range(1, mg.nl):
+            assert np.array_equal(mg.get_field("p", l), S.p[l]), f"step {s}: p level {l}"
+        assert abs(err - err_o) <= 1e-12 * abs(err_o)
+
+
+def test_parts_of_the_step_bit_exact(cavity):
+    mg = cavity
+    levels = O.levels_from_device(mg)
+    mg.set_flow(Re=400.0, courant=0.3, omega=1.0, num_relax=2, num_vcycles=1)
+    S = O.OracleSolver(levels, 400.0, 0.3, 1.0, 2, 1, jacobi=True)
+    rng = np.random.default_rng(5)
+    n = mg.n()
+    for nm in ("u", "v"):
+        vals = rng.standard_normal(n) * 0.1
+        mg.set_field(nm, vals)
+        S.f[nm][:] = vals
+    mg.intermediate_velocity()
+    S.O.orc_intermediate_velocity(S.h)
+    assert np.array_equal(mg.get_field("u_new"), S.f["u_new"])
+    assert np.array_equal(mg.get_field("v_new"), S.f["v_new"])
+    mg.mass_residual()
+    S.O.orc_mass_residual(S.h)
+    assert np.array_equal(mg.get_field("source"), S.source[0])
+
+
+def _smooth_rhs(L, seed):
+    rng = np.random.default_rng(seed)
+    a, b = rng.uniform(1, 3, 2)
+    f = np.cos(a * np.pi * L["x"]) * np.cos(b * np.pi * L["y"]) + 0.3 * np.sin(3 * L["x"] * L["y"])
+    f[L["btag"] == 1] = 0.0
+    f[0] = 0.0
+    return f
+
+
+@pytest.mark.parametrize("mode", [mgm.MODE_FP64, mgm.MODE_FP32_IR], ids=["fp64", "fp32_ir"])
+def test_poisson_converges_to_direct_solution(cavity, mode):
+    mg = cavity
+    mg.set_flow(Re=100.0, courant=0.5)
+    mg.set_solver(rel_tol=1e-8, max_iters=80)
+    g = mg.geometry(0)
+    ops = mg.operators(0)
+    b = _smooth_rhs(g, 1)
+    p, iters, rr = mg.solve_poisson(b, mode=mode)
+    assert rr < 1e-8
+    assert O.rel_residual(ops["lapP"], g["cloud"], b, p) < 2e-8
+    p_ref = O.pinned_poisson_direct(ops["lapP"], g["cloud"], b)
+    err = np.linalg.norm(p - p_ref) / np.linalg.norm(p_ref)
+    assert err < P_TOL, (err, iters)
+
+
+def test_solver_mode_steps_match_direct_solve_steps(cavity):
+    """Three fractional steps with the FP32-in-FP64 solve against the restated
+    step whose Poisson solve is an FP64 direct solve."""
+    mg = cavity
+    levels = O.levels_from_device(mg)
+    mg.set_flow(Re=100.0, courant=0.5)
+    mg.set_solver(rel_tol=1e-10, max_iters=100)
+    S = O.OracleSolver(levels, 100.0, 0.5, 1.0, 1, 1, jacobi=True)
+    mg.apply_bc(mgm.BC_LID)
+    O.lid_bc(levels[0], S.f)
+    for s in range(3):
+        mg.step(mgm.MODE_FP32_IR)
+        S.O.orc_intermediate_velocity(S.h)
+        S.O.orc_mass_residual(S.h)
+        S.p[0][:] = O.pinned_poisson_direct(levels[0].lapP, levels[0].cloud, S.source[0])
+        S.O.orc_update_velocity(S.h)
+        for nm in ("u", "v"):
+            a, b = mg.get_field(nm), S.f[nm]
+            assert np.linalg.norm(a - b) / np.linalg.norm(b) < P_TOL, (s, nm)
+        a, b = mg.get_field("p"), S.p[0]
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < P_TOL, (s, "p")
