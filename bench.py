@@ -1,0 +1,387 @@
+#!/usr/bin/env python
+"""bench.py -- NS steps/s & Poisson ms at 1M nodes, Poisson solved to a 1e-8
+relative residual: FP32-in-FP64 refinement vs plain FP64 on the GPU.
+
+Workload (the 1M-node 2D lid-driven cavity): unit square, 1000 x 1000 jittered
+Cartesian nodes (999,996 after the corner nodes are removed), 6 levels each
+coarser by 4x, PHS degree 3, polynomial degree 4 (15 terms), 30-node stencils,
+Re = 100, Courant 0.5.  A step is one fractional step (momentum, divergence,
+Poisson solve to 1e-8, velocity correction) through the C ABI.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own C implementation of the step
+(oracle/_ref/libref.so, compiled from the reference sources) on the host
+cores, on a bounded sample of the same construction, scaled to 1M nodes.
+Under torchrun each rank runs an independent replica on its own GPU
+("replicas only": the path has no exchange step); rank 0 prints the line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "NS steps/s & Poisson ms @1M nodes, 1e-8 resid: learned+FP32 vs plain FP64 GPU"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--m", type=int, default=1000, help="nodes per side of the fine cavity level")
+    ap.add_argument("--levels", type=int, default=6)
+    ap.add_argument("--k", type=int, default=30)
+    ap.add_argument("--poly", type=int, default=4)
+    ap.add_argument("--Re", type=float, default=100.0)
+    ap.add_argument("--courant", type=float, default=0.5)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--cheb-degree", type=int, default=4)
+    ap.add_argument("--cheb-ratio", type=float, default=10.0)
+    ap.add_argument("--sample-m", type=int, default=128, help="cavity size of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(a):
+    return {
+        "workload": f"2D lid-driven cavity, {a.m}x{a.m} jittered nodes, {a.levels} levels (/4), PHS3 + poly{a.poly}, "
+                    f"k={a.k}, Re={a.Re:g}, Courant {a.courant:g}, Poisson to {a.tol:g} rel. residual",
+        "nodes": a.m * a.m - 4,
+        "levels": a.levels,
+        "k": a.k,
+        "poly_degree": a.poly,
+        "Re": a.Re,
+        "courant": a.courant,
+        "rel_tol": a.tol,
+        "l2": "inputs larger than L2 (operators + hierarchy ~2 GB per step, L2 126 MB)",
+        "seed": 1,
+    }
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference's own fractional step on a bounded sample
+# ---------------------------------------------------------------------------
+def reference_sample(a, steps, warmup):
+    """Times fractional_step_explicit of the reference build (or, if it was
+    not built, the oracle restatement) on a cavity of a.sample-m nodes per side
+    with the same stencil/polynomial settings; returns per-step seconds."""
+    from multigrid_meshless_b200 import clouds
+    from oracle import oracle as O
+    nl = 3
+    cl = clouds.cavity_hierarchy(a.sample_m, nl, seed=1)
+    n = cl[0].n
+    ks, polys = [a.k] * nl, [a.poly] * nl
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    saved = os.dup(1)
+    os.dup2(devnull, 1)  # the reference prints its parameters and a line per step
+    try:
+        return _reference_sample(a, steps, warmup, cl, n, nl, ks, polys, O)
+    finally:
+        os.dup2(saved, 1)
+        os.close(devnull)
+        os.close(saved)
+
+
+def _reference_sample(a, steps, warmup, cl, n, nl, ks, polys, O):
+    t0 = time.perf_counter()
+    if O.ref_available():
+        kind = "reference"
+        levels = O.ref_pipeline(cl, ks, polys, with_weights=True)
+        R = O.ref_lib()
+        R.ref_set_flow(a.courant, a.Re, 1.0, 10, 3)
+        R.ref_fields_alloc()
+        R.ref_bc(0)
+        R.ref_dt()
+        setup_s = time.perf_counter() - t0
+        step = R.ref_step
+    else:
+        kind = "port"
+        levels = O.orc_pipeline(cl, ks, polys)
+        S = O.OracleSolver(levels, a.Re, a.courant, 1.0, 3, 10, jacobi=False)
+        O.lid_bc(levels[0], S.f)
+        setup_s = time.perf_counter() - t0
+        step = S.step
+    for _ in range(warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    per = (time.perf_counter() - t0) / max(steps, 1)
+    return {"kind": kind, "sec_per_step": per, "nodes": n, "levels": nl, "setup_s": setup_s}
+
+
+def cpu_baseline_entry(a, s, full_nodes):
+    val = (1.0 / s["sec_per_step"]) * (s["nodes"] / full_nodes)
+    return {
+        "value": val,
+        "unit": "steps/s",
+        "cores": 1,
+        "kind": s["kind"],
+        "sample": (f"fractional_step_explicit of the reference C code on a {a.sample_m}x{a.sample_m} cavity "
+                   f"({s['nodes']} nodes, {s['levels']} levels, k={a.k}, poly {a.poly}, its fixed 10 V-cycles x 3 "
+                   f"SOR sweeps, omega 1.0 -- it never reaches 1e-8), steps/s scaled by node count to "
+                   f"{full_nodes} nodes; reference set-up of the sample took {s['setup_s']:.1f} s"),
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.proc is None:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        out.update(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=max(mx) if mx else None,
+                   reasons=sorted(reasons), samples=len(rows))
+        return out
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the level-0 smoother from the committed ncu summary, scaled to this size."""
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    try:
+        d = json.load(open(path))
+        return d
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+def run_ours(a, rank, world, local_rank):
+    import numpy as np
+
+    import multigrid_meshless_b200 as mgm
+    from multigrid_meshless_b200 import api, clouds
+
+    api.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist_
+        torch.cuda.set_device(local_rank)
+        dist_.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist = dist_
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    t0 = time.perf_counter()
+    cl = clouds.cavity_hierarchy(a.m, a.levels, seed=1 + rank * 1000)
+    mg = api.Multigrid(cl, [a.k] * a.levels, [a.poly] * a.levels)
+    setup_s = time.perf_counter() - t0
+    setup_launches = api.kernel_launches()
+    print(f"setup_launches={setup_launches}", file=sys.stderr, flush=True)
+    n = mg.n()
+    mg.set_flow(Re=a.Re, courant=a.courant)
+    mg.set_solver(rel_tol=a.tol, max_iters=100, cheb_degree=a.cheb_degree, cheb_ratio=a.cheb_ratio)
+    mg.apply_bc(mgm.BC_LID)
+
+    fast = mgm.MODE_FP32_IR
+    # warm-up, then the plain FP64 arm (same steps, same state evolution)
+    mg.run_steps(fast, a.warmup)
+    barrier()
+    mg.sync()
+    plain_ms, plain_pms, plain_vc, _ = mg.run_steps(mgm.MODE_FP64, a.steps)
+    plain_ms = max_over_ranks(plain_ms)
+
+    # headline: FP32-in-FP64 refinement, device-timed on the library's stream
+    barrier()
+    mg.sync()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    l0 = api.kernel_launches()
+    mg.profile_smoother(True)
+    ms, pms, vc, err = mg.run_steps(fast, a.steps)
+    sm_ms, sm_launch, sm_bytes = mg.profile_read()
+    mg.profile_smoother(False)
+    launches = api.kernel_launches() - l0
+    ck = clocks.stop()
+    barrier()
+    ms = max_over_ranks(ms)
+
+    # end to end through the public API with page-locked host buffers:
+    # per step H2D of u, v and D2H of u, v, p (the reference's `update host(field[0])`)
+    bufs = [api.PinnedArray(n) for _ in range(5)]
+    bufs[0].array[:] = mg.get_field("u")
+    bufs[1].array[:] = mg.get_field("v")
+    barrier()
+    mg.sync()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        mg.step_host(fast, bufs[0].ptr, bufs[1].ptr, bufs[2].ptr, bufs[3].ptr, bufs[4].ptr)
+        bufs[0].array, bufs[2].array = bufs[2].array, bufs[0].array
+        bufs[0].ptr, bufs[2].ptr = bufs[2].ptr, bufs[0].ptr
+        bufs[1].array, bufs[3].array = bufs[3].array, bufs[1].array
+        bufs[1].ptr, bufs[3].ptr = bufs[3].ptr, bufs[1].ptr
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    finite = bool(np.all(np.isfinite(bufs[0].array)))
+    for b in bufs:
+        b.free()
+
+    line = None
+    if rank == 0:
+        steps_total = a.steps * world
+        value = steps_total / (ms / 1e3)
+        peak, peak_src = measured_peak()
+        avg_launch_s = (sm_ms / 1e3) / max(sm_launch, 1)
+        achieved = sm_bytes / avg_launch_s / 1e9 if sm_launch else None
+        tr = ncu_traffic()
+        traffic = None
+        if tr and tr.get("nodes"):
+            traffic = float(tr["dram_bytes_per_launch"]) * (n / float(tr["nodes"]))
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "steps/s",
+            "n_gpus": world,
+            "steps": a.steps,
+            "warmup": a.warmup,
+            "ms_per_step": ms / a.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 V-cycle inside f64 FGMRES (f64 operators, residuals, solution)",
+            "data": "synthetic (seeded jittered cloud, no mesh files)",
+            "config": workload(a),
+            "poisson_ms": pms / a.steps,
+            "vcycles_per_step": vc / a.steps,
+            "steady_err_last": err,
+            "plain_fp64": {"steps_per_s": a.steps * world / (plain_ms / 1e3), "ms_per_step": plain_ms / a.steps,
+                           "poisson_ms": plain_pms / a.steps, "vcycles_per_step": plain_vc / a.steps},
+            "learned_warm_start": None,
+            "e2e": {"value": steps_total / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": 2 * 8 * n,
+                    "d2h_bytes_per_step": 3 * 8 * n, "finite": finite},
+            "roofline": {"bound": "hbm", "kernel": "k_cheb<float> level 0 (Chebyshev smoother step)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "bytes_per_launch": sm_bytes, "launches": sm_launch,
+                         "avg_launch_us": avg_launch_s * 1e6, "peak_source": peak_src},
+            "clocks": ck,
+            "gpu_launches": launches,
+            "setup_s": setup_s,
+        }
+        if world == 1 and not a.no_cpu_baseline:
+            s = reference_sample(a, steps=3, warmup=1)
+            line["cpu_baseline"] = cpu_baseline_entry(a, s, n)
+    mg.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+def run_reference(a, rank):
+    if rank != 0:
+        return None
+    full_nodes = a.m * a.m - 4
+    s = reference_sample(a, steps=max(a.steps, 1), warmup=a.warmup)
+    cb = cpu_baseline_entry(a, s, full_nodes)
+    val = cb["value"]
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": val,
+        "unit": "steps/s",
+        "n_gpus": a.gpus,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": 1e3 / val,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded jittered cloud, no mesh files)",
+        "config": workload(a),
+        "cpu_baseline": cb,
+        "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        line = run_reference(a, rank)
+    else:
+        line = run_ours(a, rank, world, local_rank)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

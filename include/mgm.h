@@ -18,6 +18,8 @@
 #ifndef MGM_H
 #define MGM_H
 
+#include <stddef.h>
+
 #if defined(__GNUC__)
 #define MGM_API __attribute__((visibility("default")))
 #else
@@ -40,6 +42,9 @@ extern "C" {
 /* Diagnostics                                                         */
 /* ------------------------------------------------------------------ */
 MGM_API const char *mgm_last_error(void);
+/* Makes `device` the current CUDA device of the calling thread for this
+ * library (contexts are created on the current device). */
+MGM_API int mgm_set_device(int device);
 /* Number of kernels this library has launched in the calling process. */
 MGM_API long long mgm_kernel_launches(void);
 MGM_API int mgm_version(void);
@@ -200,6 +205,29 @@ MGM_API int mgm_update_velocity(mgm_ctx *ctx, double *mass_res);
  * p[0] = 0), b given on the host (b[0] and boundary rows as given), p used as
  * the initial guess and returned.  The pinned row's rhs is forced to 0. */
 MGM_API int mgm_solve_poisson(mgm_ctx *ctx, int mode, const double *b, double *p, int *iters, double *rel_res);
+
+/* Runs nsteps fractional steps (as mgm_step) back to back and reports the
+ * device time measured by CUDA events on the context's stream: total step
+ * time, total Poisson-solve time and V-cycles used.  Any output may be NULL.
+ * (No reference counterpart: measurement hook for fractional_step_explicit loops.) */
+MGM_API int mgm_run_steps(mgm_ctx *ctx, int mode, int nsteps, double *step_ms, double *poisson_ms,
+                          long long *vcycles, double *steady_err);
+
+/* One fractional step with host buffers, the shape of the reference's time
+ * loop (mg_NS_solver.c:68-91: step, then `acc update host(field[0])`):
+ * uploads the given level-0 velocity components (NULL = keep the device
+ * copy), steps, and downloads u, v, w, p into the given buffers (NULL = skip).
+ * Use mgm_host_alloc for page-locked buffers. */
+MGM_API int mgm_step_host(mgm_ctx *ctx, int mode, const double *u_in, const double *v_in, const double *w_in,
+                          double *u_out, double *v_out, double *w_out, double *p_out, double *steady_err);
+MGM_API void *mgm_host_alloc(size_t bytes);
+MGM_API void mgm_host_free(void *ptr);
+
+/* Per-launch device timing of the level-0 smoother kernel (the dominant
+ * kernel of the FP32-in-FP64 solve).  bytes_per_launch is its algorithmic
+ * traffic (operator, index and vector bytes, each counted once). */
+MGM_API int mgm_profile_smoother(mgm_ctx *ctx, int enable);
+MGM_API int mgm_profile_read(mgm_ctx *ctx, double *ms_total, long long *launches, long long *bytes_per_launch);
 
 /* Synchronises the context's stream. */
 MGM_API int mgm_sync(mgm_ctx *ctx);

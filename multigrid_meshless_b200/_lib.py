@@ -29,6 +29,7 @@ FIELD = {"u": 0, "v": 1, "w": 2, "p": 3, "u_new": 4, "v_new": 5, "w_new": 6, "re
 # every exported entry point and its argument types (restype int unless noted)
 SIGNATURES = {
     "mgm_last_error": ([], C.c_char_p),
+    "mgm_set_device": ([C.c_int], C.c_int),
     "mgm_kernel_launches": ([], C.c_longlong),
     "mgm_version": ([], C.c_int),
     "mgm_knn_cloud": ([C.c_int, C.c_int, C.c_int, dp, dp, dp, u8p, C.c_int, ip], C.c_int),
@@ -66,6 +67,13 @@ SIGNATURES = {
     "mgm_update_velocity": ([vp, C.POINTER(C.c_double)], C.c_int),
     "mgm_solve_poisson": ([vp, C.c_int, dp, dp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
     "mgm_sync": ([vp], C.c_int),
+    "mgm_run_steps": ([vp, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                       C.POINTER(C.c_double)], C.c_int),
+    "mgm_step_host": ([vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, C.POINTER(C.c_double)], C.c_int),
+    "mgm_host_alloc": ([C.c_size_t], vp),
+    "mgm_host_free": ([vp], None),
+    "mgm_profile_smoother": ([vp, C.c_int], C.c_int),
+    "mgm_profile_read": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int),
 }
 
 _LIB = None

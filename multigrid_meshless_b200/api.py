@@ -128,6 +128,10 @@ def kernel_launches() -> int:
     return int(load().mgm_kernel_launches())
 
 
+def set_device(device: int):
+    check(load().mgm_set_device(device))
+
+
 class Multigrid:
     """A device-resident multigrid hierarchy (the reference's PointStructure
     array after read_complete_mesh_data + create_derivative_matrices, and its
@@ -251,3 +255,42 @@ class Multigrid:
 
     def sync(self):
         check(self.L.mgm_sync(self.h))
+
+    def run_steps(self, mode, nsteps):
+        """nsteps fractional steps timed on the device: (step_ms, poisson_ms, vcycles, steady_err)."""
+        sm, pm, vc, e = C.c_double(), C.c_double(), C.c_longlong(), C.c_double()
+        check(self.L.mgm_run_steps(self.h, mode, nsteps, C.byref(sm), C.byref(pm), C.byref(vc), C.byref(e)))
+        return sm.value, pm.value, vc.value, e.value
+
+    def step_host(self, mode, u_in=None, v_in=None, u_out=None, v_out=None, p_out=None):
+        """One step with host buffers (ctypes pointers / None)."""
+        e = C.c_double()
+        check(self.L.mgm_step_host(self.h, mode, u_in, v_in, None, u_out, v_out, None, p_out, C.byref(e)))
+        return e.value
+
+    def profile_smoother(self, enable=True):
+        check(self.L.mgm_profile_smoother(self.h, 1 if enable else 0))
+
+    def profile_read(self):
+        ms, nl, by = C.c_double(), C.c_longlong(), C.c_longlong()
+        check(self.L.mgm_profile_read(self.h, C.byref(ms), C.byref(nl), C.byref(by)))
+        return ms.value, nl.value, by.value
+
+
+class PinnedArray:
+    """A page-locked host array (mgm_host_alloc) viewed as numpy."""
+
+    def __init__(self, n, dtype=np.float64):
+        self.L = load()
+        nbytes = int(n) * np.dtype(dtype).itemsize
+        self.ptr = self.L.mgm_host_alloc(nbytes)
+        if not self.ptr:
+            raise _lib.MgmError(_lib.MGM_ERR_NOMEM, self.L.mgm_last_error().decode())
+        buf = (C.c_char * nbytes).from_address(self.ptr)
+        self.array = np.frombuffer(buf, dtype=dtype, count=int(n))
+
+    def free(self):
+        if self.ptr:
+            self.array = None
+            self.L.mgm_host_free(self.ptr)
+            self.ptr = None

@@ -79,6 +79,10 @@ struct mgm_ctx {
     int last_iters = 0;
     double last_relres = 0;
     double *h_pinned = nullptr;
+    SmootherProfile prof;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    double poisson_ms_acc = 0;
+    long long vcycles_acc = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -310,7 +314,7 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
         for (int j = 0; j < m; j++) {
             // z_j = M^-1 v_j
             copy_convert<T>(n, V + j * ld, levels[0].r, s);
-            vcycle<T>(levels, cs, c->cheb_deg, c->cheb_ratio, s);
+            vcycle<T>(levels, cs, c->cheb_deg, c->cheb_ratio, s, &c->prof);
             copy_out<T>(n, levels[0].e, Z + j * ld, s);
             // w = A z_j, classical Gram-Schmidt with one re-orthogonalisation
             apply64<T>(n, k, L0.idx.p, L0.A64.p, Z + j * ld, w, s);
@@ -322,6 +326,7 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
             scale_by(n, w, V + (j + 1) * ld, c->kscal.p + 2 * kMaxKrylov + 4, 1, s);
             MGM_CUDA(cudaMemcpyAsync(hp, c->kscal.p, sizeof(double) * (2 * kMaxKrylov + 5), cudaMemcpyDeviceToHost, s));
             MGM_CUDA(cudaStreamSynchronize(s));
+            if (c->prof.on) c->prof.harvest();
             double *col = &H[(size_t)j * (m + 1)];
             for (int i = 0; i <= j; i++) col[i] = hp[i] + hp[kMaxKrylov + 2 + i];
             col[j + 1] = sqrt(std::max(hp[2 * kMaxKrylov + 4], 0.0));
@@ -381,6 +386,33 @@ void poisson(mgm_ctx *c, int mode)
     else throw Error{MGM_ERR_ARG, "unknown Poisson mode"};
 }
 
+void ensure_events(mgm_ctx *c)
+{
+    for (auto &e : c->ev)
+        if (!e) MGM_CUDA(cudaEventCreate(&e));
+}
+
+// one fractional step (fractional_step_explicit) with the Poisson solve timed by events
+double step_timed(mgm_ctx *c, int mode)
+{
+    ensure_events(c);
+    StepArgs a = step_args(c);
+    launch_momentum(a, c->dim, c->s);
+    launch_divergence(a, c->dim, c->s);
+    MGM_CUDA(cudaEventRecord(c->ev[2], c->s));
+    poisson(c, mode);
+    MGM_CUDA(cudaEventRecord(c->ev[3], c->s));
+    launch_correct(a, c->dim, c->partial.p, c->scal.p, c->s);
+    MGM_CUDA(cudaMemcpyAsync(c->h_pinned, c->scal.p, sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    MGM_CUDA(cudaStreamSynchronize(c->s));
+    float pm = 0;
+    MGM_CUDA(cudaEventElapsedTime(&pm, c->ev[2], c->ev[3]));
+    c->poisson_ms_acc += pm;
+    c->vcycles_acc += mode == MGM_MODE_REFERENCE ? (long long)c->num_vcycles : c->last_iters;
+    if (c->prof.on) c->prof.harvest();
+    return c->h_pinned[0];
+}
+
 void alloc_solver_buffers(mgm_ctx *c)
 {
     const int n = c->L[0].n;
@@ -403,6 +435,10 @@ void alloc_solver_buffers(mgm_ctx *c)
 extern "C" {
 
 const char *mgm_last_error(void) { return t_err.c_str(); }
+int mgm_set_device(int device)
+{
+    return guard([&] { MGM_CUDA(cudaSetDevice(device)); });
+}
 long long mgm_kernel_launches(void) { return g_launches; }
 int mgm_version(void) { return 1; }
 
@@ -995,14 +1031,94 @@ int mgm_step(mgm_ctx *c, int mode, double *steady_err)
     return guard([&] {
         check_ctx(c);
         MGM_REQUIRE(c->setup_done && c->dt > 0, "mgm_step: call mgm_setup and mgm_set_flow first");
-        StepArgs a = step_args(c);
-        launch_momentum(a, c->dim, c->s);
-        launch_divergence(a, c->dim, c->s);
-        poisson(c, mode);
-        launch_correct(a, c->dim, c->partial.p, c->scal.p, c->s);
-        c->scal.download(c->h_pinned, 1, c->s);
+        const double e = step_timed(c, mode);
+        if (steady_err) *steady_err = e;
+    });
+}
+
+int mgm_run_steps(mgm_ctx *c, int mode, int nsteps, double *step_ms, double *poisson_ms, long long *vcycles,
+                  double *steady_err)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done && c->dt > 0, "mgm_run_steps: call mgm_setup and mgm_set_flow first");
+        MGM_REQUIRE(nsteps >= 0, "mgm_run_steps: nsteps < 0");
+        ensure_events(c);
+        c->poisson_ms_acc = 0;
+        c->vcycles_acc = 0;
+        double e = 0;
+        MGM_CUDA(cudaEventRecord(c->ev[0], c->s));
+        for (int t = 0; t < nsteps; t++) e = step_timed(c, mode);
+        MGM_CUDA(cudaEventRecord(c->ev[1], c->s));
+        MGM_CUDA(cudaEventSynchronize(c->ev[1]));
+        float ms = 0;
+        MGM_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+        if (step_ms) *step_ms = ms;
+        if (poisson_ms) *poisson_ms = c->poisson_ms_acc;
+        if (vcycles) *vcycles = c->vcycles_acc;
+        if (steady_err) *steady_err = e;
+    });
+}
+
+int mgm_step_host(mgm_ctx *c, int mode, const double *u_in, const double *v_in, const double *w_in, double *u_out,
+                  double *v_out, double *w_out, double *p_out, double *steady_err)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done && c->dt > 0, "mgm_step_host: call mgm_setup and mgm_set_flow first");
+        const size_t nb = sizeof(double) * c->L[0].n;
+        cudaStream_t s = c->s;
+        if (u_in) MGM_CUDA(cudaMemcpyAsync(c->u.p, u_in, nb, cudaMemcpyHostToDevice, s));
+        if (v_in) MGM_CUDA(cudaMemcpyAsync(c->v.p, v_in, nb, cudaMemcpyHostToDevice, s));
+        if (w_in) MGM_CUDA(cudaMemcpyAsync(c->w.p, w_in, nb, cudaMemcpyHostToDevice, s));
+        const double e = step_timed(c, mode);
+        if (u_out) MGM_CUDA(cudaMemcpyAsync(u_out, c->u.p, nb, cudaMemcpyDeviceToHost, s));
+        if (v_out) MGM_CUDA(cudaMemcpyAsync(v_out, c->v.p, nb, cudaMemcpyDeviceToHost, s));
+        if (w_out) MGM_CUDA(cudaMemcpyAsync(w_out, c->w.p, nb, cudaMemcpyDeviceToHost, s));
+        if (p_out) MGM_CUDA(cudaMemcpyAsync(p_out, c->L[0].p.p, nb, cudaMemcpyDeviceToHost, s));
+        MGM_CUDA(cudaStreamSynchronize(s));
+        if (steady_err) *steady_err = e;
+    });
+}
+
+void *mgm_host_alloc(size_t bytes)
+{
+    void *p = nullptr;
+    int st = guard([&] { MGM_CUDA(cudaMallocHost(&p, bytes)); });
+    return st == MGM_OK ? p : nullptr;
+}
+
+void mgm_host_free(void *p)
+{
+    if (p) cudaFreeHost(p);
+}
+
+int mgm_profile_smoother(mgm_ctx *c, int enable)
+{
+    return guard([&] {
+        check_ctx(c);
         MGM_CUDA(cudaStreamSynchronize(c->s));
-        if (steady_err) *steady_err = c->h_pinned[0];
+        c->prof.harvest();
+        c->prof.on = enable != 0;
+        c->prof.ms = 0;
+        c->prof.launches = 0;
+    });
+}
+
+int mgm_profile_read(mgm_ctx *c, double *ms_total, long long *launches, long long *bytes_per_launch)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+        c->prof.harvest();
+        if (ms_total) *ms_total = c->prof.ms;
+        if (launches) *launches = c->prof.launches;
+        if (bytes_per_launch) {
+            // level-0 Chebyshev step (k_cheb<float> in MGM_MODE_FP32_IR): reads A, idx (k each), dinv, btag,
+            // r, e, d; writes e', d  -> n * (k * (w + 4) + 5 * w + 1 + 2 * w) with w = 4 bytes
+            const Level &L = c->L[0];
+            *bytes_per_launch = (long long)L.n * (L.k * (4 + 4) + 7 * 4 + 1);
+        }
     });
 }
 

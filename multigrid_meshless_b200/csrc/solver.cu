@@ -148,8 +148,35 @@ __global__ void __launch_bounds__(256) k_dense_solve(int n, const T *__restrict_
     if (lane == 0) e[warp] = s;
 }
 
+void SmootherProfile::mark(cudaStream_t s)
+{
+    if (used >= ev.size()) {
+        size_t old = ev.size();
+        ev.resize(std::max<size_t>(256, old * 2));
+        for (size_t i = old; i < ev.size(); i++) MGM_CUDA(cudaEventCreate(&ev[i]));
+    }
+    MGM_CUDA(cudaEventRecord(ev[used++], s));
+}
+
+void SmootherProfile::harvest()
+{
+    for (size_t i = 0; i + 1 < used; i += 2) {
+        float t = 0;
+        MGM_CUDA(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+        ms += t;
+        launches++;
+    }
+    used = 0;
+}
+
+SmootherProfile::~SmootherProfile()
+{
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+}
+
 template <class T>
-static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, cudaStream_t s)
+static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, cudaStream_t s,
+                   SmootherProfile *prof)
 {
     const double lM = 1.05 * L.lmax, lm = L.lmax / ratio;
     const double th = 0.5 * (lM + lm), de = 0.5 * (lM - lm), sig = th / de;
@@ -170,9 +197,11 @@ static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, 
             c2 = 2.0 * rn / de;
             rho = rn;
         }
+        if (prof) prof->mark(s);
         k_cheb<T><<<nb, 256, 0, s>>>(L.n, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d, (T)c1, (T)c2,
                                      step == 0 ? 1 : 0);
         MGM_LAUNCHED();
+        if (prof) prof->mark(s);
         std::swap(L.e, L.e2);
         k_bnd_exact<T><<<nbb, 256, 0, s>>>(L.nb_list, L.bnd_list, L.n, L.k, L.idx, L.A, L.dinv, L.r, L.e, 0);
         MGM_LAUNCHED();
@@ -181,8 +210,9 @@ static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, 
 
 template <class T>
 static void vcycle_rec(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int l, int deg, double ratio,
-                       cudaStream_t s)
+                       cudaStream_t s, SmootherProfile *prof)
 {
+    SmootherProfile *lp = (l == 0 && prof && prof->on) ? prof : nullptr;
     SolveLevel<T> &L = Ls[l];
     const int nl = (int)Ls.size();
     if (l == nl - 1) {
@@ -191,27 +221,29 @@ static void vcycle_rec(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs,
         return;
     }
     MGM_CUDA(cudaMemsetAsync(L.e, 0, sizeof(T) * L.n, s));
-    smooth(L, deg, ratio, true, s);
+    smooth(L, deg, ratio, true, s, lp);
     SolveLevel<T> &C = Ls[l + 1];
     k_residual<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.idx, L.A, L.btag, L.r, L.e, L.q);
     MGM_LAUNCHED();
     k_restrict<T><<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
     MGM_LAUNCHED();
-    vcycle_rec(Ls, cs, l + 1, deg, ratio, s);
+    vcycle_rec(Ls, cs, l + 1, deg, ratio, s, prof);
     k_prolong<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.kp, L.p_idx, L.p_w, C.e, L.e);
     MGM_LAUNCHED();
-    smooth(L, deg, ratio, false, s);
+    smooth(L, deg, ratio, false, s, lp);
 }
 
 template <class T>
 void vcycle(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int cheb_degree, double cheb_ratio,
-            cudaStream_t s)
+            cudaStream_t s, SmootherProfile *prof)
 {
-    vcycle_rec(Ls, cs, 0, cheb_degree, cheb_ratio, s);
+    vcycle_rec(Ls, cs, 0, cheb_degree, cheb_ratio, s, prof);
 }
 
-template void vcycle<double>(std::vector<SolveLevel<double>> &, const CoarseSolve<double> &, int, double, cudaStream_t);
-template void vcycle<float>(std::vector<SolveLevel<float>> &, const CoarseSolve<float> &, int, double, cudaStream_t);
+template void vcycle<double>(std::vector<SolveLevel<double>> &, const CoarseSolve<double> &, int, double, cudaStream_t,
+                             SmootherProfile *);
+template void vcycle<float>(std::vector<SolveLevel<float>> &, const CoarseSolve<float> &, int, double, cudaStream_t,
+                            SmootherProfile *);
 
 // ---------------------------------------------------------------------------
 // spectral radius of D^-1 A restricted to interior rows (power iteration)

@@ -72,9 +72,22 @@ struct CoarseSolve {
     const T *inv;  // dense inverse of the pinned coarsest operator, row-major [n][n]
 };
 
+// Records CUDA events around the level-0 Chebyshev kernels (the dominant
+// kernel of a solve) so that their device time can be read back.
+struct SmootherProfile {
+    bool on = false;
+    std::vector<cudaEvent_t> ev;  // pairs
+    size_t used = 0;
+    double ms = 0;
+    long long launches = 0;
+    void mark(cudaStream_t s);    // records the next event of a pair
+    void harvest();               // accumulates finished pairs (stream must be idle)
+    ~SmootherProfile();
+};
+
 template <class T>
 void vcycle(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int cheb_degree, double cheb_ratio,
-            cudaStream_t s);
+            cudaStream_t s, SmootherProfile *prof = nullptr);
 template <class T>
 void estimate_lmax(SolveLevel<T> &L, cudaStream_t s);
 
