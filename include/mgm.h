@@ -190,6 +190,9 @@ MGM_API int mgm_step(mgm_ctx *ctx, int mode, double *steady_err);
 
 /* Solver controls for MGM_MODE_FP64 / MGM_MODE_FP32_IR. */
 MGM_API int mgm_set_solver(mgm_ctx *ctx, double rel_tol, int max_iters, int cheb_degree, double cheb_ratio);
+/* Replay each V-cycle from a captured CUDA graph (default on) or launch its
+ * kernels one by one (enable = 0).  Results are identical either way. */
+MGM_API int mgm_use_graphs(mgm_ctx *ctx, int enable);
 /* Statistics of the last Poisson solve: outer iterations (V-cycles) and the
  * true relative residual ||b - A p|| / ||b|| over rows != 0 (FP64). */
 MGM_API int mgm_last_solve(mgm_ctx *ctx, int *iters, double *rel_res);

@@ -80,6 +80,15 @@ struct mgm_ctx {
     double last_relres = 0;
     double *h_pinned = nullptr;
     SmootherProfile prof;
+    // captured V-cycles, [0] FP64, [1] FP32 (re-captured when solver settings change)
+    struct VGraph {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t x = nullptr;
+        void *out = nullptr;        // level-0 correction buffer the graph writes
+        bool prof = false;          // graph records smoother events
+        size_t ev_first = 0, ev_pairs = 0;
+    } vg[2];
+    bool use_graphs = true;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     double poisson_ms_acc = 0;
     long long vcycles_acc = 0;
@@ -271,6 +280,65 @@ std::vector<RefLevel> ref_levels(mgm_ctx *c)
     return out;
 }
 
+void drop_graphs(mgm_ctx *c)
+{
+    for (auto &g : c->vg) {
+        if (g.x) cudaGraphExecDestroy(g.x);
+        if (g.g) cudaGraphDestroy(g.g);
+        g = mgm_ctx::VGraph();
+    }
+}
+
+// One V-cycle: replayed from a captured CUDA graph (about a hundred kernels,
+// most of them on launch-latency-bound coarse levels).  Returns the level-0
+// correction buffer.
+template <class T>
+const T *run_vcycle(mgm_ctx *c, std::vector<SolveLevel<T>> &levels, const CoarseSolve<T> &cs)
+{
+    cudaStream_t s = c->s;
+    if (!c->use_graphs) {
+        vcycle<T>(levels, cs, c->cheb_deg, c->cheb_ratio, s, &c->prof);
+        return levels[0].e;
+    }
+    auto &G = c->vg[sizeof(T) == 4 ? 1 : 0];
+    if (G.x && G.prof != c->prof.on) {
+        cudaGraphExecDestroy(G.x);
+        cudaGraphDestroy(G.g);
+        G = mgm_ctx::VGraph();
+    }
+    if (!G.x) {
+        std::vector<SolveLevel<T>> cap = levels;
+        if (c->prof.on) {
+            MGM_CUDA(cudaStreamSynchronize(s));
+            c->prof.harvest();
+        }
+        const size_t first = c->prof.used;
+        MGM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        try {
+            vcycle<T>(cap, cs, c->cheb_deg, c->cheb_ratio, s, c->prof.on ? &c->prof : nullptr);
+        } catch (...) {
+            cudaGraph_t junk = nullptr;
+            cudaStreamEndCapture(s, &junk);
+            if (junk) cudaGraphDestroy(junk);
+            throw;
+        }
+        MGM_CUDA(cudaStreamEndCapture(s, &G.g));
+        MGM_CUDA(cudaGraphInstantiate(&G.x, G.g, 0));
+        G.out = (void *)cap[0].e;
+        G.prof = c->prof.on;
+        G.ev_first = first;
+        G.ev_pairs = (c->prof.used - first) / 2;
+        // the graph owns these event slots from now on
+        c->prof.used = first;
+        if (G.prof) {
+            // keep the slots out of the eager recorder's way
+            c->prof.used = first + 2 * G.ev_pairs;
+        }
+    }
+    MGM_CUDA(cudaGraphLaunch(G.x, s));
+    return (const T *)G.out;
+}
+
 // Flexible GMRES(m) in FP64 right-preconditioned by one V-cycle in precision T.
 // Solves A p = b (pinned level-0 operator); p is the initial guess.
 template <class T>
@@ -314,8 +382,8 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
         for (int j = 0; j < m; j++) {
             // z_j = M^-1 v_j
             copy_convert<T>(n, V + j * ld, levels[0].r, s);
-            vcycle<T>(levels, cs, c->cheb_deg, c->cheb_ratio, s, &c->prof);
-            copy_out<T>(n, levels[0].e, Z + j * ld, s);
+            const T *zout = run_vcycle<T>(c, levels, cs);
+            copy_out<T>(n, zout, Z + j * ld, s);
             // w = A z_j, classical Gram-Schmidt with one re-orthogonalisation
             apply64<T>(n, k, L0.idx.p, L0.A64.p, Z + j * ld, w, s);
             multidot(n, j + 1, V, ld, w, c->kpart.p, c->kscal.p, s);
@@ -326,7 +394,11 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
             scale_by(n, w, V + (j + 1) * ld, c->kscal.p + 2 * kMaxKrylov + 4, 1, s);
             MGM_CUDA(cudaMemcpyAsync(hp, c->kscal.p, sizeof(double) * (2 * kMaxKrylov + 5), cudaMemcpyDeviceToHost, s));
             MGM_CUDA(cudaStreamSynchronize(s));
-            if (c->prof.on) c->prof.harvest();
+            if (c->prof.on) {
+                auto &G = c->vg[sizeof(T) == 4 ? 1 : 0];
+                if (c->use_graphs && G.x && G.prof) c->prof.harvest_graph(G.ev_first, G.ev_pairs);
+                else c->prof.harvest();
+            }
             double *col = &H[(size_t)j * (m + 1)];
             for (int i = 0; i <= j; i++) col[i] = hp[i] + hp[kMaxKrylov + 2 + i];
             col[j + 1] = sqrt(std::max(hp[2 * kMaxKrylov + 4], 0.0));
@@ -409,7 +481,6 @@ double step_timed(mgm_ctx *c, int mode)
     MGM_CUDA(cudaEventElapsedTime(&pm, c->ev[2], c->ev[3]));
     c->poisson_ms_acc += pm;
     c->vcycles_acc += mode == MGM_MODE_REFERENCE ? (long long)c->num_vcycles : c->last_iters;
-    if (c->prof.on) c->prof.harvest();
     return c->h_pinned[0];
 }
 
@@ -658,6 +729,7 @@ void mgm_destroy(mgm_ctx *c)
     cudaSetDevice(c->device);
     if (c->s) cudaStreamSynchronize(c->s);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
+    drop_graphs(c);
     c->L.clear();
     if (c->s) cudaStreamDestroy(c->s);
     delete c;
@@ -962,11 +1034,23 @@ int mgm_set_solver(mgm_ctx *c, double rel_tol, int max_iters, int cheb_degree, d
         check_ctx(c);
         MGM_REQUIRE(rel_tol > 0 && max_iters >= 1 && max_iters <= kMaxKrylov && cheb_degree >= 1 && cheb_degree <= 16 &&
                         cheb_ratio > 1, "mgm_set_solver: bad parameters");
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+        drop_graphs(c);
         c->tol = rel_tol; c->cheb_deg = cheb_degree; c->cheb_ratio = cheb_ratio;
         if (max_iters != c->max_iters) {
             c->max_iters = max_iters;
             if (c->setup_done) alloc_solver_buffers(c);
         }
+    });
+}
+
+int mgm_use_graphs(mgm_ctx *c, int enable)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+        drop_graphs(c);
+        c->use_graphs = enable != 0;
     });
 }
 
@@ -1099,6 +1183,8 @@ int mgm_profile_smoother(mgm_ctx *c, int enable)
         check_ctx(c);
         MGM_CUDA(cudaStreamSynchronize(c->s));
         c->prof.harvest();
+        drop_graphs(c);
+        c->prof.used = 0;
         c->prof.on = enable != 0;
         c->prof.ms = 0;
         c->prof.launches = 0;
@@ -1110,7 +1196,6 @@ int mgm_profile_read(mgm_ctx *c, double *ms_total, long long *launches, long lon
     return guard([&] {
         check_ctx(c);
         MGM_CUDA(cudaStreamSynchronize(c->s));
-        c->prof.harvest();
         if (ms_total) *ms_total = c->prof.ms;
         if (launches) *launches = c->prof.launches;
         if (bytes_per_launch) {

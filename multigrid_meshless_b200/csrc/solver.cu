@@ -169,6 +169,16 @@ void SmootherProfile::harvest()
     used = 0;
 }
 
+void SmootherProfile::harvest_graph(size_t first, size_t pairs)
+{
+    for (size_t q = 0; q < pairs; q++) {
+        float t = 0;
+        MGM_CUDA(cudaEventElapsedTime(&t, ev[first + 2 * q], ev[first + 2 * q + 1]));
+        ms += t;
+        launches++;
+    }
+}
+
 SmootherProfile::~SmootherProfile()
 {
     for (cudaEvent_t e : ev) cudaEventDestroy(e);

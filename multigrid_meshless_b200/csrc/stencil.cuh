@@ -74,6 +74,8 @@ struct CoarseSolve {
 
 // Records CUDA events around the level-0 Chebyshev kernels (the dominant
 // kernel of a solve) so that their device time can be read back.
+// In a captured CUDA graph the same event pairs are re-recorded on every
+// replay: harvest_graph() reads them without releasing them.
 struct SmootherProfile {
     bool on = false;
     std::vector<cudaEvent_t> ev;  // pairs
@@ -82,6 +84,7 @@ struct SmootherProfile {
     long long launches = 0;
     void mark(cudaStream_t s);    // records the next event of a pair
     void harvest();               // accumulates finished pairs (stream must be idle)
+    void harvest_graph(size_t first, size_t pairs);  // accumulates pairs recorded by a graph replay
     ~SmootherProfile();
 };
 
