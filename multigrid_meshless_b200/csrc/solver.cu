@@ -155,7 +155,11 @@ void SmootherProfile::mark(cudaStream_t s)
         ev.resize(std::max<size_t>(256, old * 2));
         for (size_t i = old; i < ev.size(); i++) MGM_CUDA(cudaEventCreate(&ev[i]));
     }
-    MGM_CUDA(cudaEventRecord(ev[used++], s));
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    MGM_CUDA(cudaStreamIsCapturing(s, &st));
+    // inside a capture the record must become an event-record node of the graph
+    if (st == cudaStreamCaptureStatusActive) MGM_CUDA(cudaEventRecordWithFlags(ev[used++], s, cudaEventRecordExternal));
+    else MGM_CUDA(cudaEventRecord(ev[used++], s));
 }
 
 void SmootherProfile::harvest()
