@@ -204,11 +204,15 @@ def measured_peak():
 
 
 def ncu_traffic():
-    """DRAM bytes per launch of the level-0 smoother from the committed ncu summary, scaled to this size."""
-    path = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    """DRAM bytes per launch of the level-0 smoother from the committed ncu summary
+    (profiles/k_cheb_float_cavity640k.md), to be scaled by node count."""
+    import re
+    path = os.path.join(ROOT, "profiles", "k_cheb_float_cavity640k.md")
     try:
-        d = json.load(open(path))
-        return d
+        txt = open(path).read()
+        b = re.search(r"dram_bytes_per_launch:\s*(\d+)", txt)
+        nn = re.search(r"nodes:\s*(\d+)", txt)
+        return {"dram_bytes_per_launch": float(b.group(1)), "nodes": float(nn.group(1))}
     except Exception:
         return None
 

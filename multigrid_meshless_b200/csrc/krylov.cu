@@ -28,12 +28,7 @@ __global__ void __launch_bounds__(256) k_resid64(int n, int k, const int *__rest
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double rr = 0, bb = 0;
     if (i < n) {
-        double s = 0.0;
-        for (int j = 0; j < k; j++) {
-            const long o = (long)j * n + i;
-            s = fma(A[o], x[idx[o]], s);
-        }
-        const double ri = b[i] - s;
+        const double ri = b[i] - ell_row_dot(idx, A, x, n, k, i);
         r[i] = ri;
         rr = ri * ri;
         bb = b[i] * b[i];
@@ -50,12 +45,7 @@ __global__ void __launch_bounds__(256) k_apply64(int n, int k, const int *__rest
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double s = 0.0;
-    for (int j = 0; j < k; j++) {
-        const long o = (long)j * n + i;
-        s = fma(A[o], (double)z[idx[o]], s);
-    }
-    w[i] = s;
+    w[i] = ell_row_dot(idx, A, z, n, k, i);
 }
 
 // partial dot products h_c = V_c . w for c < cnt; part[c * nblk + blk]

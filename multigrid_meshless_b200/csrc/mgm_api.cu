@@ -42,6 +42,9 @@ struct Level {
     DBuf<double> A64, dinv64;
     DBuf<float> A32, dinv32;
     DBuf<int> bnd_list;
+    DBuf<int> bnd_idx;           // boundary rows' stencils, row-major [nbl][k]
+    DBuf<double> bnd_A64;
+    DBuf<float> bnd_A32;
     int nbl = 0;
     double lmax = 2.0;
     // reference-mode state
@@ -87,6 +90,7 @@ struct mgm_ctx {
         void *out = nullptr;        // level-0 correction buffer the graph writes
         bool prof = false;          // graph records smoother events
         size_t ev_first = 0, ev_pairs = 0;
+        long long kernels = 0;      // kernel nodes in the graph
     } vg[2];
     bool use_graphs = true;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -168,6 +172,20 @@ __global__ void k_bc(int n, int kind, const double *x, const double *y, double *
 
 __global__ void k_zero_pinned(double *b) { b[0] = 0.0; }
 
+// compact copies of the boundary rows of the pinned operator: out[w][j] = A[j][list[w]]
+__global__ void k_gather_rows(int nbl, const int *__restrict__ list, int n, int k, const int *__restrict__ idx,
+                              const double *__restrict__ A, int *__restrict__ bidx, double *__restrict__ bA64,
+                              float *__restrict__ bA32)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)nbl * k) return;
+    const int w = (int)(t / k), j = (int)(t % k);
+    const long o = (long)j * n + list[w];
+    bidx[t] = idx[o];
+    bA64[t] = A[o];
+    bA32[t] = (float)A[o];
+}
+
 void knn_clouds(Level &L, int dim, cudaStream_t s)
 {
     const int n = L.n, k = L.k, nb = L.nb;
@@ -226,6 +244,7 @@ std::vector<SolveLevel<double>> solve_levels<double>(mgm_ctx *c)
         SolveLevel<double> S{};
         S.n = L.n; S.k = L.k; S.nb_list = L.nbl;
         S.idx = L.idx.p; S.A = L.A64.p; S.dinv = L.dinv64.p; S.btag = L.btag.p; S.bnd_list = L.bnd_list.p;
+        S.bnd_idx = L.bnd_idx.p; S.bnd_A = L.bnd_A64.p;
         S.r = L.r64.p; S.e = L.e64.p; S.e2 = L.e64b.p; S.d = L.d64.p; S.q = L.q64.p;
         S.kr = l > 0 ? c->L[l - 1].k : 0; S.r_idx = L.s_r_idx.p; S.r_w = L.s_r_w64.p;
         S.kp = l < c->nl - 1 ? c->L[l + 1].k : 0; S.p_idx = L.s_p_idx.p; S.p_w = L.s_p_w64.p;
@@ -244,6 +263,7 @@ std::vector<SolveLevel<float>> solve_levels<float>(mgm_ctx *c)
         SolveLevel<float> S{};
         S.n = L.n; S.k = L.k; S.nb_list = L.nbl;
         S.idx = L.idx.p; S.A = L.A32.p; S.dinv = L.dinv32.p; S.btag = L.btag.p; S.bnd_list = L.bnd_list.p;
+        S.bnd_idx = L.bnd_idx.p; S.bnd_A = L.bnd_A32.p;
         S.r = L.r32.p; S.e = L.e32.p; S.e2 = L.e32b.p; S.d = L.d32.p; S.q = L.q32.p;
         S.kr = l > 0 ? c->L[l - 1].k : 0; S.r_idx = L.s_r_idx.p; S.r_w = L.s_r_w32.p;
         S.kp = l < c->nl - 1 ? c->L[l + 1].k : 0; S.p_idx = L.s_p_idx.p; S.p_w = L.s_p_w32.p;
@@ -313,6 +333,7 @@ const T *run_vcycle(mgm_ctx *c, std::vector<SolveLevel<T>> &levels, const Coarse
             c->prof.harvest();
         }
         const size_t first = c->prof.used;
+        const long long launches_before = g_launches;
         MGM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         try {
             vcycle<T>(cap, cs, c->cheb_deg, c->cheb_ratio, s, c->prof.on ? &c->prof : nullptr);
@@ -324,6 +345,9 @@ const T *run_vcycle(mgm_ctx *c, std::vector<SolveLevel<T>> &levels, const Coarse
         }
         MGM_CUDA(cudaStreamEndCapture(s, &G.g));
         MGM_CUDA(cudaGraphInstantiate(&G.x, G.g, 0));
+        // captured launches did not run: count them once per replay instead
+        G.kernels = g_launches - launches_before;
+        g_launches = launches_before;
         G.out = (void *)cap[0].e;
         G.prof = c->prof.on;
         G.ev_first = first;
@@ -336,6 +360,7 @@ const T *run_vcycle(mgm_ctx *c, std::vector<SolveLevel<T>> &levels, const Coarse
         }
     }
     MGM_CUDA(cudaGraphLaunch(G.x, s));
+    g_launches += G.kernels;
     return (const T *)G.out;
 }
 
@@ -833,6 +858,13 @@ int mgm_setup(mgm_ctx *c, int flags)
             for (int i = 0; i < L.n; i++) if (hb[i]) bl.push_back(i);
             L.nbl = (int)bl.size();
             L.bnd_list.upload(bl.data(), bl.size(), s);
+            L.bnd_idx.alloc((size_t)L.nbl * L.k);
+            L.bnd_A64.alloc((size_t)L.nbl * L.k);
+            L.bnd_A32.alloc((size_t)L.nbl * L.k);
+            k_gather_rows<<<blocks_for((long)L.nbl * L.k, 256), 256, 0, s>>>(L.nbl, L.bnd_list.p, L.n, L.k, L.idx.p,
+                                                                           L.A64.p, L.bnd_idx.p, L.bnd_A64.p,
+                                                                           L.bnd_A32.p);
+            MGM_LAUNCHED();
             for (DBuf<double> *b : {&L.p, &L.ptmp, &L.src, &L.res, &L.r64, &L.e64, &L.e64b, &L.d64, &L.q64}) { b->alloc(L.n); b->zero(s); }
             for (DBuf<float> *b : {&L.r32, &L.e32, &L.e32b, &L.d32, &L.q32}) { b->alloc(L.n); b->zero(s); }
         }

@@ -47,6 +47,34 @@ constexpr int kMaxN = 192;     // k + num_poly_terms capacity of the batched sol
 
 inline int blocks_for(long n, int bs) { return (int)((n + bs - 1) / bs); }
 
+// sum_j A[j][i] * x[idx[j][i]] over an ELL row (column-major by stencil slot).
+// Slots are fetched in chunks of 8 (16 independent loads in flight per
+// thread, then 8 gathers) to hide DRAM latency; the products are summed in
+// slot order.  For kernels that need no particular rounding sequence.
+template <class T, class X>
+__device__ __forceinline__ T ell_row_dot(const int *__restrict__ idx, const T *__restrict__ A,
+                                         const X *__restrict__ x, long n, int k, long i)
+{
+    T s = T(0);
+    int j = 0;
+    for (; j + 8 <= k; j += 8) {
+        int c[8];
+        T a[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            c[q] = __ldg(idx + (long)(j + q) * n + i);
+            a[q] = __ldg(A + (long)(j + q) * n + i);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) s += a[q] * (T)__ldg(x + c[q]);
+    }
+    for (; j < k; j++) {
+        const long o = (long)j * n + i;
+        s += A[o] * (T)x[idx[o]];
+    }
+    return s;
+}
+
 // device buffer with RAII
 template <class T>
 struct DBuf {

@@ -37,22 +37,27 @@ __device__ __forceinline__ double block_sum_d(double v, double *sm)
 // ---------------------------------------------------------------------------
 // smoother
 // ---------------------------------------------------------------------------
+// Exact solve of the boundary rows, one warp per row.  A boundary row couples
+// only to itself and interior nodes, so rows can be updated in place.  The
+// rows are stored compactly (row-major [nbl][k]) so that a warp reads them
+// with coalesced loads.
 template <class T>
-__global__ void __launch_bounds__(256) k_bnd_exact(int nbl, const int *__restrict__ list, int n, int k,
-                                                   const int *__restrict__ idx, const T *__restrict__ A,
+__global__ void __launch_bounds__(256) k_bnd_exact(int nbl, const int *__restrict__ list, int k,
+                                                   const int *__restrict__ bidx, const T *__restrict__ bA,
                                                    const T *__restrict__ dinv, const T *__restrict__ r,
                                                    T *__restrict__ e, int zero_start)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nbl) return;
-    const int i = list[t];
-    if (zero_start) { e[i] = r[i] * dinv[i]; return; }
-    T s = T(0);
-    for (int j = 0; j < k; j++) {
-        const long o = (long)j * n + i;
-        s += A[o] * e[idx[o]];
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= nbl) return;
+    const int i = list[w];
+    if (zero_start) {
+        if (lane == 0) e[i] = r[i] * dinv[i];
+        return;
     }
-    e[i] = e[i] + (r[i] - s) * dinv[i];
+    T s = T(0);
+    for (int j = lane; j < k; j += 32) s += bA[(long)w * k + j] * e[bidx[(long)w * k + j]];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) e[i] = e[i] + (r[i] - s) * dinv[i];
 }
 
 // One Chebyshev step on interior rows: q = r - A e, d = c1*d + c2*D^-1 q, e' = e + d.
@@ -67,12 +72,7 @@ __global__ void __launch_bounds__(256) k_cheb(int n, int k, const int *__restric
     if (i >= n) return;
     const T ei = e[i];
     if (btag[i]) { eout[i] = ei; return; }
-    T s = T(0);
-    for (int j = 0; j < k; j++) {
-        const long o = (long)j * n + i;
-        s += A[o] * e[idx[o]];
-    }
-    const T q = r[i] - s;
+    const T q = r[i] - ell_row_dot(idx, A, e, n, k, i);
     const T di = first ? c2 * dinv[i] * q : c1 * d[i] + c2 * dinv[i] * q;
     d[i] = di;
     eout[i] = ei + di;
@@ -87,12 +87,7 @@ __global__ void __launch_bounds__(256) k_residual(int n, int k, const int *__res
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (btag[i]) { q[i] = T(0); return; }
-    T s = T(0);
-    for (int j = 0; j < k; j++) {
-        const long o = (long)j * n + i;
-        s += A[o] * e[idx[o]];
-    }
-    q[i] = r[i] - s;
+    q[i] = r[i] - ell_row_dot(idx, A, e, n, k, i);
 }
 
 // coarse rhs: r_c[i] = sum_j Rw[j][i] q_f[Ridx[j][i]] on interior coarse rows, 0 elsewhere
@@ -104,12 +99,7 @@ __global__ void __launch_bounds__(256) k_restrict(int n, int k, const int *__res
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (btag[i] || i == 0) { rc[i] = T(0); return; }
-    T s = T(0);
-    for (int j = 0; j < k; j++) {
-        const long o = (long)j * n + i;
-        s += rw[o] * qf[ridx[o]];
-    }
-    rc[i] = s;
+    rc[i] = ell_row_dot(ridx, rw, qf, n, k, i);
 }
 
 // e_f[i] += (P e_c)[i] - (P e_c)[0]  (the shift keeps the pinned node uncorrected)
@@ -126,12 +116,7 @@ __global__ void __launch_bounds__(256) k_prolong(int n, int k, const int *__rest
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    T s = T(0);
-    for (int j = 0; j < k; j++) {
-        const long o = (long)j * n + i;
-        s += pw[o] * ec[pidx[o]];
-    }
-    ef[i] += s - shift;
+    ef[i] += ell_row_dot(pidx, pw, ec, n, k, i) - shift;
 }
 
 // e = inv * r, one warp per row of the dense coarsest inverse
@@ -195,8 +180,9 @@ static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, 
     const double lM = 1.05 * L.lmax, lm = L.lmax / ratio;
     const double th = 0.5 * (lM + lm), de = 0.5 * (lM - lm), sig = th / de;
     double rho = 1.0 / sig;
-    const int nb = blocks_for(L.n, 256), nbb = blocks_for(L.nb_list, 256);
-    k_bnd_exact<T><<<nbb, 256, 0, s>>>(L.nb_list, L.bnd_list, L.n, L.k, L.idx, L.A, L.dinv, L.r, L.e, zero_start ? 1 : 0);
+    const int nb = blocks_for(L.n, 256), nbb = blocks_for((long)L.nb_list * 32, 256);
+    k_bnd_exact<T><<<nbb, 256, 0, s>>>(L.nb_list, L.bnd_list, L.k, L.bnd_idx, L.bnd_A, L.dinv, L.r, L.e,
+                                       zero_start ? 1 : 0);
     MGM_LAUNCHED();
     if (zero_start) {
         // interior entries of e must be zero before the first step reads them
@@ -217,7 +203,7 @@ static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, 
         MGM_LAUNCHED();
         if (prof) prof->mark(s);
         std::swap(L.e, L.e2);
-        k_bnd_exact<T><<<nbb, 256, 0, s>>>(L.nb_list, L.bnd_list, L.n, L.k, L.idx, L.A, L.dinv, L.r, L.e, 0);
+        k_bnd_exact<T><<<nbb, 256, 0, s>>>(L.nb_list, L.bnd_list, L.k, L.bnd_idx, L.bnd_A, L.dinv, L.r, L.e, 0);
         MGM_LAUNCHED();
     }
 }

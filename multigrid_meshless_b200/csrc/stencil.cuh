@@ -54,6 +54,8 @@ struct SolveLevel {
     const T *dinv;                // 1 / diagonal
     const uint8_t *btag;
     const int *bnd_list;          // boundary rows (incl. the pinned row 0)
+    const int *bnd_idx;           // their stencils, row-major [nb_list][k]
+    const T *bnd_A;
     T *r, *e, *e2, *d, *q;        // rhs, correction (double-buffered), Chebyshev direction, residual
     // restriction into this level (coarse row i <- fine interior residual), ELL [kf][n]
     int kr;
