@@ -88,6 +88,22 @@ MGM_API int mgm_correct_normals(int n, int k, const double *x, const double *y, 
 MGM_API int mgm_avg_dx(int n, int k, int dim, const double *x, const double *y, const double *z,
                const unsigned char *btag, const int *cloud, double *d_avg);
 
+/* No counterpart in the reference.  mgm_avg_dx for callers that cannot let a
+ * library allocate device memory (their device memory is owned by another
+ * allocator or a fixed arena, or they cannot afford cudaMalloc's device-wide
+ * synchronisation).  All pointers are DEVICE pointers owned by the caller:
+ * coordinates and tags [n], cloud row-major [n][k], d_avg one double.  Runs
+ * asynchronously on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream) and calls no cudaMalloc/cudaFree: its scratch is a fixed device
+ * array of MGM_NOALLOC_MAX_NODES doubles (16 MiB) that every GPU loading this
+ * library keeps until exit.  n above that limit is rejected with MGM_ERR_ARG.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  Calls share the array: calls that
+ * overlap on the GPU race. */
+#define MGM_NOALLOC_MAX_NODES 2097152
+MGM_API int mgm_avg_dx_noalloc(int n, int k, int dim, const double *d_x, const double *d_y, const double *d_z,
+                               const unsigned char *d_btag, const int *d_cloud, double *d_avg, void *stream);
+
 /* create_derivative_matrices (header_files/rbf.h:401-421) including
  * create_laplacian_for_Poisson (rbf.h:382-399).  Outputs [n][k]; Dz is only
  * written when dim == 3 (may be NULL otherwise). */

@@ -22,6 +22,7 @@ vp = C.c_void_p
 # status codes (include/mgm.h)
 MGM_OK, MGM_ERR_CUDA, MGM_ERR_ARG, MGM_ERR_DIVERGED, MGM_ERR_TIMEOUT, MGM_ERR_NOMEM, MGM_ERR_STATE = range(7)
 MODE_REFERENCE, MODE_FP64, MODE_FP32_IR = 0, 1, 2
+NOALLOC_MAX_NODES = 2097152  # MGM_NOALLOC_MAX_NODES
 BC_LID, BC_TAYLOR_COUETTE = 0, 1
 SETUP_REFERENCE_TRANSFER = 1
 FIELD = {"u": 0, "v": 1, "w": 2, "p": 3, "u_new": 4, "v_new": 5, "w_new": 6, "res": 10, "source": 11, "dpdn": 12}
@@ -38,6 +39,7 @@ SIGNATURES = {
     "mgm_apply_order": ([C.c_int, C.c_int, ip, dp, dp, dp, dp, dp, dp, u8p, ip], C.c_int),
     "mgm_correct_normals": ([C.c_int, C.c_int, dp, dp, dp, u8p, ip, dp, dp, dp], C.c_int),
     "mgm_avg_dx": ([C.c_int, C.c_int, C.c_int, dp, dp, dp, u8p, ip, C.POINTER(C.c_double)], C.c_int),
+    "mgm_avg_dx_noalloc": ([C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp], C.c_int),
     "mgm_derivative_weights": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, dp, dp, u8p, ip,
                                 dp, dp, vp, dp, dp], C.c_int),
     "mgm_transfer_weights": ([C.c_int, dp, dp, dp, u8p, ip, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
