@@ -154,6 +154,21 @@ MGM_API int mgm_set_level(mgm_ctx *ctx, int lev, int n, int nb, const double *x,
  * smoother bounds).  flags: MGM_SETUP_*. */
 MGM_API int mgm_setup(mgm_ctx *ctx, int flags);
 
+/* Loads a level whose set-up was done elsewhere (e.g. by the stateless calls
+ * above into the reference's host structures): geometry after the reorder,
+ * cloud [n][k], operators [n][k] (Dz only in 3D), restriction/prolongation
+ * points and d_avg.  Then optionally the reference's transfer matrices
+ * (restr [n][k of lev-1], prol [n][k of lev+1]; NULL to skip), and
+ * mgm_prepare() builds the solver's data (the copyin_*_to_gpu step,
+ * openACC_functions.h:96-120). */
+MGM_API int mgm_load_level(mgm_ctx *ctx, int lev, int n, int nb, const double *x, const double *y, const double *z,
+                           const double *nx, const double *ny, const double *nz, const unsigned char *btag,
+                           int poly_degree, int k, const int *cloud, const double *Dx, const double *Dy,
+                           const double *Dz, const double *lap, const double *lapP, const int *rpts, const int *ppts,
+                           double d_avg);
+MGM_API int mgm_load_transfer(mgm_ctx *ctx, int lev, const double *restr, const double *prol);
+MGM_API int mgm_prepare(mgm_ctx *ctx);
+
 MGM_API int mgm_level_size(mgm_ctx *ctx, int lev, int *n, int *nb, int *k, int *num_poly_terms);
 MGM_API int mgm_level_d_avg(mgm_ctx *ctx, int lev, double *d_avg);
 
@@ -219,6 +234,8 @@ MGM_API int mgm_intermediate_velocity(mgm_ctx *ctx);
 MGM_API int mgm_mass_residual(mgm_ctx *ctx);
 MGM_API int mgm_poisson(mgm_ctx *ctx, int mode);
 MGM_API int mgm_update_velocity(mgm_ctx *ctx, double *mass_res);
+/* sqrt(sum |u - u_old|^2 / n) of the last velocity update (fractional_step_solver.h:63-69). */
+MGM_API int mgm_last_steady_error(mgm_ctx *ctx, double *steady_err);
 
 /* Poisson solve of A p = b on level 0 (A = lap_Poison with row 0 replaced by
  * p[0] = 0), b given on the host (b[0] and boundary rows as given), p used as

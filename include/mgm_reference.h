@@ -1,0 +1,173 @@
+/*
+ * mgm_reference.h -- drop-in replacement of the reference's C call surface
+ * for the hot path (Multigrid_meshless header_files/*.h), backed by the
+ * sm_100a kernels of libmgm.so.
+ *
+ * A program written against the reference includes this header instead of
+ * header_files/fractional_step_solver.h (+ openACC_functions.h) and links
+ * -lmgm.  The structures below have the members, types and order of
+ * header_files/structures.h:15-106 so that code filling or reading them is
+ * unchanged; the global `parameters` is defined by the library.
+ *
+ * Differences from the reference, by design:
+ *  - every function runs its compute on the GPU (no OpenACC, no CPU path);
+ *  - node sets must be in the state read_PointStructure leaves them
+ *    (boundary nodes first, no corner nodes); corner-tagged nodes are rejected;
+ *  - exactly equal kNN distances are ordered by lower node index;
+ *  - fatal errors print the library's message and exit(1), as the reference
+ *    does on input errors (mesh_functions.h:43-47);
+ *  - fractional_step_explicit keeps the fields on the device and copies the
+ *    level-0 velocity, pressure and intermediate velocity back after each
+ *    step (the reference's managed-memory view, mg_NS_solver.c:75).
+ */
+#ifndef MGM_REFERENCE_H
+#define MGM_REFERENCE_H
+
+#include <stdbool.h>
+
+#include "mgm.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* structures.h:15-41 */
+struct parameters {
+    short dimension;
+    short poly_degree;
+    short phs_degree;
+    short cloud_size_multiplier;
+    short test;
+    double courant_number;
+    double steady_state_tolerance;
+    double poisson_solver_tolerance;
+    short num_vcycles;
+    short num_relax;
+    int num_time_steps;
+    short num_levels;
+    int write_interval;
+    bool neumann_flag_boundary;
+    float omega;
+    double dt;
+    short iter_momentum;
+    short iter_timple;
+    double rho;
+    double mu;
+    double Re;
+    double facRe;
+    double facdt;
+    double nu;
+};
+MGM_API extern struct parameters parameters;
+
+/* structures.h:44-78 */
+typedef struct PointStructure {
+    char mesh_filename[50];
+    int num_nodes;
+    int num_corners;
+    int num_boundary_nodes;
+    int num_elem;
+    double d_avg;
+    short num_poly_terms;
+    short num_cloud_points;
+    short poly_degree;
+    double *x;
+    double *y;
+    double *z;
+    int *point_index;
+    double *x_normal;
+    double *y_normal;
+    double *z_normal;
+    bool *boundary_tag;
+    bool *corner_tag;
+    short *pow_x;
+    short *pow_y;
+    short *pow_z;
+    int **cloud_index;
+    int *prolongation_points;
+    int *restriction_points;
+    double **Dx;
+    double **Dy;
+    double **Dz;
+    double **lap;
+    double **lap_Poison;
+    double **restr_mat;
+    double **prol_mat;
+    int **prolongation_points2;
+    int **restriction_points2;
+} PointStructure;
+
+/* structures.h:80-106 */
+typedef struct FieldVariables {
+    double *u;
+    double *v;
+    double *w;
+    double *p;
+    double *u_new;
+    double *v_new;
+    double *w_new;
+    double *u_old;
+    double *v_old;
+    double *w_old;
+    double *p_old;
+    double *pprime;
+    double *res;
+    double *source;
+    double *T;
+    double *dpdn;
+    double *dpdx;
+    double *dpdy;
+    double *dpdz;
+    double rho;
+    double mu;
+    double nu;
+    double Re;
+} FieldVariables;
+
+/* structures.h:114-172 */
+MGM_API void AllocateMemoryPointStructure(PointStructure *myPointStruct, int nodes);
+MGM_API void AllocateMemoryFieldVariables(FieldVariables **field, PointStructure *myPointStruct, int num_levels);
+/* mesh_functions.h:37-129, 131-170 */
+MGM_API void read_flow_parameters(char *filename);
+MGM_API void read_grid_filenames(PointStructure **myPointStruct, char *filename, short *num_levels);
+MGM_API void calculate_parameters(PointStructure *myPointStruct);
+/* kdtree_functions.h:113-175 */
+MGM_API void find_cloud_index(PointStructure *myPointStruct1);
+MGM_API int *find_nearest_point(PointStructure *myPointStruct1, PointStructure *myPointStruct2, int num_cloud_points);
+/* mesh_functions.h:478-527, 533-670, 774-872, 874-910 */
+MGM_API void rcm_reordering_with_boundarynodes(PointStructure *myPointstruct);
+MGM_API void correct_normal_directions(PointStructure *myPointStruct);
+MGM_API void calculate_avg_dx(PointStructure *myPointStruct);
+MGM_API void create_restriction_matrix(PointStructure *myPointStruct_f, PointStructure *myPointStruct_c);
+MGM_API void create_prolongation_matrix(PointStructure *myPointStruct_f, PointStructure *myPointStruct_c);
+MGM_API void create_prolongation_and_restriction_matrices(PointStructure *myPointStruct, short num_levels);
+/* rbf.h:32-40, 401-421 */
+MGM_API double calculate_phs_rbf(double *pt1, double *pt2, int phs, int dimension);
+MGM_API void create_derivative_matrices(PointStructure *myPointStruct);
+/* mat_lib.h:80-89 */
+MGM_API void multiply_sparse_matrix_vector_gpu(double **D_coeff, double *f, double *dfdx, int **cloud, int n_rows_D,
+                                               int n_cols_D);
+/* general_functions.h:34-41 */
+MGM_API double calculate_dt(PointStructure *myPointStruct);
+/* openACC_functions.h:26-120 */
+MGM_API void copyin_parameters_to_gpu(void);
+MGM_API void copyin_essentials_to_gpu(PointStructure *myPointStruct);
+MGM_API void copyin_field_to_gpu(FieldVariables *field, PointStructure *myPointStruct);
+/* fractional_step_solver.h:28-37 */
+MGM_API double fractional_step_explicit(PointStructure *myPointStruct, FieldVariables *field);
+MGM_API void calculate_intermediate_velocity(PointStructure *myPointStruct, FieldVariables *field);
+MGM_API void calculate_mass_residual(PointStructure *myPointStruct, FieldVariables *field);
+MGM_API void calculate_boundary_dpdn(PointStructure *myPointStruct, FieldVariables *field);
+MGM_API void multigrid_Poisson_solver(PointStructure *myPointStruct, FieldVariables *field);
+MGM_API void update_velocity(PointStructure *myPointStruct, FieldVariables *field);
+
+/* No counterpart in the reference: which Poisson solve multigrid_Poisson_solver
+ * and fractional_step_explicit run (MGM_MODE_REFERENCE, the default: the
+ * reference's fixed V-cycles; MGM_MODE_FP64 / MGM_MODE_FP32_IR: the
+ * convergent solve to parameters.poisson_solver_tolerance). */
+MGM_API void mgm_reference_set_poisson_mode(int mode);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

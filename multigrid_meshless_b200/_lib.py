@@ -49,6 +49,10 @@ SIGNATURES = {
     "mgm_destroy": ([vp], None),
     "mgm_set_level": ([vp, C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, dp, dp, u8p, C.c_int, C.c_int], C.c_int),
     "mgm_setup": ([vp, C.c_int], C.c_int),
+    "mgm_load_level": ([vp, C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, dp, dp, u8p, C.c_int, C.c_int, ip, dp, dp, vp,
+                        dp, dp, ip, ip, C.c_double], C.c_int),
+    "mgm_load_transfer": ([vp, C.c_int, vp, vp], C.c_int),
+    "mgm_prepare": ([vp], C.c_int),
     "mgm_level_size": ([vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                         C.POINTER(C.c_int)], C.c_int),
     "mgm_level_d_avg": ([vp, C.c_int, C.POINTER(C.c_double)], C.c_int),
@@ -68,8 +72,10 @@ SIGNATURES = {
     "mgm_mass_residual": ([vp], C.c_int),
     "mgm_poisson": ([vp, C.c_int], C.c_int),
     "mgm_update_velocity": ([vp, C.POINTER(C.c_double)], C.c_int),
+    "mgm_last_steady_error": ([vp, C.POINTER(C.c_double)], C.c_int),
     "mgm_solve_poisson": ([vp, C.c_int, dp, dp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
     "mgm_sync": ([vp], C.c_int),
+    "mgm_reference_set_poisson_mode": ([C.c_int], None),
     "mgm_run_steps": ([vp, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                        C.POINTER(C.c_double)], C.c_int),
     "mgm_step_host": ([vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, C.POINTER(C.c_double)], C.c_int),

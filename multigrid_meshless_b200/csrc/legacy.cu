@@ -1,0 +1,442 @@
+// legacy.cu -- the reference's C call surface (include/mgm_reference.h) on top
+// of the C ABI (include/mgm.h).  Host code only: it packs the reference's
+// jagged rows into [n][k] arrays, calls the GPU entry points and unpacks the
+// results into freshly malloc'd rows, as the reference's functions do.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/mgm_reference.h"
+#include "mgm_math.h"
+
+struct parameters parameters;
+
+namespace {
+
+mgm_ctx *g_ctx = nullptr;
+int g_levels = 0;
+int g_mode = MGM_MODE_REFERENCE;
+
+void die_if(int status, const char *what)
+{
+    if (status != MGM_OK) {
+        std::printf("Error: %s: %s\n", what, mgm_last_error());
+        std::exit(1);
+    }
+}
+
+std::vector<unsigned char> tags(const bool *b, int n)
+{
+    std::vector<unsigned char> t(n);
+    for (int i = 0; i < n; i++) t[i] = b[i] ? 1 : 0;
+    return t;
+}
+
+std::vector<int> pack_rows(int *const *rows, int n, int k)
+{
+    std::vector<int> out((size_t)n * k);
+    for (int i = 0; i < n; i++) std::memcpy(&out[(size_t)i * k], rows[i], sizeof(int) * k);
+    return out;
+}
+
+std::vector<double> pack_rows(double *const *rows, int n, int k)
+{
+    std::vector<double> out((size_t)n * k);
+    for (int i = 0; i < n; i++) std::memcpy(&out[(size_t)i * k], rows[i], sizeof(double) * k);
+    return out;
+}
+
+template <class T>
+T **unpack_rows(const std::vector<T> &flat, int n, int k)
+{
+    T **rows = (T **)std::malloc(sizeof(T *) * (size_t)n);
+    for (int i = 0; i < n; i++) {
+        rows[i] = (T *)std::malloc(sizeof(T) * (size_t)k);
+        std::memcpy(rows[i], &flat[(size_t)i * k], sizeof(T) * k);
+    }
+    return rows;
+}
+
+void require_no_corners(const PointStructure *p, const char *fn)
+{
+    for (int i = 0; i < p->num_nodes; i++)
+        if (p->corner_tag && p->corner_tag[i]) {
+            std::printf("Error: %s: corner-tagged node %d present (remove corner nodes first, as read_PointStructure does)\n",
+                        fn, i);
+            std::exit(1);
+        }
+}
+
+}  // namespace
+
+extern "C" {
+
+void mgm_reference_set_poisson_mode(int mode) { g_mode = mode; }
+
+// structures.h:114-126
+void AllocateMemoryPointStructure(PointStructure *p, int nodes)
+{
+    p->x_normal = (double *)std::malloc(nodes * sizeof(double));
+    p->y_normal = (double *)std::malloc(nodes * sizeof(double));
+    p->z_normal = (double *)std::malloc(nodes * sizeof(double));
+    p->x = (double *)std::malloc(nodes * sizeof(double));
+    p->y = (double *)std::malloc(nodes * sizeof(double));
+    p->z = (double *)std::malloc(nodes * sizeof(double));
+    p->point_index = (int *)std::malloc(nodes * sizeof(int));
+    p->boundary_tag = (bool *)std::malloc(nodes * sizeof(bool));
+    p->corner_tag = (bool *)std::malloc(nodes * sizeof(bool));
+    p->num_nodes = nodes;
+    p->num_elem = 0;
+}
+
+// structures.h:128-172: every member array zero-filled
+void AllocateMemoryFieldVariables(FieldVariables **field, PointStructure *ps, int num_levels)
+{
+    *field = (FieldVariables *)std::calloc((size_t)num_levels, sizeof(FieldVariables));
+    for (int l = 0; l < num_levels; l++) {
+        const size_t n = (size_t)ps[l].num_nodes;
+        FieldVariables *f = &(*field)[l];
+        double **arrs[] = {&f->u, &f->v, &f->w, &f->u_new, &f->v_new, &f->w_new, &f->pprime, &f->p, &f->u_old,
+                           &f->v_old, &f->w_old, &f->p_old, &f->res, &f->source, &f->dpdn, &f->dpdx, &f->dpdy,
+                           &f->dpdz, &f->T};
+        for (double **a : arrs) *a = (double *)std::calloc(n, sizeof(double));
+    }
+}
+
+// mesh_functions.h:37-100: positional "name,value" lines in this order
+void read_flow_parameters(char *filename)
+{
+    FILE *f = std::fopen(filename, "r");
+    if (!f) { std::printf("Error: Unable to open the file\n"); std::exit(1); }
+    char name[100];
+    int itmp = 0, r = 0;
+    r = std::fscanf(f, "%[^,],%hd\n", name, &parameters.dimension);
+    r = std::fscanf(f, "%[^,],%hd\n", name, &parameters.poly_degree);
+    r = std::fscanf(f, "%[^,],%hd\n", name, &parameters.phs_degree);
+    r = std::fscanf(f, "%[^,],%hd\n", name, &parameters.cloud_size_multiplier);
+    r = std::fscanf(f, "%[^,],%hd\n", name, &parameters.test);
+    r = std::fscanf(f, "%[^,],%lf\n", name, &parameters.courant_number);
+    r = std::fscanf(f, "%[^,],%lf\n", name, &parameters.steady_state_tolerance);
+    r = std::fscanf(f, "%[^,],%lf\n", name, &parameters.poisson_solver_tolerance);
+    r = std::fscanf(f, "%[^,],%f\n", name, &parameters.omega);
+    r = std::fscanf(f, "%[^,],%hd\n", name, &parameters.num_vcycles);
+    r = std::fscanf(f, "%[^,],%hd\n", name, &parameters.num_relax);
+    r = std::fscanf(f, "%[^,],%d\n", name, &parameters.num_time_steps);
+    r = std::fscanf(f, "%[^,],%d\n", name, &parameters.write_interval);
+    r = std::fscanf(f, "%[^,],%d\n", name, &itmp);
+    parameters.neumann_flag_boundary = itmp == 1;
+    r = std::fscanf(f, "%[^,],%lf\n", name, &parameters.dt);
+    r = std::fscanf(f, "%[^,],%hd\n", name, &parameters.iter_momentum);
+    r = std::fscanf(f, "%[^,],%hd\n", name, &parameters.iter_timple);
+    r = std::fscanf(f, "%[^,],%lf\n", name, &parameters.Re);
+    r = std::fscanf(f, "%[^,],%lf\n", name, &parameters.facRe);
+    r = std::fscanf(f, "%[^,],%lf\n", name, &parameters.facdt);
+    std::fclose(f);
+    if (r == EOF) { std::printf("Error: Unable to read the file\n"); std::exit(1); }
+    parameters.rho = 1;
+    parameters.mu = parameters.rho / parameters.Re;
+    parameters.nu = parameters.mu / parameters.rho;
+}
+
+// mesh_functions.h:102-129
+void read_grid_filenames(PointStructure **ps, char *filename, short *num_levels)
+{
+    FILE *f = std::fopen(filename, "r");
+    if (!f) { std::printf("Error: Unable to open the file\n"); std::exit(1); }
+    char name[100];
+    if (std::fscanf(f, "%[^,],%hd\n", name, num_levels) == EOF) { std::printf("Error: Unable to read the file\n"); std::exit(1); }
+    *ps = (PointStructure *)std::calloc((size_t)*num_levels, sizeof(PointStructure));
+    for (short l = 0; l < *num_levels; l++)
+        if (std::fscanf(f, "%49s\n", (*ps)[l].mesh_filename) == EOF) {
+            std::printf("Error: Unable to read the meshfile names\n");
+            std::exit(1);
+        }
+    std::fclose(f);
+}
+
+// mesh_functions.h:131-170
+void calculate_parameters(PointStructure *p)
+{
+    const int d = p->poly_degree;
+    p->num_poly_terms = parameters.dimension == 3 ? (d + 1) * (d + 2) * (d + 3) / 6 : (d + 1) * (d + 2) / 2;
+    p->num_cloud_points = parameters.cloud_size_multiplier * p->num_poly_terms;
+    p->pow_x = (short *)std::malloc(p->num_poly_terms * sizeof(short));
+    p->pow_y = (short *)std::malloc(p->num_poly_terms * sizeof(short));
+    p->pow_z = (short *)std::malloc(p->num_poly_terms * sizeof(short));
+    int c = 0;
+    for (int i = 0; i <= d; i++)
+        for (int j = 0; j <= d - i; j++) {
+            if (parameters.dimension == 3) {
+                for (int l = 0; l <= d - i - j; l++) { p->pow_x[c] = i; p->pow_y[c] = j; p->pow_z[c] = l; c++; }
+            } else { p->pow_x[c] = i; p->pow_y[c] = j; p->pow_z[c] = 0; c++; }
+        }
+}
+
+void find_cloud_index(PointStructure *p)
+{
+    require_no_corners(p, "find_cloud_index");
+    const int n = p->num_nodes, k = p->num_cloud_points;
+    std::vector<unsigned char> bt = tags(p->boundary_tag, n);
+    std::vector<int> cl((size_t)n * k);
+    die_if(mgm_knn_cloud(n, p->num_boundary_nodes, parameters.dimension, p->x, p->y, p->z, bt.data(), k, cl.data()),
+           "find_cloud_index");
+    p->cloud_index = unpack_rows(cl, n, k);
+}
+
+int *find_nearest_point(PointStructure *p1, PointStructure *p2, int num_cloud_points)
+{
+    (void)num_cloud_points;  // the reference asks for 3 and keeps the first
+    int *out = (int *)std::malloc(sizeof(int) * (size_t)p1->num_nodes);
+    die_if(mgm_nearest_points(p1->num_nodes, p1->x, p1->y, p1->z, p2->num_nodes, p2->x, p2->y, p2->z,
+                              parameters.dimension, out),
+           "find_nearest_point");
+    return out;
+}
+
+void rcm_reordering_with_boundarynodes(PointStructure *p)
+{
+    const int n = p->num_nodes, k = p->num_cloud_points;
+    std::vector<int> cl = pack_rows(p->cloud_index, n, k), q1(n);
+    die_if(mgm_bfs_order(n, k, cl.data(), q1.data()), "rcm_reordering_with_boundarynodes");
+    std::vector<unsigned char> bt = tags(p->boundary_tag, n);
+    die_if(mgm_apply_order(n, k, q1.data(), p->x, p->y, p->z, p->x_normal, p->y_normal, p->z_normal, bt.data(),
+                           cl.data()),
+           "rcm_reordering_with_boundarynodes");
+    for (int i = 0; i < n; i++) {
+        p->boundary_tag[i] = bt[i] != 0;
+        std::memcpy(p->cloud_index[i], &cl[(size_t)i * k], sizeof(int) * k);
+    }
+}
+
+void correct_normal_directions(PointStructure *p)
+{
+    const int n = p->num_nodes, k = p->num_cloud_points;
+    std::vector<int> cl = pack_rows(p->cloud_index, n, k);
+    std::vector<unsigned char> bt = tags(p->boundary_tag, n);
+    die_if(mgm_correct_normals(n, k, p->x, p->y, p->z, bt.data(), cl.data(), p->x_normal, p->y_normal, p->z_normal),
+           "correct_normal_directions");
+}
+
+void calculate_avg_dx(PointStructure *p)
+{
+    const int n = p->num_nodes, k = p->num_cloud_points;
+    std::vector<int> cl = pack_rows(p->cloud_index, n, k);
+    std::vector<unsigned char> bt = tags(p->boundary_tag, n);
+    die_if(mgm_avg_dx(n, k, parameters.dimension, p->x, p->y, p->z, bt.data(), cl.data(), &p->d_avg), "calculate_avg_dx");
+}
+
+void create_restriction_matrix(PointStructure *f, PointStructure *c)
+{
+    const int kf = f->num_cloud_points;
+    std::vector<int> scl = pack_rows(f->cloud_index, f->num_nodes, kf);
+    std::vector<unsigned char> bt = tags(c->boundary_tag, c->num_nodes);
+    std::vector<double> W((size_t)c->num_nodes * kf);
+    die_if(mgm_transfer_weights(c->num_nodes, c->x, c->y, c->z, bt.data(), c->restriction_points, c->num_boundary_nodes,
+                                0, f->num_nodes, kf, parameters.dimension, parameters.phs_degree, f->poly_degree, f->x,
+                                f->y, f->z, scl.data(), W.data()),
+           "create_restriction_matrix");
+    c->restr_mat = unpack_rows(W, c->num_nodes, kf);
+}
+
+void create_prolongation_matrix(PointStructure *f, PointStructure *c)
+{
+    const int kc = c->num_cloud_points;
+    std::vector<int> scl = pack_rows(c->cloud_index, c->num_nodes, kc);
+    std::vector<unsigned char> bt = tags(f->boundary_tag, f->num_nodes);
+    std::vector<double> W((size_t)f->num_nodes * kc);
+    die_if(mgm_transfer_weights(f->num_nodes, f->x, f->y, f->z, bt.data(), f->prolongation_points, f->num_boundary_nodes,
+                                0, c->num_nodes, kc, parameters.dimension, parameters.phs_degree, c->poly_degree, c->x,
+                                c->y, c->z, scl.data(), W.data()),
+           "create_prolongation_matrix");
+    f->prol_mat = unpack_rows(W, f->num_nodes, kc);
+}
+
+// mesh_functions.h:874-893
+void create_prolongation_and_restriction_matrices(PointStructure *ps, short num_levels)
+{
+    for (short l = 0; l < num_levels; l++) {
+        if (l == num_levels - 1) ps[l].prolongation_points = find_nearest_point(&ps[l], &ps[l], 1);
+        else {
+            ps[l].prolongation_points = find_nearest_point(&ps[l], &ps[l + 1], 1);
+            create_prolongation_matrix(&ps[l], &ps[l + 1]);
+        }
+        if (l == 0) ps[l].restriction_points = find_nearest_point(&ps[l], &ps[l], 1);
+        else {
+            ps[l].restriction_points = find_nearest_point(&ps[l], &ps[l - 1], 1);
+            create_restriction_matrix(&ps[l - 1], &ps[l]);
+        }
+    }
+}
+
+double calculate_phs_rbf(double *pt1, double *pt2, int phs, int dimension)
+{
+    return mgm_phs_rbf(pt1, pt2, phs, dimension);
+}
+
+void create_derivative_matrices(PointStructure *p)
+{
+    require_no_corners(p, "create_derivative_matrices");
+    const int n = p->num_nodes, k = p->num_cloud_points, dim = parameters.dimension;
+    std::vector<int> cl = pack_rows(p->cloud_index, n, k);
+    std::vector<unsigned char> bt = tags(p->boundary_tag, n);
+    std::vector<double> Dx((size_t)n * k), Dy((size_t)n * k), Dz(dim == 3 ? (size_t)n * k : 0), lap((size_t)n * k),
+        lapP((size_t)n * k);
+    die_if(mgm_derivative_weights(n, k, dim, parameters.phs_degree, p->poly_degree, p->x, p->y, p->z, p->x_normal,
+                                  p->y_normal, p->z_normal, bt.data(), cl.data(), Dx.data(), Dy.data(),
+                                  dim == 3 ? Dz.data() : nullptr, lap.data(), lapP.data()),
+           "create_derivative_matrices");
+    p->Dx = unpack_rows(Dx, n, k);
+    p->Dy = unpack_rows(Dy, n, k);
+    p->Dz = dim == 3 ? unpack_rows(Dz, n, k) : nullptr;
+    p->lap = unpack_rows(lap, n, k);
+    p->lap_Poison = unpack_rows(lapP, n, k);
+}
+
+void multiply_sparse_matrix_vector_gpu(double **D, double *f, double *dfdx, int **cloud, int n, int k)
+{
+    std::vector<double> W = pack_rows(D, n, k);
+    std::vector<int> cl = pack_rows(cloud, n, k);
+    die_if(mgm_spmv(n, k, W.data(), cl.data(), f, dfdx), "multiply_sparse_matrix_vector_gpu");
+}
+
+// general_functions.h:34-41
+double calculate_dt(PointStructure *p)
+{
+    const double d = p->d_avg;
+    const double termd = 2 * parameters.nu / (d * d);
+    const double termc = 1 / d;
+    const double dt = 0.5 / (termd + termc);
+    return dt * parameters.courant_number;
+}
+
+void copyin_parameters_to_gpu(void)
+{
+    if (g_ctx)
+        die_if(mgm_set_flow(g_ctx, parameters.Re, parameters.courant_number, parameters.omega, parameters.num_relax,
+                            parameters.num_vcycles, parameters.dt),
+               "copyin_parameters_to_gpu");
+}
+
+// openACC_functions.h:96-120: the level data of every level on the device
+void copyin_essentials_to_gpu(PointStructure *ps)
+{
+    if (g_ctx) mgm_destroy(g_ctx);
+    g_levels = parameters.num_levels;
+    g_ctx = mgm_create(parameters.dimension, parameters.phs_degree, g_levels);
+    if (!g_ctx) { std::printf("Error: copyin_essentials_to_gpu: %s\n", mgm_last_error()); std::exit(1); }
+    for (int l = 0; l < g_levels; l++) {
+        PointStructure *p = &ps[l];
+        const int n = p->num_nodes, k = p->num_cloud_points;
+        std::vector<int> cl = pack_rows(p->cloud_index, n, k);
+        std::vector<unsigned char> bt = tags(p->boundary_tag, n);
+        std::vector<double> Dx = pack_rows(p->Dx, n, k), Dy = pack_rows(p->Dy, n, k), lap = pack_rows(p->lap, n, k),
+                            lapP = pack_rows(p->lap_Poison, n, k);
+        std::vector<double> Dz;
+        if (parameters.dimension == 3) Dz = pack_rows(p->Dz, n, k);
+        die_if(mgm_load_level(g_ctx, l, n, p->num_boundary_nodes, p->x, p->y, p->z, p->x_normal, p->y_normal,
+                              p->z_normal, bt.data(), p->poly_degree, k, cl.data(), Dx.data(), Dy.data(),
+                              parameters.dimension == 3 ? Dz.data() : nullptr, lap.data(), lapP.data(),
+                              p->restriction_points, p->prolongation_points, p->d_avg),
+               "copyin_essentials_to_gpu");
+    }
+    for (int l = 0; l < g_levels; l++) {
+        PointStructure *p = &ps[l];
+        std::vector<double> restr, prol;
+        if (l > 0 && p->restr_mat) restr = pack_rows(p->restr_mat, p->num_nodes, ps[l - 1].num_cloud_points);
+        if (l < g_levels - 1 && p->prol_mat) prol = pack_rows(p->prol_mat, p->num_nodes, ps[l + 1].num_cloud_points);
+        die_if(mgm_load_transfer(g_ctx, l, restr.empty() ? nullptr : restr.data(), prol.empty() ? nullptr : prol.data()),
+               "copyin_essentials_to_gpu");
+    }
+    die_if(mgm_prepare(g_ctx), "copyin_essentials_to_gpu");
+    die_if(mgm_set_solver(g_ctx, parameters.poisson_solver_tolerance > 0 ? parameters.poisson_solver_tolerance : 1e-8,
+                          100, 4, 10.0),
+           "copyin_essentials_to_gpu");
+}
+
+// openACC_functions.h:67-90: level-0 fields (the coarse levels start at zero, as allocated)
+void copyin_field_to_gpu(FieldVariables *field, PointStructure *ps)
+{
+    (void)ps;
+    if (!g_ctx) { std::printf("Error: copyin_field_to_gpu before copyin_essentials_to_gpu\n"); std::exit(1); }
+    copyin_parameters_to_gpu();
+    const FieldVariables *f = &field[0];
+    die_if(mgm_set_field(g_ctx, 0, MGM_FIELD_U, f->u), "copyin_field_to_gpu");
+    die_if(mgm_set_field(g_ctx, 0, MGM_FIELD_V, f->v), "copyin_field_to_gpu");
+    die_if(mgm_set_field(g_ctx, 0, MGM_FIELD_W, f->w), "copyin_field_to_gpu");
+    die_if(mgm_set_field(g_ctx, 0, MGM_FIELD_U_NEW, f->u_new), "copyin_field_to_gpu");
+    die_if(mgm_set_field(g_ctx, 0, MGM_FIELD_V_NEW, f->v_new), "copyin_field_to_gpu");
+    die_if(mgm_set_field(g_ctx, 0, MGM_FIELD_P, f->p), "copyin_field_to_gpu");
+    die_if(mgm_set_field(g_ctx, 0, MGM_FIELD_SOURCE, f->source), "copyin_field_to_gpu");
+}
+
+static void need_ctx(const char *fn)
+{
+    if (!g_ctx) { std::printf("Error: %s before copyin_essentials_to_gpu\n", fn); std::exit(1); }
+}
+
+void calculate_intermediate_velocity(PointStructure *p, FieldVariables *f)
+{
+    (void)p;
+    need_ctx("calculate_intermediate_velocity");
+    die_if(mgm_intermediate_velocity(g_ctx), "calculate_intermediate_velocity");
+    // `acc update host(u_new, v_new)` (fractional_step_solver.h:113)
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_U_NEW, f->u_new), "calculate_intermediate_velocity");
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_V_NEW, f->v_new), "calculate_intermediate_velocity");
+}
+
+void calculate_mass_residual(PointStructure *p, FieldVariables *f)
+{
+    (void)p; (void)f;
+    need_ctx("calculate_mass_residual");
+    die_if(mgm_mass_residual(g_ctx), "calculate_mass_residual");  // also writes the boundary dp/dn
+}
+
+void calculate_boundary_dpdn(PointStructure *p, FieldVariables *f)
+{
+    (void)p; (void)f;  // computed together with the mass residual (one pass over the stencils)
+}
+
+void multigrid_Poisson_solver(PointStructure *p, FieldVariables *f)
+{
+    (void)p; (void)f;
+    need_ctx("multigrid_Poisson_solver");
+    die_if(mgm_poisson(g_ctx, g_mode), "multigrid_Poisson_solver");
+}
+
+void update_velocity(PointStructure *p, FieldVariables *f)
+{
+    need_ctx("update_velocity");
+    double mass = 0;
+    die_if(mgm_update_velocity(g_ctx, &mass), "update_velocity");
+    std::printf("Mass residual: %e\n", mass);
+    (void)p; (void)f;
+}
+
+// fractional_step_solver.h:47-71
+double fractional_step_explicit(PointStructure *ps, FieldVariables *field)
+{
+    need_ctx("fractional_step_explicit");
+    FieldVariables *f = &field[0];
+    const int n = ps[0].num_nodes;
+    std::memcpy(f->u_old, f->u, sizeof(double) * n);
+    std::memcpy(f->v_old, f->v, sizeof(double) * n);
+    if (parameters.dimension == 3) std::memcpy(f->w_old, f->w, sizeof(double) * n);
+    calculate_intermediate_velocity(&ps[0], f);
+    calculate_mass_residual(&ps[0], f);
+    calculate_boundary_dpdn(&ps[0], f);
+    multigrid_Poisson_solver(ps, field);
+    update_velocity(&ps[0], f);
+    double err = 0;
+    die_if(mgm_last_steady_error(g_ctx, &err), "fractional_step_explicit");
+    // managed-memory view of level 0 (mg_NS_solver.c:75)
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_U, f->u), "fractional_step_explicit");
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_V, f->v), "fractional_step_explicit");
+    if (parameters.dimension == 3) die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_W, f->w), "fractional_step_explicit");
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_P, f->p), "fractional_step_explicit");
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_SOURCE, f->source), "fractional_step_explicit");
+    return err;
+}
+
+}  // extern "C"

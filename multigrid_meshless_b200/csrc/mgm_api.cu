@@ -787,106 +787,234 @@ int mgm_set_level(mgm_ctx *c, int lev, int n, int nb, const double *x, const dou
     });
 }
 
+}  // extern "C"
+
+namespace {
+
+// read_complete_mesh_data (mesh_functions.h:914-928) after the reader: kNN
+// clouds, breadth-first reorder, normals, average spacing, per level
+void pipeline_geometry(mgm_ctx *c)
+{
+    cudaStream_t s = c->s;
+    for (int l = 0; l < c->nl; l++) {
+        Level &L = c->L[l];
+        knn_clouds(L, c->dim, s);
+        DBuf<int> q1(L.n);
+        int reached = bfs_order(L.n, L.k, L.cloud.p, q1.p, s);
+        MGM_REQUIRE(reached == L.n, "mgm_setup: stencil graph of level " + std::to_string(l) + " is disconnected");
+        apply_order(L.n, L.k, q1.p, L.x.p, L.y.p, L.z.p, L.nx.p, L.ny.p, L.nz.p, L.btag.p, L.cloud.p, s);
+        correct_normals(L.n, L.k, L.x.p, L.y.p, L.z.p, L.btag.p, L.cloud.p, L.nx.p, L.ny.p, L.nz.p, s);
+        DBuf<double> d(1);
+        avg_dx(L.n, L.k, c->dim, L.x.p, L.y.p, L.z.p, L.btag.p, L.cloud.p, d.p, s);
+        d.download(&L.d_avg, 1, s);
+        L.idx.alloc((size_t)L.n * L.k);
+        transpose_rowmajor_to_ell_i(L.cloud.p, L.idx.p, L.n, L.k, s);
+    }
+    MGM_CUDA(cudaStreamSynchronize(s));
+    // create_prolongation_and_restriction_matrices (mesh_functions.h:874-893): points
+    for (int l = 0; l < c->nl; l++) {
+        Level &L = c->L[l];
+        nearest_of(L, l < c->nl - 1 ? c->L[l + 1] : L, c->dim, L.ppts, s);
+        nearest_of(L, l > 0 ? c->L[l - 1] : L, c->dim, L.rpts, s);
+    }
+}
+
+// transfer weights: the reference's rows (rows >= nb, optional) and the solver's rows
+void pipeline_transfer(mgm_ctx *c, bool reference_rows)
+{
+    cudaStream_t s = c->s;
+    for (int l = 0; l < c->nl; l++) {
+        Level &L = c->L[l];
+        if (l < c->nl - 1) {
+            Level &C = c->L[l + 1];
+            if (reference_rows)
+                build_transfer(L, C, L.ppts, L.nb, 0, c->dim, c->phs, L.ref_p_idx, L.ref_prol, nullptr, s);
+            build_transfer(L, C, L.ppts, 0, 0, c->dim, c->phs, L.s_p_idx, L.s_p_w64, &L.s_p_w32, s);
+        }
+        if (l > 0) {
+            Level &F = c->L[l - 1];
+            if (reference_rows)
+                build_transfer(L, F, L.rpts, L.nb, 0, c->dim, c->phs, L.ref_r_idx, L.ref_restr, nullptr, s);
+            build_transfer(L, F, L.rpts, 0, 1, c->dim, c->phs, L.s_r_idx, L.s_r_w64, &L.s_r_w32, s);
+        }
+    }
+}
+
+// create_derivative_matrices (rbf.h:401-421) on every level, into ELL
+void pipeline_derivatives(mgm_ctx *c)
+{
+    cudaStream_t s = c->s;
+    for (int l = 0; l < c->nl; l++) {
+        Level &L = c->L[l];
+        const size_t nk = (size_t)L.n * L.k;
+        DBuf<double> rm[5];
+        for (int t = 0; t < 5; t++) rm[t].alloc(nk);
+        Monomials mono = monomials(c->dim, L.poly);
+        derivative_weights(L.n, L.k, c->dim, c->phs, mono, L.x.p, L.y.p, L.z.p, L.nx.p, L.ny.p, L.nz.p, L.btag.p,
+                           L.cloud.p, rm[0].p, rm[1].p, c->dim == 3 ? rm[2].p : nullptr, rm[3].p, rm[4].p, s);
+        DBuf<double> *dst[5] = {&L.Dx, &L.Dy, &L.Dz, &L.lap, &L.lapP};
+        for (int t = 0; t < 5; t++) {
+            if (t == 2 && c->dim != 3) continue;
+            dst[t]->alloc(nk);
+            transpose_rowmajor_to_ell_d(rm[t].p, dst[t]->p, L.n, L.k, s);
+        }
+        MGM_CUDA(cudaStreamSynchronize(s));
+    }
+}
+
+// pinned operators, boundary rows, smoother bounds, coarsest inverse, fields
+void prepare_solver(mgm_ctx *c)
+{
+    cudaStream_t s = c->s;
+    drop_graphs(c);
+    for (int l = 0; l < c->nl; l++) {
+        Level &L = c->L[l];
+        const size_t nk = (size_t)L.n * L.k;
+        L.A64.alloc(nk); L.A32.alloc(nk); L.dinv64.alloc(L.n); L.dinv32.alloc(L.n);
+        k_pin_operator<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.lapP.p, L.A64.p, L.A32.p, L.dinv64.p,
+                                                               L.dinv32.p);
+        MGM_LAUNCHED();
+        std::vector<uint8_t> hb(L.n);
+        L.btag.download(hb.data(), L.n, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+        std::vector<int> bl;
+        for (int i = 0; i < L.n; i++) if (hb[i]) bl.push_back(i);
+        L.nbl = (int)bl.size();
+        L.bnd_list.upload(bl.data(), bl.size(), s);
+        L.bnd_idx.alloc((size_t)L.nbl * L.k);
+        L.bnd_A64.alloc((size_t)L.nbl * L.k);
+        L.bnd_A32.alloc((size_t)L.nbl * L.k);
+        k_gather_rows<<<blocks_for((long)L.nbl * L.k, 256), 256, 0, s>>>(L.nbl, L.bnd_list.p, L.n, L.k, L.idx.p,
+                                                                       L.A64.p, L.bnd_idx.p, L.bnd_A64.p,
+                                                                       L.bnd_A32.p);
+        MGM_LAUNCHED();
+        for (DBuf<double> *b : {&L.p, &L.ptmp, &L.src, &L.res, &L.r64, &L.e64, &L.e64b, &L.d64, &L.q64}) { b->alloc(L.n); b->zero(s); }
+        for (DBuf<float> *b : {&L.r32, &L.e32, &L.e32b, &L.d32, &L.q32}) { b->alloc(L.n); b->zero(s); }
+    }
+    for (int l = 0; l < c->nl - 1; l++) {
+        auto lv = solve_levels<double>(c);
+        estimate_lmax<double>(lv[l], s);
+        c->L[l].lmax = lv[l].lmax;
+    }
+    Level &Lc = c->L[c->nl - 1];
+    MGM_REQUIRE(Lc.n <= 8192, "mgm_setup: coarsest level too large for the dense solve (use more levels)");
+    c->cinv64.alloc((size_t)Lc.n * Lc.n);
+    c->cinv32.alloc((size_t)Lc.n * Lc.n);
+    dense_inverse(Lc.n, Lc.k, Lc.idx.p, Lc.A64.p, c->cinv64.p, c->cinv32.p, s);
+    const int n0 = c->L[0].n;
+    for (DBuf<double> *b : {&c->u, &c->v, &c->w, &c->u_new, &c->v_new, &c->w_new, &c->dpdn}) { b->alloc(n0); b->zero(s); }
+    c->partial.alloc(blocks_for(n0, 256) + 8);
+    c->scal.alloc(8);
+    alloc_solver_buffers(c);
+    MGM_CUDA(cudaStreamSynchronize(s));
+    c->setup_done = true;
+}
+
+}  // namespace
+
+extern "C" {
+
 int mgm_setup(mgm_ctx *c, int flags)
 {
     return guard([&] {
         check_ctx(c);
-        cudaStream_t s = c->s;
         for (int l = 0; l < c->nl; l++) MGM_REQUIRE(c->L[l].n > 0, "mgm_setup: level " + std::to_string(l) + " not set");
-        // read_complete_mesh_data (mesh_functions.h:914-928), per level after the reader
-        for (int l = 0; l < c->nl; l++) {
-            Level &L = c->L[l];
-            knn_clouds(L, c->dim, s);
-            DBuf<int> q1(L.n);
-            int reached = bfs_order(L.n, L.k, L.cloud.p, q1.p, s);
-            MGM_REQUIRE(reached == L.n, "mgm_setup: stencil graph of level " + std::to_string(l) + " is disconnected");
-            apply_order(L.n, L.k, q1.p, L.x.p, L.y.p, L.z.p, L.nx.p, L.ny.p, L.nz.p, L.btag.p, L.cloud.p, s);
-            correct_normals(L.n, L.k, L.x.p, L.y.p, L.z.p, L.btag.p, L.cloud.p, L.nx.p, L.ny.p, L.nz.p, s);
-            DBuf<double> d(1);
-            avg_dx(L.n, L.k, c->dim, L.x.p, L.y.p, L.z.p, L.btag.p, L.cloud.p, d.p, s);
-            d.download(&L.d_avg, 1, s);
-            L.idx.alloc((size_t)L.n * L.k);
-            transpose_rowmajor_to_ell_i(L.cloud.p, L.idx.p, L.n, L.k, s);
-        }
-        MGM_CUDA(cudaStreamSynchronize(s));
-        // create_prolongation_and_restriction_matrices (mesh_functions.h:874-893)
-        for (int l = 0; l < c->nl; l++) {
-            Level &L = c->L[l];
-            nearest_of(L, l < c->nl - 1 ? c->L[l + 1] : L, c->dim, L.ppts, s);
-            nearest_of(L, l > 0 ? c->L[l - 1] : L, c->dim, L.rpts, s);
-        }
+        c->setup_done = false;
+        pipeline_geometry(c);
         c->have_ref_transfer = (flags & MGM_SETUP_REFERENCE_TRANSFER) != 0;
-        for (int l = 0; l < c->nl; l++) {
-            Level &L = c->L[l];
-            if (l < c->nl - 1) {
-                Level &C = c->L[l + 1];
-                if (c->have_ref_transfer)
-                    build_transfer(L, C, L.ppts, L.nb, 0, c->dim, c->phs, L.ref_p_idx, L.ref_prol, nullptr, s);
-                build_transfer(L, C, L.ppts, 0, 0, c->dim, c->phs, L.s_p_idx, L.s_p_w64, &L.s_p_w32, s);
-            }
-            if (l > 0) {
-                Level &F = c->L[l - 1];
-                if (c->have_ref_transfer)
-                    build_transfer(L, F, L.rpts, L.nb, 0, c->dim, c->phs, L.ref_r_idx, L.ref_restr, nullptr, s);
-                build_transfer(L, F, L.rpts, 0, 1, c->dim, c->phs, L.s_r_idx, L.s_r_w64, &L.s_r_w32, s);
-            }
-        }
-        // create_derivative_matrices (rbf.h:401-421) on every level
-        for (int l = 0; l < c->nl; l++) {
-            Level &L = c->L[l];
-            const size_t nk = (size_t)L.n * L.k;
-            DBuf<double> rm[5];
-            for (int t = 0; t < 5; t++) rm[t].alloc(nk);
-            Monomials mono = monomials(c->dim, L.poly);
-            derivative_weights(L.n, L.k, c->dim, c->phs, mono, L.x.p, L.y.p, L.z.p, L.nx.p, L.ny.p, L.nz.p, L.btag.p,
-                               L.cloud.p, rm[0].p, rm[1].p, c->dim == 3 ? rm[2].p : nullptr, rm[3].p, rm[4].p, s);
-            DBuf<double> *dst[5] = {&L.Dx, &L.Dy, &L.Dz, &L.lap, &L.lapP};
-            for (int t = 0; t < 5; t++) {
-                if (t == 2 && c->dim != 3) continue;
-                dst[t]->alloc(nk);
-                transpose_rowmajor_to_ell_d(rm[t].p, dst[t]->p, L.n, L.k, s);
-            }
-            // pinned solver operator, boundary row list, work vectors
-            L.A64.alloc(nk); L.A32.alloc(nk); L.dinv64.alloc(L.n); L.dinv32.alloc(L.n);
-            k_pin_operator<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.lapP.p, L.A64.p, L.A32.p, L.dinv64.p,
-                                                                   L.dinv32.p);
-            MGM_LAUNCHED();
-            std::vector<uint8_t> hb(L.n);
-            L.btag.download(hb.data(), L.n, s);
+        pipeline_transfer(c, c->have_ref_transfer);
+        pipeline_derivatives(c);
+        prepare_solver(c);
+    });
+}
+
+int mgm_load_level(mgm_ctx *c, int lev, int n, int nb, const double *x, const double *y, const double *z,
+                   const double *nx, const double *ny, const double *nz, const unsigned char *btag, int poly_degree,
+                   int k, const int *cloud, const double *Dx, const double *Dy, const double *Dz, const double *lap,
+                   const double *lapP, const int *rpts, const int *ppts, double d_avg)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(lev >= 0 && lev < c->nl, "mgm_load_level: level out of range");
+        MGM_REQUIRE(n > 0 && nb >= 0 && nb <= n && k >= 2 && k <= kMaxK, "mgm_load_level: bad sizes");
+        MGM_REQUIRE(x && y && z && nx && ny && nz && btag && cloud && Dx && Dy && lap && lapP && rpts && ppts,
+                    "mgm_load_level: null pointer");
+        MGM_REQUIRE(c->dim == 2 || Dz, "mgm_load_level: Dz required in 3D");
+        for (long t = 0; t < (long)n * k; t++) MGM_REQUIRE(cloud[t] >= 0 && cloud[t] < n, "mgm_load_level: cloud index out of range");
+        Level &L = c->L[lev];
+        L = Level();
+        Monomials mono = monomials(c->dim, poly_degree);
+        L.n = n; L.nb = nb; L.k = k; L.poly = poly_degree; L.np = mono.np; L.d_avg = d_avg;
+        cudaStream_t s = c->s;
+        L.x.upload(x, n, s); L.y.upload(y, n, s); L.z.upload(z, n, s);
+        L.nx.upload(nx, n, s); L.ny.upload(ny, n, s); L.nz.upload(nz, n, s);
+        L.btag.upload(btag, n, s);
+        L.cloud.upload(cloud, (size_t)n * k, s);
+        L.idx.alloc((size_t)n * k);
+        transpose_rowmajor_to_ell_i(L.cloud.p, L.idx.p, n, k, s);
+        const double *h[5] = {Dx, Dy, Dz, lap, lapP};
+        DBuf<double> *dst[5] = {&L.Dx, &L.Dy, &L.Dz, &L.lap, &L.lapP};
+        DBuf<double> tmp((size_t)n * k);
+        for (int t = 0; t < 5; t++) {
+            if (t == 2 && c->dim != 3) continue;
+            tmp.upload(h[t], (size_t)n * k, s);
+            dst[t]->alloc((size_t)n * k);
+            transpose_rowmajor_to_ell_d(tmp.p, dst[t]->p, n, k, s);
             MGM_CUDA(cudaStreamSynchronize(s));
-            std::vector<int> bl;
-            for (int i = 0; i < L.n; i++) if (hb[i]) bl.push_back(i);
-            L.nbl = (int)bl.size();
-            L.bnd_list.upload(bl.data(), bl.size(), s);
-            L.bnd_idx.alloc((size_t)L.nbl * L.k);
-            L.bnd_A64.alloc((size_t)L.nbl * L.k);
-            L.bnd_A32.alloc((size_t)L.nbl * L.k);
-            k_gather_rows<<<blocks_for((long)L.nbl * L.k, 256), 256, 0, s>>>(L.nbl, L.bnd_list.p, L.n, L.k, L.idx.p,
-                                                                           L.A64.p, L.bnd_idx.p, L.bnd_A64.p,
-                                                                           L.bnd_A32.p);
-            MGM_LAUNCHED();
-            for (DBuf<double> *b : {&L.p, &L.ptmp, &L.src, &L.res, &L.r64, &L.e64, &L.e64b, &L.d64, &L.q64}) { b->alloc(L.n); b->zero(s); }
-            for (DBuf<float> *b : {&L.r32, &L.e32, &L.e32b, &L.d32, &L.q32}) { b->alloc(L.n); b->zero(s); }
         }
-        // smoother bounds and the coarsest-level inverse
-        for (int l = 0; l < c->nl - 1; l++) {
-            auto lv = solve_levels<double>(c);
-            estimate_lmax<double>(lv[l], s);
-            c->L[l].lmax = lv[l].lmax;
-        }
-        Level &Lc = c->L[c->nl - 1];
-        MGM_REQUIRE(Lc.n <= 8192, "mgm_setup: coarsest level too large for the dense solve (use more levels)");
-        c->cinv64.alloc((size_t)Lc.n * Lc.n);
-        c->cinv32.alloc((size_t)Lc.n * Lc.n);
-        dense_inverse(Lc.n, Lc.k, Lc.idx.p, Lc.A64.p, c->cinv64.p, c->cinv32.p, s);
-        // level-0 fields
-        const int n0 = c->L[0].n;
-        for (DBuf<double> *b : {&c->u, &c->v, &c->w, &c->u_new, &c->v_new, &c->w_new, &c->dpdn}) { b->alloc(n0); b->zero(s); }
-        c->partial.alloc(blocks_for(n0, 256) + 8);
-        c->scal.alloc(8);
-        alloc_solver_buffers(c);
+        L.rpts.upload(rpts, n, s);
+        L.ppts.upload(ppts, n, s);
         MGM_CUDA(cudaStreamSynchronize(s));
-        c->setup_done = true;
+        c->setup_done = false;
+        c->have_ref_transfer = false;
+    });
+}
+
+int mgm_load_transfer(mgm_ctx *c, int lev, const double *restr, const double *prol)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(lev >= 0 && lev < c->nl && c->L[lev].n > 0, "mgm_load_transfer: level not loaded");
+        Level &L = c->L[lev];
+        cudaStream_t s = c->s;
+        if (restr && lev > 0) {
+            Level &F = c->L[lev - 1];
+            DBuf<double> tmp;
+            tmp.upload(restr, (size_t)L.n * F.k, s);
+            L.ref_restr.alloc((size_t)L.n * F.k);
+            transpose_rowmajor_to_ell_d(tmp.p, L.ref_restr.p, L.n, F.k, s);
+            L.ref_r_idx.alloc((size_t)L.n * F.k);
+            k_gather_idx<<<blocks_for((long)L.n * F.k, 256), 256, 0, s>>>(L.n, F.k, L.rpts.p, F.cloud.p, L.ref_r_idx.p);
+            MGM_LAUNCHED();
+            MGM_CUDA(cudaStreamSynchronize(s));
+        }
+        if (prol && lev < c->nl - 1) {
+            Level &C = c->L[lev + 1];
+            DBuf<double> tmp;
+            tmp.upload(prol, (size_t)L.n * C.k, s);
+            L.ref_prol.alloc((size_t)L.n * C.k);
+            transpose_rowmajor_to_ell_d(tmp.p, L.ref_prol.p, L.n, C.k, s);
+            L.ref_p_idx.alloc((size_t)L.n * C.k);
+            k_gather_idx<<<blocks_for((long)L.n * C.k, 256), 256, 0, s>>>(L.n, C.k, L.ppts.p, C.cloud.p, L.ref_p_idx.p);
+            MGM_LAUNCHED();
+            MGM_CUDA(cudaStreamSynchronize(s));
+        }
+    });
+}
+
+int mgm_prepare(mgm_ctx *c)
+{
+    return guard([&] {
+        check_ctx(c);
+        for (int l = 0; l < c->nl; l++) MGM_REQUIRE(c->L[l].n > 0 && c->L[l].lapP.p, "mgm_prepare: level " + std::to_string(l) + " not loaded");
+        bool ref_ok = true;
+        for (int l = 0; l < c->nl; l++) {
+            if (l > 0 && !c->L[l].ref_restr.p) ref_ok = false;
+            if (l < c->nl - 1 && !c->L[l].ref_prol.p) ref_ok = false;
+        }
+        pipeline_transfer(c, false);
+        c->have_ref_transfer = ref_ok;
+        prepare_solver(c);
     });
 }
 
@@ -1139,6 +1267,17 @@ int mgm_update_velocity(mgm_ctx *c, double *mass_res)
             *mass_res = c->h_pinned[1];
         }
         MGM_CUDA(cudaStreamSynchronize(c->s));
+    });
+}
+
+int mgm_last_steady_error(mgm_ctx *c, double *steady_err)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done, "mgm_last_steady_error: not ready");
+        c->scal.download(c->h_pinned, 1, c->s);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+        *steady_err = c->h_pinned[0];
     });
 }
 

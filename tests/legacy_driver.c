@@ -1,0 +1,157 @@
+/*
+ * legacy_driver.c -- a program written against the reference's call surface
+ * (the flow of mg_NS_solver.c:17-103 with the mesh reader replaced by a node
+ * file), linked against libmgm.so through include/mgm_reference.h.
+ *
+ *   legacy_driver <input.bin> <output_dir>
+ *
+ * input.bin: int32 nl, dim, phs, poly, multiplier, nsteps, num_vcycles,
+ *            num_relax, mode; double Re, courant, omega; per level: int32 n,
+ *            nb; double x[n], y[n], z[n], nx[n], ny[n], nz[n]; uint8 btag[n].
+ * Writes raw arrays into output_dir (read back by tests/test_gpu_legacy.py).
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "mgm_reference.h"
+
+static void rd(void *p, size_t sz, size_t n, FILE *f)
+{
+    if (fread(p, sz, n, f) != n) { fprintf(stderr, "short read\n"); exit(2); }
+}
+
+static void wr(const char *dir, const char *name, const void *p, size_t bytes)
+{
+    char path[512];
+    snprintf(path, sizeof(path), "%s/%s", dir, name);
+    FILE *f = fopen(path, "wb");
+    if (!f || fwrite(p, 1, bytes, f) != bytes) { fprintf(stderr, "write %s failed\n", path); exit(3); }
+    fclose(f);
+}
+
+static void wr_rows_d(const char *dir, const char *name, double **rows, int n, int k)
+{
+    double *flat = malloc(sizeof(double) * (size_t)n * k);
+    for (int i = 0; i < n; i++) memcpy(flat + (size_t)i * k, rows[i], sizeof(double) * k);
+    wr(dir, name, flat, sizeof(double) * (size_t)n * k);
+    free(flat);
+}
+
+static void wr_rows_i(const char *dir, const char *name, int **rows, int n, int k)
+{
+    int *flat = malloc(sizeof(int) * (size_t)n * k);
+    for (int i = 0; i < n; i++) memcpy(flat + (size_t)i * k, rows[i], sizeof(int) * k);
+    wr(dir, name, flat, sizeof(int) * (size_t)n * k);
+    free(flat);
+}
+
+int main(int argc, char **argv)
+{
+    if (argc < 3) { fprintf(stderr, "usage: legacy_driver input.bin outdir\n"); return 1; }
+    FILE *f = fopen(argv[1], "rb");
+    if (!f) { fprintf(stderr, "cannot open %s\n", argv[1]); return 1; }
+    const char *out = argv[2];
+    int hdr[9];
+    double flow[3];
+    rd(hdr, sizeof(int), 9, f);
+    rd(flow, sizeof(double), 3, f);
+    const int nl = hdr[0], nsteps = hdr[5];
+    memset(&parameters, 0, sizeof(parameters));
+    parameters.dimension = (short)hdr[1];
+    parameters.phs_degree = (short)hdr[2];
+    parameters.poly_degree = (short)hdr[3];
+    parameters.cloud_size_multiplier = (short)hdr[4];
+    parameters.num_vcycles = (short)hdr[6];
+    parameters.num_relax = (short)hdr[7];
+    parameters.num_levels = (short)nl;
+    parameters.Re = flow[0];
+    parameters.courant_number = flow[1];
+    parameters.omega = (float)flow[2];
+    parameters.poisson_solver_tolerance = 1e-10;
+    parameters.rho = 1;
+    parameters.mu = parameters.rho / parameters.Re;
+    parameters.nu = parameters.mu / parameters.rho;
+    mgm_reference_set_poisson_mode(hdr[8]);
+
+    /* read_complete_mesh_data (mesh_functions.h:914-928), nodes from the file */
+    PointStructure *ps = calloc(nl, sizeof(PointStructure));
+    for (int l = 0; l < nl; l++) {
+        int nn[2];
+        rd(nn, sizeof(int), 2, f);
+        PointStructure *p = &ps[l];
+        p->poly_degree = parameters.poly_degree;
+        calculate_parameters(p);
+        AllocateMemoryPointStructure(p, nn[0]);
+        rd(p->x, sizeof(double), nn[0], f);
+        rd(p->y, sizeof(double), nn[0], f);
+        rd(p->z, sizeof(double), nn[0], f);
+        rd(p->x_normal, sizeof(double), nn[0], f);
+        rd(p->y_normal, sizeof(double), nn[0], f);
+        rd(p->z_normal, sizeof(double), nn[0], f);
+        unsigned char *bt = malloc(nn[0]);
+        rd(bt, 1, nn[0], f);
+        for (int i = 0; i < nn[0]; i++) {
+            p->boundary_tag[i] = bt[i] != 0;
+            p->corner_tag[i] = false;
+            p->point_index[i] = i;
+        }
+        free(bt);
+        p->num_boundary_nodes = nn[1];
+        p->num_corners = 0;
+        find_cloud_index(p);
+        rcm_reordering_with_boundarynodes(p);
+        correct_normal_directions(p);
+        calculate_avg_dx(p);
+    }
+    fclose(f);
+    create_prolongation_and_restriction_matrices(ps, (short)nl);
+    for (int l = 0; l < nl; l++) create_derivative_matrices(&ps[l]);
+
+    /* mg_NS_solver.c:47-59 with the lid-driven cavity conditions (init_LDC.c) */
+    FieldVariables *field;
+    AllocateMemoryFieldVariables(&field, ps, nl);
+    for (int i = 0; i < ps[0].num_nodes; i++)
+        if (fabs(ps[0].y[i] - 1.0) < 1e-9) field[0].u[i] = 1.0;
+    parameters.dt = calculate_dt(&ps[0]);
+    copyin_essentials_to_gpu(ps);
+    copyin_field_to_gpu(field, ps);
+    copyin_parameters_to_gpu();
+
+    double *errs = malloc(sizeof(double) * (nsteps > 0 ? nsteps : 1));
+    for (int s = 0; s < nsteps; s++) errs[s] = fractional_step_explicit(ps, field);
+
+    for (int l = 0; l < nl; l++) {
+        PointStructure *p = &ps[l];
+        const int n = p->num_nodes, k = p->num_cloud_points;
+        char nm[64];
+        unsigned char *bt = malloc(n);
+        for (int i = 0; i < n; i++) bt[i] = p->boundary_tag[i];
+#define W(tag, ptr, bytes) do { snprintf(nm, sizeof(nm), "l%d_%s", l, tag); wr(out, nm, ptr, bytes); } while (0)
+        W("x", p->x, sizeof(double) * n);
+        W("y", p->y, sizeof(double) * n);
+        W("nx", p->x_normal, sizeof(double) * n);
+        W("ny", p->y_normal, sizeof(double) * n);
+        W("btag", bt, n);
+        W("d_avg", &p->d_avg, sizeof(double));
+        W("rpts", p->restriction_points, sizeof(int) * n);
+        W("ppts", p->prolongation_points, sizeof(int) * n);
+#undef W
+        snprintf(nm, sizeof(nm), "l%d_cloud", l); wr_rows_i(out, nm, p->cloud_index, n, k);
+        snprintf(nm, sizeof(nm), "l%d_Dx", l); wr_rows_d(out, nm, p->Dx, n, k);
+        snprintf(nm, sizeof(nm), "l%d_Dy", l); wr_rows_d(out, nm, p->Dy, n, k);
+        snprintf(nm, sizeof(nm), "l%d_lap", l); wr_rows_d(out, nm, p->lap, n, k);
+        snprintf(nm, sizeof(nm), "l%d_lapP", l); wr_rows_d(out, nm, p->lap_Poison, n, k);
+        if (l > 0) { snprintf(nm, sizeof(nm), "l%d_restr", l); wr_rows_d(out, nm, p->restr_mat, n, ps[l - 1].num_cloud_points); }
+        if (l < nl - 1) { snprintf(nm, sizeof(nm), "l%d_prol", l); wr_rows_d(out, nm, p->prol_mat, n, ps[l + 1].num_cloud_points); }
+        free(bt);
+    }
+    wr(out, "dt", &parameters.dt, sizeof(double));
+    wr(out, "errs", errs, sizeof(double) * nsteps);
+    wr(out, "u", field[0].u, sizeof(double) * ps[0].num_nodes);
+    wr(out, "v", field[0].v, sizeof(double) * ps[0].num_nodes);
+    wr(out, "p", field[0].p, sizeof(double) * ps[0].num_nodes);
+    printf("legacy driver done: %d levels, %d steps\n", nl, nsteps);
+    return 0;
+}

@@ -22,6 +22,23 @@ def declared_symbols():
     return names
 
 
+def reference_surface_symbols():
+    txt = open(os.path.join(ROOT, "include", "mgm_reference.h")).read()
+    return set(re.findall(r"MGM_API\s+(?:extern\s+)?[\w\s\*]*?\b([A-Za-z_]\w*)\s*[\(;]", txt))
+
+
+def test_reference_surface_exported():
+    """Every function of the reference's call surface (and the `parameters`
+    global) that include/mgm_reference.h declares is exported."""
+    names = reference_surface_symbols()
+    for must in ("find_cloud_index", "create_derivative_matrices", "fractional_step_explicit",
+                 "multiply_sparse_matrix_vector_gpu", "copyin_essentials_to_gpu", "parameters"):
+        assert must in names
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [nm for nm in sorted(names) if not hasattr(lib, nm)]
+    assert not missing, missing
+
+
 def test_header_declares_entry_points():
     names = declared_symbols()
     assert "mgm_knn_cloud" in names and "mgm_step" in names and "mgm_solve_poisson" in names

@@ -1,0 +1,90 @@
+"""A C program written against the reference's call surface
+(include/mgm_reference.h: find_cloud_index, rcm_reordering_with_boundarynodes,
+create_derivative_matrices, copyin_*_to_gpu, fractional_step_explicit, ...)
+runs on the GPU through libmgm.so and reproduces the oracle.
+
+The driver (tests/legacy_driver.c) is compiled here with gcc against the
+in-tree library; its outputs are compared bit for bit with the oracle
+restatement (correctly-rounded-power build for the weights; same sweep order
+for the fractional step)."""
+import os
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+from multigrid_meshless_b200 import clouds
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "multigrid_meshless_b200")
+
+
+def _compile(tmp):
+    exe = os.path.join(tmp, "legacy_driver")
+    subprocess.run(["gcc", "-O2", "-std=c11", "-I", os.path.join(ROOT, "include"), "-o", exe,
+                    os.path.join(ROOT, "tests", "legacy_driver.c"), "-L", PKG, "-lmgm", f"-Wl,-rpath,{PKG}", "-lm"],
+                   check=True)
+    return exe
+
+
+def _write_input(path, cl, poly, mult, nsteps, nv, nr, mode, Re, courant, omega):
+    with open(path, "wb") as f:
+        f.write(struct.pack("9i", len(cl), cl[0].dim, 3, poly, mult, nsteps, nv, nr, mode))
+        f.write(struct.pack("3d", Re, courant, omega))
+        for c in cl:
+            f.write(struct.pack("2i", c.n, c.nb))
+            for a in (c.x, c.y, c.z, c.nx, c.ny, c.nz):
+                f.write(np.ascontiguousarray(a, np.float64).tobytes())
+            f.write(np.ascontiguousarray(c.btag, np.uint8).tobytes())
+
+
+def _read(out, name, dtype, shape=None):
+    a = np.fromfile(os.path.join(out, name), dtype=dtype)
+    return a.reshape(shape) if shape else a
+
+
+def test_reference_call_surface_end_to_end(require_gpu, tmp_path):
+    exe = _compile(str(tmp_path))
+    cl = clouds.cavity_hierarchy(36, 2, seed=13)
+    k, poly = 20, 3
+    inp = str(tmp_path / "in.bin")
+    out = str(tmp_path / "out")
+    os.makedirs(out)
+    _write_input(inp, cl, poly, 2, 2, 2, 3, 0, 100.0, 0.5, 1.2)
+    r = subprocess.run([exe, inp, out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.count("Mass residual") == 2
+
+    P = O.orc_pipeline(cl, [k, k], [poly, poly], crpow=True)
+    levels = []
+    for l, L in enumerate(P):
+        n = L.n
+        assert np.array_equal(_read(out, f"l{l}_cloud", np.int32, (n, k)), L.cloud)
+        for nm in ("x", "y", "nx", "ny"):
+            assert np.array_equal(_read(out, f"l{l}_{nm}", np.float64), getattr(L, nm)), nm
+        assert np.array_equal(_read(out, f"l{l}_btag", np.uint8), L.btag)
+        assert _read(out, f"l{l}_d_avg", np.float64)[0] == L.d_avg
+        assert np.array_equal(_read(out, f"l{l}_rpts", np.int32), L.rpts)
+        assert np.array_equal(_read(out, f"l{l}_ppts", np.int32), L.ppts)
+        for nm in ("Dx", "Dy", "lap", "lapP"):
+            assert np.array_equal(_read(out, f"l{l}_{nm}", np.float64, (n, k)), getattr(L, nm)), nm
+        if l > 0:
+            assert np.array_equal(_read(out, f"l{l}_restr", np.float64, (n, k)), L.restr)
+        if l < len(P) - 1:
+            assert np.array_equal(_read(out, f"l{l}_prol", np.float64, (n, k)), L.prol)
+
+    # two fractional steps in the reference's semantics (sweeps in Jacobi order)
+    S = O.OracleSolver(P, 100.0, 0.5, 1.2, 3, 2, jacobi=True)
+    assert S.dt == _read(out, "dt", np.float64)[0]
+    O.lid_bc(P[0], S.f)
+    errs = _read(out, "errs", np.float64)
+    for s in range(2):
+        e, _ = S.step()
+        assert abs(errs[s] - e) <= 1e-12 * abs(e)
+    assert np.array_equal(_read(out, "u", np.float64), S.f["u"])
+    assert np.array_equal(_read(out, "v", np.float64), S.f["v"])
+    assert np.array_equal(_read(out, "p", np.float64), S.p[0])
