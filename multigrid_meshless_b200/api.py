@@ -211,6 +211,9 @@ class Multigrid:
     def set_solver(self, rel_tol=1e-8, max_iters=60, cheb_degree=3, cheb_ratio=6.0):
         check(self.L.mgm_set_solver(self.h, rel_tol, max_iters, cheb_degree, cheb_ratio))
 
+    def use_compact(self, enable=True):
+        check(self.L.mgm_use_compact(self.h, 1 if enable else 0))
+
     def use_graphs(self, enable=True):
         check(self.L.mgm_use_graphs(self.h, 1 if enable else 0))
 

@@ -79,11 +79,13 @@ def _smooth_rhs(L, seed):
     return f
 
 
-@pytest.mark.parametrize("mode", [mgm.MODE_FP64, mgm.MODE_FP32_IR], ids=["fp64", "fp32_ir"])
-def test_poisson_converges_to_direct_solution(cavity, mode):
+@pytest.mark.parametrize("mode,compact", [(mgm.MODE_FP64, True), (mgm.MODE_FP32_IR, True), (mgm.MODE_FP32_IR, False)],
+                         ids=["fp64", "fp32_ir_compact", "fp32_ir_plain"])
+def test_poisson_converges_to_direct_solution(cavity, mode, compact):
     mg = cavity
     mg.set_flow(Re=100.0, courant=0.5)
     mg.set_solver(rel_tol=1e-8, max_iters=80)
+    mg.use_compact(compact)
     g = mg.geometry(0)
     ops = mg.operators(0)
     b = _smooth_rhs(g, 1)
@@ -92,6 +94,7 @@ def test_poisson_converges_to_direct_solution(cavity, mode):
     assert O.rel_residual(ops["lapP"], g["cloud"], b, p) < 2e-8
     p_ref = O.pinned_poisson_direct(ops["lapP"], g["cloud"], b)
     err = np.linalg.norm(p - p_ref) / np.linalg.norm(p_ref)
+    mg.use_compact(True)
     assert err < P_TOL, (err, iters)
 
 
