@@ -47,8 +47,8 @@ def parse():
     ap.add_argument("--Re", type=float, default=100.0)
     ap.add_argument("--courant", type=float, default=0.5)
     ap.add_argument("--tol", type=float, default=1e-8)
-    ap.add_argument("--cheb-degree", type=int, default=4)
-    ap.add_argument("--cheb-ratio", type=float, default=10.0)
+    ap.add_argument("--cheb-degree", type=int, default=3)
+    ap.add_argument("--cheb-ratio", type=float, default=20.0)
     ap.add_argument("--episode", type=int, default=10,
                     help="steps per episode from rest (the explicit scheme is unstable beyond ~12 steps at 1M nodes)")
     ap.add_argument("--sample-m", type=int, default=128, help="cavity size of the CPU baseline sample")
@@ -355,7 +355,7 @@ def run_ours(a, rank, world, local_rank):
             "learned_warm_start": None,
             "e2e": {"value": steps_total / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": 2 * 8 * n,
                     "d2h_bytes_per_step": 3 * 8 * n, "finite": finite},
-            "roofline": {"bound": "hbm", "kernel": "k_cheb<float> level 0 (Chebyshev smoother step)",
+            "roofline": {"bound": "hbm", "kernel": "k_cheb_o level 0 (FP32 Chebyshev smoother step, int16 offsets)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "bytes_per_launch": sm_bytes, "launches": sm_launch,

@@ -221,10 +221,10 @@ MGM_API int mgm_step(mgm_ctx *ctx, int mode, double *steady_err);
 
 /* Solver controls for MGM_MODE_FP64 / MGM_MODE_FP32_IR. */
 MGM_API int mgm_set_solver(mgm_ctx *ctx, double rel_tol, int max_iters, int cheb_degree, double cheb_ratio);
-/* MGM_MODE_FP32_IR preconditioner storage: compact (default; D^-1 A and the
- * transfer weights in FP16, neighbour indices as 16-bit offsets where the
- * reordered bandwidth allows) or plain FP32 with 32-bit indices (enable = 0).
- * The outer FP64 iteration is unchanged, so the converged answer is too. */
+/* MGM_MODE_FP32_IR preconditioner indices: compact (default; neighbour
+ * indices as 16-bit offsets from the row, transfer gathers as 16-bit offsets
+ * from the row's nearest node, wherever the reordered bandwidth allows) or
+ * 32-bit (enable = 0).  Results are identical either way. */
 MGM_API int mgm_use_compact(mgm_ctx *ctx, int enable);
 /* Replay each V-cycle from a captured CUDA graph (default on) or launch its
  * kernels one by one (enable = 0).  Results are identical either way. */

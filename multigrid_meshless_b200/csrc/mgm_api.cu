@@ -47,10 +47,8 @@ struct Level {
     DBuf<float> bnd_A32;
     int nbl = 0;
     double lmax = 2.0;
-    // compact FP32-path storage (FP16 row-scaled weights, int16 offsets)
-    DBuf<__half> As16, rs16, ps16;
+    // compact FP32-path indices (int16 offsets)
     DBuf<short> off16, r_off16, p_off16;
-    DBuf<float> diag32;
     bool off_ok = false, r_off_ok = false, p_off_ok = false;
     // reference-mode state
     DBuf<double> p, ptmp, src, res;
@@ -178,31 +176,14 @@ __global__ void k_bc(int n, int kind, const double *x, const double *y, double *
 
 __global__ void k_zero_pinned(double *b) { b[0] = 0.0; }
 
-// FP16 copy of D^-1 A (row-scaled pinned operator), diagonal, int16 offsets c - i
-__global__ void k_make_compact_A(int n, int k, const int *__restrict__ idx, const double *__restrict__ A,
-                                 const double *__restrict__ dinv, __half *__restrict__ As, float *__restrict__ diag,
-                                 short *__restrict__ off, int *__restrict__ overflow)
-{
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)n * k) return;
-    const int j = (int)(t / n), i = (int)(t % n);
-    As[t] = __double2half(A[t] * dinv[i]);
-    const int d = idx[t] - i;
-    if (d > 32767 || d < -32768) atomicOr(overflow, 1);
-    off[t] = (short)d;
-    if (j == 0) diag[i] = (float)A[t];
-}
-
-// FP16 transfer weights, int16 offsets from a per-row base node
-__global__ void k_make_compact_T(int n, int k, const int *__restrict__ gidx, const double *__restrict__ W,
-                                 const int *__restrict__ base, __half *__restrict__ Ws, short *__restrict__ off,
-                                 int *__restrict__ overflow)
+// int16 offsets of a gather index from a per-row base node (base = nullptr: the row itself)
+__global__ void k_make_offsets(int n, int k, const int *__restrict__ gidx, const int *__restrict__ base,
+                               short *__restrict__ off, int *__restrict__ overflow)
 {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)n * k) return;
     const int i = (int)(t % n);
-    Ws[t] = __double2half(W[t]);
-    const int d = gidx[t] - base[i];
+    const int d = gidx[t] - (base ? base[i] : i);
     if (d > 32767 || d < -32768) atomicOr(overflow, 1);
     off[t] = (short)d;
 }
@@ -303,10 +284,10 @@ std::vector<SolveLevel<float>> solve_levels<float>(mgm_ctx *c)
         S.kr = l > 0 ? c->L[l - 1].k : 0; S.r_idx = L.s_r_idx.p; S.r_w = L.s_r_w32.p;
         S.kp = l < c->nl - 1 ? c->L[l + 1].k : 0; S.p_idx = L.s_p_idx.p; S.p_w = L.s_p_w32.p;
         S.lmax = L.lmax;
-        if (c->compact && L.As16.p) {
-            S.As = L.As16.p; S.diag = L.diag32.p; S.off = L.off_ok ? L.off16.p : nullptr;
-            S.r_ws = L.rs16.p; S.r_off = L.r_off_ok ? L.r_off16.p : nullptr; S.r_base = L.rpts.p;
-            S.p_ws = L.ps16.p; S.p_off = L.p_off_ok ? L.p_off16.p : nullptr; S.p_base = L.ppts.p;
+        if (c->compact) {
+            S.off = L.off_ok ? L.off16.p : nullptr;
+            S.r_off = L.r_off_ok ? L.r_off16.p : nullptr; S.r_base = L.rpts.p;
+            S.p_off = L.p_off_ok ? L.p_off16.p : nullptr; S.p_base = L.ppts.p;
         }
         out.push_back(S);
     }
@@ -928,28 +909,25 @@ void prepare_solver(mgm_ctx *c)
                                                                        L.A64.p, L.bnd_idx.p, L.bnd_A64.p,
                                                                        L.bnd_A32.p);
         MGM_LAUNCHED();
-        // compact FP32-path storage
+        // compact FP32-path indices
         {
             DBuf<int> ovf(3);
             ovf.zero(s);
-            L.As16.alloc(nk); L.off16.alloc(nk); L.diag32.alloc(L.n);
-            k_make_compact_A<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.idx.p, L.A64.p, L.dinv64.p,
-                                                                     L.As16.p, L.diag32.p, L.off16.p, ovf.p);
+            L.off16.alloc(nk);
+            k_make_offsets<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.idx.p, nullptr, L.off16.p, ovf.p);
             MGM_LAUNCHED();
             if (l > 0) {
                 const int kr = c->L[l - 1].k;
-                L.rs16.alloc((size_t)L.n * kr); L.r_off16.alloc((size_t)L.n * kr);
-                k_make_compact_T<<<blocks_for((long)L.n * kr, 256), 256, 0, s>>>(L.n, kr, L.s_r_idx.p, L.s_r_w64.p,
-                                                                               L.rpts.p, L.rs16.p, L.r_off16.p,
-                                                                               ovf.p + 1);
+                L.r_off16.alloc((size_t)L.n * kr);
+                k_make_offsets<<<blocks_for((long)L.n * kr, 256), 256, 0, s>>>(L.n, kr, L.s_r_idx.p, L.rpts.p,
+                                                                             L.r_off16.p, ovf.p + 1);
                 MGM_LAUNCHED();
             }
             if (l < c->nl - 1) {
                 const int kp = c->L[l + 1].k;
-                L.ps16.alloc((size_t)L.n * kp); L.p_off16.alloc((size_t)L.n * kp);
-                k_make_compact_T<<<blocks_for((long)L.n * kp, 256), 256, 0, s>>>(L.n, kp, L.s_p_idx.p, L.s_p_w64.p,
-                                                                               L.ppts.p, L.ps16.p, L.p_off16.p,
-                                                                               ovf.p + 2);
+                L.p_off16.alloc((size_t)L.n * kp);
+                k_make_offsets<<<blocks_for((long)L.n * kp, 256), 256, 0, s>>>(L.n, kp, L.s_p_idx.p, L.ppts.p,
+                                                                             L.p_off16.p, ovf.p + 2);
                 MGM_LAUNCHED();
             }
             int h_ovf[3] = {0, 0, 0};
@@ -1455,8 +1433,7 @@ int mgm_profile_read(mgm_ctx *c, double *ms_total, long long *launches, long lon
             // per slot the weight and the index; per node r, dinv, e read, e' written,
             // d written, d read by all but the first step of a smoothing pass, btag
             const Level &L = c->L[0];
-            const bool cmp = c->compact && L.As16.p;
-            const double slot = cmp ? 2.0 + (L.off_ok ? 2.0 : 4.0) : 8.0;
+            const double slot = (c->compact && L.off_ok) ? 6.0 : 8.0;
             const double dread = 4.0 * (c->cheb_deg - 1) / (double)c->cheb_deg;
             *bytes_per_launch = (long long)((double)L.n * (L.k * slot + 4 * 5 + 1 + dread));
         }

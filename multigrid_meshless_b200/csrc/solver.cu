@@ -120,13 +120,12 @@ __global__ void __launch_bounds__(256) k_prolong(int n, int k, const int *__rest
 }
 
 // ---------------------------------------------------------------------------
-// compact FP32 path: FP16 row-scaled weights, int16 neighbour offsets
+// compact FP32 path: FP32 weights, neighbours stored as int16 offsets c - base
+// (6 bytes per stencil slot instead of 8)
 // ---------------------------------------------------------------------------
-// sum_j As[j][i] * x[i + off[j][i]]  (or x[idx[j][i]] when off is null)
 template <class X>
-__device__ __forceinline__ float ell_row_dot_c(const short *__restrict__ off, const int *__restrict__ idx,
-                                               const __half *__restrict__ A, const X *__restrict__ x, long n, int k,
-                                               long i, long base)
+__device__ __forceinline__ float ell_row_dot_o(const short *__restrict__ off, const float *__restrict__ A,
+                                               const X *__restrict__ x, long n, int k, long i, int base)
 {
     float s = 0.f;
     int j = 0;
@@ -136,72 +135,67 @@ __device__ __forceinline__ float ell_row_dot_c(const short *__restrict__ off, co
 #pragma unroll
         for (int q = 0; q < 8; q++) {
             const long o = (long)(j + q) * n + i;
-            c[q] = off ? (int)(base + __ldg(off + o)) : __ldg(idx + o);
-            a[q] = __half2float(__ldg(A + o));
+            c[q] = base + (int)__ldg(off + o);
+            a[q] = __ldg(A + o);
         }
 #pragma unroll
         for (int q = 0; q < 8; q++) s += a[q] * (float)__ldg(x + c[q]);
     }
     for (; j < k; j++) {
         const long o = (long)j * n + i;
-        const int c = off ? (int)(base + off[o]) : idx[o];
-        s += __half2float(A[o]) * (float)x[c];
+        s += A[o] * (float)x[base + (int)off[o]];
     }
     return s;
 }
 
-// Chebyshev step on D^-1 A: q' = D^-1 r - (D^-1 A) e
-__global__ void __launch_bounds__(256) k_cheb_c(int n, int k, const short *__restrict__ off,
-                                                const int *__restrict__ idx, const __half *__restrict__ As,
-                                                const float *__restrict__ dinv, const uint8_t *__restrict__ btag,
-                                                const float *__restrict__ r, const float *__restrict__ e,
-                                                float *__restrict__ eout, float *__restrict__ d, float c1, float c2,
-                                                int first)
+__global__ void __launch_bounds__(256) k_cheb_o(int n, int k, const short *__restrict__ off,
+                                                const float *__restrict__ A, const float *__restrict__ dinv,
+                                                const uint8_t *__restrict__ btag, const float *__restrict__ r,
+                                                const float *__restrict__ e, float *__restrict__ eout,
+                                                float *__restrict__ d, float c1, float c2, int first)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float ei = e[i];
     if (btag[i]) { eout[i] = ei; return; }
-    const float q = r[i] * dinv[i] - ell_row_dot_c(off, idx, As, e, n, k, i, i);
-    const float di = first ? c2 * q : c1 * d[i] + c2 * q;
+    const float q = r[i] - ell_row_dot_o(off, A, e, n, k, i, i);
+    const float di = first ? c2 * dinv[i] * q : c1 * d[i] + c2 * dinv[i] * q;
     d[i] = di;
     eout[i] = ei + di;
 }
 
-__global__ void __launch_bounds__(256) k_residual_c(int n, int k, const short *__restrict__ off,
-                                                    const int *__restrict__ idx, const __half *__restrict__ As,
-                                                    const float *__restrict__ diag, const uint8_t *__restrict__ btag,
+__global__ void __launch_bounds__(256) k_residual_o(int n, int k, const short *__restrict__ off,
+                                                    const float *__restrict__ A, const uint8_t *__restrict__ btag,
                                                     const float *__restrict__ r, const float *__restrict__ e,
                                                     float *__restrict__ q)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (btag[i]) { q[i] = 0.f; return; }
-    q[i] = r[i] - diag[i] * ell_row_dot_c(off, idx, As, e, n, k, i, i);
+    q[i] = r[i] - ell_row_dot_o(off, A, e, n, k, i, i);
 }
 
-__global__ void __launch_bounds__(256) k_restrict_c(int n, int k, const short *__restrict__ off,
-                                                    const int *__restrict__ ridx, const int *__restrict__ base,
-                                                    const __half *__restrict__ rw, const uint8_t *__restrict__ btag,
-                                                    const float *__restrict__ qf, float *__restrict__ rc)
+__global__ void __launch_bounds__(256) k_restrict_o(int n, int k, const short *__restrict__ off,
+                                                    const int *__restrict__ base, const float *__restrict__ rw,
+                                                    const uint8_t *__restrict__ btag, const float *__restrict__ qf,
+                                                    float *__restrict__ rc)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (btag[i] || i == 0) { rc[i] = 0.f; return; }
-    rc[i] = ell_row_dot_c(off, ridx, rw, qf, n, k, i, off ? base[i] : 0);
+    rc[i] = ell_row_dot_o(off, rw, qf, n, k, i, base[i]);
 }
 
-__global__ void __launch_bounds__(256) k_prolong_c(int n, int k, const short *__restrict__ off,
-                                                   const int *__restrict__ pidx, const int *__restrict__ base,
-                                                   const __half *__restrict__ pw, const float *__restrict__ ec,
-                                                   float *__restrict__ ef)
+__global__ void __launch_bounds__(256) k_prolong_o(int n, int k, const short *__restrict__ off,
+                                                   const int *__restrict__ base, const float *__restrict__ pw,
+                                                   const float *__restrict__ ec, float *__restrict__ ef)
 {
     __shared__ float shift;
-    if (threadIdx.x == 0) shift = ell_row_dot_c(off, pidx, pw, ec, n, k, 0, off ? base[0] : 0);
+    if (threadIdx.x == 0) shift = ell_row_dot_o(off, pw, ec, n, k, 0, base[0]);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    ef[i] += ell_row_dot_c(off, pidx, pw, ec, n, k, i, off ? base[i] : 0) - shift;
+    ef[i] += ell_row_dot_o(off, pw, ec, n, k, i, base[i]) - shift;
 }
 
 // e = inv * r, one warp per row of the dense coarsest inverse
@@ -284,9 +278,9 @@ static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, 
         }
         if (prof) prof->mark(s);
         if constexpr (sizeof(T) == 4) {
-            if (L.As) {
-                k_cheb_c<<<nb, 256, 0, s>>>(L.n, L.k, L.off, L.idx, L.As, L.dinv, L.btag, L.r, L.e, L.e2, L.d,
-                                            (float)c1, (float)c2, step == 0 ? 1 : 0);
+            if (L.off) {
+                k_cheb_o<<<nb, 256, 0, s>>>(L.n, L.k, L.off, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d, (float)c1,
+                                            (float)c2, step == 0 ? 1 : 0);
             } else {
                 k_cheb<T><<<nb, 256, 0, s>>>(L.n, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d, (T)c1,
                                              (T)c2, step == 0 ? 1 : 0);
@@ -318,28 +312,25 @@ static void vcycle_rec(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs,
     MGM_CUDA(cudaMemsetAsync(L.e, 0, sizeof(T) * L.n, s));
     smooth(L, deg, ratio, true, s, lp);
     SolveLevel<T> &C = Ls[l + 1];
-    bool compact = false;
-    if constexpr (sizeof(T) == 4) compact = L.As != nullptr;
     if constexpr (sizeof(T) == 4) {
-        if (compact) {
-            k_residual_c<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.off, L.idx, L.As, L.diag, L.btag, L.r, L.e,
-                                                              L.q);
-            MGM_LAUNCHED();
-            k_restrict_c<<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.kr, C.r_off, C.r_idx, C.r_base, C.r_ws, C.btag,
-                                                              L.q, C.r);
-            MGM_LAUNCHED();
-        }
-    }
-    if (!compact) {
+        if (L.off) k_residual_o<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.off, L.A, L.btag, L.r, L.e, L.q);
+        else k_residual<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.idx, L.A, L.btag, L.r, L.e, L.q);
+        MGM_LAUNCHED();
+        if (C.r_off) k_restrict_o<<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.kr, C.r_off, C.r_base, C.r_w, C.btag, L.q, C.r);
+        else k_restrict<T><<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
+        MGM_LAUNCHED();
+    } else {
         k_residual<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.idx, L.A, L.btag, L.r, L.e, L.q);
         MGM_LAUNCHED();
         k_restrict<T><<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
         MGM_LAUNCHED();
     }
     vcycle_rec(Ls, cs, l + 1, deg, ratio, s, prof);
-    if (compact) {
+    bool poff = false;
+    if constexpr (sizeof(T) == 4) poff = L.p_off != nullptr;
+    if (poff) {
         if constexpr (sizeof(T) == 4)
-            k_prolong_c<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.kp, L.p_off, L.p_idx, L.p_base, L.p_ws, C.e, L.e);
+            k_prolong_o<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.kp, L.p_off, L.p_base, L.p_w, C.e, L.e);
     } else {
         k_prolong<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.kp, L.p_idx, L.p_w, C.e, L.e);
     }

@@ -68,17 +68,12 @@ struct SolveLevel {
     const int *p_idx;
     const T *p_w;
     double lmax;                  // spectral radius estimate of D^-1 A on interior rows
-    // compact storage (FP32 path only; used when As != nullptr):
-    //   As   = D^-1 A in FP16 [k][n] (unit diagonal, O(1) entries), diag = A_ii
-    //   off  = neighbour offsets c - i as int16 [k][n] (nullptr: use idx)
-    //   transfer weights in FP16 with offsets from a per-row base node
-    const __half *As = nullptr;
-    const T *diag = nullptr;
+    // compact indices (FP32 path only; each used when non-null): neighbours as
+    // int16 offsets c - i [k][n]; transfer gathers as int16 offsets from a
+    // per-row base node (restriction: rpts, prolongation: ppts)
     const short *off = nullptr;
-    const __half *r_ws = nullptr;
     const short *r_off = nullptr;
     const int *r_base = nullptr;
-    const __half *p_ws = nullptr;
     const short *p_off = nullptr;
     const int *p_base = nullptr;
 };

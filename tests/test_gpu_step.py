@@ -138,3 +138,9 @@ def test_graph_replay_matches_eager_launches(cavity):
         mg.use_graphs(True)
         assert it1 == it2
         assert np.array_equal(p1, p2) and np.array_equal(p1, p1b)
+    # 16-bit neighbour offsets address the same entries: identical results
+    mg.use_compact(False)
+    p3, _, _ = mg.solve_poisson(b, mode=mgm.MODE_FP32_IR)
+    mg.use_compact(True)
+    p4, _, _ = mg.solve_poisson(b, mode=mgm.MODE_FP32_IR)
+    assert np.array_equal(p3, p4)
