@@ -270,6 +270,31 @@ MGM_API void mgm_host_free(void *ptr);
 MGM_API int mgm_profile_smoother(mgm_ctx *ctx, int enable);
 MGM_API int mgm_profile_read(mgm_ctx *ctx, double *ms_total, long long *launches, long long *bytes_per_launch);
 
+/* ------------------------------------------------------------------ */
+/* Learned warm start (no counterpart in the reference)                */
+/* ------------------------------------------------------------------ */
+/* A 4-layer message-passing network (hidden width 64, BF16 weights and
+ * activations, FP32 accumulation) on the level-0 stencil graph predicts the
+ * pressure increment of a Poisson solve from (b, previous p, coordinates).
+ * With the warm start on, the prediction is the first search direction of
+ * the FP64 flexible GMRES; the V-cycles then run to the same tolerance.
+ * mgm_mpnn_init allocates it (seeded weights) and a dataset ring of
+ * dataset_capacity samples; mgm_mpnn_collect runs time steps with a solver
+ * mode and records (b, p_prev, p_new - p_prev); mgm_mpnn_train runs Adam on a
+ * range of samples (losses[it] per iteration, may be NULL); mgm_mpnn_eval
+ * returns the mean loss on a range.  Params: mgm_mpnn_num_params() floats. */
+MGM_API int mgm_mpnn_init(mgm_ctx *ctx, unsigned long long seed, int dataset_capacity);
+MGM_API int mgm_mpnn_num_params(void);
+MGM_API int mgm_mpnn_params(mgm_ctx *ctx, float *get, const float *set);
+MGM_API int mgm_mpnn_loss_grad(mgm_ctx *ctx, const float *b_hat, const float *p_hat, const float *target,
+                               double *loss, float *grads, float *prediction);
+MGM_API int mgm_mpnn_collect(mgm_ctx *ctx, int mode, int nsteps);
+MGM_API int mgm_mpnn_dataset_size(mgm_ctx *ctx, int *count);
+MGM_API int mgm_mpnn_train(mgm_ctx *ctx, int first, int count, int iters, float lr, unsigned long long seed,
+                           double *losses);
+MGM_API int mgm_mpnn_eval(mgm_ctx *ctx, int first, int count, double *mean_loss);
+MGM_API int mgm_set_warm_start(mgm_ctx *ctx, int enable);
+
 /* Synchronises the context's stream. */
 MGM_API int mgm_sync(mgm_ctx *ctx);
 

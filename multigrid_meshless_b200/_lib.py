@@ -77,6 +77,15 @@ SIGNATURES = {
     "mgm_solve_poisson": ([vp, C.c_int, dp, dp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
     "mgm_sync": ([vp], C.c_int),
     "mgm_reference_set_poisson_mode": ([C.c_int], None),
+    "mgm_mpnn_init": ([vp, C.c_ulonglong, C.c_int], C.c_int),
+    "mgm_mpnn_num_params": ([], C.c_int),
+    "mgm_mpnn_params": ([vp, vp, vp], C.c_int),
+    "mgm_mpnn_loss_grad": ([vp, vp, vp, vp, C.POINTER(C.c_double), vp, vp], C.c_int),
+    "mgm_mpnn_collect": ([vp, C.c_int, C.c_int], C.c_int),
+    "mgm_mpnn_dataset_size": ([vp, C.POINTER(C.c_int)], C.c_int),
+    "mgm_mpnn_train": ([vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_ulonglong, vp], C.c_int),
+    "mgm_mpnn_eval": ([vp, C.c_int, C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "mgm_set_warm_start": ([vp, C.c_int], C.c_int),
     "mgm_run_steps": ([vp, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                        C.POINTER(C.c_double)], C.c_int),
     "mgm_step_host": ([vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, C.POINTER(C.c_double)], C.c_int),

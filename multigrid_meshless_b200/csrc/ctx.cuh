@@ -1,0 +1,92 @@
+// ctx.cuh -- the per-level device data and the solver context behind the C ABI.
+#pragma once
+#include "../../include/mgm.h"
+#include "krylov.cuh"
+#include "stencil.cuh"
+
+namespace mgm {
+
+struct MpnnState;  // learned warm start (mpnn.cu)
+
+struct Level {
+    int n = 0, nb = 0, k = 0, poly = 0, np = 0;
+    double d_avg = 0;
+    DBuf<double> x, y, z, nx, ny, nz;
+    DBuf<uint8_t> btag;
+    DBuf<int> cloud;  // row-major [n][k] after the reorder
+    DBuf<int> idx;    // ELL [k][n]
+    DBuf<double> Dx, Dy, Dz, lap, lapP;  // ELL
+    DBuf<int> rpts, ppts;
+    // reference-semantics transfer rows (rows >= nb), ELL
+    DBuf<int> ref_r_idx, ref_p_idx;
+    DBuf<double> ref_restr, ref_prol;
+    // solver transfer: restriction into this level (interior rows), prolongation into this level (all rows)
+    DBuf<int> s_r_idx, s_p_idx;
+    DBuf<double> s_r_w64, s_p_w64;
+    DBuf<float> s_r_w32, s_p_w32;
+    // pinned operator
+    DBuf<double> A64, dinv64;
+    DBuf<float> A32, dinv32;
+    DBuf<int> bnd_list;
+    DBuf<int> bnd_idx;           // boundary rows' stencils, row-major [nbl][k]
+    DBuf<double> bnd_A64;
+    DBuf<float> bnd_A32;
+    int nbl = 0;
+    double lmax = 2.0;
+    // compact FP32-path indices (int16 offsets)
+    DBuf<short> off16, r_off16, p_off16;
+    bool off_ok = false, r_off_ok = false, p_off_ok = false;
+    // reference-mode state
+    DBuf<double> p, ptmp, src, res;
+    // solver work vectors
+    DBuf<double> r64, e64, e64b, d64, q64;
+    DBuf<float> r32, e32, e32b, d32, q32;
+};
+
+}  // namespace mgm
+
+using namespace mgm;
+
+struct mgm_ctx {
+    mgm::MpnnState *mpnn = nullptr;
+    int dim = 2, phs = 3, nl = 0;
+    int device = 0;
+    cudaStream_t s = nullptr;
+    std::vector<Level> L;
+    bool setup_done = false;
+    bool have_ref_transfer = false;
+    // flow
+    double Re = 100, courant = 0.5, dt = 0, nu = 0.01, rho = 1;
+    float omega = 1.0f;
+    int num_relax = 3, num_vcycles = 10;
+    // level-0 fields
+    DBuf<double> u, v, w, u_new, v_new, w_new, dpdn, partial, scal;
+    // solver controls and state
+    double tol = 1e-8;
+    int max_iters = 60, cheb_deg = 3;
+    double cheb_ratio = 6.0;
+    DBuf<double> cinv64;
+    DBuf<float> cinv32;
+    DBuf<double> V, Z64, wv, kpart, kscal, bvec;
+    DBuf<float> Z32;
+    int last_iters = 0;
+    double last_relres = 0;
+    long long vcycles_in_solve = 0;   // V-cycles of the last solve (iterations minus learned directions)
+    double *h_pinned = nullptr;
+    SmootherProfile prof;
+    // captured V-cycles, [0] FP64, [1] FP32 (re-captured when solver settings change)
+    struct VGraph {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t x = nullptr;
+        void *out = nullptr;        // level-0 correction buffer the graph writes
+        bool prof = false;          // graph records smoother events
+        size_t ev_first = 0, ev_pairs = 0;
+        long long kernels = 0;      // kernel nodes in the graph
+    } vg[2];
+    bool use_graphs = true;
+    bool compact = true;    // FP32 V-cycle on compact storage
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    double poisson_ms_acc = 0;
+    long long vcycles_acc = 0;
+};
+

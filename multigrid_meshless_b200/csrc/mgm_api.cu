@@ -8,9 +8,7 @@
 #include <cstring>
 #include <memory>
 
-#include "../../include/mgm.h"
-#include "krylov.cuh"
-#include "stencil.cuh"
+#include "ctx.cuh"
 
 namespace mgm {
 
@@ -22,85 +20,9 @@ void set_error(int code, const std::string &msg)
     t_err = msg;
 }
 
-struct Level {
-    int n = 0, nb = 0, k = 0, poly = 0, np = 0;
-    double d_avg = 0;
-    DBuf<double> x, y, z, nx, ny, nz;
-    DBuf<uint8_t> btag;
-    DBuf<int> cloud;  // row-major [n][k] after the reorder
-    DBuf<int> idx;    // ELL [k][n]
-    DBuf<double> Dx, Dy, Dz, lap, lapP;  // ELL
-    DBuf<int> rpts, ppts;
-    // reference-semantics transfer rows (rows >= nb), ELL
-    DBuf<int> ref_r_idx, ref_p_idx;
-    DBuf<double> ref_restr, ref_prol;
-    // solver transfer: restriction into this level (interior rows), prolongation into this level (all rows)
-    DBuf<int> s_r_idx, s_p_idx;
-    DBuf<double> s_r_w64, s_p_w64;
-    DBuf<float> s_r_w32, s_p_w32;
-    // pinned operator
-    DBuf<double> A64, dinv64;
-    DBuf<float> A32, dinv32;
-    DBuf<int> bnd_list;
-    DBuf<int> bnd_idx;           // boundary rows' stencils, row-major [nbl][k]
-    DBuf<double> bnd_A64;
-    DBuf<float> bnd_A32;
-    int nbl = 0;
-    double lmax = 2.0;
-    // compact FP32-path indices (int16 offsets)
-    DBuf<short> off16, r_off16, p_off16;
-    bool off_ok = false, r_off_ok = false, p_off_ok = false;
-    // reference-mode state
-    DBuf<double> p, ptmp, src, res;
-    // solver work vectors
-    DBuf<double> r64, e64, e64b, d64, q64;
-    DBuf<float> r32, e32, e32b, d32, q32;
-};
-
 }  // namespace mgm
 
 using namespace mgm;
-
-struct mgm_ctx {
-    int dim = 2, phs = 3, nl = 0;
-    int device = 0;
-    cudaStream_t s = nullptr;
-    std::vector<Level> L;
-    bool setup_done = false;
-    bool have_ref_transfer = false;
-    // flow
-    double Re = 100, courant = 0.5, dt = 0, nu = 0.01, rho = 1;
-    float omega = 1.0f;
-    int num_relax = 3, num_vcycles = 10;
-    // level-0 fields
-    DBuf<double> u, v, w, u_new, v_new, w_new, dpdn, partial, scal;
-    // solver controls and state
-    double tol = 1e-8;
-    int max_iters = 60, cheb_deg = 3;
-    double cheb_ratio = 6.0;
-    DBuf<double> cinv64;
-    DBuf<float> cinv32;
-    DBuf<double> V, Z64, wv, kpart, kscal, bvec;
-    DBuf<float> Z32;
-    int last_iters = 0;
-    double last_relres = 0;
-    double *h_pinned = nullptr;
-    SmootherProfile prof;
-    // captured V-cycles, [0] FP64, [1] FP32 (re-captured when solver settings change)
-    struct VGraph {
-        cudaGraph_t g = nullptr;
-        cudaGraphExec_t x = nullptr;
-        void *out = nullptr;        // level-0 correction buffer the graph writes
-        bool prof = false;          // graph records smoother events
-        size_t ev_first = 0, ev_pairs = 0;
-        long long kernels = 0;      // kernel nodes in the graph
-    } vg[2];
-    bool use_graphs = true;
-    bool compact = true;    // FP32 V-cycle on compact storage
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    double poisson_ms_acc = 0;
-    long long vcycles_acc = 0;
-};
 
 // ---------------------------------------------------------------------------
 namespace {
@@ -321,6 +243,18 @@ std::vector<RefLevel> ref_levels(mgm_ctx *c)
     return out;
 }
 
+}  // namespace
+
+// learned warm start (mpnn.cu)
+namespace mgm {
+bool warm_start_enabled(mgm_ctx *c);
+template <class T>
+void warm_direction(mgm_ctx *c, const double *b, const double *p, T *out, cudaStream_t s);
+void destroy_mpnn(mgm_ctx *c);
+}  // namespace mgm
+
+namespace {
+
 void drop_graphs(mgm_ctx *c)
 {
     for (auto &g : c->vg) {
@@ -405,6 +339,7 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
     double *hp = c->h_pinned;  // pinned host scratch [2*kMaxKrylov+8]
     std::vector<double> H((size_t)(m + 1) * m, 0.0), cs_(m), sn_(m), g(m + 1);
     int total_it = 0;
+    c->vcycles_in_solve = 0;
     double bnorm = 0, relres = 1;
     const int max_restarts = 4;
     for (int restart = 0; restart <= max_restarts; restart++) {
@@ -425,11 +360,21 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
         int j_done = 0;
+        // With the learned warm start the first search direction is the
+        // network's predicted increment and every later z_j is the V-cycle of
+        // v_{j-1} (flexible GMRES allows any z_j): the learned direction is
+        // added to the Krylov space, no V-cycle direction is dropped.
+        const bool learned = restart == 0 && warm_start_enabled(c);
         for (int j = 0; j < m; j++) {
-            // z_j = M^-1 v_j
-            copy_convert<T>(n, V + j * ld, levels[0].r, s);
-            const T *zout = run_vcycle<T>(c, levels, cs);
-            copy_out<T>(n, zout, Z + j * ld, s);
+            if (learned && j == 0) {
+                warm_direction<T>(c, b, p, Z, s);
+            } else {
+                const int src = learned ? j - 1 : j;
+                copy_convert<T>(n, V + src * ld, levels[0].r, s);
+                const T *zout = run_vcycle<T>(c, levels, cs);
+                copy_out<T>(n, zout, Z + j * ld, s);
+                c->vcycles_in_solve++;
+            }
             // w = A z_j, classical Gram-Schmidt with one re-orthogonalisation
             apply64<T>(n, k, L0.idx.p, L0.A64.p, Z + j * ld, w, s);
             multidot(n, j + 1, V, ld, w, c->kpart.p, c->kscal.p, s);
@@ -478,7 +423,7 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
         MGM_CUDA(cudaMemcpyAsync(c->kscal.p, hp, sizeof(double) * j_done, cudaMemcpyHostToDevice, s));
         combine<T>(n, j_done, Z, ld, c->kscal.p, p, s);
     }
-    c->last_iters = total_it;
+    c->last_iters = (int)c->vcycles_in_solve;  // V-cycles (learned directions are not V-cycles)
     c->last_relres = relres;
     if (!(relres < c->tol) && bnorm > 0)
         throw Error{MGM_ERR_DIVERGED, "Poisson solve did not reach the tolerance (rel. residual " +
@@ -776,6 +721,7 @@ void mgm_destroy(mgm_ctx *c)
     if (c->s) cudaStreamSynchronize(c->s);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     drop_graphs(c);
+    destroy_mpnn(c);
     c->L.clear();
     if (c->s) cudaStreamDestroy(c->s);
     delete c;
