@@ -276,8 +276,9 @@ MGM_API int mgm_profile_read(mgm_ctx *ctx, double *ms_total, long long *launches
 /* A 4-layer message-passing network (hidden width 64, BF16 weights and
  * activations, FP32 accumulation) on the level-0 stencil graph predicts the
  * pressure increment of a Poisson solve from (b, previous p, coordinates).
- * With the warm start on, the prediction is the first search direction of
- * the FP64 flexible GMRES; the V-cycles then run to the same tolerance.
+ * With the warm start on, each solve first steps along the prediction with
+ * the length that minimises the FP64 residual; the V-cycle-preconditioned
+ * FGMRES then runs to the same tolerance as without it.
  * mgm_mpnn_init allocates it (seeded weights) and a dataset ring of
  * dataset_capacity samples; mgm_mpnn_collect runs time steps with a solver
  * mode and records (b, p_prev, p_new - p_prev); mgm_mpnn_train runs Adam on a
@@ -293,6 +294,10 @@ MGM_API int mgm_mpnn_dataset_size(mgm_ctx *ctx, int *count);
 MGM_API int mgm_mpnn_train(mgm_ctx *ctx, int first, int count, int iters, float lr, unsigned long long seed,
                            double *losses);
 MGM_API int mgm_mpnn_eval(mgm_ctx *ctx, int first, int count, double *mean_loss);
+/* Training loss w_mse * mean (y - t)^2 + w_res * |A (t - y)|^2 / |A t|^2,
+ * t the normalised increment, A the pinned Poisson operator: the second term
+ * is the starting residual the prediction leaves (default 1, 0). */
+MGM_API int mgm_mpnn_set_loss(mgm_ctx *ctx, float w_mse, float w_res);
 MGM_API int mgm_set_warm_start(mgm_ctx *ctx, int enable);
 
 /* Synchronises the context's stream. */

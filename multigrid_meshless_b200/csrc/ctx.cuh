@@ -67,11 +67,12 @@ struct mgm_ctx {
     double cheb_ratio = 6.0;
     DBuf<double> cinv64;
     DBuf<float> cinv32;
-    DBuf<double> V, Z64, wv, kpart, kscal, bvec;
+    DBuf<double> V, Z64, wv, kpart, kscal, bvec, wdir;
     DBuf<float> Z32;
     int last_iters = 0;
     double last_relres = 0;
-    long long vcycles_in_solve = 0;   // V-cycles of the last solve (iterations minus learned directions)
+    long long vcycles_in_solve = 0;
+    double last_learned_alpha = 0;    // step length the last solve took along the learned direction   // V-cycles of the last solve (iterations minus learned directions)
     double *h_pinned = nullptr;
     SmootherProfile prof;
     // captured V-cycles, [0] FP64, [1] FP32 (re-captured when solver settings change)

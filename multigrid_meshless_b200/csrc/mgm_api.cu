@@ -342,6 +342,24 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
     c->vcycles_in_solve = 0;
     double bnorm = 0, relres = 1;
     const int max_restarts = 4;
+    if (warm_start_enabled(c)) {
+        // learned warm start: p += alpha d along the network's predicted
+        // increment d, alpha minimising |b - A (p + alpha d)|_2 (never worse
+        // than p); the FGMRES below then runs unchanged to the tolerance
+        double *d = c->wdir.p, *r0 = V, *Ad = w;
+        warm_direction<double>(c, b, p, d, s);
+        resid64(n, k, L0.idx.p, L0.A64.p, b, p, r0, c->kpart.p, s);
+        apply64<double>(n, k, L0.idx.p, L0.A64.p, d, Ad, s);
+        multidot(n, 1, r0, ld, Ad, c->kpart.p, c->kscal.p, s);
+        multidot(n, 1, Ad, ld, Ad, c->kpart.p, c->kscal.p + 1, s);
+        MGM_CUDA(cudaMemcpyAsync(hp, c->kscal.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+        MGM_CUDA(cudaStreamSynchronize(s));
+        const double alpha = hp[1] > 0 && std::isfinite(hp[0] / hp[1]) ? hp[0] / hp[1] : 0.0;
+        c->last_learned_alpha = alpha;
+        hp[0] = alpha;
+        MGM_CUDA(cudaMemcpyAsync(c->kscal.p, hp, sizeof(double), cudaMemcpyHostToDevice, s));
+        combine<double>(n, 1, d, ld, c->kscal.p, p, s);
+    }
     for (int restart = 0; restart <= max_restarts; restart++) {
         // r0 = b - A p  -> V_0 (unnormalised), norms
         resid64(n, k, L0.idx.p, L0.A64.p, b, p, V, c->kpart.p, s);
@@ -360,17 +378,9 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
         int j_done = 0;
-        // With the learned warm start the first search direction is the
-        // network's predicted increment and every later z_j is the V-cycle of
-        // v_{j-1} (flexible GMRES allows any z_j): the learned direction is
-        // added to the Krylov space, no V-cycle direction is dropped.
-        const bool learned = restart == 0 && warm_start_enabled(c);
         for (int j = 0; j < m; j++) {
-            if (learned && j == 0) {
-                warm_direction<T>(c, b, p, Z, s);
-            } else {
-                const int src = learned ? j - 1 : j;
-                copy_convert<T>(n, V + src * ld, levels[0].r, s);
+            {
+                copy_convert<T>(n, V + j * ld, levels[0].r, s);
                 const T *zout = run_vcycle<T>(c, levels, cs);
                 copy_out<T>(n, zout, Z + j * ld, s);
                 c->vcycles_in_solve++;
@@ -483,6 +493,7 @@ void alloc_solver_buffers(mgm_ctx *c)
     c->Z64.alloc((size_t)m * n);
     c->Z32.alloc((size_t)m * n);
     c->wv.alloc(n);
+    c->wdir.alloc(n);
     c->bvec.alloc(n);
     c->kpart.alloc((size_t)std::max(2 * blocks_for(n, 256), (kMaxKrylov + 1) * dot_blocks(n)) + 16);
     c->kscal.alloc(3 * kMaxKrylov + 16);

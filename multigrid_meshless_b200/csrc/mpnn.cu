@@ -9,10 +9,11 @@
 // product is accumulated in FP32; the layer GEMM runs on the tensor cores
 // (mma.sync m16n8k16 BF16 -> FP32) fused with the neighbour aggregation.
 //
-// The prediction is the shape of the pressure increment p_new - p_prev.  It is
-// used as the first search direction of the FP64 flexible GMRES, which picks
-// its length and then continues with V-cycles to the same tolerance: the
-// learned guess can only add to the Krylov space, never replace the solver.
+// The prediction is the shape of the pressure increment p_new - p_prev.  The
+// solve steps along it with the length that minimises the FP64 residual, then
+// runs the V-cycle-preconditioned FGMRES to the same tolerance as without it:
+// the learned guess can only lower the starting residual, never replace the
+// solver.
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -36,8 +37,9 @@ struct MpnnState {
     DBuf<float> params, grads, am, av;
     DBuf<bf16> WT[kLayers];  // [64][192]
     DBuf<float> lapS;        // row-major [n][k]
-    DBuf<int> tptr, tsrc;    // transpose adjacency (in-edges), sorted by source
-    DBuf<float> tw;
+    DBuf<int> tptr, tpos;    // transpose adjacency: in-edges of node j as positions i*k+s, sorted
+    DBuf<float> Arm;         // pinned Poisson operator, row-major [n][k] (FP32), for the residual loss
+    float w_mse = 1.f, w_res = 0.f;
     DBuf<float> feat;        // [n][5]
     DBuf<bf16> h[kLayers + 1];
     DBuf<bf16> cat[kLayers];
@@ -151,51 +153,81 @@ __device__ __forceinline__ void mma_bf16(float *c, uint32_t a0, uint32_t a1, uin
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-constexpr int kTile = 64, kPad = 200;  // rows per CTA, padded row length (bf16) of the smem tiles
+constexpr int kTile = 64, kPad = 200;  // rows per CTA, padded row length (bf16) of the smem tile
+
+struct bf4 { __nv_bfloat162 a, b; };
 
 // One message-passing layer for 64 nodes: gather [h_i | mean h_j | sum l_ij h_j]
 // into shared memory (BF16), multiply by W (tensor cores, FP32 accumulate),
 // bias + relu + residual, store h' (BF16); in training also z and the row.
+// Aggregation: a half-warp per node (4 features per lane, one 128-byte row
+// per neighbour), 8 neighbour rows in flight.  W (24 KB) is read through L1.
 __global__ void __launch_bounds__(128) k_mp_layer(int n, int k, const int *__restrict__ cloud,
                                                   const float *__restrict__ lapS, float inv_k,
                                                   const bf16 *__restrict__ h_in, const bf16 *__restrict__ WT,
                                                   const float *__restrict__ bias, bf16 *__restrict__ h_out,
                                                   float *__restrict__ z_out, bf16 *__restrict__ cat_out)
 {
-    extern __shared__ __align__(16) unsigned char mp_smem[];
-    bf16 (*Xs)[kPad] = reinterpret_cast<bf16 (*)[kPad]>(mp_smem);
-    bf16 (*Ws)[kPad] = reinterpret_cast<bf16 (*)[kPad]>(mp_smem + sizeof(bf16) * kTile * kPad);
+    __shared__ __align__(16) bf16 Xs[kTile][kPad];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int half = lane >> 4, hl = lane & 15;
+    const unsigned hmask = 0xffffffffu;  // rows past n are clamped, so all lanes stay converged
     const long base = (long)blockIdx.x * kTile;
-    for (int w = tid; w < kH * (kCat / 2); w += blockDim.x) {
-        const int r = w / (kCat / 2), cw = w % (kCat / 2);
-        reinterpret_cast<uint32_t *>(&Ws[r][0])[cw] = reinterpret_cast<const uint32_t *>(WT)[(long)r * (kCat / 2) + cw];
-    }
-    for (int rr = 0; rr < kTile / 4; rr++) {
-        const int row = warp * (kTile / 4) + rr;
-        const long i = base + row;
-        float2 self = make_float2(0.f, 0.f), mean = self, lp = self;
-        if (i < n) {
-            self = ld_bf2(h_in + i * kH + 2 * lane);
-            const int c0 = lane < k ? cloud[i * k + lane] : 0;
-            const float w0 = lane < k ? lapS[i * k + lane] : 0.f;
-            const int c1 = lane + 32 < k ? cloud[i * k + lane + 32] : 0;
-            const float w1 = lane + 32 < k ? lapS[i * k + lane + 32] : 0.f;
-            for (int j = 0; j < k; j++) {
-                const int c = __shfl_sync(0xffffffffu, j < 32 ? c0 : c1, j & 31);
-                const float wj = __shfl_sync(0xffffffffu, j < 32 ? w0 : w1, j & 31);
-                const float2 v = ld_bf2(h_in + (long)c * kH + 2 * lane);
-                mean.x += v.x; mean.y += v.y;
-                lp.x += wj * v.x; lp.y += wj * v.y;
+    for (int rr = 0; rr < kTile / 8; rr++) {
+        const int row = warp * (kTile / 4) + 2 * rr + half;
+        const bool valid = base + row < n;
+        const long i = valid ? base + row : (long)n - 1;
+        float sf[4] = {0, 0, 0, 0}, mn[4] = {0, 0, 0, 0}, lp[4] = {0, 0, 0, 0};
+        {
+            const bf4 sv = *reinterpret_cast<const bf4 *>(h_in + i * kH + 4 * hl);
+            const float2 s0 = __bfloat1622float2(sv.a), s1 = __bfloat1622float2(sv.b);
+            sf[0] = s0.x; sf[1] = s0.y; sf[2] = s1.x; sf[3] = s1.y;
+            const int c0 = hl < k ? cloud[i * k + hl] : 0;
+            const float w0 = hl < k ? lapS[i * k + hl] : 0.f;
+            const int c1 = hl + 16 < k ? cloud[i * k + hl + 16] : 0;
+            const float w1 = hl + 16 < k ? lapS[i * k + hl + 16] : 0.f;
+            const int c2 = hl + 32 < k ? cloud[i * k + hl + 32] : 0;
+            const float w2 = hl + 32 < k ? lapS[i * k + hl + 32] : 0.f;
+            const int c3 = hl + 48 < k ? cloud[i * k + hl + 48] : 0;
+            const float w3 = hl + 48 < k ? lapS[i * k + hl + 48] : 0.f;
+            for (int j0 = 0; j0 < k; j0 += 8) {
+                bf4 v[8];
+                float wj[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const int j = j0 + q;
+                    const int src = j & 15, sel = j >> 4;
+                    const int cs = __shfl_sync(hmask, sel == 0 ? c0 : sel == 1 ? c1 : sel == 2 ? c2 : c3, src, 16);
+                    wj[q] = __shfl_sync(hmask, sel == 0 ? w0 : sel == 1 ? w1 : sel == 2 ? w2 : w3, src, 16);
+                    if (j < k) v[q] = *reinterpret_cast<const bf4 *>(h_in + (long)cs * kH + 4 * hl);
+                    else { wj[q] = 0.f; v[q].a = v[q].b = __floats2bfloat162_rn(0.f, 0.f); }
+                }
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    if (j0 + q >= k) break;
+                    const float2 a = __bfloat1622float2(v[q].a), b = __bfloat1622float2(v[q].b);
+                    mn[0] += a.x; mn[1] += a.y; mn[2] += b.x; mn[3] += b.y;
+                    lp[0] += wj[q] * a.x; lp[1] += wj[q] * a.y; lp[2] += wj[q] * b.x; lp[3] += wj[q] * b.y;
+                }
             }
-            mean.x *= inv_k; mean.y *= inv_k;
+#pragma unroll
+            for (int q = 0; q < 4; q++) mn[q] *= inv_k;
+            if (!valid) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) sf[q] = mn[q] = lp[q] = 0.f;
+            }
         }
-        st_bf2(&Xs[row][2 * lane], self.x, self.y);
-        st_bf2(&Xs[row][kH + 2 * lane], mean.x, mean.y);
-        st_bf2(&Xs[row][2 * kH + 2 * lane], lp.x, lp.y);
+        bf4 o;
+        o.a = __floats2bfloat162_rn(sf[0], sf[1]); o.b = __floats2bfloat162_rn(sf[2], sf[3]);
+        *reinterpret_cast<bf4 *>(&Xs[row][4 * hl]) = o;
+        o.a = __floats2bfloat162_rn(mn[0], mn[1]); o.b = __floats2bfloat162_rn(mn[2], mn[3]);
+        *reinterpret_cast<bf4 *>(&Xs[row][kH + 4 * hl]) = o;
+        o.a = __floats2bfloat162_rn(lp[0], lp[1]); o.b = __floats2bfloat162_rn(lp[2], lp[3]);
+        *reinterpret_cast<bf4 *>(&Xs[row][2 * kH + 4 * hl]) = o;
     }
     __syncthreads();
     const int g = lane >> 2, t = lane & 3, r0 = warp * 16;
+    const uint32_t *W32 = reinterpret_cast<const uint32_t *>(WT);  // [64][96] words
     float acc[8][4];
 #pragma unroll
     for (int q = 0; q < 8; q++) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = 0.f;
@@ -208,8 +240,8 @@ __global__ void __launch_bounds__(128) k_mp_layer(int n, int k, const int *__res
         const uint32_t a3 = *reinterpret_cast<const uint32_t *>(&Xs[r0 + g + 8][k0 + 2 * t + 8]);
 #pragma unroll
         for (int nt = 0; nt < 8; nt++) {
-            const uint32_t b0 = *reinterpret_cast<const uint32_t *>(&Ws[nt * 8 + g][k0 + 2 * t]);
-            const uint32_t b1 = *reinterpret_cast<const uint32_t *>(&Ws[nt * 8 + g][k0 + 2 * t + 8]);
+            const uint32_t b0 = __ldg(W32 + (nt * 8 + g) * (kCat / 2) + (k0 >> 1) + t);
+            const uint32_t b1 = __ldg(W32 + (nt * 8 + g) * (kCat / 2) + (k0 >> 1) + t + 4);
             mma_bf16(acc[nt], a0, a1, a2, a3, b0, b1);
         }
     }
@@ -361,15 +393,16 @@ __global__ void __launch_bounds__(192) k_dcat(int n, const float *dz, const bf16
 }
 
 // dHin[j] += sum over in-edges (i, l_ij): dm_mean[i] / k + l_ij dm_lap[i]
-__global__ void __launch_bounds__(256) k_scatter_T(int n, float inv_k, const int *tptr, const int *tsrc,
-                                                   const float *tw, const float *dm, float *dHin)
+__global__ void __launch_bounds__(256) k_scatter_T(int n, int k, float inv_k, const int *tptr, const int *tpos,
+                                                   const float *lapS, const float *dm, float *dHin)
 {
     const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (j >= n) return;
     float a0 = 0, a1 = 0;
     for (int e = tptr[j]; e < tptr[j + 1]; e++) {
-        const long i = tsrc[e];
-        const float w = tw[e];
+        const int pos = tpos[e];
+        const long i = pos / k;
+        const float w = lapS[pos];
         const float *r = dm + i * 128;
         a0 += inv_k * r[2 * lane] + w * r[kH + 2 * lane];
         a1 += inv_k * r[2 * lane + 1] + w * r[kH + 2 * lane + 1];
@@ -442,32 +475,72 @@ __global__ void k_count_in(int n, int k, const int *cloud, int *deg)
     if (t < (long)n * k) atomicAdd(&deg[cloud[t]], 1);
 }
 
-__global__ void k_fill_in(int n, int k, const int *cloud, const float *lapS, int *fill, int *tsrc, float *tw)
+__global__ void k_fill_in(int n, int k, const int *cloud, int *fill, int *tpos)
 {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)n * k) return;
     const int pos = atomicAdd(&fill[cloud[t]], 1);
-    tsrc[pos] = (int)(t / k);
-    tw[pos] = lapS[t];
+    tpos[pos] = (int)t;
 }
 
-// deterministic order of each node's in-edges: by (source, weight)
-__global__ void k_sort_in(int n, const int *tptr, int *tsrc, float *tw)
+// deterministic order of each node's in-edges: by position i*k+s
+__global__ void k_sort_in(int n, const int *tptr, int *tpos)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     for (int a = tptr[j] + 1; a < tptr[j + 1]; a++) {
-        const int s = tsrc[a];
-        const float w = tw[a];
+        const int v = tpos[a];
         int b = a;
-        while (b > tptr[j] && (tsrc[b - 1] > s || (tsrc[b - 1] == s && tw[b - 1] > w))) {
-            tsrc[b] = tsrc[b - 1];
-            tw[b] = tw[b - 1];
-            b--;
-        }
-        tsrc[b] = s;
-        tw[b] = w;
+        while (b > tptr[j] && tpos[b - 1] > v) { tpos[b] = tpos[b - 1]; b--; }
+        tpos[b] = v;
     }
+}
+
+// row-major FP32 copy of an ELL FP64 operator
+__global__ void k_rowmajor_f(int n, int k, const double *A, float *out)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)n * k) return;
+    const int i = (int)(t / k), j = (int)(t % k);
+    out[t] = (float)A[(long)j * n + i];
+}
+
+// residual loss, forward: r = A (t - y), q = A t ; sums of squares -> acc[0], acc[1]
+__global__ void k_res_fwd(int n, int k, const int *cloud, const float *Arm, const float *t, const float *y, float *r,
+                          double *acc)
+{
+    __shared__ double sm[32];
+    double sr = 0, sq = 0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        float a = 0.f, b = 0.f;
+        for (int s = 0; s < k; s++) {
+            const long o = i * k + s;
+            const int c = cloud[o];
+            a += Arm[o] * (t[c] - y[c]);
+            b += Arm[o] * t[c];
+        }
+        r[i] = a;
+        sr += (double)a * a;
+        sq += (double)b * b;
+    }
+    sr = bsum_d<256>(sr, sm);
+    sq = bsum_d<256>(sq, sm);
+    if (threadIdx.x == 0) { atomicAdd(acc, sr); atomicAdd(acc + 1, sq); }
+}
+
+// dy = w_res * (-2 A^T r / |A t|^2) + w_mse * 2 (y - t) / n ; loss += w_res |r|^2/|A t|^2 (mse part added by k_loss)
+__global__ void k_res_bwd(int n, int k, const int *tptr, const int *tpos, const float *Arm, const float *r,
+                          const double *acc, float w_res, float *dy)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const double Q = acc[1] > 0 ? acc[1] : 1.0;
+    float s = 0.f;
+    for (int e = tptr[j]; e < tptr[j + 1]; e++) {
+        const int pos = tpos[e];
+        s += Arm[pos] * r[pos / k];
+    }
+    dy[j] += (float)(w_res * (-2.0 * s / Q));
 }
 
 // dataset record: slot <- (b/rms b, p/rms p, (p_new - p_prev)/rms) ; scal[0..2] = sumsq of b, p_prev, dp
@@ -514,14 +587,8 @@ static void forward(MpnnState &M, bool train, cudaStream_t s)
     const float *P = M.params.p;
     k_encode<<<warp_blocks(n), 256, 0, s>>>(n, M.feat.p, P, M.h[0].p, train ? M.z[0].p : nullptr);
     MGM_LAUNCHED();
-    const size_t smem = sizeof(bf16) * (kTile + kH) * kPad;
-    static bool attr_set = false;
-    if (!attr_set) {
-        MGM_CUDA(cudaFuncSetAttribute(k_mp_layer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-    }
     for (int l = 0; l < kLayers; l++) {
-        k_mp_layer<<<blocks_for(n, kTile), 128, smem, s>>>(n, M.k, M.cloud, M.lapS.p, 1.f / M.k, M.h[l].p, M.WT[l].p,
+        k_mp_layer<<<blocks_for(n, kTile), 128, 0, s>>>(n, M.k, M.cloud, M.lapS.p, 1.f / M.k, M.h[l].p, M.WT[l].p,
                                                        P + P_L0 + l * kLayerParams + kCat * kH, M.h[l + 1].p,
                                                        train ? M.z[l + 1].p : nullptr, train ? M.cat[l].p : nullptr);
         MGM_LAUNCHED();
@@ -530,15 +597,44 @@ static void forward(MpnnState &M, bool train, cudaStream_t s)
     MGM_LAUNCHED();
 }
 
+// loss w_mse * mean (y - t)^2 + w_res * |A (t - y)|^2 / |A t|^2 and dL/dy; loss -> M.scal[2]
+__global__ void k_scale_mse(int n, float w, float *dy)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dy[i] *= w;
+}
+__global__ void k_add_loss(const double *acc, double w_mse, double w_res, double *loss)
+{
+    const double Q = acc[1] > 0 ? acc[1] : 1.0;
+    *loss = w_mse * (*loss) + w_res * acc[0] / Q;
+}
+
+static void loss_head(MpnnState &M, const float *t, cudaStream_t s)
+{
+    const int n = M.n;
+    MGM_CUDA(cudaMemsetAsync(M.scal.p + 2, 0, 3 * sizeof(double), s));
+    k_loss<<<red_blocks(n), 256, 0, s>>>(n, M.y.p, t, M.dy.p, M.scal.p + 2);
+    MGM_LAUNCHED();
+    k_scale_mse<<<blocks_for(n, 256), 256, 0, s>>>(n, M.w_mse, M.dy.p);
+    MGM_LAUNCHED();
+    if (M.w_res > 0.f) {
+        k_res_fwd<<<red_blocks(n), 256, 0, s>>>(n, M.k, M.cloud, M.Arm.p, t, M.y.p, M.dz.p, M.scal.p + 3);
+        MGM_LAUNCHED();
+        k_res_bwd<<<blocks_for(n, 256), 256, 0, s>>>(n, M.k, M.tptr.p, M.tpos.p, M.Arm.p, M.dz.p, M.scal.p + 3,
+                                                    M.w_res, M.dy.p);
+        MGM_LAUNCHED();
+    }
+    k_add_loss<<<1, 1, 0, s>>>(M.scal.p + 3, M.w_mse, M.w_res, M.scal.p + 2);
+    MGM_LAUNCHED();
+}
+
 // loss against target t and the full gradient into M.grads (zeroed here); loss -> M.scal[2]
 static void loss_and_grad(MpnnState &M, const float *t, cudaStream_t s)
 {
     const int n = M.n;
     MGM_CUDA(cudaMemsetAsync(M.grads.p, 0, sizeof(float) * kNumParams, s));
-    MGM_CUDA(cudaMemsetAsync(M.scal.p + 2, 0, sizeof(double), s));
     forward(M, true, s);
-    k_loss<<<red_blocks(n), 256, 0, s>>>(n, M.y.p, t, M.dy.p, M.scal.p + 2);
-    MGM_LAUNCHED();
+    loss_head(M, t, s);
     float *G = M.grads.p;
     k_decode_bwd<<<red_blocks(n), 256, 0, s>>>(n, M.h[kLayers].p, M.dy.p, M.params.p, M.dH.p, G);
     MGM_LAUNCHED();
@@ -551,7 +647,7 @@ static void loss_and_grad(MpnnState &M, const float *t, cudaStream_t s)
         MGM_LAUNCHED();
         k_dcat<<<std::min(blocks_for(n, 16), 148 * 8), 192, 0, s>>>(n, M.dz.p, M.WT[l].p, M.dHin.p, M.dm.p);
         MGM_LAUNCHED();
-        k_scatter_T<<<warp_blocks(n), 256, 0, s>>>(n, 1.f / M.k, M.tptr.p, M.tsrc.p, M.tw.p, M.dm.p, M.dHin.p);
+        k_scatter_T<<<warp_blocks(n), 256, 0, s>>>(n, M.k, 1.f / M.k, M.tptr.p, M.tpos.p, M.lapS.p, M.dm.p, M.dHin.p);
         MGM_LAUNCHED();
         std::swap(M.dH.p, M.dHin.p);
     }
@@ -675,15 +771,17 @@ int mgm_mpnn_init(mgm_ctx *c, unsigned long long seed, int dataset_capacity)
         DBuf<int> deg(n), fill(n);
         deg.zero(s);
         M.tptr.alloc(n + 1);
-        M.tsrc.alloc(nk);
-        M.tw.alloc(nk);
+        M.tpos.alloc(nk);
+        M.Arm.alloc(nk);
+        k_rowmajor_f<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.A64.p, M.Arm.p);
+        MGM_LAUNCHED();
         k_count_in<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.cloud.p, deg.p);
         MGM_LAUNCHED();
         scan_exclusive(deg.p, M.tptr.p, L.n, M.tptr.p + n, s);
         MGM_CUDA(cudaMemcpyAsync(fill.p, M.tptr.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
-        k_fill_in<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.cloud.p, M.lapS.p, fill.p, M.tsrc.p, M.tw.p);
+        k_fill_in<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.cloud.p, fill.p, M.tpos.p);
         MGM_LAUNCHED();
-        k_sort_in<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, M.tptr.p, M.tsrc.p, M.tw.p);
+        k_sort_in<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, M.tptr.p, M.tpos.p);
         MGM_LAUNCHED();
         M.feat.alloc(n * kFin);
         for (auto &h : M.h) h.alloc(n * kH);
@@ -837,14 +935,26 @@ int mgm_mpnn_eval(mgm_ctx *c, int first, int count, double *mean_loss)
             k_features_ds<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, slot, slot + M.n, L.x.p, L.y.p, L.btag.p, M.feat.p);
             MGM_LAUNCHED();
             forward(M, false, s);
-            MGM_CUDA(cudaMemsetAsync(M.scal.p + 2, 0, sizeof(double), s));
-            k_loss<<<red_blocks(M.n), 256, 0, s>>>(M.n, M.y.p, slot + 2 * M.n, dyv.p, M.scal.p + 2);
-            MGM_LAUNCHED();
+            loss_head(M, slot + 2 * M.n, s);
             M.scal.download(c->h_pinned, 3, s);
             MGM_CUDA(cudaStreamSynchronize(s));
             tot += c->h_pinned[2];
         }
         *mean_loss = tot / count;
+        return MGM_OK;
+    } catch (const Error &e) {
+        set_error(e.code, e.msg);
+        return e.code;
+    }
+}
+
+int mgm_mpnn_set_loss(mgm_ctx *c, float w_mse, float w_res)
+{
+    try {
+        MpnnState &M = state(c);
+        MGM_REQUIRE(w_mse >= 0 && w_res >= 0 && w_mse + w_res > 0, "mgm_mpnn_set_loss: weights must be >= 0, not both 0");
+        M.w_mse = w_mse;
+        M.w_res = w_res;
         return MGM_OK;
     } catch (const Error &e) {
         set_error(e.code, e.msg);

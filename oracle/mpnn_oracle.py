@@ -79,14 +79,25 @@ def forward(P, feat, G: Graph, use_bf16=True):
     return y, dict(h=h, z=zs, cat=cats, feat=feat)
 
 
-def loss_grad(P, feat, target, G: Graph, use_bf16=True):
+def loss_grad(P, feat, target, G: Graph, use_bf16=True, w_mse=1.0, w_res=0.0, A=None):
+    """loss = w_mse mean (y - t)^2 + w_res |A (t - y)|^2 / |A t|^2 ; A row-major [n][k] on G.cloud."""
     We, ce, Ws, cs, wd, cd = unpack(P)
     rnd = (lambda a: bf16(a).astype(np.float64)) if use_bf16 else (lambda a: np.asarray(a, np.float64))
     y, st = forward(P, feat, G, use_bf16)
     n = len(y)
-    r = y - np.asarray(target, np.float64)
-    loss = float(np.mean(r * r))
-    dy = 2 * r / n
+    t = np.asarray(target, np.float64)
+    r = y - t
+    loss = w_mse * float(np.mean(r * r))
+    dy = w_mse * 2 * r / n
+    if w_res > 0:
+        A = np.asarray(A, np.float64)
+        rr = (A * (t - y)[G.cloud]).sum(1)
+        q = (A * t[G.cloud]).sum(1)
+        Q = float(q @ q)
+        loss += w_res * float(rr @ rr) / Q
+        ATr = np.zeros(n)
+        np.add.at(ATr, G.cloud.ravel(), (A * rr[:, None]).ravel())
+        dy = dy + w_res * (-2.0 * ATr / Q)
     g = np.zeros(NUM_PARAMS)
     h = st["h"]
     g[P_WD:P_WD + H] = h[-1].T @ dy
@@ -106,13 +117,13 @@ def loss_grad(P, feat, target, G: Graph, use_bf16=True):
     return loss, g, y
 
 
-def fd_check(P, feat, target, G: Graph, idx, eps=1e-6):
+def fd_check(P, feat, target, G: Graph, idx, eps=1e-6, **kw):
     """Central differences of the exact (float64) loss at parameter indices idx."""
     out = []
     for i in idx:
         Pp = np.array(P, np.float64); Pp[i] += eps
         Pm = np.array(P, np.float64); Pm[i] -= eps
-        lp, _, _ = loss_grad(Pp, feat, target, G, use_bf16=False)
-        lm, _, _ = loss_grad(Pm, feat, target, G, use_bf16=False)
+        lp, _, _ = loss_grad(Pp, feat, target, G, use_bf16=False, **kw)
+        lm, _, _ = loss_grad(Pm, feat, target, G, use_bf16=False, **kw)
         out.append((lp - lm) / (2 * eps))
     return np.array(out)
