@@ -299,6 +299,11 @@ MGM_API int mgm_mpnn_eval(mgm_ctx *ctx, int first, int count, double *mean_loss)
  * is the starting residual the prediction leaves (default 1, 0). */
 MGM_API int mgm_mpnn_set_loss(mgm_ctx *ctx, float w_mse, float w_res);
 MGM_API int mgm_set_warm_start(mgm_ctx *ctx, int enable);
+/* Fine-level Chebyshev steps applied to the learned direction before the
+ * minimal-residual step (default 3; 0 = use the raw prediction), and the step
+ * length the last solve took along it. */
+MGM_API int mgm_set_warm_smoothing(mgm_ctx *ctx, int steps);
+MGM_API int mgm_last_learned_alpha(mgm_ctx *ctx, double *alpha);
 
 /* Synchronises the context's stream. */
 MGM_API int mgm_sync(mgm_ctx *ctx);

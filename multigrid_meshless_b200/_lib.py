@@ -87,6 +87,8 @@ SIGNATURES = {
     "mgm_mpnn_eval": ([vp, C.c_int, C.c_int, C.POINTER(C.c_double)], C.c_int),
     "mgm_set_warm_start": ([vp, C.c_int], C.c_int),
     "mgm_mpnn_set_loss": ([vp, C.c_float, C.c_float], C.c_int),
+    "mgm_set_warm_smoothing": ([vp, C.c_int], C.c_int),
+    "mgm_last_learned_alpha": ([vp, C.POINTER(C.c_double)], C.c_int),
     "mgm_run_steps": ([vp, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                        C.POINTER(C.c_double)], C.c_int),
     "mgm_step_host": ([vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, C.POINTER(C.c_double)], C.c_int),

@@ -72,7 +72,8 @@ struct mgm_ctx {
     int last_iters = 0;
     double last_relres = 0;
     long long vcycles_in_solve = 0;
-    double last_learned_alpha = 0;    // step length the last solve took along the learned direction   // V-cycles of the last solve (iterations minus learned directions)
+    double last_learned_alpha = 0;
+    int warm_smooth_steps = 3;        // Chebyshev steps that clean the learned direction    // step length the last solve took along the learned direction   // V-cycles of the last solve (iterations minus learned directions)
     double *h_pinned = nullptr;
     SmootherProfile prof;
     // captured V-cycles, [0] FP64, [1] FP32 (re-captured when solver settings change)

@@ -343,11 +343,24 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
     double bnorm = 0, relres = 1;
     const int max_restarts = 4;
     if (warm_start_enabled(c)) {
-        // learned warm start: p += alpha d along the network's predicted
-        // increment d, alpha minimising |b - A (p + alpha d)|_2 (never worse
-        // than p); the FGMRES below then runs unchanged to the tolerance
-        double *d = c->wdir.p, *r0 = V, *Ad = w;
+        // learned warm start.  The network's increment d carries BF16-level
+        // grid-scale noise that the Laplacian amplifies, so it is first cleaned
+        // by Chebyshev smoothing of A e = b - A (p + d) on the fine level
+        // (d <- d + e), then p += alpha d with alpha minimising
+        // |b - A (p + alpha d)|_2 (never worse than p).  The FGMRES below then
+        // runs unchanged to the tolerance.
+        double *d = c->wdir.p, *r0 = V, *Ad = w, *pd = V + ld;
         warm_direction<double>(c, b, p, d, s);
+        if (c->warm_smooth_steps > 0) {
+            copy_out<double>(n, p, pd, s);
+            hp[0] = 1.0;
+            MGM_CUDA(cudaMemcpyAsync(c->kscal.p, hp, sizeof(double), cudaMemcpyHostToDevice, s));
+            combine<double>(n, 1, d, ld, c->kscal.p, pd, s);                 // pd = p + d
+            resid64(n, k, L0.idx.p, L0.A64.p, b, pd, r0, c->kpart.p, s);     // r0 = b - A (p + d)
+            copy_convert<T>(n, r0, levels[0].r, s);
+            const T *e = smooth_from_zero<T>(levels[0], c->warm_smooth_steps, c->cheb_ratio, s);
+            combine<T>(n, 1, e, ld, c->kscal.p, d, s);                      // d += e
+        }
         resid64(n, k, L0.idx.p, L0.A64.p, b, p, r0, c->kpart.p, s);
         apply64<double>(n, k, L0.idx.p, L0.A64.p, d, Ad, s);
         multidot(n, 1, r0, ld, Ad, c->kpart.p, c->kscal.p, s);
@@ -1227,6 +1240,22 @@ int mgm_use_graphs(mgm_ctx *c, int enable)
         MGM_CUDA(cudaStreamSynchronize(c->s));
         drop_graphs(c);
         c->use_graphs = enable != 0;
+    });
+}
+
+int mgm_set_warm_smoothing(mgm_ctx *c, int steps)
+{
+    return guard([&] {
+        MGM_REQUIRE(c && steps >= 0 && steps <= 16, "mgm_set_warm_smoothing: 0..16 steps");
+        c->warm_smooth_steps = steps;
+    });
+}
+
+int mgm_last_learned_alpha(mgm_ctx *c, double *alpha)
+{
+    return guard([&] {
+        MGM_REQUIRE(c, "null context");
+        *alpha = c->last_learned_alpha;
     });
 }
 

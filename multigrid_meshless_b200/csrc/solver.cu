@@ -345,6 +345,18 @@ void vcycle(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int cheb_d
     vcycle_rec(Ls, cs, 0, cheb_degree, cheb_ratio, s, prof);
 }
 
+// Chebyshev smoothing of A e = r on one level from e = 0 (r already in L.r);
+// returns the buffer holding e.
+template <class T>
+const T *smooth_from_zero(SolveLevel<T> &L, int degree, double ratio, cudaStream_t s)
+{
+    MGM_CUDA(cudaMemsetAsync(L.e, 0, sizeof(T) * L.n, s));
+    smooth(L, degree, ratio, true, s, nullptr);
+    return L.e;
+}
+template const double *smooth_from_zero<double>(SolveLevel<double> &, int, double, cudaStream_t);
+template const float *smooth_from_zero<float>(SolveLevel<float> &, int, double, cudaStream_t);
+
 template void vcycle<double>(std::vector<SolveLevel<double>> &, const CoarseSolve<double> &, int, double, cudaStream_t,
                              SmootherProfile *);
 template void vcycle<float>(std::vector<SolveLevel<float>> &, const CoarseSolve<float> &, int, double, cudaStream_t,

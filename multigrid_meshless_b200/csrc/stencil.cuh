@@ -105,5 +105,7 @@ void vcycle(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int cheb_d
             cudaStream_t s, SmootherProfile *prof = nullptr);
 template <class T>
 void estimate_lmax(SolveLevel<T> &L, cudaStream_t s);
+template <class T>
+const T *smooth_from_zero(SolveLevel<T> &L, int degree, double ratio, cudaStream_t s);
 
 }  // namespace mgm
