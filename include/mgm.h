@@ -308,6 +308,58 @@ MGM_API int mgm_last_learned_alpha(mgm_ctx *ctx, double *alpha);
 /* Synchronises the context's stream. */
 MGM_API int mgm_sync(mgm_ctx *ctx);
 
+/* ------------------------------------------------------------------ */
+/* Batched hierarchies: per-node stencil sizes, one-launch weight      */
+/* assembly, many right-hand sides through one V-cycle.               */
+/* No counterpart in the reference, which has one stencil size per    */
+/* level (structures.h:15-78, mesh_functions.h:131-170) and one       */
+/* right-hand side per solve (fractional_step_solver.h:150-166).      */
+/* ------------------------------------------------------------------ */
+typedef struct mgm_batch mgm_batch;
+MGM_API mgm_batch *mgm_batch_create(int dim, int phs_degree, int num_levels);
+MGM_API void mgm_batch_destroy(mgm_batch *b);
+/* Level input as for mgm_set_level (boundary nodes first, no corners), with
+ * the stencil size of every node: k_per_node[i] nearest nodes (self first;
+ * boundary node: itself then k-1 interior nodes, kdtree_functions.h:141-149). */
+MGM_API int mgm_batch_set_level(mgm_batch *b, int lev, int n, int nb, const double *x, const double *y,
+                                const double *z, const double *nx, const double *ny, const double *nz,
+                                const unsigned char *btag, int poly_degree, const int *k_per_node);
+#define MGM_BATCH_AUTOTUNE 1 /* time candidate team widths / CTA budgets before the launch */
+/* kNN lists, breadth-first reorder, normals, nearest points, then every
+ * derivative row (rbf.h:401-421), restriction row and prolongation row
+ * (mesh_functions.h:533-670) of every level in ONE persistent launch, then the
+ * solver set-up (pinned operators, smoother bounds, coarsest inverse). */
+MGM_API int mgm_batch_setup(mgm_batch *b, int flags);
+/* The weight launch: its device time, the autotuner's time, systems, tiles,
+ * shared memory per CTA and resident CTAs per SM. */
+MGM_API int mgm_batch_weights_report(mgm_batch *b, double *weights_ms, double *tuning_ms, long long *systems,
+                                     int *tiles, int *smem_bytes, int *ctas_per_sm);
+/* Size classes (largest system order first): order N = k + np, systems,
+ * threads per system chosen, measured microseconds per system (0 untuned). */
+MGM_API int mgm_batch_num_classes(mgm_batch *b, int *count);
+MGM_API int mgm_batch_class(mgm_batch *b, int idx, int *order, long long *systems, int *team_threads,
+                            double *us_per_system);
+MGM_API int mgm_batch_level_size(mgm_batch *b, int lev, int *n, int *nb, long long *nnz, long long *r_nnz,
+                                 long long *p_nnz);
+/* Level data after the reorder (CSR: row i = col[row_ptr[i] .. row_ptr[i+1])).
+ * Any output may be NULL. */
+MGM_API int mgm_batch_get_level(mgm_batch *b, int lev, double *x, double *y, double *z, double *nx, double *ny,
+                                double *nz, unsigned char *btag, int *k_per_node, int *row_ptr, int *col,
+                                double *Dx, double *Dy, double *Dz, double *lap, double *lapP);
+/* Restriction into level lev (row i interpolates level lev-1 at node i; rows
+ * of boundary nodes and node 0 are empty) and prolongation into level lev
+ * (from level lev+1, every row).  Any output may be NULL. */
+MGM_API int mgm_batch_get_transfer(mgm_batch *b, int lev, int *rpts, int *ppts, int *r_ptr, int *r_col,
+                                   double *r_w, int *p_ptr, int *p_col, double *p_w);
+/* rel_tol, Krylov restart length (<= 32), Chebyshev degree and ratio. */
+MGM_API int mgm_batch_set_solver(mgm_batch *b, double rel_tol, int restart, int cheb_degree, double cheb_ratio);
+/* Solves the pinned Poisson system (row 0 -> p[0] = 0) for nrhs <= 64
+ * right-hand sides at once: rhs and sol are host arrays [nrhs][n0] in the
+ * reordered node order; rel_res[nrhs].  mode: MGM_MODE_FP64 or
+ * MGM_MODE_FP32_IR.  solve_ms: device time with the right-hand sides in HBM. */
+MGM_API int mgm_batch_solve(mgm_batch *b, int mode, int nrhs, const double *rhs, double *sol, int *vcycles,
+                            double *rel_res, double *solve_ms);
+
 #ifdef __cplusplus
 }
 #endif

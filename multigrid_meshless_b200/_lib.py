@@ -25,6 +25,7 @@ MODE_REFERENCE, MODE_FP64, MODE_FP32_IR = 0, 1, 2
 NOALLOC_MAX_NODES = 2097152  # MGM_NOALLOC_MAX_NODES
 BC_LID, BC_TAYLOR_COUETTE = 0, 1
 SETUP_REFERENCE_TRANSFER = 1
+BATCH_AUTOTUNE = 1
 FIELD = {"u": 0, "v": 1, "w": 2, "p": 3, "u_new": 4, "v_new": 5, "w_new": 6, "res": 10, "source": 11, "dpdn": 12}
 
 # every exported entry point and its argument types (restype int unless noted)
@@ -96,6 +97,21 @@ SIGNATURES = {
     "mgm_host_free": ([vp], None),
     "mgm_profile_smoother": ([vp, C.c_int], C.c_int),
     "mgm_profile_read": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int),
+    "mgm_batch_create": ([C.c_int, C.c_int, C.c_int], vp),
+    "mgm_batch_destroy": ([vp], None),
+    "mgm_batch_set_level": ([vp, C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, dp, dp, u8p, C.c_int, ip], C.c_int),
+    "mgm_batch_setup": ([vp, C.c_int], C.c_int),
+    "mgm_batch_weights_report": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                                  C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    "mgm_batch_num_classes": ([vp, C.POINTER(C.c_int)], C.c_int),
+    "mgm_batch_class": ([vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_int),
+                         C.POINTER(C.c_double)], C.c_int),
+    "mgm_batch_level_size": ([vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong),
+                              C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int),
+    "mgm_batch_get_level": ([vp, C.c_int] + [vp] * 15, C.c_int),
+    "mgm_batch_get_transfer": ([vp, C.c_int] + [vp] * 8, C.c_int),
+    "mgm_batch_set_solver": ([vp, C.c_double, C.c_int, C.c_int, C.c_double], C.c_int),
+    "mgm_batch_solve": ([vp, C.c_int, C.c_int, dp, dp, C.POINTER(C.c_int), dp, C.POINTER(C.c_double)], C.c_int),
 }
 
 _LIB = None

@@ -300,3 +300,98 @@ class PinnedArray:
             self.array = None
             self.L.mgm_host_free(self.ptr)
             self.ptr = None
+
+
+class Batch:
+    """A hierarchy with a stencil size per node, assembled in one persistent
+    weight launch, solving many Poisson right-hand sides through one V-cycle
+    (mgm_batch_* in include/mgm.h).  Node arrays come back in the reordered
+    order; operators are CSR (row_ptr, col, values)."""
+
+    def __init__(self, clouds, k_per_node, polys, phs=3, autotune=True):
+        self.L = load()
+        self.nl = len(clouds)
+        self.dim = clouds[0].dim
+        h = self.L.mgm_batch_create(self.dim, phs, self.nl)
+        if not h:
+            raise _lib.MgmError(-1, self.L.mgm_last_error().decode())
+        self.h = h
+        for l, c in enumerate(clouds):
+            check(self.L.mgm_batch_set_level(h, l, c.n, c.nb, _f(c.x), _f(c.y), _f(c.z), _f(c.nx), _f(c.ny),
+                                             _f(c.nz), _u8(c.btag), polys[l], _i(k_per_node[l])))
+        check(self.L.mgm_batch_setup(h, _lib.BATCH_AUTOTUNE if autotune else 0))
+        self.sizes = []
+        for l in range(self.nl):
+            n, nb = C.c_int(), C.c_int()
+            nnz, rn, pn = C.c_longlong(), C.c_longlong(), C.c_longlong()
+            check(self.L.mgm_batch_level_size(h, l, C.byref(n), C.byref(nb), C.byref(nnz), C.byref(rn), C.byref(pn)))
+            self.sizes.append((n.value, nb.value, nnz.value, rn.value, pn.value))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mgm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def n(self, l=0):
+        return self.sizes[l][0]
+
+    def weights_report(self):
+        wm, tm = C.c_double(), C.c_double()
+        ns = C.c_longlong()
+        nt, sm, cta = C.c_int(), C.c_int(), C.c_int()
+        check(self.L.mgm_batch_weights_report(self.h, C.byref(wm), C.byref(tm), C.byref(ns), C.byref(nt),
+                                              C.byref(sm), C.byref(cta)))
+        cnt = C.c_int()
+        check(self.L.mgm_batch_num_classes(self.h, C.byref(cnt)))
+        classes = []
+        for i in range(cnt.value):
+            N, s, t, us = C.c_int(), C.c_longlong(), C.c_int(), C.c_double()
+            check(self.L.mgm_batch_class(self.h, i, C.byref(N), C.byref(s), C.byref(t), C.byref(us)))
+            classes.append({"order": N.value, "systems": s.value, "team_threads": t.value,
+                            "us_per_system": us.value})
+        return {"weights_ms": wm.value, "tuning_ms": tm.value, "systems": ns.value, "tiles": nt.value,
+                "smem_bytes": sm.value, "ctas_per_sm": cta.value, "classes": classes}
+
+    def level(self, l):
+        n, nb, nnz, _, _ = self.sizes[l]
+        a = {nm: np.zeros(n) for nm in ("x", "y", "z", "nx", "ny", "nz")}
+        a["btag"] = np.zeros(n, np.uint8)
+        a["k"] = np.zeros(n, np.int32)
+        a["row_ptr"] = np.zeros(n + 1, np.int32)
+        a["col"] = np.zeros(max(nnz, 1), np.int32)
+        for nm in ("Dx", "Dy", "Dz", "lap", "lapP"):
+            a[nm] = np.zeros(max(nnz, 1)) if (nm != "Dz" or self.dim == 3) else None
+        check(self.L.mgm_batch_get_level(self.h, l, *(ptr(a[nm]) for nm in (
+            "x", "y", "z", "nx", "ny", "nz", "btag", "k", "row_ptr", "col", "Dx", "Dy", "Dz", "lap", "lapP"))))
+        return a
+
+    def transfer(self, l):
+        n, _, _, rn, pn = self.sizes[l]
+        a = {"rpts": np.zeros(n, np.int32), "ppts": np.zeros(n, np.int32)}
+        if l > 0:
+            a.update(r_ptr=np.zeros(n + 1, np.int32), r_col=np.zeros(max(rn, 1), np.int32), r_w=np.zeros(max(rn, 1)))
+        if l < self.nl - 1:
+            a.update(p_ptr=np.zeros(n + 1, np.int32), p_col=np.zeros(max(pn, 1), np.int32), p_w=np.zeros(max(pn, 1)))
+        check(self.L.mgm_batch_get_transfer(self.h, l, *(ptr(a.get(nm)) for nm in (
+            "rpts", "ppts", "r_ptr", "r_col", "r_w", "p_ptr", "p_col", "p_w"))))
+        return a
+
+    def set_solver(self, rel_tol=1e-8, restart=24, cheb_degree=3, cheb_ratio=20.0):
+        check(self.L.mgm_batch_set_solver(self.h, rel_tol, restart, cheb_degree, cheb_ratio))
+
+    def solve(self, rhs, mode=_lib.MODE_FP32_IR):
+        """rhs [nrhs][n0] -> (solutions [nrhs][n0], V-cycles, rel. residuals [nrhs], device ms)."""
+        rhs = _f(np.atleast_2d(rhs))
+        nrhs = rhs.shape[0]
+        sol = np.zeros_like(rhs)
+        vc = C.c_int()
+        rr = np.zeros(nrhs)
+        ms = C.c_double()
+        check(self.L.mgm_batch_solve(self.h, mode, nrhs, rhs, sol, C.byref(vc), rr, C.byref(ms)))
+        return sol, vc.value, rr, ms.value

@@ -17,6 +17,10 @@ Kinds
   cube3d(m)        unit cube, m^3 nodes, interior jittered by U(-0.25h, 0.25h),
                    face nodes evenly spaced, edge and corner nodes removed
                    (Gmsh line/point elements are corner-tagged, mesh_functions.h:396-413).
+  shell3d(h)       spherical shell r in [0.5, 1]: interior nodes by rejection
+                   of a jittered Cartesian lattice of spacing h (uniform
+                   density), boundary nodes on both spheres by a Fibonacci
+                   lattice of matching spacing.
 """
 from __future__ import annotations
 
@@ -184,4 +188,86 @@ def cube_hierarchy(m: int, levels: int, seed: int = 1) -> list[Cloud]:
     for l in range(levels):
         out.append(cube3d(m, seed + l))
         m = max(3, m // 2)
+    return out
+
+
+def _fibonacci_sphere(count: int, r: float):
+    i = np.arange(count, dtype=np.float64) + 0.5
+    zc = 1.0 - 2.0 * i / count
+    rho = np.sqrt(np.maximum(0.0, 1.0 - zc * zc))
+    th = math.pi * (3.0 - math.sqrt(5.0)) * i
+    return rho * np.cos(th), rho * np.sin(th), zc
+
+
+def shell3d(h: float, seed: int = 1, r_in: float = 0.5, r_out: float = 1.0) -> Cloud:
+    """Shell r in [r_in, r_out]; nodes at spacing about h.  Interior: lattice
+    points of spacing h jittered by U(-0.25h, 0.25h), kept when their radius
+    lies in [r_in + 0.5h, r_out - 0.5h].  Boundary: Fibonacci points on each
+    sphere, one per h^2 of area, normals pointing out of the fluid."""
+    m = int(math.ceil(2.0 * r_out / h)) + 1
+    g = (np.arange(m, dtype=np.float64) - 0.5 * (m - 1)) * h
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    X = X.ravel(); Y = Y.ravel(); Z = Z.ravel()
+    nt = X.shape[0]
+    X = X + (uniform(seed, 0, nt) - 0.5) * 0.5 * h
+    Y = Y + (uniform(seed, 1, nt) - 0.5) * 0.5 * h
+    Z = Z + (uniform(seed, 2, nt) - 0.5) * 0.5 * h
+    R = np.sqrt(X * X + Y * Y + Z * Z)
+    keep = (R >= r_in + 0.5 * h) & (R <= r_out - 0.5 * h)
+    ix, iy, iz = X[keep], Y[keep], Z[keep]
+    bxs, bys, bzs, nxs, nys, nzs = [], [], [], [], [], []
+    for r, sgn in ((r_in, -1.0), (r_out, 1.0)):
+        cnt = max(12, int(round(4.0 * math.pi * r * r / (h * h))))
+        ux, uy, uz = _fibonacci_sphere(cnt, r)
+        bxs.append(r * ux); bys.append(r * uy); bzs.append(r * uz)
+        nxs.append(sgn * ux); nys.append(sgn * uy); nzs.append(sgn * uz)
+    bx = np.concatenate(bxs); by = np.concatenate(bys); bz = np.concatenate(bzs)
+    nb = bx.shape[0]
+    x = np.concatenate([bx, ix]); y = np.concatenate([by, iy]); z = np.concatenate([bz, iz])
+    n = x.shape[0]
+    btag = np.zeros(n, np.uint8); btag[:nb] = 1
+    nx = np.zeros(n); ny = np.zeros(n); nz = np.zeros(n)
+    nx[:nb] = np.concatenate(nxs); ny[:nb] = np.concatenate(nys); nz[:nb] = np.concatenate(nzs)
+    return Cloud(x, y, z, nx, ny, nz, btag, nb, 3, h, "shell3d", {"h": h, "seed": seed, "r_in": r_in, "r_out": r_out})
+
+
+def shell_h_for_nodes(n_target: int, r_in: float = 0.5, r_out: float = 1.0) -> float:
+    """Spacing giving about n_target interior plus boundary nodes."""
+    vol = 4.0 / 3.0 * math.pi * (r_out ** 3 - r_in ** 3)
+    return (vol / n_target) ** (1.0 / 3.0)
+
+
+def shell_hierarchy(h: float, levels: int, seed: int = 1) -> list[Cloud]:
+    """Fine spacing h, each coarser level at twice the spacing (8x fewer nodes)."""
+    return [shell3d(h * (2 ** l), seed + l) for l in range(levels)]
+
+
+def shell_stencil_sizes(c: Cloud, k_interior: int, k_boundary: int, band: float = 1.5):
+    """Per-node stencil size: k_boundary for boundary nodes and nodes within
+    band*h of either sphere, k_interior elsewhere."""
+    r = np.sqrt(c.x * c.x + c.y * c.y + c.z * c.z)
+    near = (r - c.meta["r_in"] < band * c.h) | (c.meta["r_out"] - r < band * c.h) | (c.btag != 0)
+    return np.where(near, k_boundary, k_interior).astype(np.int32)
+
+
+def gaussian_fields(c: Cloud, count: int, seed: int = 1, bumps: int = 8, wmin: float = 0.1, wmax: float = 0.3):
+    """count smooth fields [count][n], each a sum of `bumps` Gaussians with
+    amplitude N(0,1), width U(wmin, wmax) and centres uniform in the shell."""
+    out = np.zeros((count, c.n))
+    r_in, r_out = c.meta.get("r_in", 0.0), c.meta.get("r_out", 1.0)
+    for f in range(count):
+        u = uniform(seed, 1000 + f, 16 * bumps)
+        k = 0
+        for b in range(bumps):
+            # amplitude N(0,1) by Box-Muller
+            a = math.sqrt(-2.0 * math.log(max(u[k], 1e-300))) * math.cos(2.0 * math.pi * u[k + 1]); k += 2
+            w = wmin + (wmax - wmin) * u[k]; k += 1
+            # centre: uniform in the shell (radius by inverse CDF, direction uniform)
+            rr = (r_in ** 3 + u[k] * (r_out ** 3 - r_in ** 3)) ** (1.0 / 3.0); k += 1
+            cz = 1.0 - 2.0 * u[k]; k += 1
+            ph = 2.0 * math.pi * u[k]; k += 1
+            s = math.sqrt(max(0.0, 1.0 - cz * cz))
+            cx, cy, cz = rr * s * math.cos(ph), rr * s * math.sin(ph), rr * cz
+            d2 = (c.x - cx) ** 2 + (c.y - cy) ** 2 + (c.z - cz) ** 2
+            out[f] += a * np.exp(-d2 / (w * w))
     return out

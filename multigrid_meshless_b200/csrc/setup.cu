@@ -9,6 +9,7 @@
 #include <climits>
 
 #include "mgm_internal.cuh"
+#include "weights.cuh"
 
 namespace mgm {
 
@@ -485,133 +486,6 @@ Monomials monomials(int dim, int deg)
     return m;
 }
 
-struct MonoDev {
-    int np;
-    short px[kMaxPoly], py[kMaxPoly], pz[kMaxPoly];
-};
-
-static MonoDev to_dev(const Monomials &m)
-{
-    MonoDev d;
-    d.np = m.np;
-    for (int i = 0; i < kMaxPoly; i++) { d.px[i] = m.px[i]; d.py[i] = m.py[i]; d.pz[i] = m.pz[i]; }
-    return d;
-}
-
-// Shared-memory layout of one system (doubles): aug[N][2N] | sx[k] sy[k] sz[k] | L[4][N] | t[N] ; ints: perm[N]
-__device__ __forceinline__ void stage_cloud(const int *cl, int m, const double *x, const double *y, const double *z,
-                                            double *sx, double *sy, double *sz)
-{
-    for (int j = threadIdx.x; j < m; j += blockDim.x) { int c = cl[j]; sx[j] = x[c]; sy[j] = y[c]; sz[j] = z[c]; }
-}
-
-// create_A_matrix_from_cloud_indices (rbf.h:42-77) into the left half of aug,
-// identity into the right half.
-__device__ void build_aug(int m, int np, int dim, int phs, const MonoDev &mono, const double *sx, const double *sy,
-                          const double *sz, double *aug, int N)
-{
-    const int W2 = 2 * N;
-    for (int e = threadIdx.x; e < N * W2; e += blockDim.x) {
-        int i = e / W2, j = e % W2;
-        double v;
-        if (j >= N) v = (j - N == i) ? 1.0 : 0.0;
-        else if (i < m && j < m) {
-            if (i == j) v = 0;
-            else {
-                int a = min(i, j), b = max(i, j);  // the reference evaluates (cloud[a], cloud[b]) with a < b
-                double p1[3] = {sx[a], sy[a], sz[a]}, p2[3] = {sx[b], sy[b], sz[b]};
-                v = mgm_phs_rbf(p1, p2, phs, dim);
-            }
-        } else if (i < m || j < m) {
-            int node = i < m ? i : j, t = i < m ? j - m : i - m;
-            v = 1;
-            if (mono.px[t] != 0) v = MGM_MUL(v, mgm_pow_int(MGM_SUB(sx[node], sx[0]), mono.px[t]));
-            if (mono.py[t] != 0) v = MGM_MUL(v, mgm_pow_int(MGM_SUB(sy[node], sy[0]), mono.py[t]));
-            if (mono.pz[t] != 0) v = MGM_MUL(v, mgm_pow_int(MGM_SUB(sz[node], sz[0]), mono.pz[t]));
-        } else v = 0;
-        aug[e] = v;
-    }
-}
-
-// In-place Gauss-Jordan; on return aug[perm[i]][N + j] holds inverse[i][j].
-__device__ void gauss_jordan(double *aug, int *perm, double *t, int N)
-{
-    const int W2 = 2 * N;
-    if (threadIdx.x == 0) {
-        for (int i = 0; i < N; i++) perm[i] = i;
-        for (int i = N - 1; i > 0; i--)
-            if (aug[perm[i - 1] * W2] < aug[perm[i] * W2]) { int tmp = perm[i]; perm[i] = perm[i - 1]; perm[i - 1] = tmp; }
-    }
-    __syncthreads();
-    for (int i = 0; i < N; i++) {
-        const double *pr = aug + perm[i] * W2;
-        const double piv = pr[i];
-        for (int j = threadIdx.x; j < N; j += blockDim.x) t[j] = (j == i) ? 0.0 : MGM_DIV(aug[perm[j] * W2 + i], piv);
-        __syncthreads();
-        for (int e = threadIdx.x; e < N * W2; e += blockDim.x) {
-            int j = e / W2, c = e % W2;
-            if (j == i) continue;
-            double *rj = aug + perm[j] * W2;
-            rj[c] = MGM_SUB(rj[c], MGM_MUL(pr[c], t[j]));
-        }
-        __syncthreads();
-    }
-    for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
-        int i = e / N, j = e % N;
-        double *ri = aug + perm[i] * W2;
-        ri[N + j] = MGM_DIV(ri[N + j], ri[i]);
-    }
-    __syncthreads();
-}
-
-// Row 0 of gradx/grady/gradz/laplacian_matrix (rbf.h:79-270) at the seed.
-__device__ void operator_row0(int op, int m, int np, int dim, int phs, const MonoDev &mono, const double *sx,
-                              const double *sy, const double *sz, double *L)
-{
-    const int N = m + np;
-    const double p1[3] = {sx[0], sy[0], sz[0]};
-    for (int c = threadIdx.x; c < N; c += blockDim.x) {
-        double v = 0;
-        if (c < m) {
-            const double p2[3] = {sx[c], sy[c], sz[c]};
-            if (op <= 2) v = MGM_MUL(MGM_MUL((double)phs, MGM_SUB(p1[op], p2[op])), mgm_phs_rbf(p1, p2, phs - 2, dim));
-            else v = MGM_MUL((double)(phs * phs), mgm_phs_rbf(p1, p2, phs - 2, dim));
-            if ((op == 1 || op == 2) && c == 0) v = 0;  // rbf.h:141, :180 zero column 0
-        } else {
-            const int j = c - m;
-            const double d0 = MGM_SUB(p1[0], sx[0]), d1 = MGM_SUB(p1[1], sy[0]), d2 = MGM_SUB(p1[2], sz[0]);
-            const int ex = mono.px[j], ey = mono.py[j], ez = mono.pz[j];
-            if (op == 0) {
-                if (j == 0 || ex == 0) v = 0;
-                else { v = MGM_MUL((double)ex, mgm_pow_int(d0, ex - 1)); v = MGM_MUL(v, mgm_pow_int(d1, ey)); v = MGM_MUL(v, mgm_pow_int(d2, ez)); }
-            } else if (op == 1) {
-                if (j == 0 || ey == 0) v = 0;  // grad[i][m] is never written by grady_matrix: zero from create_matrix
-                else { v = MGM_MUL((double)ey, mgm_pow_int(d1, ey - 1)); v = MGM_MUL(v, mgm_pow_int(d0, ex)); v = MGM_MUL(v, mgm_pow_int(d2, ez)); }
-            } else if (op == 2) {
-                if (j == 0 || ez == 0) v = 0;
-                else { v = MGM_MUL((double)ez, mgm_pow_int(d2, ez - 1)); v = MGM_MUL(v, mgm_pow_int(d1, ey)); v = MGM_MUL(v, mgm_pow_int(d0, ex)); }
-            } else {
-                double tx = 0, ty = 0, tz = 0;
-                if (ex > 1) {
-                    tx = MGM_MUL((double)(ex * (ex - 1)), mgm_pow_int(d0, ex - 2));
-                    tx = MGM_MUL(tx, mgm_pow_int(d1, ey));
-                    if (dim == 3) tx = MGM_MUL(tx, mgm_pow_int(d2, ez));
-                } else if (ey > 1) {
-                    ty = MGM_MUL((double)(ey * (ey - 1)), mgm_pow_int(d1, ey - 2));
-                    ty = MGM_MUL(ty, mgm_pow_int(d0, ex));
-                    if (dim == 3) ty = MGM_MUL(ty, mgm_pow_int(d2, ez));
-                } else if (dim == 3 && ez > 1) {
-                    tz = MGM_MUL((double)(ez * (ez - 1)), mgm_pow_int(d2, ez - 2));
-                    tz = MGM_MUL(tz, mgm_pow_int(d0, ex));
-                    tz = MGM_MUL(tz, mgm_pow_int(d1, ey));
-                }
-                v = dim == 3 ? MGM_ADD(MGM_ADD(tx, ty), tz) : MGM_ADD(tx, ty);
-            }
-        }
-        L[c] = v;
-    }
-}
-
 __global__ void k_derivative_weights(int n, int k, int dim, int phs, MonoDev mono, const double *__restrict__ x,
                                      const double *__restrict__ y, const double *__restrict__ z,
                                      const double *__restrict__ nx, const double *__restrict__ ny,
@@ -628,21 +502,19 @@ __global__ void k_derivative_weights(int n, int k, int dim, int phs, MonoDev mon
     double *wout = t + N;         // [4][k]
     int *perm = (int *)(wout + 4 * k);
     const int nops = dim == 3 ? 4 : 3;
+    const Team tm = Team::block();
     for (long node = blockIdx.x; node < n; node += gridDim.x) {
         const int *cl = cloud + node * k;
-        stage_cloud(cl, m, x, y, z, sx, sy, sz);
-        __syncthreads();
-        build_aug(m, np, dim, phs, mono, sx, sy, sz, aug, N);
-        for (int o = 0; o < nops; o++) operator_row0(o == nops - 1 ? 3 : o, m, np, dim, phs, mono, sx, sy, sz, L + o * N);
-        __syncthreads();
-        gauss_jordan(aug, perm, t, N);
+        stage_cloud(tm, cl, m, x, y, z, sx, sy, sz);
+        tm.sync();
+        build_aug(tm, m, np, dim, phs, mono, sx, sy, sz, aug, N);
+        for (int o = 0; o < nops; o++) operator_row0(tm, o == nops - 1 ? 3 : o, m, np, dim, phs, mono, sx, sy, sz, L + o * N);
+        tm.sync();
+        gauss_jordan(tm, aug, perm, t, N);
         // weights: D[j] = sum_c L[c] * inverse[c][j], c ascending (multiply_matrices, mat_lib.h:214-228)
         for (int e = threadIdx.x; e < nops * m; e += blockDim.x) {
             const int o = e / m, j = e % m;
-            const double *Lo = L + o * N;
-            double s = 0;
-            for (int c = 0; c < N; c++) s = MGM_ADD(s, MGM_MUL(Lo[c], aug[perm[c] * 2 * N + N + j]));
-            wout[o * k + j] = s;
+            wout[o * k + j] = row_times_inverse(L + o * N, aug, perm, N, j);
         }
         __syncthreads();
         const bool bnd = btag[node] != 0;
@@ -663,11 +535,7 @@ __global__ void k_derivative_weights(int n, int k, int dim, int phs, MonoDev mon
     }
 }
 
-static size_t weights_smem(int k, int np)
-{
-    const int N = k + np;
-    return sizeof(double) * ((size_t)N * 2 * N + 3 * k + 4 * N + N + 4 * k) + sizeof(int) * N;
-}
+static size_t weights_smem(int k, int np) { return system_bytes(k, np); }
 
 static int weights_grid(long rows)
 {
@@ -702,6 +570,7 @@ __global__ void k_transfer_weights(int nt, const double *__restrict__ tx, const 
     double *tmp = sz + m;  // [N]
     double *t = tmp + N;   // [N]
     int *perm = (int *)(t + N);
+    const Team tm = Team::block();
     for (long i = blockIdx.x; i < nt; i += gridDim.x) {
         const bool skip = only_interior ? (tbtag[i] != 0) : (i < rows_from);
         if (skip) {
@@ -710,32 +579,16 @@ __global__ void k_transfer_weights(int nt, const double *__restrict__ tx, const 
         }
         const int ip = src_pt[i];
         const int *cl = scloud + (long)ip * ks;
-        stage_cloud(cl, m, sxg, syg, szg, sx, sy, sz);
-        __syncthreads();
-        build_aug(m, np, dim, phs, mono, sx, sy, sz, aug, N);
+        stage_cloud(tm, cl, m, sxg, syg, szg, sx, sy, sz);
+        tm.sync();
+        build_aug(tm, m, np, dim, phs, mono, sx, sy, sz, aug, N);
         const double p1[3] = {tx[i], ty[i], tz[i]};
         const double seed[3] = {sxg[ip], syg[ip], szg[ip]};
-        for (int c = threadIdx.x; c < N; c += blockDim.x) {
-            double v;
-            if (c < m) {
-                const double p2[3] = {sx[c], sy[c], sz[c]};
-                v = mgm_phs_rbf(p1, p2, phs, dim);
-            } else {
-                const int j = c - m;
-                v = MGM_MUL(MGM_MUL(mgm_pow_int(MGM_SUB(p1[0], seed[0]), mono.px[j]),
-                                    mgm_pow_int(MGM_SUB(p1[1], seed[1]), mono.py[j])),
-                            mgm_pow_int(MGM_SUB(p1[2], seed[2]), mono.pz[j]));
-            }
-            tmp[c] = v;
-        }
-        __syncthreads();
-        gauss_jordan(aug, perm, t, N);
+        transfer_row(tm, m, np, dim, phs, mono, sx, sy, sz, p1, seed, tmp);
+        tm.sync();
+        gauss_jordan(tm, aug, perm, t, N);
         // multiply_vector_matrix_columnwise (mat_lib.h:720-726)
-        for (int c = threadIdx.x; c < m; c += blockDim.x) {
-            double s = 0;
-            for (int j = 0; j < N; j++) s = MGM_ADD(s, MGM_MUL(tmp[j], aug[perm[j] * 2 * N + N + c]));
-            W[i * ks + c] = s;
-        }
+        for (int c = threadIdx.x; c < m; c += blockDim.x) W[i * ks + c] = row_times_inverse(tmp, aug, perm, N, c);
         __syncthreads();
     }
 }
