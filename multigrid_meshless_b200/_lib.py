@@ -69,6 +69,7 @@ SIGNATURES = {
     "mgm_set_solver": ([vp, C.c_double, C.c_int, C.c_int, C.c_double], C.c_int),
     "mgm_use_graphs": ([vp, C.c_int], C.c_int),
     "mgm_use_compact": ([vp, C.c_int], C.c_int),
+    "mgm_use_tiled": ([vp, C.c_int], C.c_int),
     "mgm_last_solve": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
     "mgm_intermediate_velocity": ([vp], C.c_int),
     "mgm_mass_residual": ([vp], C.c_int),

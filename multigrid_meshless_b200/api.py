@@ -214,6 +214,9 @@ class Multigrid:
     def use_compact(self, enable=True):
         check(self.L.mgm_use_compact(self.h, 1 if enable else 0))
 
+    def use_tiled(self, enable=True):
+        check(self.L.mgm_use_tiled(self.h, 1 if enable else 0))
+
     def use_graphs(self, enable=True):
         check(self.L.mgm_use_graphs(self.h, 1 if enable else 0))
 

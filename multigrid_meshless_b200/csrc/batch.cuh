@@ -82,7 +82,7 @@ struct mgm_batch {
     int B = 0;
     mgm::BVecs<double> v64[mgm::kBatchMaxLevels];
     mgm::BVecs<float> v32[mgm::kBatchMaxLevels];
-    mgm::DBuf<double> X, Bv, W, V, part, hsc;
+    mgm::DBuf<double> X, Bv, V, part, hsc;
     mgm::DBuf<float> Z32;
     mgm::DBuf<double> Z64;
     int V_cols = 0, Z_cols32 = 0, Z_cols64 = 0;

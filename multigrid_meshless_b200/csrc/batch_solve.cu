@@ -83,7 +83,15 @@ __device__ __forceinline__ void row_dot_b(const int *__restrict__ col, const T *
     }
 }
 
-__device__ __forceinline__ int warp_row() { return (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5); }
+// Row-kernel shape: a CTA of 8 warps owns kRowsPerCta consecutive rows and
+// its warps step through them together (warp w: rows w, w + 8, ...).  In the
+// breadth-first order consecutive rows share most neighbours, so the gathered
+// neighbour rows of one CTA are served from L1 after their first use.
+constexpr int kRowsPerCta = 64;
+inline int rows_grid(long rows) { return blocks_for(rows, kRowsPerCta); }
+#define MGM_CTA_ROWS(r, count)                                                                     \
+    for (int r##_k = (int)(threadIdx.x >> 5), r = blockIdx.x * kRowsPerCta + r##_k;                \
+         r##_k < kRowsPerCta && r < (count); r##_k += 8, r += 8)
 
 // exact solve of the boundary rows (they couple only to themselves and interior nodes)
 template <class T, int Q>
@@ -92,24 +100,25 @@ __global__ void __launch_bounds__(256) k_b_bnd(int nbl, const int *__restrict__ 
                                                const T *__restrict__ dinv, const T *__restrict__ r, T *e, int B,
                                                int zero_start)
 {
-    const int w = warp_row(), lane = threadIdx.x & 31;
-    if (w >= nbl) return;
-    const int i = list[w];
-    const long o = (long)i * B + lane * Q;
-    T rv[Q], ev[Q];
-    ldq<T, Q>(r + o, rv);
-    const T di = dinv[i];
-    if (zero_start) {
+    const int lane = threadIdx.x & 31;
+    MGM_CTA_ROWS(w, nbl) {
+        const int i = list[w];
+        const long o = (long)i * B + lane * Q;
+        T rv[Q], ev[Q];
+        ldq<T, Q>(r + o, rv);
+        const T di = dinv[i];
+        if (zero_start) {
 #pragma unroll
-        for (int q = 0; q < Q; q++) ev[q] = rv[q] * di;
-    } else {
-        T acc[Q];
-        row_dot_b<T, Q, T>(col, A, rp[i], rp[i + 1] - rp[i], e, B, lane, acc);
-        ldq<T, Q>(e + o, ev);
+            for (int q = 0; q < Q; q++) ev[q] = rv[q] * di;
+        } else {
+            T acc[Q];
+            row_dot_b<T, Q, T>(col, A, rp[i], rp[i + 1] - rp[i], e, B, lane, acc);
+            ldq<T, Q>(e + o, ev);
 #pragma unroll
-        for (int q = 0; q < Q; q++) ev[q] = ev[q] + (rv[q] - acc[q]) * di;
+            for (int q = 0; q < Q; q++) ev[q] = ev[q] + (rv[q] - acc[q]) * di;
+        }
+        stq<T, Q>(e + o, ev);
     }
-    stq<T, Q>(e + o, ev);
 }
 
 // one Chebyshev step on interior rows: q = r - A e, d = c1 d + c2 D^-1 q, e' = e + d
@@ -120,25 +129,26 @@ __global__ void __launch_bounds__(256) k_b_cheb(int n, const int *__restrict__ r
                                                 const T *__restrict__ e, T *__restrict__ eout, T *__restrict__ d,
                                                 int B, T c1, T c2, int first)
 {
-    const int i = warp_row(), lane = threadIdx.x & 31;
-    if (i >= n) return;
-    const long o = (long)i * B + lane * Q;
-    T ev[Q];
-    ldq<T, Q>(e + o, ev);
-    if (btag[i]) { stq<T, Q>(eout + o, ev); return; }
-    T acc[Q], rv[Q], dv[Q];
-    row_dot_b<T, Q, T>(col, A, rp[i], rp[i + 1] - rp[i], e, B, lane, acc);
-    ldq<T, Q>(r + o, rv);
-    if (!first) ldq<T, Q>(d + o, dv);
-    const T di = dinv[i];
+    const int lane = threadIdx.x & 31;
+    MGM_CTA_ROWS(i, n) {
+        const long o = (long)i * B + lane * Q;
+        T ev[Q];
+        ldq<T, Q>(e + o, ev);
+        if (btag[i]) { stq<T, Q>(eout + o, ev); continue; }
+        T acc[Q], rv[Q], dv[Q];
+        row_dot_b<T, Q, T>(col, A, rp[i], rp[i + 1] - rp[i], e, B, lane, acc);
+        ldq<T, Q>(r + o, rv);
+        if (!first) ldq<T, Q>(d + o, dv);
+        const T di = dinv[i];
 #pragma unroll
-    for (int q = 0; q < Q; q++) {
-        const T qv = rv[q] - acc[q];
-        dv[q] = first ? c2 * di * qv : c1 * dv[q] + c2 * di * qv;
-        ev[q] += dv[q];
+        for (int q = 0; q < Q; q++) {
+            const T qv = rv[q] - acc[q];
+            dv[q] = first ? c2 * di * qv : c1 * dv[q] + c2 * di * qv;
+            ev[q] += dv[q];
+        }
+        stq<T, Q>(d + o, dv);
+        stq<T, Q>(eout + o, ev);
     }
-    stq<T, Q>(d + o, dv);
-    stq<T, Q>(eout + o, ev);
 }
 
 template <class T, int Q>
@@ -147,21 +157,22 @@ __global__ void __launch_bounds__(256) k_b_residual(int n, const int *__restrict
                                                     const T *__restrict__ r, const T *__restrict__ e,
                                                     T *__restrict__ qo, int B)
 {
-    const int i = warp_row(), lane = threadIdx.x & 31;
-    if (i >= n) return;
-    const long o = (long)i * B + lane * Q;
-    T out[Q];
-    if (btag[i]) {
+    const int lane = threadIdx.x & 31;
+    MGM_CTA_ROWS(i, n) {
+        const long o = (long)i * B + lane * Q;
+        T out[Q];
+        if (btag[i]) {
 #pragma unroll
-        for (int q = 0; q < Q; q++) out[q] = T(0);
-    } else {
-        T acc[Q], rv[Q];
-        row_dot_b<T, Q, T>(col, A, rp[i], rp[i + 1] - rp[i], e, B, lane, acc);
-        ldq<T, Q>(r + o, rv);
+            for (int q = 0; q < Q; q++) out[q] = T(0);
+        } else {
+            T acc[Q], rv[Q];
+            row_dot_b<T, Q, T>(col, A, rp[i], rp[i + 1] - rp[i], e, B, lane, acc);
+            ldq<T, Q>(r + o, rv);
 #pragma unroll
-        for (int q = 0; q < Q; q++) out[q] = rv[q] - acc[q];
+            for (int q = 0; q < Q; q++) out[q] = rv[q] - acc[q];
+        }
+        stq<T, Q>(qo + o, out);
     }
-    stq<T, Q>(qo + o, out);
 }
 
 // y = M x for a CSR transfer matrix (empty rows give 0)
@@ -170,11 +181,12 @@ __global__ void __launch_bounds__(256) k_b_restrict(int n, const int *__restrict
                                                     const T *__restrict__ w, const T *__restrict__ x,
                                                     T *__restrict__ y, int B)
 {
-    const int i = warp_row(), lane = threadIdx.x & 31;
-    if (i >= n) return;
-    T acc[Q];
-    row_dot_b<T, Q, T>(col, w, rp[i], rp[i + 1] - rp[i], x, B, lane, acc);
-    stq<T, Q>(y + (long)i * B + lane * Q, acc);
+    const int lane = threadIdx.x & 31;
+    MGM_CTA_ROWS(i, n) {
+        T acc[Q];
+        row_dot_b<T, Q, T>(col, w, rp[i], rp[i + 1] - rp[i], x, B, lane, acc);
+        stq<T, Q>(y + (long)i * B + lane * Q, acc);
+    }
 }
 
 // ef += P ec - (P ec)[row 0]
@@ -192,15 +204,15 @@ __global__ void __launch_bounds__(256) k_b_prolong(int n, const int *__restrict_
         for (int q = 0; q < Q; q++) shift[lane * Q + q] = acc[q];
     }
     __syncthreads();
-    const int i = warp_row();
-    if (i >= n) return;
-    T acc[Q], ev[Q];
-    row_dot_b<T, Q, T>(col, w, rp[i], rp[i + 1] - rp[i], ec, B, lane, acc);
-    const long o = (long)i * B + lane * Q;
-    ldq<T, Q>(ef + o, ev);
+    MGM_CTA_ROWS(i, n) {
+        T acc[Q], ev[Q];
+        row_dot_b<T, Q, T>(col, w, rp[i], rp[i + 1] - rp[i], ec, B, lane, acc);
+        const long o = (long)i * B + lane * Q;
+        ldq<T, Q>(ef + o, ev);
 #pragma unroll
-    for (int q = 0; q < Q; q++) ev[q] += acc[q] - shift[lane * Q + q];
-    stq<T, Q>(ef + o, ev);
+        for (int q = 0; q < Q; q++) ev[q] += acc[q] - shift[lane * Q + q];
+        stq<T, Q>(ef + o, ev);
+    }
 }
 
 // E[n][B] = inv[n][n] R[n][B]; block: 32 rows x B columns, K tiles of 32
@@ -281,11 +293,12 @@ __global__ void __launch_bounds__(256) k_b_apply64(int n, const int *__restrict_
                                                    const double *__restrict__ A, const X *__restrict__ z,
                                                    double *__restrict__ w, int B)
 {
-    const int i = warp_row(), lane = threadIdx.x & 31;
-    if (i >= n) return;
-    double acc[Q];
-    row_dot_b<double, Q, X>(col, A, rp[i], rp[i + 1] - rp[i], z, B, lane, acc);
-    stq<double, Q>(w + (long)i * B + lane * Q, acc);
+    const int lane = threadIdx.x & 31;
+    MGM_CTA_ROWS(i, n) {
+        double acc[Q];
+        row_dot_b<double, Q, X>(col, A, rp[i], rp[i + 1] - rp[i], z, B, lane, acc);
+        stq<double, Q>(w + (long)i * B + lane * Q, acc);
+    }
 }
 
 // part[(blk*cnt + c)*B + b] = sum over this block's rows of V_c[i][b] W[i][b]
@@ -319,30 +332,52 @@ __global__ void __launch_bounds__(256) k_b_multidot(int n, int B, int cnt, const
     }
 }
 
-// out[c*B + b] = sum_blk part[(blk*cnt + c)*B + b]
-__global__ void k_b_reduce(const double *__restrict__ part, int nblk, int cnt, int B, double *__restrict__ out)
+// out[c*B + b] = sum_blk part[(blk*cnt + c)*B + b]; one CTA per (c, 32 columns),
+// 8 warps summing interleaved blocks, then a fixed-order sum of the 8 partials.
+__global__ void __launch_bounds__(256) k_b_reduce(const double *__restrict__ part, int nblk, int cnt, int B,
+                                                  double *__restrict__ out)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= cnt * B) return;
-    const int c = t / B, b = t % B;
+    __shared__ double sm[8][33];
+    const int chunks = (B + 31) / 32;
+    const int c = blockIdx.x / chunks, b = (blockIdx.x % chunks) * 32 + (threadIdx.x & 31), w = threadIdx.x >> 5;
     double s = 0;
-    for (int k = 0; k < nblk; k++) s += part[((long)k * cnt + c) * B + b];
-    out[t] = s;
+    if (b < B)
+        for (int k = w; k < nblk; k += 8) s += part[((long)k * cnt + c) * B + b];
+    sm[w][threadIdx.x & 31] = s;
+    __syncthreads();
+    if (w == 0 && b < B) {
+        double t = 0;
+        for (int q = 0; q < 8; q++) t += sm[q][threadIdx.x];
+        out[c * B + b] = t;
+    }
 }
 
-// W -= sum_c h[c][b] V_c
-__global__ void __launch_bounds__(256) k_b_orth(long nB, int B, int cnt, const double *__restrict__ V, long ldv,
-                                                const double *__restrict__ h, double *__restrict__ W)
+// W -= sum_c h[c][b] V_c, and per-block partial |W_b|^2 of the result:
+// part[blk*B + b].  Grid-stride over elements; the stride is a multiple of B,
+// so a thread keeps one right-hand side.
+__global__ void __launch_bounds__(256) k_b_orth_norm(long nB, int B, int cnt, const double *__restrict__ V, long ldv,
+                                                     const double *__restrict__ h, double *__restrict__ W,
+                                                     double *__restrict__ part)
 {
     __shared__ double hs[kBatchMaxRestart + 1][64];
+    __shared__ double sq[256];
     for (int t = threadIdx.x; t < cnt * B; t += blockDim.x) hs[t / B][t % B] = h[t];
     __syncthreads();
-    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nB) return;
-    const int b = (int)(e % B);
-    double s = W[e];
-    for (int c = 0; c < cnt; c++) s = fma(-hs[c][b], V[c * ldv + e], s);
-    W[e] = s;
+    const int b = threadIdx.x % B;
+    double acc = 0.0;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < nB; e += (long)gridDim.x * blockDim.x) {
+        double s = W[e];
+        for (int c = 0; c < cnt; c++) s = fma(-hs[c][b], V[c * ldv + e], s);
+        W[e] = s;
+        acc = fma(s, s, acc);
+    }
+    sq[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x < B) {
+        double a = 0;
+        for (int q = threadIdx.x; q < (int)blockDim.x; q += B) a += sq[q];
+        part[(long)blockIdx.x * B + threadIdx.x] = a;
+    }
 }
 
 // out = in / nrm_b  (nrm holds |.|^2 when is_sq)
@@ -535,7 +570,7 @@ void batch_free_solver(mgm_batch *b)
         b->v64[l] = BVecs<double>();
         b->v32[l] = BVecs<float>();
     }
-    b->X.release(); b->Bv.release(); b->W.release(); b->V.release(); b->part.release(); b->hsc.release();
+    b->X.release(); b->Bv.release(); b->V.release(); b->part.release(); b->hsc.release();
     b->Z32.release(); b->Z64.release();
     b->V_cols = b->Z_cols32 = b->Z_cols64 = 0;
     b->B = 0;
@@ -584,7 +619,6 @@ std::vector<BLev<T>> blevels(mgm_batch *b)
     return out;
 }
 
-inline int warps_grid(long rows) { return blocks_for(rows * 32, 256); }
 
 template <class T, int Q>
 void bsmooth(mgm_batch *b, BLev<T> &L, bool zero_start)
@@ -594,7 +628,7 @@ void bsmooth(mgm_batch *b, BLev<T> &L, bool zero_start)
     const double lM = 1.05 * L.lmax, lm = L.lmax / b->cheb_ratio;
     const double th = 0.5 * (lM + lm), de = 0.5 * (lM - lm), sig = th / de;
     double rho = 1.0 / sig;
-    k_b_bnd<T, Q><<<warps_grid(L.nbl), 256, 0, s>>>(L.nbl, L.bnd_list, L.rp, L.col, L.A, L.dinv, L.r, L.e, B,
+    k_b_bnd<T, Q><<<rows_grid(L.nbl), 256, 0, s>>>(L.nbl, L.bnd_list, L.rp, L.col, L.A, L.dinv, L.r, L.e, B,
                                                     zero_start ? 1 : 0);
     MGM_LAUNCHED();
     for (int step = 0; step < b->cheb_deg; step++) {
@@ -606,11 +640,11 @@ void bsmooth(mgm_batch *b, BLev<T> &L, bool zero_start)
             c2 = 2.0 * rn / de;
             rho = rn;
         }
-        k_b_cheb<T, Q><<<warps_grid(L.n), 256, 0, s>>>(L.n, L.rp, L.col, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d,
+        k_b_cheb<T, Q><<<rows_grid(L.n), 256, 0, s>>>(L.n, L.rp, L.col, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d,
                                                        B, (T)c1, (T)c2, step == 0 ? 1 : 0);
         MGM_LAUNCHED();
         std::swap(L.e, L.e2);
-        k_b_bnd<T, Q><<<warps_grid(L.nbl), 256, 0, s>>>(L.nbl, L.bnd_list, L.rp, L.col, L.A, L.dinv, L.r, L.e, B, 0);
+        k_b_bnd<T, Q><<<rows_grid(L.nbl), 256, 0, s>>>(L.nbl, L.bnd_list, L.rp, L.col, L.A, L.dinv, L.r, L.e, B, 0);
         MGM_LAUNCHED();
     }
 }
@@ -631,12 +665,12 @@ void bvcycle(mgm_batch *b, std::vector<BLev<T>> &Ls, int l)
     MGM_CUDA(cudaMemsetAsync(L.e, 0, sizeof(T) * (size_t)L.n * B, s));
     bsmooth<T, Q>(b, L, true);
     BLev<T> &C = Ls[l + 1];
-    k_b_residual<T, Q><<<warps_grid(L.n), 256, 0, s>>>(L.n, L.rp, L.col, L.A, L.btag, L.r, L.e, L.q, B);
+    k_b_residual<T, Q><<<rows_grid(L.n), 256, 0, s>>>(L.n, L.rp, L.col, L.A, L.btag, L.r, L.e, L.q, B);
     MGM_LAUNCHED();
-    k_b_restrict<T, Q><<<warps_grid(C.n), 256, 0, s>>>(C.n, C.r_rp, C.r_col, C.r_w, L.q, C.r, B);
+    k_b_restrict<T, Q><<<rows_grid(C.n), 256, 0, s>>>(C.n, C.r_rp, C.r_col, C.r_w, L.q, C.r, B);
     MGM_LAUNCHED();
     bvcycle<T, Q>(b, Ls, l + 1);
-    k_b_prolong<T, Q><<<warps_grid(L.n), 256, 0, s>>>(L.n, L.p_rp, L.p_col, L.p_w, C.e, L.e, B);
+    k_b_prolong<T, Q><<<rows_grid(L.n), 256, 0, s>>>(L.n, L.p_rp, L.p_col, L.p_w, C.e, L.e, B);
     MGM_LAUNCHED();
     bsmooth<T, Q>(b, L, false);
 }
@@ -652,7 +686,7 @@ void ensure_vecs(mgm_batch *b, int B, int m)
         if (V.r.n != nB) for (DBuf<T> *x : {&V.r, &V.e, &V.e2, &V.d, &V.q}) { x->alloc(nB); x->zero(b->s); }
     }
     const size_t nB = (size_t)b->L[0].n * B;
-    if (b->X.n != nB) { b->X.alloc(nB); b->Bv.alloc(nB); b->W.alloc(nB); }
+    if (b->X.n != nB) { b->X.alloc(nB); b->Bv.alloc(nB); }
     if (b->V_cols < m + 1) { b->V.alloc(nB * (m + 1)); b->V_cols = m + 1; }
     if constexpr (sizeof(T) == 4) { if (b->Z_cols32 < m) { b->Z32.alloc(nB * m); b->Z_cols32 = m; } }
     else { if (b->Z_cols64 < m) { b->Z64.alloc(nB * m); b->Z_cols64 = m; } }
@@ -680,11 +714,11 @@ void bfgmres(mgm_batch *b, int nrhs, int *vcycles, double *rel_res)
     auto Ls = blevels<T>(b);
     T *Z;
     if constexpr (sizeof(T) == 8) Z = b->Z64.p; else Z = b->Z32.p;
-    double *V = b->V.p, *W = b->W.p, *X = b->X.p, *hp = b->h_pinned, *dsc = b->hsc.p;
+    double *V = b->V.p, *X = b->X.p, *hp = b->h_pinned, *dsc = b->hsc.p;
     const int gres = dot_grid(n);
     const int gdot = (int)std::max(1L, std::min<long>((n + (256 / B) - 1) / (256 / B), 148L * 8));
-    if (b->part.n < (size_t)gres * 2 * B || b->part.n < (size_t)gdot * 8 * B)
-        b->part.alloc(std::max((size_t)gres * 2 * B, (size_t)gdot * 8 * B) * 2);
+    const size_t part_need = std::max({(size_t)gres * 2 * B, (size_t)gdot * 8 * B, (size_t)148 * 16 * B});
+    if (b->part.n < part_need) b->part.alloc(part_need);
     std::vector<double> bnorm(B, 0.0), relres(B, 0.0);
     std::vector<double> H((size_t)B * (m + 1) * m), cs((size_t)B * m), sn((size_t)B * m), g((size_t)B * (m + 1));
     long long vc = 0;
@@ -695,14 +729,14 @@ void bfgmres(mgm_batch *b, int nrhs, int *vcycles, double *rel_res)
             const int cc = std::min(8, cnt - c0);
             k_b_multidot<<<gdot, 256, 0, s>>>(n, B, cc, Vb + (long)c0 * nB, nB, Wv, b->part.p);
             MGM_LAUNCHED();
-            k_b_reduce<<<blocks_for((long)cc * B, 256), 256, 0, s>>>(b->part.p, gdot, cc, B, dsc + off + c0 * B);
+            k_b_reduce<<<cc * ((B + 31) / 32), 256, 0, s>>>(b->part.p, gdot, cc, B, dsc + off + c0 * B);
             MGM_LAUNCHED();
         }
     };
     for (int restart = 0; restart <= max_restarts; restart++) {
         k_b_resid64<double, Q><<<gres, 256, 0, s>>>(n, L0.rp.p, L0.col.p, L0.A64.p, b->Bv.p, X, V, b->part.p, B);
         MGM_LAUNCHED();
-        k_b_reduce<<<blocks_for(2L * B, 256), 256, 0, s>>>(b->part.p, gres, 2, B, dsc);
+        k_b_reduce<<<2 * ((B + 31) / 32), 256, 0, s>>>(b->part.p, gres, 2, B, dsc);
         MGM_LAUNCHED();
         MGM_CUDA(cudaMemcpyAsync(hp, dsc, sizeof(double) * 2 * B, cudaMemcpyDeviceToHost, s));
         MGM_CUDA(cudaStreamSynchronize(s));
@@ -731,20 +765,37 @@ void bfgmres(mgm_batch *b, int nrhs, int *vcycles, double *rel_res)
             vc++;
             k_b_convert<T, T><<<blocks_for(nB, 256), 256, 0, s>>>(nB, cyc[0].e, Z + (long)j * nB);
             MGM_LAUNCHED();
-            k_b_apply64<T, Q><<<warps_grid(n), 256, 0, s>>>(n, L0.rp.p, L0.col.p, L0.A64.p, Z + (long)j * nB, W, B);
+            // w = A z_j, written into the slot of V_{j+1}; classical Gram-Schmidt with
+            // the norm of w in the same pass, a second pass only when the first one
+            // cancelled more than 1 - 1/sqrt(2) of |w| for some right-hand side
+            // (the Daniel-Gragg-Kaufman-Stewart test)
+            double *Wn = V + (long)(j + 1) * nB;
+            k_b_apply64<T, Q><<<rows_grid(n), 256, 0, s>>>(n, L0.rp.p, L0.col.p, L0.A64.p, Z + (long)j * nB, Wn, B);
             MGM_LAUNCHED();
             const int h1 = 0, h2 = (kBatchMaxRestart + 2) * B, h3 = 2 * (kBatchMaxRestart + 2) * B;
-            multidot(j + 1, V, W, h1);
-            k_b_orth<<<blocks_for(nB, 256), 256, 0, s>>>(nB, B, j + 1, V, nB, dsc + h1, W);
+            multidot(j + 2, V, Wn, h1);  // dots with V_0..V_j, then |w|^2
+            const int gorth = (int)std::min<long>(blocks_for(nB, 256), 148L * 16);
+            k_b_orth_norm<<<gorth, 256, 0, s>>>(nB, B, j + 1, V, nB, dsc + h1, Wn, b->part.p);
             MGM_LAUNCHED();
-            multidot(j + 1, V, W, h2);
-            k_b_orth<<<blocks_for(nB, 256), 256, 0, s>>>(nB, B, j + 1, V, nB, dsc + h2, W);
-            MGM_LAUNCHED();
-            multidot(1, W, W, h3);
-            k_b_scale<<<blocks_for(nB, 256), 256, 0, s>>>(nB, B, W, V + (long)(j + 1) * nB, dsc + h3, 1);
+            k_b_reduce<<<(B + 31) / 32, 256, 0, s>>>(b->part.p, gorth, 1, B, dsc + h3);
             MGM_LAUNCHED();
             MGM_CUDA(cudaMemcpyAsync(hp, dsc, sizeof(double) * (h3 + B), cudaMemcpyDeviceToHost, s));
             MGM_CUDA(cudaStreamSynchronize(s));
+            bool again = false;
+            for (int q = 0; q < B; q++)
+                if (hp[h3 + q] < 0.5 * hp[h1 + (j + 1) * B + q]) again = true;
+            for (int i = 0; i <= j; i++) for (int q = 0; q < B; q++) hp[h2 + i * B + q] = 0.0;
+            if (again) {
+                multidot(j + 1, V, Wn, h2);
+                k_b_orth_norm<<<gorth, 256, 0, s>>>(nB, B, j + 1, V, nB, dsc + h2, Wn, b->part.p);
+                MGM_LAUNCHED();
+                k_b_reduce<<<(B + 31) / 32, 256, 0, s>>>(b->part.p, gorth, 1, B, dsc + h3);
+                MGM_LAUNCHED();
+                MGM_CUDA(cudaMemcpyAsync(hp + h2, dsc + h2, sizeof(double) * (h3 - h2 + B), cudaMemcpyDeviceToHost, s));
+                MGM_CUDA(cudaStreamSynchronize(s));
+            }
+            k_b_scale<<<blocks_for(nB, 256), 256, 0, s>>>(nB, B, Wn, Wn, dsc + h3, 1);
+            MGM_LAUNCHED();
             double worst = 0;
             for (int q = 0; q < B; q++) {
                 double *col = &H[((size_t)q * m + j) * (m + 1)];

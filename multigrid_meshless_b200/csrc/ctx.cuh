@@ -36,6 +36,11 @@ struct Level {
     // compact FP32-path indices (int16 offsets)
     DBuf<short> off16, r_off16, p_off16;
     bool off_ok = false, r_off_ok = false, p_off_ok = false;
+    // the compact operator again, tile-major ([ld / kTileRows][k][kTileRows],
+    // rows padded to ld), streamed tile by tile into shared memory by bulk copies
+    DBuf<float> A32t;
+    DBuf<short> off16t;
+    int ldt = 0;
     // reference-mode state
     DBuf<double> p, ptmp, src, res;
     // solver work vectors
@@ -71,9 +76,11 @@ struct mgm_ctx {
     DBuf<float> Z32;
     int last_iters = 0;
     double last_relres = 0;
-    long long vcycles_in_solve = 0;
-    double last_learned_alpha = 0;
-    int warm_smooth_steps = 3;        // Chebyshev steps that clean the learned direction    // step length the last solve took along the learned direction   // V-cycles of the last solve (iterations minus learned directions)
+    long long vcycles_in_solve = 0;   // V-cycles of the last solve
+    double last_learned_alpha = 0;    // step length the last solve took along the learned direction
+    int warm_smooth_steps = 3;        // Chebyshev steps that clean the learned direction
+    bool use_tma = true;              // tile-streamed level kernels where a level has them
+    DBuf<int> tma_err;                // set by a tile-streamed kernel whose bounded wait ran out
     double *h_pinned = nullptr;
     SmootherProfile prof;
     // captured V-cycles, [0] FP64, [1] FP32 (re-captured when solver settings change)

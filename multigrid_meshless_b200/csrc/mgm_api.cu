@@ -110,6 +110,19 @@ __global__ void k_make_offsets(int n, int k, const int *__restrict__ gidx, const
     off[t] = (short)d;
 }
 
+// tile-major copy of an ELL array: out[(t*k + j)*kTileRows + r] = in[j][t*kTileRows + r], zero past row n
+template <class T>
+__global__ void k_tile_major(int n, int k, int ld, const T *__restrict__ in, T *__restrict__ out)
+{
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long)k * ld) return;
+    const int r = (int)(e % kTileRows);
+    const long tj = e / kTileRows;
+    const int j = (int)(tj % k);
+    const long row = (tj / k) * kTileRows + r;
+    out[e] = row < n ? in[(long)j * n + row] : T(0);
+}
+
 // compact copies of the boundary rows of the pinned operator: out[w][j] = A[j][list[w]]
 __global__ void k_gather_rows(int nbl, const int *__restrict__ list, int n, int k, const int *__restrict__ idx,
                               const double *__restrict__ A, int *__restrict__ bidx, double *__restrict__ bA64,
@@ -210,6 +223,9 @@ std::vector<SolveLevel<float>> solve_levels<float>(mgm_ctx *c)
             S.off = L.off_ok ? L.off16.p : nullptr;
             S.r_off = L.r_off_ok ? L.r_off16.p : nullptr; S.r_base = L.rpts.p;
             S.p_off = L.p_off_ok ? L.p_off16.p : nullptr; S.p_base = L.ppts.p;
+            if (c->use_tma && L.ldt > 0) {
+                S.At = L.A32t.p; S.offt = L.off16t.p; S.ldt = L.ldt; S.tma_err = c->tma_err.p;
+            }
         }
         out.push_back(S);
     }
@@ -445,6 +461,17 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
         for (int i = 0; i < j_done; i++) hp[i] = y[i];
         MGM_CUDA(cudaMemcpyAsync(c->kscal.p, hp, sizeof(double) * j_done, cudaMemcpyHostToDevice, s));
         combine<T>(n, j_done, Z, ld, c->kscal.p, p, s);
+    }
+    if constexpr (sizeof(T) == 4) {
+        if (c->tma_err.p) {
+            int h_err = 0;
+            c->tma_err.download(&h_err, 1, s);
+            MGM_CUDA(cudaStreamSynchronize(s));
+            if (h_err) {
+                c->tma_err.zero(s);
+                throw Error{MGM_ERR_TIMEOUT, "Poisson solve: a tile-streamed level kernel timed out waiting for its copies"};
+            }
+        }
     }
     c->last_iters = (int)c->vcycles_in_solve;  // V-cycles (learned directions are not V-cycles)
     c->last_relres = relres;
@@ -907,6 +934,21 @@ void prepare_solver(mgm_ctx *c)
             L.r_off_ok = h_ovf[1] == 0;
             L.p_off_ok = h_ovf[2] == 0;
         }
+        // tile-streamed copy of the compact operator for the large levels
+        L.ldt = 0;
+        L.A32t.release();
+        L.off16t.release();
+        if (L.off_ok && L.n >= kTileMinRows && L.k <= kTileMaxK) {
+            const int ld = (L.n + kTileRows - 1) / kTileRows * kTileRows;
+            L.A32t.alloc((size_t)L.k * ld);
+            L.off16t.alloc((size_t)L.k * ld);
+            const long tot = (long)L.k * ld;
+            k_tile_major<float><<<blocks_for(tot, 256), 256, 0, s>>>(L.n, L.k, ld, L.A32.p, L.A32t.p);
+            MGM_LAUNCHED();
+            k_tile_major<short><<<blocks_for(tot, 256), 256, 0, s>>>(L.n, L.k, ld, L.off16.p, L.off16t.p);
+            MGM_LAUNCHED();
+            L.ldt = ld;
+        }
         for (DBuf<double> *b : {&L.p, &L.ptmp, &L.src, &L.res, &L.r64, &L.e64, &L.e64b, &L.d64, &L.q64}) { b->alloc(L.n); b->zero(s); }
         for (DBuf<float> *b : {&L.r32, &L.e32, &L.e32b, &L.d32, &L.q32}) { b->alloc(L.n); b->zero(s); }
     }
@@ -924,6 +966,8 @@ void prepare_solver(mgm_ctx *c)
     for (DBuf<double> *b : {&c->u, &c->v, &c->w, &c->u_new, &c->v_new, &c->w_new, &c->dpdn}) { b->alloc(n0); b->zero(s); }
     c->partial.alloc(blocks_for(n0, 256) + 8);
     c->scal.alloc(8);
+    c->tma_err.alloc(1);
+    c->tma_err.zero(s);
     alloc_solver_buffers(c);
     MGM_CUDA(cudaStreamSynchronize(s));
     c->setup_done = true;
@@ -1230,6 +1274,16 @@ int mgm_use_compact(mgm_ctx *c, int enable)
         MGM_CUDA(cudaStreamSynchronize(c->s));
         drop_graphs(c);
         c->compact = enable != 0;
+    });
+}
+
+int mgm_use_tiled(mgm_ctx *c, int enable)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+        drop_graphs(c);
+        c->use_tma = enable != 0;
     });
 }
 

@@ -198,6 +198,277 @@ __global__ void __launch_bounds__(256) k_prolong_o(int n, int k, const short *__
     ef[i] += ell_row_dot_o(off, pw, ec, n, k, i, base[i]) - shift;
 }
 
+// ---------------------------------------------------------------------------
+// tile-streamed level kernels (FP32 compact operator)
+//
+// The operator is stored tile-major ([tile][k][kTileRows]: a tile's weights,
+// and separately its int16 offsets, are contiguous).  A persistent CTA walks
+// tiles of kTileRows rows; for each tile one thread issues two bulk
+// asynchronous copies (cp.async.bulk, the TMA engine's 1-D form) into shared
+// memory, completing on an mbarrier; two stages alternate, so the next tile's
+// operator streams in while this tile's rows gather their neighbours.  A
+// thread then reads its row's stencil from shared memory and issues its
+// neighbour gathers back to back.  The products are summed in slot order, as
+// in k_cheb_o / k_residual_o, so the results are the same bits.
+//
+// Every mbarrier wait is bounded: on time-out the CTA sets *err, waits (again
+// bounded) for the copies it still has in flight, and stops.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity)
+{
+    for (int it = 0; it < (1 << 20); it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// global -> shared bulk copy; addresses 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// MODE 0: Chebyshev step (as k_cheb_o); MODE 1: residual (as k_residual_o)
+template <int MODE>
+__global__ void __launch_bounds__(kTileRows) k_level_tiled(int n, int k, const short *__restrict__ offt,
+                                                           const float *__restrict__ At, const float *__restrict__ dinv,
+                                                           const uint8_t *__restrict__ btag,
+                                                           const float *__restrict__ r, const float *__restrict__ e,
+                                                           float *__restrict__ out, float *__restrict__ d, float c1,
+                                                           float c2, int first, int *err)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int ok_flag;
+    const int tid = threadIdx.x;
+    const int ntiles = (n + kTileRows - 1) / kTileRows;
+    const unsigned a_bytes = kTileRows * sizeof(float), o_bytes = kTileRows * sizeof(short);
+    const size_t stage = (size_t)k * (a_bytes + o_bytes);
+    // stage st: weights at smem + st * stage, offsets after them
+    auto As = [&](int st) { return (float *)(smem + st * stage); };
+    auto Os = [&](int st) { return (short *)(smem + st * stage + (size_t)k * a_bytes); };
+    unsigned pending = 0;  // bit st: stage st has copies in flight (tracked by thread 0)
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    auto issue = [&](int tile, int st) {
+        if (tid == 0) {
+            mbar_expect_tx(&bar[st], (unsigned)stage);
+            const long t0 = (long)tile * k * kTileRows;  // tile-major: the tile's [k][kTileRows] block is contiguous
+            bulk_g2s(As(st), At + t0, (unsigned)k * a_bytes, &bar[st]);
+            bulk_g2s(Os(st), offt + t0, (unsigned)k * o_bytes, &bar[st]);
+        }
+        pending |= 1u << st;
+    };
+    int it = 0;
+    if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    if (blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+        const int st = it & 1;
+        const unsigned parity = (unsigned)((it >> 1) & 1);
+        if (tid == 0) ok_flag = mbar_wait_bounded(&bar[st], parity) ? 1 : 0;
+        __syncthreads();
+        if (!ok_flag) {
+            if (tid == 0) {
+                atomicOr(err, 1);
+                // the other stage may still have a copy in flight
+                const int o = st ^ 1;
+                if (pending & (1u << o)) mbar_wait_bounded(&bar[o], (unsigned)(((it + 1) >> 1) & 1));
+            }
+            return;
+        }
+        mbar_try_wait(&bar[st], parity);  // completed: acquires the copied data for this thread
+        pending &= ~(1u << st);
+        const int i = tile * kTileRows + tid;
+        if (i < n) {
+            const float ei = e[i];
+            if (btag[i]) {
+                out[i] = MODE == 0 ? ei : 0.f;
+            } else {
+                const float *a = As(st) + tid;
+                const short *o = Os(st) + tid;
+                float s = 0.f;
+                int j = 0;
+                for (; j + 8 <= k; j += 8) {
+                    float av[8], xv[8];
+#pragma unroll
+                    for (int q = 0; q < 8; q++) {
+                        av[q] = a[(j + q) * kTileRows];
+                        xv[q] = __ldg(e + i + (int)o[(j + q) * kTileRows]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 8; q++) s += av[q] * xv[q];
+                }
+                for (; j < k; j++) s += a[j * kTileRows] * e[i + (int)o[j * kTileRows]];
+                if (MODE == 0) {
+                    const float q = r[i] - s;
+                    const float di = first ? c2 * dinv[i] * q : c1 * d[i] + c2 * dinv[i] * q;
+                    d[i] = di;
+                    out[i] = ei + di;
+                } else {
+                    out[i] = r[i] - s;
+                }
+            }
+        }
+        __syncthreads();  // every thread is done with stage st
+        if (tile + 2 * gridDim.x < ntiles) issue(tile + 2 * gridDim.x, st);
+    }
+}
+
+// Register variant for k <= 32: a thread copies its row's whole stencil from
+// shared memory into registers, the CTA syncs, the freed stage starts the
+// copies of the tile after next, and the threads issue all k neighbour
+// gathers at once (k gathers in flight per row instead of 8).
+template <int MODE>
+__global__ void __launch_bounds__(kTileRows, 2) k_level_tiled_r(int n, int k, const short *__restrict__ offt,
+                                                              const float *__restrict__ At,
+                                                              const float *__restrict__ dinv,
+                                                              const uint8_t *__restrict__ btag,
+                                                              const float *__restrict__ r,
+                                                              const float *__restrict__ e, float *__restrict__ out,
+                                                              float *__restrict__ d, float c1, float c2, int first,
+                                                              int *err)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int ok_flag;
+    const int tid = threadIdx.x;
+    const int ntiles = (n + kTileRows - 1) / kTileRows;
+    const unsigned a_bytes = kTileRows * sizeof(float), o_bytes = kTileRows * sizeof(short);
+    const size_t stage = (size_t)k * (a_bytes + o_bytes);
+    auto As = [&](int st) { return (float *)(smem + st * stage); };
+    auto Os = [&](int st) { return (short *)(smem + st * stage + (size_t)k * a_bytes); };
+    unsigned pending = 0;  // bit st: stage st has copies in flight (tracked by thread 0)
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    auto issue = [&](int tile, int st) {
+        if (tid == 0) {
+            mbar_expect_tx(&bar[st], (unsigned)stage);
+            const long t0 = (long)tile * k * kTileRows;
+            bulk_g2s(As(st), At + t0, (unsigned)k * a_bytes, &bar[st]);
+            bulk_g2s(Os(st), offt + t0, (unsigned)k * o_bytes, &bar[st]);
+        }
+        pending |= 1u << st;
+    };
+    if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    if (blockIdx.x + gridDim.x < ntiles) issue(blockIdx.x + gridDim.x, 1);
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+        const int st = it & 1;
+        const unsigned parity = (unsigned)((it >> 1) & 1);
+        if (tid == 0) ok_flag = mbar_wait_bounded(&bar[st], parity) ? 1 : 0;
+        __syncthreads();
+        if (!ok_flag) {
+            if (tid == 0) {
+                atomicOr(err, 1);
+                const int o = st ^ 1;
+                if (pending & (1u << o)) mbar_wait_bounded(&bar[o], (unsigned)(((it + 1) >> 1) & 1));
+            }
+            return;
+        }
+        mbar_try_wait(&bar[st], parity);
+        pending &= ~(1u << st);
+        float a[32];
+        int o[32];
+        const float *as = As(st);
+        const short *os = Os(st);
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            a[j] = j < k ? as[j * kTileRows + tid] : 0.f;
+            o[j] = j < k ? (int)os[j * kTileRows + tid] : 0;
+        }
+        __syncthreads();  // stage st is free again
+        if (tile + 2 * (int)gridDim.x < ntiles) issue(tile + 2 * gridDim.x, st);
+        const int i = tile * kTileRows + tid;
+        if (i < n) {
+            const float ei = e[i];
+            if (btag[i]) {
+                out[i] = MODE == 0 ? ei : 0.f;
+            } else {
+                float x[32];
+#pragma unroll
+                for (int j = 0; j < 32; j++) x[j] = j < k ? __ldg(e + i + o[j]) : 0.f;
+                float s = 0.f;
+#pragma unroll
+                for (int j = 0; j < 32; j++)
+                    if (j < k) s += a[j] * x[j];
+                if (MODE == 0) {
+                    const float q = r[i] - s;
+                    const float di = first ? c2 * dinv[i] * q : c1 * d[i] + c2 * dinv[i] * q;
+                    d[i] = di;
+                    out[i] = ei + di;
+                } else {
+                    out[i] = r[i] - s;
+                }
+            }
+        }
+    }
+}
+
+template <class K>
+static int tiled_grid(K kernel, int n, size_t smem)
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        MGM_CUDA(cudaGetDevice(&dev));
+        MGM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    int per_sm = 0;
+    MGM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTileRows, smem));
+    const int tiles = (n + kTileRows - 1) / kTileRows;
+    return std::max(1, std::min(tiles, sms * std::max(1, per_sm)));
+}
+
+template <int MODE>
+static void launch_tiled(const SolveLevel<float> &L, const float *e, float *out, float c1, float c2, int first,
+                         cudaStream_t s)
+{
+    const size_t per_stage = (size_t)L.k * kTileRows * (sizeof(float) + sizeof(short));
+    if (L.k <= 32) {
+        MGM_CUDA(cudaFuncSetAttribute(k_level_tiled_r<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(2 * 32 * kTileRows * (sizeof(float) + sizeof(short)))));
+        k_level_tiled_r<MODE><<<tiled_grid(k_level_tiled_r<MODE>, L.n, 2 * per_stage), kTileRows, 2 * per_stage, s>>>(
+            L.n, L.k, L.offt, L.At, L.dinv, L.btag, L.r, e, out, L.d, c1, c2, first, L.tma_err);
+    } else {
+        MGM_CUDA(cudaFuncSetAttribute(k_level_tiled<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(2 * kTileMaxK * kTileRows * (sizeof(float) + sizeof(short)))));
+        k_level_tiled<MODE><<<tiled_grid(k_level_tiled<MODE>, L.n, 2 * per_stage), kTileRows, 2 * per_stage, s>>>(
+            L.n, L.k, L.offt, L.At, L.dinv, L.btag, L.r, e, out, L.d, c1, c2, first, L.tma_err);
+    }
+    MGM_LAUNCHED();
+}
+
 // e = inv * r, one warp per row of the dense coarsest inverse
 template <class T>
 __global__ void __launch_bounds__(256) k_dense_solve(int n, const T *__restrict__ inv, const T *__restrict__ r,
@@ -278,7 +549,9 @@ static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, 
         }
         if (prof) prof->mark(s);
         if constexpr (sizeof(T) == 4) {
-            if (L.off) {
+            if (L.At) {
+                launch_tiled<0>(L, L.e, L.e2, (float)c1, (float)c2, step == 0 ? 1 : 0, s);
+            } else if (L.off) {
                 k_cheb_o<<<nb, 256, 0, s>>>(L.n, L.k, L.off, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d, (float)c1,
                                             (float)c2, step == 0 ? 1 : 0);
             } else {
@@ -313,9 +586,12 @@ static void vcycle_rec(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs,
     smooth(L, deg, ratio, true, s, lp);
     SolveLevel<T> &C = Ls[l + 1];
     if constexpr (sizeof(T) == 4) {
-        if (L.off) k_residual_o<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.off, L.A, L.btag, L.r, L.e, L.q);
-        else k_residual<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.idx, L.A, L.btag, L.r, L.e, L.q);
-        MGM_LAUNCHED();
+        if (L.At) launch_tiled<1>(L, L.e, L.q, 0.f, 0.f, 0, s);
+        else {
+            if (L.off) k_residual_o<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.off, L.A, L.btag, L.r, L.e, L.q);
+            else k_residual<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.idx, L.A, L.btag, L.r, L.e, L.q);
+            MGM_LAUNCHED();
+        }
         if (C.r_off) k_restrict_o<<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.kr, C.r_off, C.r_base, C.r_w, C.btag, L.q, C.r);
         else k_restrict<T><<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
         MGM_LAUNCHED();

@@ -76,7 +76,19 @@ struct SolveLevel {
     const int *r_base = nullptr;
     const short *p_off = nullptr;
     const int *p_base = nullptr;
+    // tile-streamed copy of (A, off), tile-major over ldt padded rows (FP32 path; used when non-null)
+    const float *At = nullptr;
+    const short *offt = nullptr;
+    int ldt = 0;
+    int *tma_err = nullptr;
 };
+
+// rows per tile of the tile-streamed level kernels
+constexpr int kTileRows = 256;
+// smallest level the tile-streamed kernels are used on (smaller levels fit in L2)
+constexpr int kTileMinRows = 65536;
+// largest stencil width the tile-streamed kernels take (two stages of k x 1.5 KB in shared memory)
+constexpr int kTileMaxK = 64;
 
 template <class T>
 struct CoarseSolve {

@@ -28,7 +28,7 @@ inline MonoDev to_dev(const Monomials &m)
     return d;
 }
 
-// A group of `size` consecutive threads starting at thread `base` of the CTA.
+// A group of `size` consecutive threads of a CTA (tid: the thread's rank in it).
 // bar 0: the whole CTA (__syncthreads); otherwise named barrier `bar`.
 struct Team {
     int tid, size, bar;
@@ -89,7 +89,8 @@ __device__ inline void build_aug(const Team &tm, int m, int np, int dim, int phs
 
 // In-place Gauss-Jordan; on return aug[perm[i]][N + j] holds inverse[i][j].
 // Elimination by column ownership: a thread keeps the pivot-row entry of its
-// column in a register and sweeps the rows.
+// column in a register and sweeps the rows (all of them, or every R-th row when
+// the team has R >= 2 threads per column).
 __device__ inline void gauss_jordan(const Team &tm, double *aug, int *perm, double *t, int N)
 {
     const int W2 = 2 * N;
@@ -104,12 +105,26 @@ __device__ inline void gauss_jordan(const Team &tm, double *aug, int *perm, doub
         const double piv = pr[i];
         for (int j = tm.tid; j < N; j += tm.size) t[j] = (j == i) ? 0.0 : MGM_DIV(aug[perm[j] * W2 + i], piv);
         tm.sync();
-        for (int c = tm.tid; c < W2; c += tm.size) {
-            const double pc = pr[c];
-            for (int j = 0; j < N; j++) {
-                if (j == i) continue;
-                double *rj = aug + perm[j] * W2;
-                rj[c] = MGM_SUB(rj[c], MGM_MUL(pc, t[j]));
+        if (tm.size >= 2 * W2) {
+            // enough threads for several row groups per column
+            const int R = tm.size / W2;
+            if (tm.tid < R * W2) {
+                const int c = tm.tid % W2;
+                const double pc = pr[c];
+                for (int j = tm.tid / W2; j < N; j += R) {
+                    if (j == i) continue;
+                    double *rj = aug + perm[j] * W2;
+                    rj[c] = MGM_SUB(rj[c], MGM_MUL(pc, t[j]));
+                }
+            }
+        } else {
+            for (int c = tm.tid; c < W2; c += tm.size) {
+                const double pc = pr[c];
+                for (int j = 0; j < N; j++) {
+                    if (j == i) continue;
+                    double *rj = aug + perm[j] * W2;
+                    rj[c] = MGM_SUB(rj[c], MGM_MUL(pc, t[j]));
+                }
             }
         }
         tm.sync();
