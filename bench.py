@@ -53,6 +53,12 @@ def parse():
                     help="steps per episode from rest (the explicit scheme is unstable beyond ~12 steps at 1M nodes)")
     ap.add_argument("--sample-m", type=int, default=128, help="cavity size of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start measurement")
+    ap.add_argument("--learn-episodes", type=int, default=12, help="training episodes (Re ~ U[100, 1000])")
+    ap.add_argument("--learn-iters", type=int, default=400, help="Adam iterations of the GPU training")
+    ap.add_argument("--workload", choices=["cavity", "annulus", "cube", "shell-batch"], default="cavity",
+                    help="cavity: the headline (1M-node cavity); annulus / cube / shell-batch: the other configs, "
+                         "each printing its own line")
     return ap.parse_args()
 
 
@@ -218,6 +224,73 @@ def ncu_traffic():
 
 
 # ---------------------------------------------------------------------------
+# learned warm start: trained on the GPU on plain-solver episodes, evaluated on
+# held-out episodes with and without it
+# ---------------------------------------------------------------------------
+def learned_arm(a, mg, mgm, n):
+    import ctypes as C
+
+    import numpy as np
+
+    from multigrid_meshless_b200 import _lib
+    from multigrid_meshless_b200.clouds import uniform
+    L = _lib.load()
+    ep_len = a.episode
+    n_train, n_eval = a.learn_episodes, 2
+    res_train = 100.0 + 900.0 * uniform(7, 0, n_train)
+    res_eval = 100.0 + 900.0 * uniform(7, 1, n_eval)
+    t0 = time.perf_counter()
+    _lib.check(L.mgm_mpnn_init(mg.h, 1, n_train * ep_len))
+    for Re in res_train:
+        mg.set_flow(Re=float(Re), courant=a.courant)
+        mg.apply_bc(mgm.BC_LID)
+        _lib.check(L.mgm_mpnn_collect(mg.h, mgm.MODE_FP32_IR, ep_len))
+    collect_s = time.perf_counter() - t0
+    cnt = C.c_int()
+    _lib.check(L.mgm_mpnn_dataset_size(mg.h, C.byref(cnt)))
+    n_fit = max(1, cnt.value - ep_len)
+    losses = np.zeros(a.learn_iters)
+    t0 = time.perf_counter()
+    _lib.check(L.mgm_mpnn_train(mg.h, 0, n_fit, a.learn_iters, 1e-3, 1, losses.ctypes.data))
+    train_s = time.perf_counter() - t0
+    held = C.c_double()
+    _lib.check(L.mgm_mpnn_eval(mg.h, n_fit, cnt.value - n_fit, C.byref(held)))
+    out = {"episodes_train": int(n_train), "steps_train": int(cnt.value), "episodes_eval": n_eval,
+           "steps_eval": n_eval * ep_len, "Re_train": "U[100, 1000] (seeded)",
+           "Re_eval": [float(r) for r in res_eval], "adam_iters": a.learn_iters,
+           "loss_first": float(losses[:20].mean()), "loss_last": float(losses[-20:].mean()),
+           "loss_held_out_samples": float(held.value), "collect_s": collect_s, "train_s": train_s}
+    arms = {}
+    pressures = {}
+    for name, mode, warm in (("fp64", mgm.MODE_FP64, 0), ("fp32", mgm.MODE_FP32_IR, 0),
+                             ("learned_fp32", mgm.MODE_FP32_IR, 1)):
+        _lib.check(L.mgm_set_warm_start(mg.h, warm))
+        tot = [0.0, 0.0, 0]
+        ps = []
+        for Re in res_eval:
+            mg.set_flow(Re=float(Re), courant=a.courant)
+            mg.apply_bc(mgm.BC_LID)
+            ms_, pms_, vc_, _ = mg.run_steps(mode, ep_len)
+            tot[0] += ms_; tot[1] += pms_; tot[2] += vc_
+            ps.append(mg.get_field("p"))
+        steps = n_eval * ep_len
+        arms[name] = {"ms_per_step": tot[0] / steps, "poisson_ms": tot[1] / steps, "vcycles_per_step": tot[2] / steps}
+        pressures[name] = ps
+    _lib.check(L.mgm_set_warm_start(mg.h, 0))
+    mg.set_flow(Re=a.Re, courant=a.courant)
+    rel = lambda x, y: max(float(np.linalg.norm(u - v) / np.linalg.norm(v)) for u, v in zip(x, y))
+    out.update(arms)
+    out["vcycles_saved_per_step"] = arms["fp32"]["vcycles_per_step"] - arms["learned_fp32"]["vcycles_per_step"]
+    out["speedup_learned_fp32_vs_fp64"] = arms["fp64"]["ms_per_step"] / arms["learned_fp32"]["ms_per_step"]
+    out["speedup_fp32_vs_fp64"] = arms["fp64"]["ms_per_step"] / arms["fp32"]["ms_per_step"]
+    out["pressure_rel_l2_learned_fp32_vs_fp64"] = rel(pressures["learned_fp32"], pressures["fp64"])
+    out["pressure_rel_l2_fp32_vs_fp64"] = rel(pressures["fp32"], pressures["fp64"])
+    out["note"] = ("held-out episodes of a.episode steps from rest at unseen Re; the FP64 arm is the plain FP64 "
+                   "V-cycle solve, pressures compared after each episode")
+    return out
+
+
+# ---------------------------------------------------------------------------
 def run_ours(a, rank, world, local_rank):
     import numpy as np
 
@@ -321,6 +394,9 @@ def run_ours(a, rank, world, local_rank):
     finite = bool(np.all(np.isfinite(bufs[0].array)))
     for b in bufs:
         b.free()
+    learned = None
+    if rank == 0 and not a.no_learned:
+        learned = learned_arm(a, mg, mgm, n)
 
     line = None
     if rank == 0:
@@ -352,7 +428,9 @@ def run_ours(a, rank, world, local_rank):
             "steady_err_last": err,
             "plain_fp64": {"steps_per_s": a.steps * world / (plain_ms / 1e3), "ms_per_step": plain_ms / a.steps,
                            "poisson_ms": plain_pms / a.steps, "vcycles_per_step": plain_vc / a.steps},
-            "learned_warm_start": None,
+            "learned_warm_start": learned,
+            "headline_arm": ("FP32 V-cycle inside FP64 FGMRES without the learned warm start (the faster arm: "
+                             "the measured learned arm is in learned_warm_start)"),
             "e2e": {"value": steps_total / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": 2 * 8 * n,
                     "d2h_bytes_per_step": 3 * 8 * n, "finite": finite},
             "roofline": {"bound": "hbm", "kernel": "k_cheb_o level 0 (FP32 Chebyshev smoother step, int16 offsets)",
@@ -372,6 +450,144 @@ def run_ours(a, rank, world, local_rank):
         dist.barrier()
         dist.destroy_process_group()
     return line
+
+
+# ---------------------------------------------------------------------------
+# the other configurations (one GPU, each its own line)
+# ---------------------------------------------------------------------------
+def run_other(a):
+    import numpy as np
+
+    import multigrid_meshless_b200 as mgm
+    from multigrid_meshless_b200 import api, clouds
+    t0 = time.perf_counter()
+    if a.workload == "annulus":
+        nl, k, poly, Re, courant, deg, ratio = 6, 30, 4, 100.0, 0.5, 4, 10.0
+        cl = clouds.annulus_hierarchy(clouds.annulus_h_for_nodes(1_000_000), nl, seed=1)
+        bc = mgm.BC_TAYLOR_COUETTE
+        desc = (f"2D Taylor-Couette annulus r in [0.5, 1], jittered polar nodes, {nl} levels (/4), PHS3 + poly{poly}, "
+                f"k={k}, Re={Re:g}, Courant {courant:g}, inner wall u_theta = 1")
+    else:
+        nl, k, poly, Re, courant, deg, ratio = 4, 35, 2, 400.0, 0.3, 4, 10.0
+        cl = clouds.cube_hierarchy(128, nl, seed=1)
+        bc = mgm.BC_LID
+        desc = (f"3D lid-driven cube, 128^3 jittered nodes (edges/corners removed), {nl} levels (/8), PHS3 + "
+                f"poly{poly}, k={k}, Re={Re:g}, Courant {courant:g}")
+    mg = api.Multigrid(cl, [k] * nl, [poly] * nl)
+    setup_s = time.perf_counter() - t0
+    n = mg.n()
+    mg.set_flow(Re=Re, courant=courant)
+    mg.set_solver(rel_tol=a.tol, max_iters=100, cheb_degree=deg, cheb_ratio=ratio)
+
+    # the explicit scheme is diffusion-unstable at these spacings; the annulus
+    # grows faster than the cavity, so its episodes are shorter
+    episode = min(a.episode, 5) if a.workload == "annulus" else a.episode
+
+    def arm(mode, steps):
+        tot = [0.0, 0.0, 0, 0.0]
+        done = 0
+        while done < steps:
+            m_ = min(episode, steps - done)
+            mg.apply_bc(bc)
+            ms_, pms_, vc_, err_ = mg.run_steps(mode, m_)
+            tot[0] += ms_; tot[1] += pms_; tot[2] += vc_; tot[3] = err_
+            done += m_
+        return tot
+    arm(mgm.MODE_FP32_IR, a.warmup)
+    arm(mgm.MODE_FP64, min(a.warmup, 2))
+    pl = arm(mgm.MODE_FP64, a.steps)
+    mg.profile_smoother(True)
+    sm0 = mg.profile_read()
+    clocks = ClockSampler(0)
+    clocks.start()
+    l0 = api.kernel_launches()
+    ms, pms, vc, err = arm(mgm.MODE_FP32_IR, a.steps)
+    launches = api.kernel_launches() - l0
+    ck = clocks.stop()
+    sm1 = mg.profile_read()
+    sm_ms, sm_launch, sm_bytes = sm1[0] - sm0[0], sm1[1] - sm0[1], sm1[2]
+    peak, peak_src = measured_peak()
+    avg = (sm_ms / 1e3) / max(sm_launch, 1)
+    ach = sm_bytes / avg / 1e9 if sm_launch else None
+    mg.close()
+    return {
+        "metric": f"NS steps/s & Poisson ms, 1e-8 resid: FP32-in-FP64 vs plain FP64 GPU ({a.workload})",
+        "value": a.steps / (ms / 1e3), "unit": "steps/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 V-cycle inside f64 FGMRES", "data": "synthetic (seeded jittered cloud, no mesh files)",
+        "config": {"workload": desc, "nodes": n, "levels": nl, "k": k, "poly_degree": poly, "rel_tol": a.tol,
+                   "cheb_degree": deg, "cheb_ratio": ratio,
+                   "episodes": f"steps in episodes of {episode} from rest"},
+        "poisson_ms": pms / a.steps, "vcycles_per_step": vc / a.steps, "steady_err_last": err,
+        "plain_fp64": {"steps_per_s": a.steps / (pl[0] / 1e3), "ms_per_step": pl[0] / a.steps,
+                       "poisson_ms": pl[1] / a.steps, "vcycles_per_step": pl[2] / a.steps},
+        "roofline": {"bound": "hbm", "kernel": "level-0 FP32 Chebyshev smoother step", "achieved": ach,
+                     "peak": peak, "unit": "GB/s", "frac": (ach / peak) if ach else None,
+                     "bytes_per_launch": sm_bytes, "launches": sm_launch, "avg_launch_us": avg * 1e6,
+                     "peak_source": peak_src},
+        "clocks": ck, "gpu_launches": launches, "setup_s": setup_s,
+    }
+
+
+def run_batch(a):
+    import numpy as np
+
+    import multigrid_meshless_b200 as mgm
+    from multigrid_meshless_b200 import api, clouds
+    nl, nrhs = 4, 64
+    t0 = time.perf_counter()
+    h = clouds.shell_h_for_nodes(int(3_000_000 * 0.875))
+    cl = clouds.shell_hierarchy(h, nl, seed=1)
+    ks = [clouds.shell_stencil_sizes(cl[0], 40, 60)] + [clouds.shell_stencil_sizes(c, 25, 35) for c in cl[1:]]
+    polys = [3] + [2] * (nl - 1)
+    b = api.Batch(cl, ks, polys, autotune=True)
+    setup_s = time.perf_counter() - t0
+    rep = b.weights_report()
+    lev = b.level(0)
+    c0 = clouds.Cloud(lev["x"], lev["y"], lev["z"], lev["nx"], lev["ny"], lev["nz"], lev["btag"], 0, 3, 0.0,
+                      "shell3d", {"r_in": 0.5, "r_out": 1.0})
+    f = clouds.gaussian_fields(c0, nrhs, seed=5)
+    inner = lev["btag"] == 0
+    f[:, ~inner] = 0.0
+    f[:, inner] -= f[:, inner].mean(1, keepdims=True)
+    f[:, 0] = 0.0
+    b.set_solver(a.tol, 24, 4, 10.0)
+    arms = {}
+    for name, mode in (("fp32", mgm.MODE_FP32_IR), ("fp64", mgm.MODE_FP64)):
+        b.solve(f, mode)  # warm-up (allocates the Krylov space)
+        dev, wall, vcs, worst = 0.0, 0.0, 0, 0.0
+        reps = max(1, min(a.steps, 3))
+        for _ in range(reps):
+            t1 = time.perf_counter()
+            sol, vc, rr, ms = b.solve(f, mode)
+            wall += time.perf_counter() - t1
+            dev += ms
+            vcs += vc
+            worst = max(worst, float(rr.max()))
+        arms[name] = {"ms_per_solve": dev / reps, "wall_ms_per_solve": wall * 1e3 / reps, "vcycles": vcs / reps,
+                      "worst_rel_res": worst, "sol": sol}
+    rel = max(float(np.linalg.norm(x - y) / np.linalg.norm(y)) for x, y in zip(arms["fp32"]["sol"], arms["fp64"]["sol"]))
+    for v in arms.values():
+        v.pop("sol")
+    n_tot = sum(c.n for c in cl)
+    b.close()
+    return {
+        "metric": "64 Poisson right-hand sides to 1e-8 through one batched V-cycle (3D shell, per-node stencils)",
+        "value": nrhs / (arms["fp32"]["ms_per_solve"] / 1e3), "unit": "RHS solved/s", "n_gpus": 1,
+        "steps": 3, "warmup": 1, "ms_per_step": arms["fp32"]["ms_per_solve"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 V-cycle inside f64 FGMRES",
+        "data": "synthetic (seeded shell cloud, seeded sums of 8 Gaussians)",
+        "config": {"workload": f"3D sphere-in-sphere shell r in [0.5, 1], {n_tot} nodes over {nl} levels (/8), "
+                               f"k 40/60 (poly 3) on the fine level and 25/35 (poly 2) below by boundary proximity",
+                   "nodes_total": n_tot, "nodes_fine": cl[0].n, "levels": nl,
+                   "nrhs": nrhs, "rel_tol": a.tol},
+        "weights": {k_: v for k_, v in rep.items()},
+        "fp32": arms["fp32"], "fp64": arms["fp64"],
+        "solution_rel_l2_fp32_vs_fp64": rel,
+        "e2e": {"value": nrhs / (arms["fp32"]["wall_ms_per_solve"] / 1e3), "unit": "RHS solved/s",
+                "h2d_bytes_per_step": nrhs * cl[0].n * 8, "d2h_bytes_per_step": nrhs * cl[0].n * 8},
+        "setup_s": setup_s,
+    }
 
 
 def run_reference(a, rank):
@@ -408,6 +624,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         line = run_reference(a, rank)
+    elif a.workload == "shell-batch":
+        line = run_batch(a) if rank == 0 else None
+    elif a.workload in ("annulus", "cube"):
+        line = run_other(a) if rank == 0 else None
     else:
         line = run_ours(a, rank, world, local_rank)
     if line is not None:
