@@ -251,7 +251,36 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
                  : "memory");
 }
 
-// MODE 0: Chebyshev step (as k_cheb_o); MODE 1: residual (as k_residual_o)
+// One pipeline stage in shared memory: the tile's weights [k][kTileRows] f32
+// and offsets [k][kTileRows] i16.
+struct TileStage {
+    int k;
+    __device__ size_t a_off() const { return 0; }
+    __device__ size_t o_off() const { return (size_t)k * kTileRows * sizeof(float); }
+    __device__ size_t bytes() const { return (size_t)k * kTileRows * (sizeof(float) + sizeof(short)); }
+};
+__host__ inline size_t tile_stage_bytes(int k) { return (size_t)k * kTileRows * (sizeof(float) + sizeof(short)); }
+
+// One thread issues the two bulk copies of tile `tile` (weights, offsets; the
+// operator is stored tile-major) into stage memory `st`; the mbarrier expects
+// exactly the bytes issued.
+__device__ __forceinline__ void tile_issue(unsigned char *st, uint64_t *bar, int tile, int k, const float *At,
+                                           const short *offt)
+{
+    const TileStage L{k};
+    // the stage may have been read by the CTA's threads (generic proxy) before
+    // the barrier that precedes this call: order those reads before the
+    // copies' writes (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(bar, (unsigned)L.bytes());
+    const long t0 = (long)tile * k * kTileRows;
+    bulk_g2s(st + L.a_off(), At + t0, (unsigned)(k * kTileRows * sizeof(float)), bar);
+    bulk_g2s(st + L.o_off(), offt + t0, (unsigned)(k * kTileRows * sizeof(short)), bar);
+}
+
+// MODE 0: Chebyshev step (as k_cheb_o); MODE 1: residual (as k_residual_o).
+// Chunked variant for any k <= kTileMaxK: the row's stencil is read from the
+// stage while its gathers run, 8 at a time.
 template <int MODE>
 __global__ void __launch_bounds__(kTileRows) k_level_tiled(int n, int k, const short *__restrict__ offt,
                                                            const float *__restrict__ At, const float *__restrict__ dinv,
@@ -265,11 +294,8 @@ __global__ void __launch_bounds__(kTileRows) k_level_tiled(int n, int k, const s
     __shared__ int ok_flag;
     const int tid = threadIdx.x;
     const int ntiles = (n + kTileRows - 1) / kTileRows;
-    const unsigned a_bytes = kTileRows * sizeof(float), o_bytes = kTileRows * sizeof(short);
-    const size_t stage = (size_t)k * (a_bytes + o_bytes);
-    // stage st: weights at smem + st * stage, offsets after them
-    auto As = [&](int st) { return (float *)(smem + st * stage); };
-    auto Os = [&](int st) { return (short *)(smem + st * stage + (size_t)k * a_bytes); };
+    const TileStage L{k};
+    const size_t stage = L.bytes();
     unsigned pending = 0;  // bit st: stage st has copies in flight (tracked by thread 0)
     if (tid == 0) {
         mbar_init(&bar[0], 1);
@@ -278,12 +304,7 @@ __global__ void __launch_bounds__(kTileRows) k_level_tiled(int n, int k, const s
     }
     __syncthreads();
     auto issue = [&](int tile, int st) {
-        if (tid == 0) {
-            mbar_expect_tx(&bar[st], (unsigned)stage);
-            const long t0 = (long)tile * k * kTileRows;  // tile-major: the tile's [k][kTileRows] block is contiguous
-            bulk_g2s(As(st), At + t0, (unsigned)k * a_bytes, &bar[st]);
-            bulk_g2s(Os(st), offt + t0, (unsigned)k * o_bytes, &bar[st]);
-        }
+        if (tid == 0) tile_issue(smem + st * stage, &bar[st], tile, k, At, offt);
         pending |= 1u << st;
     };
     int it = 0;
@@ -305,14 +326,15 @@ __global__ void __launch_bounds__(kTileRows) k_level_tiled(int n, int k, const s
         }
         mbar_try_wait(&bar[st], parity);  // completed: acquires the copied data for this thread
         pending &= ~(1u << st);
+        unsigned char *sb = smem + st * stage;
         const int i = tile * kTileRows + tid;
         if (i < n) {
             const float ei = e[i];
             if (btag[i]) {
                 out[i] = MODE == 0 ? ei : 0.f;
             } else {
-                const float *a = As(st) + tid;
-                const short *o = Os(st) + tid;
+                const float *a = (const float *)(sb + L.a_off()) + tid;
+                const short *o = (const short *)(sb + L.o_off()) + tid;
                 float s = 0.f;
                 int j = 0;
                 for (; j + 8 <= k; j += 8) {
@@ -342,9 +364,9 @@ __global__ void __launch_bounds__(kTileRows) k_level_tiled(int n, int k, const s
 }
 
 // Register variant for k <= 32: a thread copies its row's whole stencil from
-// shared memory into registers, the CTA syncs, the freed stage starts the
-// copies of the tile after next, and the threads issue all k neighbour
-// gathers at once (k gathers in flight per row instead of 8).
+// the stage into registers, the CTA syncs, the freed stage starts the copies
+// of the tile after next, and the threads issue all k neighbour gathers at
+// once (k gathers in flight per row instead of 8).
 template <int MODE>
 __global__ void __launch_bounds__(kTileRows, 2) k_level_tiled_r(int n, int k, const short *__restrict__ offt,
                                                               const float *__restrict__ At,
@@ -360,10 +382,8 @@ __global__ void __launch_bounds__(kTileRows, 2) k_level_tiled_r(int n, int k, co
     __shared__ int ok_flag;
     const int tid = threadIdx.x;
     const int ntiles = (n + kTileRows - 1) / kTileRows;
-    const unsigned a_bytes = kTileRows * sizeof(float), o_bytes = kTileRows * sizeof(short);
-    const size_t stage = (size_t)k * (a_bytes + o_bytes);
-    auto As = [&](int st) { return (float *)(smem + st * stage); };
-    auto Os = [&](int st) { return (short *)(smem + st * stage + (size_t)k * a_bytes); };
+    const TileStage L{k};
+    const size_t stage = L.bytes();
     unsigned pending = 0;  // bit st: stage st has copies in flight (tracked by thread 0)
     if (tid == 0) {
         mbar_init(&bar[0], 1);
@@ -372,12 +392,7 @@ __global__ void __launch_bounds__(kTileRows, 2) k_level_tiled_r(int n, int k, co
     }
     __syncthreads();
     auto issue = [&](int tile, int st) {
-        if (tid == 0) {
-            mbar_expect_tx(&bar[st], (unsigned)stage);
-            const long t0 = (long)tile * k * kTileRows;
-            bulk_g2s(As(st), At + t0, (unsigned)k * a_bytes, &bar[st]);
-            bulk_g2s(Os(st), offt + t0, (unsigned)k * o_bytes, &bar[st]);
-        }
+        if (tid == 0) tile_issue(smem + st * stage, &bar[st], tile, k, At, offt);
         pending |= 1u << st;
     };
     if (blockIdx.x < ntiles) issue(blockIdx.x, 0);
@@ -398,10 +413,11 @@ __global__ void __launch_bounds__(kTileRows, 2) k_level_tiled_r(int n, int k, co
         }
         mbar_try_wait(&bar[st], parity);
         pending &= ~(1u << st);
+        const unsigned char *sb = smem + st * stage;
+        const float *as = (const float *)(sb + L.a_off());
+        const short *os = (const short *)(sb + L.o_off());
         float a[32];
         int o[32];
-        const float *as = As(st);
-        const short *os = Os(st);
 #pragma unroll
         for (int j = 0; j < 32; j++) {
             a[j] = j < k ? as[j * kTileRows + tid] : 0.f;
@@ -454,16 +470,16 @@ template <int MODE>
 static void launch_tiled(const SolveLevel<float> &L, const float *e, float *out, float c1, float c2, int first,
                          cudaStream_t s)
 {
-    const size_t per_stage = (size_t)L.k * kTileRows * (sizeof(float) + sizeof(short));
+    const size_t smem = 2 * tile_stage_bytes(L.k);
     if (L.k <= 32) {
         MGM_CUDA(cudaFuncSetAttribute(k_level_tiled_r<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(2 * 32 * kTileRows * (sizeof(float) + sizeof(short)))));
-        k_level_tiled_r<MODE><<<tiled_grid(k_level_tiled_r<MODE>, L.n, 2 * per_stage), kTileRows, 2 * per_stage, s>>>(
+                                      (int)(2 * tile_stage_bytes(32))));
+        k_level_tiled_r<MODE><<<tiled_grid(k_level_tiled_r<MODE>, L.n, smem), kTileRows, smem, s>>>(
             L.n, L.k, L.offt, L.At, L.dinv, L.btag, L.r, e, out, L.d, c1, c2, first, L.tma_err);
     } else {
         MGM_CUDA(cudaFuncSetAttribute(k_level_tiled<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(2 * kTileMaxK * kTileRows * (sizeof(float) + sizeof(short)))));
-        k_level_tiled<MODE><<<tiled_grid(k_level_tiled<MODE>, L.n, 2 * per_stage), kTileRows, 2 * per_stage, s>>>(
+                                      (int)(2 * tile_stage_bytes(kTileMaxK))));
+        k_level_tiled<MODE><<<tiled_grid(k_level_tiled<MODE>, L.n, smem), kTileRows, smem, s>>>(
             L.n, L.k, L.offt, L.At, L.dinv, L.btag, L.r, e, out, L.d, c1, c2, first, L.tma_err);
     }
     MGM_LAUNCHED();
