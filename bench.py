@@ -297,6 +297,8 @@ def run_ours(a, rank, world, local_rank):
     import multigrid_meshless_b200 as mgm
     from multigrid_meshless_b200 import api, clouds
 
+    from multigrid_meshless_b200 import replicas
+
     api.set_device(local_rank)
     dist = None
     if world > 1:
@@ -305,21 +307,11 @@ def run_ours(a, rank, world, local_rank):
         torch.cuda.set_device(local_rank)
         dist_.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
         dist = dist_
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    timing = replicas.Timing(dist, f"cuda:{local_rank}")
+    barrier, max_over_ranks = timing.barrier, timing.max_over_ranks
 
     t0 = time.perf_counter()
-    cl = clouds.cavity_hierarchy(a.m, a.levels, seed=1 + rank * 1000)
+    cl = clouds.cavity_hierarchy(a.m, a.levels, seed=replicas.replica_seed(1, rank))
     mg = api.Multigrid(cl, [a.k] * a.levels, [a.poly] * a.levels)
     setup_s = time.perf_counter() - t0
     setup_launches = api.kernel_launches()
@@ -621,9 +613,8 @@ def run_reference(a, rank):
 
 def main():
     a = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    from multigrid_meshless_b200.replicas import env_rank
+    rank, world, local_rank = env_rank()
     if a.impl == "reference":
         line = run_reference(a, rank)
     elif a.workload == "shell-batch":
