@@ -63,15 +63,36 @@ __global__ void __launch_bounds__(256) k_multidot(int n, int cnt, const double *
     }
 }
 
+// out[c] = sum_t part[c * nblk + t]; one block per c
 __global__ void k_reduce_parts(const double *__restrict__ part, int nblk, int cnt, double *__restrict__ out)
 {
     __shared__ double sm[32];
-    for (int c = 0; c < cnt; c++) {
-        double s = 0.0;
-        for (int t = threadIdx.x; t < nblk; t += blockDim.x) s += part[(long)c * nblk + t];
-        s = bsum<256>(s, sm);
-        if (threadIdx.x == 0) out[c] = s;
+    const int c = blockIdx.x;
+    if (c >= cnt) return;
+    double s = 0.0;
+    for (int t = threadIdx.x; t < nblk; t += blockDim.x) s += part[(long)c * nblk + t];
+    s = bsum<256>(s, sm);
+    if (threadIdx.x == 0) out[c] = s;
+}
+
+// w -= sum_c h[c] V_c, and per-block partial |w|^2 of the result (grid-stride)
+__global__ void __launch_bounds__(256) k_orth_norm(int n, int cnt, const double *__restrict__ V, long ldv,
+                                                   const double *__restrict__ h, double *__restrict__ w,
+                                                   double *__restrict__ part)
+{
+    __shared__ double hs[kMaxKrylov + 1];
+    __shared__ double sm[32];
+    for (int c = threadIdx.x; c < cnt; c += blockDim.x) hs[c] = h[c];
+    __syncthreads();
+    double acc = 0.0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        double s = w[i];
+        for (int c = 0; c < cnt; c++) s = fma(-hs[c], V[c * ldv + i], s);
+        w[i] = s;
+        acc = fma(s, s, acc);
     }
+    acc = bsum<256>(acc, sm);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
 }
 
 // w -= sum_c h[c] V_c
@@ -149,12 +170,21 @@ void multidot(int n, int cnt, const double *V, long ldv, const double *w, double
     const int nb = dot_blocks(n);
     k_multidot<<<nb, 256, 0, s>>>(n, cnt, V, ldv, w, part);
     MGM_LAUNCHED();
-    k_reduce_parts<<<1, 256, 0, s>>>(part, nb, cnt, out);
+    k_reduce_parts<<<cnt, 256, 0, s>>>(part, nb, cnt, out);
     MGM_LAUNCHED();
 }
 void reduce_parts(const double *part, int nblk, int cnt, double *out, cudaStream_t s)
 {
-    k_reduce_parts<<<1, 256, 0, s>>>(part, nblk, cnt, out);
+    k_reduce_parts<<<cnt, 256, 0, s>>>(part, nblk, cnt, out);
+    MGM_LAUNCHED();
+}
+void orth_norm(int n, int cnt, const double *V, long ldv, const double *h, double *w, double *part, double *norm2,
+               cudaStream_t s)
+{
+    const int nb = dot_blocks(n);
+    k_orth_norm<<<nb, 256, 0, s>>>(n, cnt, V, ldv, h, w, part);
+    MGM_LAUNCHED();
+    k_reduce_parts<<<1, 256, 0, s>>>(part, nb, 1, norm2);
     MGM_LAUNCHED();
 }
 void orth_update(int n, int cnt, const double *V, long ldv, const double *h, double *w, cudaStream_t s)

@@ -16,6 +16,9 @@ int dot_blocks(int n);
 void multidot(int n, int cnt, const double *V, long ldv, const double *w, double *part, double *out, cudaStream_t s);
 void reduce_parts(const double *part, int nblk, int cnt, double *out, cudaStream_t s);
 void orth_update(int n, int cnt, const double *V, long ldv, const double *h, double *w, cudaStream_t s);
+// w -= sum_c h[c] V_c and *norm2 = |w|^2 of the result (device scalar)
+void orth_norm(int n, int cnt, const double *V, long ldv, const double *h, double *w, double *part, double *norm2,
+               cudaStream_t s);
 void scale_by(int n, const double *in, double *out, const double *nrm, int is_sq, cudaStream_t s);
 template <class T>
 void combine(int n, int cnt, const T *Z, long ldz, const double *y, double *x, cudaStream_t s);

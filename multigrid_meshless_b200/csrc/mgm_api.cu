@@ -414,16 +414,27 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
                 copy_out<T>(n, zout, Z + j * ld, s);
                 c->vcycles_in_solve++;
             }
-            // w = A z_j, classical Gram-Schmidt with one re-orthogonalisation
-            apply64<T>(n, k, L0.idx.p, L0.A64.p, Z + j * ld, w, s);
-            multidot(n, j + 1, V, ld, w, c->kpart.p, c->kscal.p, s);
-            orth_update(n, j + 1, V, ld, c->kscal.p, w, s);
-            multidot(n, j + 1, V, ld, w, c->kpart.p, c->kscal.p + kMaxKrylov + 2, s);
-            orth_update(n, j + 1, V, ld, c->kscal.p + kMaxKrylov + 2, w, s);
-            multidot(n, 1, w, ld, w, c->kpart.p, c->kscal.p + 2 * kMaxKrylov + 4, s);
-            scale_by(n, w, V + (j + 1) * ld, c->kscal.p + 2 * kMaxKrylov + 4, 1, s);
+            // w = A z_j, written into the slot of V_{j+1}; classical Gram-Schmidt:
+            // the projections and |w|^2 in one pass, the update with the norm of
+            // the result in a second, and a re-orthogonalisation only when the
+            // first pass cancelled more than 1 - 1/sqrt(2) of |w| (the
+            // Daniel-Gragg-Kaufman-Stewart test)
+            double *wn = V + (j + 1) * ld;
+            double *h2 = c->kscal.p + kMaxKrylov + 2, *nrm = c->kscal.p + 2 * kMaxKrylov + 4;
+            apply64<T>(n, k, L0.idx.p, L0.A64.p, Z + j * ld, wn, s);
+            multidot(n, j + 2, V, ld, wn, c->kpart.p, c->kscal.p, s);
+            orth_norm(n, j + 1, V, ld, c->kscal.p, wn, c->kpart.p, nrm, s);
             MGM_CUDA(cudaMemcpyAsync(hp, c->kscal.p, sizeof(double) * (2 * kMaxKrylov + 5), cudaMemcpyDeviceToHost, s));
             MGM_CUDA(cudaStreamSynchronize(s));
+            for (int i = 0; i <= j; i++) hp[kMaxKrylov + 2 + i] = 0.0;
+            if (hp[2 * kMaxKrylov + 4] < 0.5 * hp[j + 1]) {
+                multidot(n, j + 1, V, ld, wn, c->kpart.p, h2, s);
+                orth_norm(n, j + 1, V, ld, h2, wn, c->kpart.p, nrm, s);
+                MGM_CUDA(cudaMemcpyAsync(hp + kMaxKrylov + 2, h2, sizeof(double) * (kMaxKrylov + 3),
+                                         cudaMemcpyDeviceToHost, s));
+                MGM_CUDA(cudaStreamSynchronize(s));
+            }
+            scale_by(n, wn, wn, nrm, 1, s);
             if (c->prof.on) {
                 auto &G = c->vg[sizeof(T) == 4 ? 1 : 0];
                 if (c->use_graphs && G.x && G.prof) c->prof.harvest_graph(G.ev_first, G.ev_pairs);

@@ -177,3 +177,4 @@ def test_tiled_levels_match_plain_loads(require_gpu):
         assert np.linalg.norm(ref[0] - want) / np.linalg.norm(want) < P_TOL
     finally:
         mg.close()
+
