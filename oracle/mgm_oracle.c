@@ -816,3 +816,297 @@ ORC_EXPORT double orc_step(void *h, double *mass_res)
 ORC_EXPORT void orc_intermediate_velocity(void *h) { orc_ctx *c = (orc_ctx *)h; intermediate_velocity(&c->L[0], &c->f, c->dt, c->nu); }
 ORC_EXPORT void orc_mass_residual(void *h) { orc_ctx *c = (orc_ctx *)h; mass_residual(&c->L[0], &c->f, c->dt, c->rho); }
 ORC_EXPORT double orc_update_velocity(void *h) { orc_ctx *c = (orc_ctx *)h; return update_velocity(&c->L[0], &c->f, c->dt, c->rho); }
+
+/* ------------------------------------------------------------------------ */
+/* TIMPLE: the time-implicit step (timple_solver.h:40-410), the default      */
+/* solver of mg_NS_solver.c.  Per level p[l] holds pprime; p_old is level 0. */
+/* jacobi = 0: the in-place sweeps of the C build; jacobi = 1: every node   */
+/* updated from the previous sweep's values (the GPU's order).              */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    double *p_old;
+    int iter_timple, iter_momentum;
+    double facRe, facdt;
+    double *su, *sv, *sw;  /* previous-sweep copies (Jacobi order) */
+} orc_timple;
+
+static orc_timple g_timple;
+
+ORC_EXPORT void orc_ctx_timple(void *h, double *p_old, int iter_timple, int iter_momentum, double facRe, double facdt)
+{
+    orc_ctx *c = (orc_ctx *)h;
+    int n = c->L[0].n;
+    g_timple.p_old = p_old;
+    g_timple.iter_timple = iter_timple;
+    g_timple.iter_momentum = iter_momentum;
+    g_timple.facRe = facRe;
+    g_timple.facdt = facdt;
+    free(g_timple.su); free(g_timple.sv); free(g_timple.sw);
+    g_timple.su = (double *)malloc(sizeof(double) * (size_t)n);
+    g_timple.sv = (double *)malloc(sizeof(double) * (size_t)n);
+    g_timple.sw = (double *)malloc(sizeof(double) * (size_t)n);
+}
+
+/* calculate_intermediate_velocity_implicit (timple_solver.h:72-175) */
+static void timple_momentum(orc_ctx *c)
+{
+    const orc_level *L = &c->L[0];
+    orc_field *f = &c->f;
+    const orc_timple *t = &g_timple;
+    int n = L->n, k = L->k, dim = c->dim;
+    /* mu = rho / Re; with rho = 1 (mesh_functions.h:97) this is nu * rho, bit for bit */
+    double rho = c->rho, mu = c->nu * c->rho, dt = c->dt;
+    orc_spmv(n, k, L->Dx, L->cloud, t->p_old, f->dpdx);
+    orc_spmv(n, k, L->Dy, L->cloud, t->p_old, f->dpdy);
+    if (dim == 3) orc_spmv(n, k, L->Dz, L->cloud, t->p_old, f->dpdz);
+    for (int it = 0; it < t->iter_momentum; it++) {
+        const double *uin = f->u_new, *vin = f->v_new, *win = f->w_new;
+        if (c->jacobi) {
+            memcpy(t->su, f->u_new, sizeof(double) * (size_t)n); uin = t->su;
+            memcpy(t->sv, f->v_new, sizeof(double) * (size_t)n); vin = t->sv;
+            if (dim == 3) { memcpy(t->sw, f->w_new, sizeof(double) * (size_t)n); win = t->sw; }
+        }
+        for (int i = 0; i < n; i++) {
+            if (L->btag[i]) continue;
+            const size_t r = (size_t)i * k;
+            const double *comp_in[3] = {uin, vin, win};
+            double *comp_out[3] = {f->u_new, f->v_new, f->w_new};
+            const double *comp_old[3] = {f->u_old, f->v_old, f->w_old};
+            const double *grad[3] = {f->dpdx, f->dpdy, f->dpdz};
+            for (int cidx = 0; cidx < (dim == 3 ? 3 : 2); cidx++) {
+                const double *x = comp_in[cidx];
+                double temp1 = 0, temp2 = 0, temp3 = 0, temp4 = 0;
+                double advection_x = f->u[i] * L->Dx[r];
+                double advection_y = f->v[i] * L->Dy[r];
+                double diffusion = -t->facRe * mu * L->lap[r];
+                double unsteady = 1. / (dt * t->facdt);
+                double denom;
+                if (cidx < 2) {
+                    denom = rho * (advection_x + advection_y + unsteady) + diffusion;
+                    for (int j = 1; j < k; j++) {
+                        double xv = x[L->cloud[r + j]];
+                        temp1 += L->Dx[r + j] * xv;
+                        temp2 += L->Dy[r + j] * xv;
+                        temp4 += L->lap[r + j] * xv;
+                    }
+                    if (dim == 3) {
+                        denom += rho * f->w[i] * L->Dz[r];
+                        for (int j = 1; j < k; j++) temp3 += L->Dz[r + j] * x[L->cloud[r + j]];
+                    }
+                } else {
+                    double advection_z = f->w[i] * L->Dz[r];
+                    denom = rho * (advection_x + advection_y + advection_z + unsteady) + diffusion;
+                    for (int j = 1; j < k; j++) {
+                        double xv = x[L->cloud[r + j]];
+                        temp1 += L->Dx[r + j] * xv;
+                        temp2 += L->Dy[r + j] * xv;
+                        temp3 += L->Dz[r + j] * xv;
+                        temp4 += L->lap[r + j] * xv;
+                    }
+                }
+                double advection = f->u[i] * temp1 + f->v[i] * temp2 + f->w[i] * temp3;
+                unsteady = comp_old[cidx][i] / (dt * t->facdt);
+                comp_out[cidx][i] = (rho * (unsteady - advection) - (t->facRe - 1) * mu * L->lap[r] * x[i] +
+                                     mu * temp4 - grad[cidx][i]) / denom;
+            }
+        }
+    }
+}
+
+/* calculate_mass_residual_implicit (timple_solver.h:177-201) */
+static void timple_mass(orc_ctx *c)
+{
+    const orc_level *L = &c->L[0];
+    orc_field *f = &c->f;
+    int n = L->n, k = L->k;
+    orc_spmv(n, k, L->Dx, L->cloud, f->u_new, f->dpdx);
+    orc_spmv(n, k, L->Dy, L->cloud, f->v_new, f->dpdy);
+    if (c->dim == 3) orc_spmv(n, k, L->Dz, L->cloud, f->w_new, f->dpdz);
+    for (int i = 0; i < n; i++)
+        f->source[i] = L->btag[i] ? 0 : c->rho * (f->dpdx[i] + f->dpdy[i] + f->dpdz[i]) / c->dt;
+}
+
+/* relaxation (timple_solver.h:249-283): residual with lap_Poison on interior rows */
+static void timple_relaxation(const orc_level *L, double *p, const double *source, double *res, float omega,
+                              int num_relax, int jacobi, double *scratch)
+{
+    int n = L->n, k = L->k;
+    for (int it = 0; it < num_relax; it++) {
+        const double *pin = p;
+        if (jacobi) { memcpy(scratch, p, sizeof(double) * (size_t)n); pin = scratch; }
+        for (int i = 0; i < n; i++) {
+            double sum = 0.0;
+            for (int j = 1; j < k; j++) sum += L->lapP[(size_t)i * k + j] * pin[L->cloud[(size_t)i * k + j]];
+            p[i] = omega * ((source[i] - sum) / L->lapP[(size_t)i * k]) + (1 - omega) * pin[i];
+        }
+        double pref = p[0];
+        for (int i = 0; i < n; i++) p[i] = p[i] - pref;
+        for (int i = 0; i < n; i++) {
+            if (!L->btag[i]) {
+                res[i] = source[i];
+                for (int j = 0; j < k; j++) res[i] = res[i] - L->lapP[(size_t)i * k + j] * p[L->cloud[(size_t)i * k + j]];
+            } else res[i] = 0;
+        }
+    }
+}
+
+/* calculate_residuals (timple_solver.h:285-301) */
+static void timple_residuals(const orc_level *L, const double *p, const double *source, double *res)
+{
+    int n = L->n, k = L->k;
+    for (int i = 0; i < n; i++) {
+        res[i] = 0.0;
+        if (!L->btag[i]) {
+            double sum = 0;
+            for (int j = 0; j < k; j++) sum += L->lapP[(size_t)i * k + j] * p[L->cloud[(size_t)i * k + j]];
+            res[i] = source[i] - sum;
+        }
+    }
+}
+
+/* restrict_residuals (timple_solver.h:303-317): every coarse row written */
+static void timple_restrict(const orc_level *F, const orc_level *C, const double *res_f, double *source_c)
+{
+    for (int i = 0; i < C->n; i++) {
+        double results = 0.0;
+        if (!C->btag[i]) {
+            int ir = C->rpts[i];
+            for (int j = 0; j < F->k; j++) results += C->restr[(size_t)i * F->k + j] * res_f[F->cloud[(size_t)ir * F->k + j]];
+        }
+        source_c[i] = results;
+    }
+}
+
+/* prolongate_corrections (timple_solver.h:319-339): every coarse pprime reset */
+static void timple_prolongate(const orc_level *F, const orc_level *C, double *p_f, double *p_c)
+{
+    for (int i = 0; i < F->n; i++) {
+        if (F->btag[i]) continue;
+        int ip = F->ppts[i];
+        double r = 0.0;
+        for (int j = 0; j < C->k; j++) r += F->prol[(size_t)i * C->k + j] * p_c[C->cloud[(size_t)ip * C->k + j]];
+        p_f[i] = p_f[i] + r;
+    }
+    for (int i = 0; i < C->n; i++) p_c[i] = 0.0;
+}
+
+/* multigrid_Poisson_solver (timple_solver.h:203-220) */
+static void timple_multigrid(orc_ctx *c)
+{
+    int nl = c->nl;
+    for (int cyc = 0; cyc < c->num_vcycles; cyc++) {
+        for (int l = 0; l < nl; l++) {
+            timple_relaxation(&c->L[l], c->p[l], c->source[l], c->res[l], c->omega, c->num_relax, c->jacobi, c->scratch);
+            timple_residuals(&c->L[l], c->p[l], c->source[l], c->res[l]);
+            if (l != nl - 1) timple_restrict(&c->L[l], &c->L[l + 1], c->res[l], c->source[l + 1]);
+        }
+        for (int l = nl - 1; l > 0; l--) {
+            timple_prolongate(&c->L[l - 1], &c->L[l], c->p[l - 1], c->p[l]);
+            if (l != 1)
+                timple_relaxation(&c->L[l - 1], c->p[l - 1], c->source[l - 1], c->res[l - 1], c->omega, c->num_relax,
+                                  c->jacobi, c->scratch);
+        }
+    }
+}
+
+/* update_velocity_implicit (timple_solver.h:341-369) */
+static void timple_update_velocity(orc_ctx *c)
+{
+    const orc_level *L = &c->L[0];
+    orc_field *f = &c->f;
+    int n = L->n, k = L->k;
+    double *pp = c->p[0], *p_old = g_timple.p_old;
+    orc_spmv(n, k, L->Dx, L->cloud, pp, f->dpdx);
+    orc_spmv(n, k, L->Dy, L->cloud, pp, f->dpdy);
+    if (c->dim == 3) orc_spmv(n, k, L->Dz, L->cloud, pp, f->dpdz);
+    for (int i = 0; i < n; i++) {
+        if (L->btag[i]) continue;
+        f->u_new[i] = f->u_new[i] - c->dt * f->dpdx[i] / c->rho;
+        f->v_new[i] = f->v_new[i] - c->dt * f->dpdy[i] / c->rho;
+        if (c->dim == 3) f->w_new[i] = f->w_new[i] - c->dt * f->dpdz[i] / c->rho;
+        p_old[i] = p_old[i] + 1.0 * pp[i];
+    }
+    double pref = p_old[0];
+    for (int i = 0; i < n; i++) p_old[i] = p_old[i] - pref;
+}
+
+/* update_boundary_pressure (timple_solver.h:371-410).  The velocity terms are
+ * assigned, not accumulated, inside the stencil loop (:378-380), so only the
+ * last stencil slot contributes; FieldVariables.rho, which the reference never
+ * sets, is taken as rho. */
+static void timple_boundary_pressure(orc_ctx *c)
+{
+    const orc_level *L = &c->L[0];
+    orc_field *f = &c->f;
+    int n = L->n, k = L->k, dim = c->dim;
+    double *p_old = g_timple.p_old;
+    double nu = c->nu;
+    for (int i = 0; i < n; i++) {
+        if (!L->btag[i]) continue;
+        const size_t r = (size_t)i * k;
+        double temp1 = 0, temp2 = 0, temp3 = 0;
+        for (int j = 0; j < k; j++) {
+            int cj = L->cloud[r + j];
+            temp1 = nu * L->lap[r + j] * f->u_new[cj];
+            temp1 -= f->u[i] * f->u_new[cj] * L->Dx[r + j];
+            temp1 -= f->v[i] * f->u_new[cj] * L->Dy[r + j];
+            if (dim == 3) temp1 -= f->w[i] * f->u_new[cj] * L->Dz[r + j];
+            temp2 = nu * L->lap[r + j] * f->v_new[cj];
+            temp2 -= f->u[i] * f->v_new[cj] * L->Dx[r + j];
+            temp2 -= f->v[i] * f->v_new[cj] * L->Dy[r + j];
+            if (dim == 3) temp2 -= f->w[i] * f->v_new[cj] * L->Dz[r + j];
+            if (dim == 3) {
+                temp3 = nu * L->lap[r + j] * f->w_new[cj];
+                temp3 -= f->u[i] * f->w_new[cj] * L->Dx[r + j];
+                temp3 -= f->v[i] * f->w_new[cj] * L->Dy[r + j];
+                temp3 -= f->w[i] * f->w_new[cj] * L->Dz[r + j];
+            }
+        }
+        f->dpdn[i] = c->rho * (temp1 * L->nx[i] + temp2 * L->ny[i] + temp3 * L->nz[i]);
+        double sumx = 0, sumy = 0, sumz = 0, Ap = 0.0;
+        for (int j = 1; j < k; j++) {
+            sumx += L->Dx[r + j] * p_old[L->cloud[r + j]];
+            sumy += L->Dy[r + j] * p_old[L->cloud[r + j]];
+            if (dim == 3) sumz += L->Dz[r + j] * p_old[L->cloud[r + j]];
+        }
+        Ap += L->Dx[r] * L->nx[i];
+        Ap += L->Dy[r] * L->ny[i];
+        if (dim == 3) Ap += L->Dz[r] * L->nz[i];
+        p_old[i] = (f->dpdn[i] - sumx * L->nx[i] - sumy * L->ny[i] - sumz * L->nz[i]) / Ap;
+    }
+}
+
+/* time_implicit_solver (timple_solver.h:40-70) */
+ORC_EXPORT double orc_timple_step(void *h)
+{
+    orc_ctx *c = (orc_ctx *)h;
+    orc_field *f = &c->f;
+    int n = c->L[0].n, dim = c->dim;
+    double *pp = c->p[0];
+    for (int i = 0; i < n; i++) {
+        f->u_old[i] = f->u_new[i]; f->u[i] = f->u_new[i];
+        f->v_old[i] = f->v_new[i]; f->v[i] = f->v_new[i];
+        f->w_old[i] = f->w_new[i]; f->w[i] = f->w_new[i];
+        pp[i] = 0;
+    }
+    for (int it = 0; it < g_timple.iter_timple; it++) {
+        for (int i = 0; i < n; i++) { f->u[i] = f->u_new[i]; f->v[i] = f->v_new[i]; f->w[i] = f->w_new[i]; pp[i] = 0; }
+        timple_momentum(c);
+        timple_mass(c);
+        timple_multigrid(c);
+        timple_update_velocity(c);
+        timple_boundary_pressure(c);
+    }
+    double e = 0.0;
+    for (int i = 0; i < n; i++) {
+        e += pow(f->u_new[i] - f->u_old[i], 2) + pow(f->v_new[i] - f->v_old[i], 2);
+        if (dim == 3) e += pow(f->w_new[i] - f->w_old[i], 2);
+    }
+    return sqrt(e / n);
+}
+
+ORC_EXPORT void orc_timple_momentum(void *h) { timple_momentum((orc_ctx *)h); }
+ORC_EXPORT void orc_timple_mass(void *h) { timple_mass((orc_ctx *)h); }
+ORC_EXPORT void orc_timple_multigrid(void *h) { timple_multigrid((orc_ctx *)h); }
+ORC_EXPORT void orc_timple_update_velocity(void *h) { timple_update_velocity((orc_ctx *)h); }
+ORC_EXPORT void orc_timple_boundary_pressure(void *h) { timple_boundary_pressure((orc_ctx *)h); }

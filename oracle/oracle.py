@@ -17,7 +17,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 _ORC = {}
-_REF = None
+_REF = {}
 
 dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
@@ -65,18 +65,26 @@ def lib(crpow: bool = False):
             getattr(L, nm).argtypes = [C.c_void_p]
         L.orc_update_velocity.argtypes = [C.c_void_p]
         L.orc_update_velocity.restype = C.c_double
+        L.orc_ctx_timple.argtypes = [C.c_void_p, dp, C.c_int, C.c_int, C.c_double, C.c_double]
+        L.orc_timple_step.argtypes = [C.c_void_p]
+        L.orc_timple_step.restype = C.c_double
+        for nm in ("orc_timple_momentum", "orc_timple_mass", "orc_timple_multigrid", "orc_timple_update_velocity",
+                   "orc_timple_boundary_pressure"):
+            getattr(L, nm).argtypes = [C.c_void_p]
         _ORC[key] = L
     return _ORC[key]
 
 
-def ref_available() -> bool:
-    return os.path.exists(os.path.join(HERE, "_ref", "libref.so"))
+def ref_available(timple: bool = False) -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_timple.so" if timple else "libref.so"))
 
 
-def ref_lib():
-    global _REF
-    if _REF is None:
-        path = os.path.join(HERE, "_ref", "libref.so")
+def ref_lib(timple: bool = False):
+    """_ref/libref.so (fractional-step build) or _ref/libref_timple.so (the
+    reference's TIMPLE solver); each is its own library with its own globals."""
+    key = "timple" if timple else "fs"
+    if key not in _REF:
+        path = os.path.join(HERE, "_ref", "libref_timple.so" if timple else "libref.so")
         if not os.path.exists(path):
             raise RuntimeError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
         L = C.CDLL(path)
@@ -98,15 +106,20 @@ def ref_lib():
         L.ref_set_dt.argtypes = [C.c_double]
         L.ref_field_get.argtypes = [C.c_int, C.c_int, dp]
         L.ref_field_set.argtypes = [C.c_int, C.c_int, dp]
-        L.ref_step.restype = C.c_double
         L.ref_spmv.argtypes = [C.c_int, C.c_int, dp, dp]
-        _REF = L
-    return _REF
+        if timple:
+            L.ref_timple_params.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double]
+            L.ref_timple_step.restype = C.c_double
+        else:
+            L.ref_step.restype = C.c_double
+        _REF[key] = L
+    return _REF[key]
 
 
 # field ids of ref_shim.c:field_ptr
 FIELD = {"u": 0, "v": 1, "w": 2, "p": 3, "u_new": 4, "v_new": 5, "w_new": 6, "u_old": 7, "v_old": 8,
-         "w_old": 9, "res": 10, "source": 11, "dpdn": 12, "dpdx": 13, "dpdy": 14, "dpdz": 15}
+         "w_old": 9, "res": 10, "source": 11, "dpdn": 12, "dpdx": 13, "dpdy": 14, "dpdz": 15, "p_old": 16,
+         "pprime": 17}
 
 
 @dataclass
@@ -141,10 +154,11 @@ def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
-def ref_pipeline(clouds, ks, polys, phs=3, with_weights=True, search_scale=0.3):
+def ref_pipeline(clouds, ks, polys, phs=3, with_weights=True, search_scale=0.3, timple=False):
     """Runs read_complete_mesh_data's steps (minus the file reader) and
-    create_derivative_matrices through the reference's own code."""
-    R = ref_lib()
+    create_derivative_matrices through the reference's own code (in the
+    TIMPLE build when timple)."""
+    R = ref_lib(timple)
     nl = len(clouds)
     dim = clouds[0].dim
     R.ref_begin(dim, phs, nl)
@@ -303,6 +317,20 @@ class OracleSolver:
             self.O.orc_ctx_free(self.h)
         except Exception:
             pass
+
+
+class TimpleSolver(OracleSolver):
+    """Reference-semantics TIMPLE step (time_implicit_solver, timple_solver.h:40-70)
+    on restated levels: self.p[l] is pprime of level l, self.p_old the pressure."""
+
+    def __init__(self, levels, Re, courant, omega, num_relax, num_vcycles, iter_timple, iter_momentum, facRe, facdt,
+                 jacobi=True, dt=None):
+        super().__init__(levels, Re, courant, omega, num_relax, num_vcycles, jacobi=jacobi, dt=dt)
+        self.p_old = np.zeros(levels[0].n)
+        self.O.orc_ctx_timple(self.h, self.p_old, iter_timple, iter_momentum, facRe, facdt)
+
+    def step(self):
+        return self.O.orc_timple_step(self.h)
 
 
 def lid_bc(L, f):

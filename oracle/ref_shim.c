@@ -15,6 +15,8 @@
  *   create_derivative_matrices        rbf.h:401-421
  *   calculate_dt                      general_functions.h:34-41
  *   fractional_step_explicit & callees  fractional_step_solver.h:47-275
+ *   time_implicit_solver & callees    timple_solver.h:40-410 (built with
+ *                                     -DMGM_REF_TIMPLE into _ref/libref_timple.so)
  *
  * The level set-up mirrors read_complete_mesh_data (mesh_functions.h:914-928)
  * with the mesh reader replaced by arrays handed in by the caller (boundary
@@ -24,7 +26,13 @@
  */
 #include <stdio.h>
 #include <string.h>
+#ifdef MGM_REF_TIMPLE
+/* _ref/libref_timple.so: the same handle over the reference's time-implicit
+ * (TIMPLE) solver, timple_solver.h:40-410, the default of mg_NS_solver.c */
+#include "header_files/timple_solver.h"
+#else
 #include "header_files/fractional_step_solver.h"
+#endif
 #include "init/init_LDC.c"
 #undef INIT_C
 #define initial_conditions tc_initial_conditions
@@ -170,12 +178,31 @@ static double *field_ptr(int lev, int which)
 void ref_field_get(int lev, int which, double *out) { memcpy(out, field_ptr(lev, which), sizeof(double) * g_ps[lev].num_nodes); }
 void ref_field_set(int lev, int which, const double *in) { memcpy(field_ptr(lev, which), in, sizeof(double) * g_ps[lev].num_nodes); }
 
+#ifdef MGM_REF_TIMPLE
+/* TIMPLE parameters (read_flow_parameters, mesh_functions.h:82-91).  The
+ * reference never sets FieldVariables.rho, which update_boundary_pressure
+ * (timple_solver.h:365) reads; it is defined here as parameters.rho. */
+void ref_timple_params(int iter_timple, int iter_momentum, double facRe, double facdt)
+{
+    parameters.iter_timple = (short)iter_timple;
+    parameters.iter_momentum = (short)iter_momentum;
+    parameters.facRe = facRe;
+    parameters.facdt = facdt;
+    for (int l = 0; l < g_levels; l++) { g_field[l].rho = parameters.rho; g_field[l].mu = parameters.mu; }
+}
+double ref_timple_step(void) { return time_implicit_solver(g_ps, g_field); }
+void ref_timple_momentum(void) { calculate_intermediate_velocity_implicit(&g_ps[0], &g_field[0]); }
+void ref_timple_mass(void) { calculate_mass_residual_implicit(&g_ps[0], &g_field[0]); }
+void ref_timple_update_velocity(void) { update_velocity_implicit(&g_ps[0], &g_field[0]); }
+void ref_timple_boundary_pressure(void) { update_boundary_pressure(&g_ps[0], &g_field[0]); }
+#else
 double ref_step(void) { return fractional_step_explicit(g_ps, g_field); }
 void ref_intermediate_velocity(void) { calculate_intermediate_velocity(&g_ps[0], &g_field[0]); }
 void ref_mass_residual(void) { calculate_mass_residual(&g_ps[0], &g_field[0]); }
 void ref_boundary_dpdn(void) { calculate_boundary_dpdn(&g_ps[0], &g_field[0]); }
-void ref_multigrid(void) { multigrid_Poisson_solver(g_ps, g_field); }
 void ref_update_velocity(void) { update_velocity(&g_ps[0], &g_field[0]); }
+#endif
+void ref_multigrid(void) { multigrid_Poisson_solver(g_ps, g_field); }
 void ref_relaxation(int lev) { relaxation(&g_ps[lev], &g_field[lev]); }
 void ref_residuals(int lev) { calculate_residuals(&g_ps[lev], &g_field[lev]); }
 void ref_restrict(int lev) { restrict_residuals(&g_ps[lev], &g_ps[lev + 1], &g_field[lev], &g_field[lev + 1]); }
