@@ -195,9 +195,17 @@ MGM_API int mgm_get_dt(mgm_ctx *ctx, double *dt);
 #define MGM_FIELD_U_NEW 4
 #define MGM_FIELD_V_NEW 5
 #define MGM_FIELD_W_NEW 6
+#define MGM_FIELD_U_OLD 7
+#define MGM_FIELD_V_OLD 8
+#define MGM_FIELD_W_OLD 9
 #define MGM_FIELD_RES 10
 #define MGM_FIELD_SOURCE 11
 #define MGM_FIELD_DPDN 12
+#define MGM_FIELD_DPDX 13
+#define MGM_FIELD_DPDY 14
+#define MGM_FIELD_DPDZ 15
+#define MGM_FIELD_P_OLD 16  /* TIMPLE pressure (the fractional step's pressure is MGM_FIELD_P) */
+#define MGM_FIELD_PPRIME MGM_FIELD_P  /* TIMPLE: the level's pressure correction lives in the P buffer */
 MGM_API int mgm_set_field(mgm_ctx *ctx, int lev, int which, const double *values);
 MGM_API int mgm_get_field(mgm_ctx *ctx, int lev, int which, double *values);
 
@@ -206,6 +214,27 @@ MGM_API int mgm_get_field(mgm_ctx *ctx, int lev, int which, double *values);
 #define MGM_BC_LID 0
 #define MGM_BC_TAYLOR_COUETTE 1
 MGM_API int mgm_apply_bc(mgm_ctx *ctx, int kind);
+
+/* time_implicit_solver (header_files/timple_solver.h:40-70), the default solver
+ * of mg_NS_solver.c: iter_timple outer iterations of iter_momentum implicit
+ * momentum sweeps (calculate_intermediate_velocity_implicit, :72-175), the mass
+ * residual (:177-201), the pressure-correction solve, the velocity and pressure
+ * update (:341-369) and the boundary pressure (:371-410).  Velocities live in
+ * MGM_FIELD_U_NEW/V_NEW/W_NEW (the boundary conditions too), the pressure in
+ * MGM_FIELD_P_OLD.  Momentum sweeps run in data-parallel order (every node from
+ * the previous sweep's values; the reference's C build updates in place).  mode:
+ * MGM_MODE_REFERENCE = the reference's fixed V-cycles on p' (timple variant,
+ * :203-339); MGM_MODE_FP64 / MGM_MODE_FP32_IR = the convergent pinned solve. */
+MGM_API int mgm_set_timple(mgm_ctx *ctx, int iter_timple, int iter_momentum, double facRe, double facdt);
+MGM_API int mgm_timple_step(mgm_ctx *ctx, int mode, double *steady_err);
+/* One part of a TIMPLE iteration, for callers that drive the loop themselves
+ * (the reference's callees): */
+#define MGM_TIMPLE_MOMENTUM 0           /* calculate_intermediate_velocity_implicit (:72-175) */
+#define MGM_TIMPLE_MASS 1               /* calculate_mass_residual_implicit (:177-201) */
+#define MGM_TIMPLE_PRESSURE 2           /* the p' solve (multigrid_Poisson_solver, :203-220, in `mode`) */
+#define MGM_TIMPLE_UPDATE 3             /* update_velocity_implicit (:341-369) */
+#define MGM_TIMPLE_BOUNDARY_PRESSURE 4  /* update_boundary_pressure (:371-410) */
+MGM_API int mgm_timple_part(mgm_ctx *ctx, int part, int mode);
 
 /* Poisson solve modes */
 #define MGM_MODE_REFERENCE 0   /* multigrid_Poisson_solver semantics, fixed num_vcycles (Jacobi-order sweeps) */

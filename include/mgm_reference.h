@@ -161,6 +161,17 @@ MGM_API void calculate_boundary_dpdn(PointStructure *myPointStruct, FieldVariabl
 MGM_API void multigrid_Poisson_solver(PointStructure *myPointStruct, FieldVariables *field);
 MGM_API void update_velocity(PointStructure *myPointStruct, FieldVariables *field);
 
+/* timple_solver.h:40-70, 72-201, 341-410 (the default solver of mg_NS_solver.c).
+ * time_implicit_solver runs the TIMPLE variants of the multigrid routines
+ * (timple_solver.h:203-339) internally; the exported multigrid_Poisson_solver,
+ * relaxation, ... above are the fractional step's.  Momentum sweeps run in
+ * data-parallel order. */
+MGM_API double time_implicit_solver(PointStructure *myPointStruct, FieldVariables *field);
+MGM_API void calculate_intermediate_velocity_implicit(PointStructure *myPointStruct, FieldVariables *field);
+MGM_API void calculate_mass_residual_implicit(PointStructure *myPointStruct, FieldVariables *field);
+MGM_API void update_velocity_implicit(PointStructure *myPointStruct, FieldVariables *field);
+MGM_API void update_boundary_pressure(PointStructure *myPointStruct, FieldVariables *field);
+
 /* No counterpart in the reference: which Poisson solve multigrid_Poisson_solver
  * and fractional_step_explicit run (MGM_MODE_REFERENCE, the default: the
  * reference's fixed V-cycles; MGM_MODE_FP64 / MGM_MODE_FP32_IR: the

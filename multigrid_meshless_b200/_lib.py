@@ -26,7 +26,9 @@ NOALLOC_MAX_NODES = 2097152  # MGM_NOALLOC_MAX_NODES
 BC_LID, BC_TAYLOR_COUETTE = 0, 1
 SETUP_REFERENCE_TRANSFER = 1
 BATCH_AUTOTUNE = 1
-FIELD = {"u": 0, "v": 1, "w": 2, "p": 3, "u_new": 4, "v_new": 5, "w_new": 6, "res": 10, "source": 11, "dpdn": 12}
+FIELD = {"u": 0, "v": 1, "w": 2, "p": 3, "u_new": 4, "v_new": 5, "w_new": 6, "u_old": 7, "v_old": 8, "w_old": 9,
+         "res": 10, "source": 11, "dpdn": 12, "dpdx": 13, "dpdy": 14, "dpdz": 15, "p_old": 16, "pprime": 3}
+TIMPLE_PARTS = {"momentum": 0, "mass": 1, "pressure": 2, "update": 3, "boundary_pressure": 4}
 
 # every exported entry point and its argument types (restype int unless noted)
 SIGNATURES = {
@@ -70,6 +72,9 @@ SIGNATURES = {
     "mgm_use_graphs": ([vp, C.c_int], C.c_int),
     "mgm_use_compact": ([vp, C.c_int], C.c_int),
     "mgm_use_tiled": ([vp, C.c_int], C.c_int),
+    "mgm_set_timple": ([vp, C.c_int, C.c_int, C.c_double, C.c_double], C.c_int),
+    "mgm_timple_step": ([vp, C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "mgm_timple_part": ([vp, C.c_int, C.c_int], C.c_int),
     "mgm_last_solve": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
     "mgm_intermediate_velocity": ([vp], C.c_int),
     "mgm_mass_residual": ([vp], C.c_int),

@@ -214,6 +214,18 @@ class Multigrid:
     def use_compact(self, enable=True):
         check(self.L.mgm_use_compact(self.h, 1 if enable else 0))
 
+    def set_timple(self, iter_timple=1, iter_momentum=1, facRe=1.0, facdt=1.0):
+        check(self.L.mgm_set_timple(self.h, iter_timple, iter_momentum, facRe, facdt))
+
+    def timple_step(self, mode=_lib.MODE_REFERENCE):
+        """time_implicit_solver (timple_solver.h:40-70); returns the steady-state error."""
+        e = C.c_double()
+        check(self.L.mgm_timple_step(self.h, mode, C.byref(e)))
+        return e.value
+
+    def timple_part(self, part, mode=_lib.MODE_REFERENCE):
+        check(self.L.mgm_timple_part(self.h, _lib.TIMPLE_PARTS[part], mode))
+
     def use_tiled(self, enable=True):
         check(self.L.mgm_use_tiled(self.h, 1 if enable else 0))
 

@@ -66,6 +66,11 @@ struct mgm_ctx {
     int num_relax = 3, num_vcycles = 10;
     // level-0 fields
     DBuf<double> u, v, w, u_new, v_new, w_new, dpdn, partial, scal;
+    // TIMPLE state (timple_solver.h): previous time level, pressure, gradients,
+    // and the previous-sweep copies of the momentum iterations
+    DBuf<double> u_old, v_old, w_old, p_old, dpdx, dpdy, dpdz, tu, tv, tw;
+    int iter_timple = 1, iter_momentum = 1;
+    double facRe = 1.0, facdt = 1.0;
     // solver controls and state
     double tol = 1e-8;
     int max_iters = 60, cheb_deg = 3;

@@ -369,6 +369,9 @@ void copyin_field_to_gpu(FieldVariables *field, PointStructure *ps)
     die_if(mgm_set_field(g_ctx, 0, MGM_FIELD_V_NEW, f->v_new), "copyin_field_to_gpu");
     die_if(mgm_set_field(g_ctx, 0, MGM_FIELD_P, f->p), "copyin_field_to_gpu");
     die_if(mgm_set_field(g_ctx, 0, MGM_FIELD_SOURCE, f->source), "copyin_field_to_gpu");
+    // the TIMPLE step's state (timple_solver.h): w_new and the pressure p_old
+    die_if(mgm_set_field(g_ctx, 0, MGM_FIELD_W_NEW, f->w_new), "copyin_field_to_gpu");
+    die_if(mgm_set_field(g_ctx, 0, MGM_FIELD_P_OLD, f->p_old), "copyin_field_to_gpu");
 }
 
 static void need_ctx(const char *fn)
@@ -436,6 +439,82 @@ double fractional_step_explicit(PointStructure *ps, FieldVariables *field)
     if (parameters.dimension == 3) die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_W, f->w), "fractional_step_explicit");
     die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_P, f->p), "fractional_step_explicit");
     die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_SOURCE, f->source), "fractional_step_explicit");
+    return err;
+}
+
+// ---------------------------------------------------------------------------
+// the time-implicit solver (header_files/timple_solver.h), the default of
+// mg_NS_solver.c.  Its multigrid_Poisson_solver / relaxation / ... share their
+// names with the fractional step's; this library's exports of those names
+// are the fractional step's, and time_implicit_solver runs the TIMPLE
+// variants internally.
+// ---------------------------------------------------------------------------
+static void timple_params()
+{
+    die_if(mgm_set_timple(g_ctx, parameters.iter_timple > 0 ? parameters.iter_timple : 1,
+                          parameters.iter_momentum > 0 ? parameters.iter_momentum : 1, parameters.facRe,
+                          parameters.facdt > 0 ? parameters.facdt : 1.0),
+           "TIMPLE parameters");
+}
+
+static void timple_host_view(FieldVariables *f, int n)
+{
+    (void)n;
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_U_NEW, f->u_new), "TIMPLE fields");
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_V_NEW, f->v_new), "TIMPLE fields");
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_U, f->u), "TIMPLE fields");
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_V, f->v), "TIMPLE fields");
+    if (parameters.dimension == 3) {
+        die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_W_NEW, f->w_new), "TIMPLE fields");
+        die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_W, f->w), "TIMPLE fields");
+    }
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_P_OLD, f->p_old), "TIMPLE fields");
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_PPRIME, f->pprime), "TIMPLE fields");
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_SOURCE, f->source), "TIMPLE fields");
+}
+
+// timple_solver.h:72-175
+void calculate_intermediate_velocity_implicit(PointStructure *p, FieldVariables *f)
+{
+    need_ctx("calculate_intermediate_velocity_implicit");
+    timple_params();
+    die_if(mgm_timple_part(g_ctx, MGM_TIMPLE_MOMENTUM, g_mode), "calculate_intermediate_velocity_implicit");
+    timple_host_view(f, p->num_nodes);
+}
+
+// timple_solver.h:177-201
+void calculate_mass_residual_implicit(PointStructure *p, FieldVariables *f)
+{
+    need_ctx("calculate_mass_residual_implicit");
+    die_if(mgm_timple_part(g_ctx, MGM_TIMPLE_MASS, g_mode), "calculate_mass_residual_implicit");
+    timple_host_view(f, p->num_nodes);
+}
+
+// timple_solver.h:341-369
+void update_velocity_implicit(PointStructure *p, FieldVariables *f)
+{
+    need_ctx("update_velocity_implicit");
+    die_if(mgm_timple_part(g_ctx, MGM_TIMPLE_UPDATE, g_mode), "update_velocity_implicit");
+    timple_host_view(f, p->num_nodes);
+}
+
+// timple_solver.h:371-410
+void update_boundary_pressure(PointStructure *p, FieldVariables *f)
+{
+    need_ctx("update_boundary_pressure");
+    die_if(mgm_timple_part(g_ctx, MGM_TIMPLE_BOUNDARY_PRESSURE, g_mode), "update_boundary_pressure");
+    timple_host_view(f, p->num_nodes);
+}
+
+// timple_solver.h:40-70
+double time_implicit_solver(PointStructure *ps, FieldVariables *field)
+{
+    need_ctx("time_implicit_solver");
+    timple_params();
+    double err = 0;
+    die_if(mgm_timple_step(g_ctx, g_mode, &err), "time_implicit_solver");
+    // managed-memory view of level 0 (mg_NS_solver.c:75)
+    timple_host_view(&field[0], ps[0].num_nodes);
     return err;
 }
 

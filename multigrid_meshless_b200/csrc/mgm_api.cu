@@ -88,7 +88,8 @@ __global__ void k_bc(int n, int kind, const double *x, const double *y, double *
     if (kind == MGM_BC_LID) {
         if (fabs(y[i] - 1.0) < 1e-9) { u[i] = 1.0; v[i] = 0.0; }
     } else {
-        const double r = sqrt(x[i] * x[i] + y[i] * y[i]);
+        // init_TC.c:37: every product and sum rounded separately, as in the C build
+        const double r = sqrt(MGM_ADD(MGM_MUL(x[i], x[i]), MGM_MUL(y[i], y[i])));
         if (fabs(r - 0.5) < 1e-9) {
             u[i] = -y[i] / r; v[i] = x[i] / r;
             un[i] = u[i]; vn[i] = v[i];
@@ -491,14 +492,14 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
                                           std::to_string(relres) + " after " + std::to_string(total_it) + " V-cycles)"};
 }
 
-void poisson(mgm_ctx *c, int mode)
+void poisson(mgm_ctx *c, int mode, bool timple = false)
 {
     Level &L0 = c->L[0];
     if (mode == MGM_MODE_REFERENCE) {
         MGM_REQUIRE(c->have_ref_transfer || c->nl == 1, "reference mode needs mgm_setup(..., MGM_SETUP_REFERENCE_TRANSFER)");
         auto R = ref_levels(c);
         const double w1 = (double)c->omega, w2 = (double)(1 - c->omega);
-        ref_multigrid(R, w1, w2, c->num_relax, c->num_vcycles, c->s);
+        ref_multigrid(R, w1, w2, c->num_relax, c->num_vcycles, c->s, timple);
         return;
     }
     // b = source with the pinned row's rhs 0 (boundary rows keep their (zero) source)
@@ -552,6 +553,11 @@ void alloc_solver_buffers(mgm_ctx *c)
 }
 
 }  // namespace
+
+namespace mgm {
+// The Poisson solve of a step on L0.src -> L0.p (the TIMPLE step uses it for p').
+void poisson_solve(mgm_ctx *c, int mode, bool timple) { poisson(c, mode, timple); }
+}  // namespace mgm
 
 // ===========================================================================
 // C ABI
@@ -974,7 +980,11 @@ void prepare_solver(mgm_ctx *c)
     c->cinv32.alloc((size_t)Lc.n * Lc.n);
     dense_inverse(Lc.n, Lc.k, Lc.idx.p, Lc.A64.p, c->cinv64.p, c->cinv32.p, s);
     const int n0 = c->L[0].n;
-    for (DBuf<double> *b : {&c->u, &c->v, &c->w, &c->u_new, &c->v_new, &c->w_new, &c->dpdn}) { b->alloc(n0); b->zero(s); }
+    for (DBuf<double> *b : {&c->u, &c->v, &c->w, &c->u_new, &c->v_new, &c->w_new, &c->dpdn, &c->u_old, &c->v_old,
+                            &c->w_old, &c->p_old, &c->dpdx, &c->dpdy, &c->dpdz, &c->tu, &c->tv, &c->tw}) {
+        b->alloc(n0);
+        b->zero(s);
+    }
     c->partial.alloc(blocks_for(n0, 256) + 8);
     c->scal.alloc(8);
     c->tma_err.alloc(1);
@@ -1216,6 +1226,13 @@ static DBuf<double> *field_buf(mgm_ctx *c, int lev, int which)
         case MGM_FIELD_V_NEW: return &c->v_new;
         case MGM_FIELD_W_NEW: return &c->w_new;
         case MGM_FIELD_DPDN: return &c->dpdn;
+        case MGM_FIELD_U_OLD: return &c->u_old;
+        case MGM_FIELD_V_OLD: return &c->v_old;
+        case MGM_FIELD_W_OLD: return &c->w_old;
+        case MGM_FIELD_DPDX: return &c->dpdx;
+        case MGM_FIELD_DPDY: return &c->dpdy;
+        case MGM_FIELD_DPDZ: return &c->dpdz;
+        case MGM_FIELD_P_OLD: return &c->p_old;
         }
     }
     switch (which) {

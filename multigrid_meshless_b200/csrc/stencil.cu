@@ -240,34 +240,43 @@ __global__ void __launch_bounds__(256) k_ref_sweep(int n, int k, const int *__re
     pout[i] = MGM_ADD(MGM_MUL(w1, MGM_DIV(MGM_SUB(src[i], sum), lapP[i])), MGM_MUL(w2, pin[i]));
 }
 
-// p -= p[0] (:180-183) fused with the all-node residual (:185-191)
+// p -= p[0] (:180-183) fused with the all-node residual (:185-191).  TIMPLE
+// form (timple_solver.h:265-281): the residual uses lap_Poison (passed as lap)
+// on interior rows and is 0 on boundary rows (btag non-null).
 __global__ void __launch_bounds__(256) k_ref_shift_residual(int n, int k, const int *__restrict__ idx,
                                                             const double *__restrict__ lap,
                                                             const double *__restrict__ src,
                                                             const double *__restrict__ pin, double *__restrict__ pout,
-                                                            double *__restrict__ res)
+                                                            double *__restrict__ res, const uint8_t *__restrict__ btag)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double pref = pin[0];
+    pout[i] = MGM_SUB(pin[i], pref);
+    if (btag && btag[i]) { res[i] = 0.0; return; }
     double r = src[i];
     for (int j = 0; j < k; j++) {
         const long o = (long)j * n + i;
         r = MGM_SUB(r, MGM_MUL(lap[o], MGM_SUB(pin[idx[o]], pref)));
     }
     res[i] = r;
-    pout[i] = MGM_SUB(pin[i], pref);
 }
 
-// calculate_residuals (:236-246): interior rows only
+// calculate_residuals (:236-246): interior rows only.  TIMPLE form
+// (timple_solver.h:285-301, zero_boundary): lap_Poison, boundary rows set to 0.
 __global__ void __launch_bounds__(256) k_ref_residual_interior(int n, int k, const int *__restrict__ idx,
                                                                const double *__restrict__ lap,
                                                                const uint8_t *__restrict__ btag,
                                                                const double *__restrict__ src,
-                                                               const double *__restrict__ p, double *__restrict__ res)
+                                                               const double *__restrict__ p, double *__restrict__ res,
+                                                               int zero_boundary)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || btag[i]) return;
+    if (i >= n) return;
+    if (btag[i]) {
+        if (zero_boundary) res[i] = 0.0;
+        return;
+    }
     double sum = 0;
     for (int j = 0; j < k; j++) {
         const long o = (long)j * n + i;
@@ -277,14 +286,20 @@ __global__ void __launch_bounds__(256) k_ref_residual_interior(int n, int k, con
 }
 
 // restrict_residuals (:198-212) / the sum of prolongate_corrections (:216-227):
-// out[i] (+)= sum_j W[j][i] * in[gidx[j][i]] on rows whose tag is 0.
+// out[i] (+)= sum_j W[j][i] * in[gidx[j][i]] on rows whose tag is 0; rows
+// with a tag are left alone, or set to 0 with zero_tagged (the TIMPLE
+// restriction writes every coarse row, timple_solver.h:303-317).
 __global__ void __launch_bounds__(256) k_ref_transfer(int n, int k, const int *__restrict__ gidx,
                                                       const double *__restrict__ W, const uint8_t *__restrict__ btag,
                                                       const double *__restrict__ in, double *__restrict__ out,
-                                                      int accumulate)
+                                                      int accumulate, int zero_tagged)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || btag[i]) return;
+    if (i >= n) return;
+    if (btag[i]) {
+        if (zero_tagged) out[i] = 0.0;
+        return;
+    }
     double r = 0.0;
     for (int j = 0; j < k; j++) {
         const long o = (long)j * n + i;
@@ -299,50 +314,60 @@ __global__ void k_zero_interior(int n, const uint8_t *__restrict__ btag, double 
     if (i < n && !btag[i]) p[i] = 0.0;
 }
 
-void ref_relaxation(const RefLevel &L, double w1, double w2, int num_relax, cudaStream_t s)
+void ref_relaxation(const RefLevel &L, double w1, double w2, int num_relax, cudaStream_t s, bool timple)
 {
     const int nb = blocks_for(L.n, 256);
     for (int it = 0; it < num_relax; it++) {
         k_ref_sweep<<<nb, 256, 0, s>>>(L.n, L.k, L.idx, L.lapP, L.src, L.p, L.ptmp, w1, w2);
         MGM_LAUNCHED();
-        k_ref_shift_residual<<<nb, 256, 0, s>>>(L.n, L.k, L.idx, L.lap, L.src, L.ptmp, L.p, L.res);
+        k_ref_shift_residual<<<nb, 256, 0, s>>>(L.n, L.k, L.idx, timple ? L.lapP : L.lap, L.src, L.ptmp, L.p, L.res,
+                                                timple ? L.btag : nullptr);
         MGM_LAUNCHED();
     }
 }
 
-void ref_residual_interior(const RefLevel &L, cudaStream_t s)
+void ref_residual_interior(const RefLevel &L, cudaStream_t s, bool timple)
 {
-    k_ref_residual_interior<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.idx, L.lap, L.btag, L.src, L.p, L.res);
+    k_ref_residual_interior<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.idx, timple ? L.lapP : L.lap, L.btag,
+                                                                 L.src, L.p, L.res, timple ? 1 : 0);
     MGM_LAUNCHED();
 }
 
-void ref_restrict(const RefLevel &F, const RefLevel &C, cudaStream_t s)
+void ref_restrict(const RefLevel &F, const RefLevel &C, cudaStream_t s, bool timple)
 {
-    k_ref_transfer<<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, F.k, C.r_idx, C.restr, C.btag, F.res, C.src, 0);
+    k_ref_transfer<<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, F.k, C.r_idx, C.restr, C.btag, F.res, C.src, 0,
+                                                        timple ? 1 : 0);
     MGM_LAUNCHED();
 }
 
-void ref_prolongate(const RefLevel &F, const RefLevel &C, cudaStream_t s)
+void ref_prolongate(const RefLevel &F, const RefLevel &C, cudaStream_t s, bool timple)
 {
-    k_ref_transfer<<<blocks_for(F.n, 256), 256, 0, s>>>(F.n, C.k, F.p_idx, F.prol, F.btag, C.p, F.p, 1);
+    k_ref_transfer<<<blocks_for(F.n, 256), 256, 0, s>>>(F.n, C.k, F.p_idx, F.prol, F.btag, C.p, F.p, 1, 0);
     MGM_LAUNCHED();
-    k_zero_interior<<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.btag, C.p);
-    MGM_LAUNCHED();
+    if (timple) {
+        // every coarse correction reset (timple_solver.h:333-338)
+        MGM_CUDA(cudaMemsetAsync(C.p, 0, sizeof(double) * C.n, s));
+    } else {
+        k_zero_interior<<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.btag, C.p);
+        MGM_LAUNCHED();
+    }
 }
 
-// multigrid_Poisson_solver (:150-166)
-void ref_multigrid(std::vector<RefLevel> &Ls, double w1, double w2, int num_relax, int num_vcycles, cudaStream_t s)
+// multigrid_Poisson_solver (fractional_step_solver.h:150-166; the TIMPLE
+// variant timple_solver.h:203-220 has the same cycle over its own routines)
+void ref_multigrid(std::vector<RefLevel> &Ls, double w1, double w2, int num_relax, int num_vcycles, cudaStream_t s,
+                   bool timple)
 {
     const int nl = (int)Ls.size();
     for (int cyc = 0; cyc < num_vcycles; cyc++) {
         for (int l = 0; l < nl; l++) {
-            ref_relaxation(Ls[l], w1, w2, num_relax, s);
-            ref_residual_interior(Ls[l], s);
-            if (l != nl - 1) ref_restrict(Ls[l], Ls[l + 1], s);
+            ref_relaxation(Ls[l], w1, w2, num_relax, s, timple);
+            ref_residual_interior(Ls[l], s, timple);
+            if (l != nl - 1) ref_restrict(Ls[l], Ls[l + 1], s, timple);
         }
         for (int l = nl - 1; l > 0; l--) {
-            ref_prolongate(Ls[l - 1], Ls[l], s);
-            if (l != 1) ref_relaxation(Ls[l - 1], w1, w2, num_relax, s);
+            ref_prolongate(Ls[l - 1], Ls[l], s, timple);
+            if (l != 1) ref_relaxation(Ls[l - 1], w1, w2, num_relax, s, timple);
         }
     }
 }

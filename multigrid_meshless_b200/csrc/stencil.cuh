@@ -38,11 +38,13 @@ struct RefLevel {
     const double *prol;
 };
 
-void ref_relaxation(const RefLevel &L, double w1, double w2, int num_relax, cudaStream_t s);
-void ref_residual_interior(const RefLevel &L, cudaStream_t s);
-void ref_restrict(const RefLevel &F, const RefLevel &C, cudaStream_t s);
-void ref_prolongate(const RefLevel &F, const RefLevel &C, cudaStream_t s);
-void ref_multigrid(std::vector<RefLevel> &Ls, double w1, double w2, int num_relax, int num_vcycles, cudaStream_t s);
+// timple: the TIMPLE solver's variants (timple_solver.h:203-339)
+void ref_relaxation(const RefLevel &L, double w1, double w2, int num_relax, cudaStream_t s, bool timple = false);
+void ref_residual_interior(const RefLevel &L, cudaStream_t s, bool timple = false);
+void ref_restrict(const RefLevel &F, const RefLevel &C, cudaStream_t s, bool timple = false);
+void ref_prolongate(const RefLevel &F, const RefLevel &C, cudaStream_t s, bool timple = false);
+void ref_multigrid(std::vector<RefLevel> &Ls, double w1, double w2, int num_relax, int num_vcycles, cudaStream_t s,
+                   bool timple = false);
 
 // ---------------------------------------------------------------------------
 // convergent solver (solver.cu)

@@ -3,7 +3,12 @@
  * (the flow of mg_NS_solver.c:17-103 with the mesh reader replaced by a node
  * file), linked against libmgm.so through include/mgm_reference.h.
  *
- *   legacy_driver <input.bin> <output_dir>
+ *   legacy_driver <input.bin> <output_dir> [timple]
+ *
+ * With "timple" the time loop is the reference main's default,
+ * time_implicit_solver (timple_solver.h:40-70), on the Taylor-Couette
+ * conditions of init_TC.c (iter_timple = iter_momentum = 2, facRe = facdt = 1);
+ * otherwise fractional_step_explicit on the lid-driven cavity (init_LDC.c).
  *
  * input.bin: int32 nl, dim, phs, poly, multiplier, nsteps, num_vcycles,
  *            num_relax, mode; double Re, courant, omega; per level: int32 n,
@@ -49,7 +54,8 @@ static void wr_rows_i(const char *dir, const char *name, int **rows, int n, int 
 
 int main(int argc, char **argv)
 {
-    if (argc < 3) { fprintf(stderr, "usage: legacy_driver input.bin outdir\n"); return 1; }
+    if (argc < 3) { fprintf(stderr, "usage: legacy_driver input.bin outdir [timple]\n"); return 1; }
+    const int timple = argc > 3 && strcmp(argv[3], "timple") == 0;
     FILE *f = fopen(argv[1], "rb");
     if (!f) { fprintf(stderr, "cannot open %s\n", argv[1]); return 1; }
     const char *out = argv[2];
@@ -109,18 +115,34 @@ int main(int argc, char **argv)
     create_prolongation_and_restriction_matrices(ps, (short)nl);
     for (int l = 0; l < nl; l++) create_derivative_matrices(&ps[l]);
 
-    /* mg_NS_solver.c:47-59 with the lid-driven cavity conditions (init_LDC.c) */
+    /* mg_NS_solver.c:47-59 with the lid-driven cavity conditions (init_LDC.c)
+     * or, for TIMPLE, the Taylor-Couette ones (init_TC.c:33-52) */
     FieldVariables *field;
     AllocateMemoryFieldVariables(&field, ps, nl);
-    for (int i = 0; i < ps[0].num_nodes; i++)
-        if (fabs(ps[0].y[i] - 1.0) < 1e-9) field[0].u[i] = 1.0;
+    for (int i = 0; i < ps[0].num_nodes; i++) {
+        if (!timple) {
+            if (fabs(ps[0].y[i] - 1.0) < 1e-9) field[0].u[i] = 1.0;
+        } else {
+            const double x = ps[0].x[i], y = ps[0].y[i], r = sqrt(x * x + y * y);
+            if (fabs(r - 0.5) < 1e-9) {
+                field[0].u[i] = -y / r; field[0].v[i] = x / r;
+                field[0].u_new[i] = -y / r; field[0].v_new[i] = x / r;
+            }
+        }
+    }
+    if (timple) {
+        parameters.iter_timple = 2;
+        parameters.iter_momentum = 2;
+        parameters.facRe = 1.0;
+        parameters.facdt = 1.0;
+    }
     parameters.dt = calculate_dt(&ps[0]);
     copyin_essentials_to_gpu(ps);
     copyin_field_to_gpu(field, ps);
     copyin_parameters_to_gpu();
 
     double *errs = malloc(sizeof(double) * (nsteps > 0 ? nsteps : 1));
-    for (int s = 0; s < nsteps; s++) errs[s] = fractional_step_explicit(ps, field);
+    for (int s = 0; s < nsteps; s++) errs[s] = timple ? time_implicit_solver(ps, field) : fractional_step_explicit(ps, field);
 
     for (int l = 0; l < nl; l++) {
         PointStructure *p = &ps[l];
@@ -152,6 +174,9 @@ int main(int argc, char **argv)
     wr(out, "u", field[0].u, sizeof(double) * ps[0].num_nodes);
     wr(out, "v", field[0].v, sizeof(double) * ps[0].num_nodes);
     wr(out, "p", field[0].p, sizeof(double) * ps[0].num_nodes);
+    wr(out, "u_new", field[0].u_new, sizeof(double) * ps[0].num_nodes);
+    wr(out, "v_new", field[0].v_new, sizeof(double) * ps[0].num_nodes);
+    wr(out, "p_old", field[0].p_old, sizeof(double) * ps[0].num_nodes);
     printf("legacy driver done: %d levels, %d steps\n", nl, nsteps);
     return 0;
 }

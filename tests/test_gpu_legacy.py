@@ -88,3 +88,49 @@ def test_reference_call_surface_end_to_end(require_gpu, tmp_path):
     assert np.array_equal(_read(out, "u", np.float64), S.f["u"])
     assert np.array_equal(_read(out, "v", np.float64), S.f["v"])
     assert np.array_equal(_read(out, "p", np.float64), S.p[0])
+
+
+def test_reference_call_surface_timple(require_gpu, tmp_path):
+    """The reference main's default loop, time_implicit_solver, called by name
+    from C through libmgm.so (reference-semantics multigrid on p'), against
+    the TIMPLE restatement in the same data-parallel sweep order.  The coarse
+    annulus holds node pairs one gap apart across the channel (squared
+    distance 0.25 (1 - 2^-53), whose power 1.5 lies 2^-107 from a rounding
+    midpoint), so the set-up comparison also covers the near-midpoint
+    rounding of the power helpers."""
+    exe = _compile(str(tmp_path))
+    cl = clouds.annulus_hierarchy(0.06, 2, seed=3)
+    k, poly = 20, 3
+    inp = str(tmp_path / "in.bin")
+    out = str(tmp_path / "out")
+    os.makedirs(out)
+    _write_input(inp, cl, poly, 2, 3, 3, 2, 0, 100.0, 0.5, 1.0)
+    r = subprocess.run([exe, inp, out, "timple"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    P = O.orc_pipeline(cl, [k, k], [poly, poly], crpow=True)
+    levels = []
+    for l, L in enumerate(P):
+        n = L.n
+        assert np.array_equal(_read(out, f"l{l}_cloud", np.int32, (n, k)), L.cloud), (l, "cloud")
+        for nm in ("x", "y", "nx", "ny"):
+            assert np.array_equal(_read(out, f"l{l}_{nm}", np.float64), getattr(L, nm)), (l, nm)
+        ops = {nm: _read(out, f"l{l}_{nm}", np.float64, (n, k)) for nm in ("Dx", "Dy", "lap", "lapP")}
+        for nm, v in ops.items():
+            assert np.array_equal(v, getattr(L, nm)), (l, nm)
+        restr = _read(out, f"l{l}_restr", np.float64, (n, k)) if l > 0 else None
+        prol = _read(out, f"l{l}_prol", np.float64, (n, k)) if l < len(P) - 1 else None
+        for nm, got, want in (("restr", restr, L.restr), ("prol", prol, L.prol)):
+            if got is not None:
+                assert np.array_equal(got, want), (l, nm)
+        levels.append(O.Level(n, L.nb, k, 2, poly, L.x, L.y, L.z, L.nx, L.ny, L.nz, L.btag, L.cloud, L.d_avg,
+                              ops["Dx"], ops["Dy"], None, ops["lap"], ops["lapP"], L.rpts, L.ppts, restr, prol))
+    S = O.TimpleSolver(levels, 100.0, 0.5, 1.0, 2, 3, 2, 2, 1.0, 1.0, jacobi=True)
+    assert S.dt == _read(out, "dt", np.float64)[0]
+    O.tc_bc(levels[0], S.f)
+    errs = _read(out, "errs", np.float64)
+    for s in range(3):
+        e = S.step()
+        assert abs(errs[s] - e) <= 1e-12 * abs(e)
+    for nm in ("u_new", "v_new"):
+        assert np.array_equal(_read(out, nm, np.float64), S.f[nm]), nm
+    assert np.array_equal(_read(out, "p_old", np.float64), S.p_old)
