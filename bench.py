@@ -211,9 +211,9 @@ def measured_peak():
 
 def ncu_traffic():
     """DRAM bytes per launch of the level-0 smoother from the committed ncu summary
-    (profiles/k_level_tiled_r_cavity1m.md), to be scaled by node count."""
+    (profiles/k_level_v4_cavity1m.md), to be scaled by node count."""
     import re
-    path = os.path.join(ROOT, "profiles", "k_level_tiled_r_cavity1m.md")
+    path = os.path.join(ROOT, "profiles", "k_level_v4_cavity1m.md")
     try:
         txt = open(path).read()
         b = re.search(r"dram_bytes_per_launch:\s*(\d+)", txt)
@@ -425,8 +425,9 @@ def run_ours(a, rank, world, local_rank):
                              "the measured learned arm is in learned_warm_start)"),
             "e2e": {"value": steps_total / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": 2 * 8 * n,
                     "d2h_bytes_per_step": 3 * 8 * n, "finite": finite},
-            "roofline": {"bound": "hbm", "kernel": ("level-0 FP32 Chebyshev smoother step (k_level_tiled_r: int16 "
-                                                    "offsets, operator tiles streamed by bulk async copies)"),
+            "roofline": {"bound": "hbm", "kernel": ("level-0 FP32 Chebyshev smoother step (k_level_v4<0>: FP32 "
+                                                    "weights + int16 offsets, slots sorted by neighbour, four rows "
+                                                    "per thread with vector loads)"),
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "bytes_per_launch": sm_bytes, "launches": sm_launch,

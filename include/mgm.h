@@ -259,8 +259,9 @@ MGM_API int mgm_use_compact(mgm_ctx *ctx, int enable);
  * kernels one by one (enable = 0).  Results are identical either way. */
 MGM_API int mgm_use_graphs(mgm_ctx *ctx, int enable);
 /* FP32 compact path: on levels of at least 65,536 rows, stream the operator
- * tile by tile into shared memory with bulk asynchronous copies (default 1);
- * 0 = plain loads.  Same results either way. */
+ * tile by tile into shared memory with bulk asynchronous copies (enable = 1),
+ * or read it with plain vector loads, four rows per thread (enable = 0, the
+ * default, faster on B200).  Same results either way. */
 MGM_API int mgm_use_tiled(mgm_ctx *ctx, int enable);
 /* Statistics of the last Poisson solve: outer iterations (V-cycles) and the
  * true relative residual ||b - A p|| / ||b|| over rows != 0 (FP64). */

@@ -24,16 +24,20 @@ struct Level {
     DBuf<int> s_r_idx, s_p_idx;
     DBuf<double> s_r_w64, s_p_w64;
     DBuf<float> s_r_w32, s_p_w32;
-    // pinned operator
+    // pinned operator: FP64 in the level's slot order [k][n]; FP32 with each
+    // row's slots sorted by neighbour index, [k][ld4] (rows padded to a
+    // multiple of 4 with zero weights), indices in sidx
     DBuf<double> A64, dinv64;
     DBuf<float> A32, dinv32;
+    DBuf<int> sidx;
+    int ld4 = 0;
     DBuf<int> bnd_list;
     DBuf<int> bnd_idx;           // boundary rows' stencils, row-major [nbl][k]
     DBuf<double> bnd_A64;
     DBuf<float> bnd_A32;
     int nbl = 0;
     double lmax = 2.0;
-    // compact FP32-path indices (int16 offsets)
+    // compact FP32-path indices (int16 offsets): off16 [k][ld4] (sorted slots), r_off16/p_off16 [k][n]
     DBuf<short> off16, r_off16, p_off16;
     bool off_ok = false, r_off_ok = false, p_off_ok = false;
     // the compact operator again, tile-major ([ld / kTileRows][k][kTileRows],
@@ -84,7 +88,7 @@ struct mgm_ctx {
     long long vcycles_in_solve = 0;   // V-cycles of the last solve
     double last_learned_alpha = 0;    // step length the last solve took along the learned direction
     int warm_smooth_steps = 3;        // Chebyshev steps that clean the learned direction
-    bool use_tma = true;              // tile-streamed level kernels where a level has them
+    bool use_tma = false;             // tile-streamed level kernels where a level has them (else 4 rows per thread)
     DBuf<int> tma_err;                // set by a tile-streamed kernel whose bounded wait ran out
     double *h_pinned = nullptr;
     SmootherProfile prof;

@@ -69,7 +69,7 @@ __global__ void k_gather_idx(int n, int k, const int *__restrict__ pts, const in
 }
 
 __global__ void k_pin_operator(int n, int k, const double *__restrict__ lapP, double *__restrict__ A64,
-                               float *__restrict__ A32, double *__restrict__ d64, float *__restrict__ d32)
+                               double *__restrict__ d64, float *__restrict__ d32)
 {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)n * k) return;
@@ -77,7 +77,6 @@ __global__ void k_pin_operator(int n, int k, const double *__restrict__ lapP, do
     double a = lapP[t];
     if (i == 0) a = (j == 0) ? 1.0 : 0.0;  // pinned row p[0] = 0
     A64[t] = a;
-    A32[t] = (float)a;
     if (j == 0) { d64[i] = 1.0 / a; d32[i] = (float)(1.0 / a); }
 }
 
@@ -100,20 +99,49 @@ __global__ void k_bc(int n, int kind, const double *x, const double *y, double *
 __global__ void k_zero_pinned(double *b) { b[0] = 0.0; }
 
 // int16 offsets of a gather index from a per-row base node (base = nullptr: the row itself)
-__global__ void k_make_offsets(int n, int k, const int *__restrict__ gidx, const int *__restrict__ base,
+// ELL [k][ld] int16 offsets gidx - base (base: per-row node, or the row itself);
+// padding rows (n <= i < ld) get offset 0
+__global__ void k_make_offsets(int n, int ld, int k, const int *__restrict__ gidx, const int *__restrict__ base,
                                short *__restrict__ off, int *__restrict__ overflow)
 {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)n * k) return;
-    const int i = (int)(t % n);
+    if (t >= (long)ld * k) return;
+    const int i = (int)(t % ld);
+    if (i >= n) { off[t] = 0; return; }
     const int d = gidx[t] - (base ? base[i] : i);
     if (d > 32767 || d < -32768) atomicOr(overflow, 1);
     off[t] = (short)d;
 }
 
-// tile-major copy of an ELL array: out[(t*k + j)*kTileRows + r] = in[j][t*kTileRows + r], zero past row n
+// The FP32 solver operator with each row's slots sorted by neighbour index
+// (consecutive rows then gather from nearby addresses in the same slot), [k][ld]
+// with ld >= n a multiple of 4; padding rows get weight 0 and index 0.
+__global__ void __launch_bounds__(128) k_sort_slots(int n, int k, int ld, const int *__restrict__ idx,
+                                                    const double *__restrict__ A64, int *__restrict__ sidx,
+                                                    float *__restrict__ A32)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ld) return;
+    if (i >= n) {
+        for (int j = 0; j < k; j++) { sidx[(long)j * ld + i] = 0; A32[(long)j * ld + i] = 0.f; }
+        return;
+    }
+    int c[kMaxK];
+    float a[kMaxK];
+    for (int j = 0; j < k; j++) {
+        const int cj = idx[(long)j * n + i];
+        const float aj = (float)A64[(long)j * n + i];
+        int p = j;
+        while (p > 0 && c[p - 1] > cj) { c[p] = c[p - 1]; a[p] = a[p - 1]; p--; }
+        c[p] = cj;
+        a[p] = aj;
+    }
+    for (int j = 0; j < k; j++) { sidx[(long)j * ld + i] = c[j]; A32[(long)j * ld + i] = a[j]; }
+}
+
+// tile-major copy of an ELL array [k][ldin]: out[(t*k + j)*kTileRows + r] = in[j][t*kTileRows + r], zero past row n
 template <class T>
-__global__ void k_tile_major(int n, int k, int ld, const T *__restrict__ in, T *__restrict__ out)
+__global__ void k_tile_major(int n, int k, int ld, int ldin, const T *__restrict__ in, T *__restrict__ out)
 {
     const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (long)k * ld) return;
@@ -121,7 +149,7 @@ __global__ void k_tile_major(int n, int k, int ld, const T *__restrict__ in, T *
     const long tj = e / kTileRows;
     const int j = (int)(tj % k);
     const long row = (tj / k) * kTileRows + r;
-    out[e] = row < n ? in[(long)j * n + row] : T(0);
+    out[e] = row < n ? in[(long)j * ldin + row] : T(0);
 }
 
 // compact copies of the boundary rows of the pinned operator: out[w][j] = A[j][list[w]]
@@ -194,7 +222,7 @@ std::vector<SolveLevel<double>> solve_levels<double>(mgm_ctx *c)
     for (int l = 0; l < c->nl; l++) {
         Level &L = c->L[l];
         SolveLevel<double> S{};
-        S.n = L.n; S.k = L.k; S.nb_list = L.nbl;
+        S.n = L.n; S.k = L.k; S.ld = L.n; S.nb_list = L.nbl;
         S.idx = L.idx.p; S.A = L.A64.p; S.dinv = L.dinv64.p; S.btag = L.btag.p; S.bnd_list = L.bnd_list.p;
         S.bnd_idx = L.bnd_idx.p; S.bnd_A = L.bnd_A64.p;
         S.r = L.r64.p; S.e = L.e64.p; S.e2 = L.e64b.p; S.d = L.d64.p; S.q = L.q64.p;
@@ -213,8 +241,8 @@ std::vector<SolveLevel<float>> solve_levels<float>(mgm_ctx *c)
     for (int l = 0; l < c->nl; l++) {
         Level &L = c->L[l];
         SolveLevel<float> S{};
-        S.n = L.n; S.k = L.k; S.nb_list = L.nbl;
-        S.idx = L.idx.p; S.A = L.A32.p; S.dinv = L.dinv32.p; S.btag = L.btag.p; S.bnd_list = L.bnd_list.p;
+        S.n = L.n; S.k = L.k; S.ld = L.ld4; S.nb_list = L.nbl;
+        S.idx = L.sidx.p; S.A = L.A32.p; S.dinv = L.dinv32.p; S.btag = L.btag.p; S.bnd_list = L.bnd_list.p;
         S.bnd_idx = L.bnd_idx.p; S.bnd_A = L.bnd_A32.p;
         S.r = L.r32.p; S.e = L.e32.p; S.e2 = L.e32b.p; S.d = L.d32.p; S.q = L.q32.p;
         S.kr = l > 0 ? c->L[l - 1].k : 0; S.r_idx = L.s_r_idx.p; S.r_w = L.s_r_w32.p;
@@ -905,9 +933,13 @@ void prepare_solver(mgm_ctx *c)
     for (int l = 0; l < c->nl; l++) {
         Level &L = c->L[l];
         const size_t nk = (size_t)L.n * L.k;
-        L.A64.alloc(nk); L.A32.alloc(nk); L.dinv64.alloc(L.n); L.dinv32.alloc(L.n);
-        k_pin_operator<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.lapP.p, L.A64.p, L.A32.p, L.dinv64.p,
+        L.ld4 = (L.n + 3) & ~3;
+        const size_t nk4 = (size_t)L.ld4 * L.k;
+        L.A64.alloc(nk); L.A32.alloc(nk4); L.sidx.alloc(nk4); L.dinv64.alloc(L.n); L.dinv32.alloc(L.n);
+        k_pin_operator<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.lapP.p, L.A64.p, L.dinv64.p,
                                                                L.dinv32.p);
+        MGM_LAUNCHED();
+        k_sort_slots<<<blocks_for(L.ld4, 128), 128, 0, s>>>(L.n, L.k, L.ld4, L.idx.p, L.A64.p, L.sidx.p, L.A32.p);
         MGM_LAUNCHED();
         std::vector<uint8_t> hb(L.n);
         L.btag.download(hb.data(), L.n, s);
@@ -927,20 +959,21 @@ void prepare_solver(mgm_ctx *c)
         {
             DBuf<int> ovf(3);
             ovf.zero(s);
-            L.off16.alloc(nk);
-            k_make_offsets<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.idx.p, nullptr, L.off16.p, ovf.p);
+            L.off16.alloc(nk4);
+            k_make_offsets<<<blocks_for((long)nk4, 256), 256, 0, s>>>(L.n, L.ld4, L.k, L.sidx.p, nullptr, L.off16.p,
+                                                                    ovf.p);
             MGM_LAUNCHED();
             if (l > 0) {
                 const int kr = c->L[l - 1].k;
                 L.r_off16.alloc((size_t)L.n * kr);
-                k_make_offsets<<<blocks_for((long)L.n * kr, 256), 256, 0, s>>>(L.n, kr, L.s_r_idx.p, L.rpts.p,
+                k_make_offsets<<<blocks_for((long)L.n * kr, 256), 256, 0, s>>>(L.n, L.n, kr, L.s_r_idx.p, L.rpts.p,
                                                                              L.r_off16.p, ovf.p + 1);
                 MGM_LAUNCHED();
             }
             if (l < c->nl - 1) {
                 const int kp = c->L[l + 1].k;
                 L.p_off16.alloc((size_t)L.n * kp);
-                k_make_offsets<<<blocks_for((long)L.n * kp, 256), 256, 0, s>>>(L.n, kp, L.s_p_idx.p, L.ppts.p,
+                k_make_offsets<<<blocks_for((long)L.n * kp, 256), 256, 0, s>>>(L.n, L.n, kp, L.s_p_idx.p, L.ppts.p,
                                                                              L.p_off16.p, ovf.p + 2);
                 MGM_LAUNCHED();
             }
@@ -960,9 +993,9 @@ void prepare_solver(mgm_ctx *c)
             L.A32t.alloc((size_t)L.k * ld);
             L.off16t.alloc((size_t)L.k * ld);
             const long tot = (long)L.k * ld;
-            k_tile_major<float><<<blocks_for(tot, 256), 256, 0, s>>>(L.n, L.k, ld, L.A32.p, L.A32t.p);
+            k_tile_major<float><<<blocks_for(tot, 256), 256, 0, s>>>(L.n, L.k, ld, L.ld4, L.A32.p, L.A32t.p);
             MGM_LAUNCHED();
-            k_tile_major<short><<<blocks_for(tot, 256), 256, 0, s>>>(L.n, L.k, ld, L.off16.p, L.off16t.p);
+            k_tile_major<short><<<blocks_for(tot, 256), 256, 0, s>>>(L.n, L.k, ld, L.ld4, L.off16.p, L.off16t.p);
             MGM_LAUNCHED();
             L.ldt = ld;
         }

@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(256) k_bnd_exact(int nbl, const int *__restric
 // One Chebyshev step on interior rows: q = r - A e, d = c1*d + c2*D^-1 q, e' = e + d.
 // Boundary rows copy e.  zero_start: e is zero except on boundary rows.
 template <class T>
-__global__ void __launch_bounds__(256) k_cheb(int n, int k, const int *__restrict__ idx, const T *__restrict__ A,
+__global__ void __launch_bounds__(256) k_cheb(int n, int ld, int k, const int *__restrict__ idx, const T *__restrict__ A,
                                               const T *__restrict__ dinv, const uint8_t *__restrict__ btag,
                                               const T *__restrict__ r, const T *__restrict__ e, T *__restrict__ eout,
                                               T *__restrict__ d, T c1, T c2, int first)
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(256) k_cheb(int n, int k, const int *__restric
     if (i >= n) return;
     const T ei = e[i];
     if (btag[i]) { eout[i] = ei; return; }
-    const T q = r[i] - ell_row_dot(idx, A, e, n, k, i);
+    const T q = r[i] - ell_row_dot(idx, A, e, ld, k, i);
     const T di = first ? c2 * dinv[i] * q : c1 * d[i] + c2 * dinv[i] * q;
     d[i] = di;
     eout[i] = ei + di;
@@ -80,14 +80,14 @@ __global__ void __launch_bounds__(256) k_cheb(int n, int k, const int *__restric
 
 // residual on interior rows (boundary rows are solved exactly: 0)
 template <class T>
-__global__ void __launch_bounds__(256) k_residual(int n, int k, const int *__restrict__ idx, const T *__restrict__ A,
-                                                  const uint8_t *__restrict__ btag, const T *__restrict__ r,
-                                                  const T *__restrict__ e, T *__restrict__ q)
+__global__ void __launch_bounds__(256) k_residual(int n, int ld, int k, const int *__restrict__ idx,
+                                                  const T *__restrict__ A, const uint8_t *__restrict__ btag,
+                                                  const T *__restrict__ r, const T *__restrict__ e, T *__restrict__ q)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (btag[i]) { q[i] = T(0); return; }
-    q[i] = r[i] - ell_row_dot(idx, A, e, n, k, i);
+    q[i] = r[i] - ell_row_dot(idx, A, e, ld, k, i);
 }
 
 // coarse rhs: r_c[i] = sum_j Rw[j][i] q_f[Ridx[j][i]] on interior coarse rows, 0 elsewhere
@@ -148,31 +148,110 @@ __device__ __forceinline__ float ell_row_dot_o(const short *__restrict__ off, co
     return s;
 }
 
-__global__ void __launch_bounds__(256) k_cheb_o(int n, int k, const short *__restrict__ off,
-                                                const float *__restrict__ A, const float *__restrict__ dinv,
-                                                const uint8_t *__restrict__ btag, const float *__restrict__ r,
-                                                const float *__restrict__ e, float *__restrict__ eout,
-                                                float *__restrict__ d, float c1, float c2, int first)
+// Compact level kernels (FP32 weights, int16 offsets, ELL [k][ld]).
+//
+// k_level_v4: four consecutive rows per thread; the weights and offsets of
+// rows i0..i0+3 come in as one 16-byte and one 8-byte load per stencil slot
+// (ld a multiple of 4; streamed past L1 with evict-first loads), so a thread
+// has 8 operator loads and 16 gathers in flight per 4 slots.  For the large
+// levels, which are bandwidth-bound.
+// k_level_c1: one row per thread, for the small levels, which are latency-
+// bound and need the threads more than the wide loads.
+// Each row's sum runs in slot order in both, as in every other FP32 level
+// kernel, so all of them give the same bits.  MODE 0: Chebyshev step
+// q = r - A e, d = c1 d + c2 D^-1 q, e' = e + d on interior rows (boundary
+// rows copy e); MODE 1: residual q = r - A e on interior rows, 0 on boundary rows.
+template <int MODE>
+__device__ __forceinline__ void level_row_out(int i, float s, const float *__restrict__ dinv,
+                                              const uint8_t *__restrict__ btag, const float *__restrict__ r,
+                                              const float *__restrict__ e, float *__restrict__ out,
+                                              float *__restrict__ d, float c1, float c2, int first)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float ei = e[i];
-    if (btag[i]) { eout[i] = ei; return; }
-    const float q = r[i] - ell_row_dot_o(off, A, e, n, k, i, i);
-    const float di = first ? c2 * dinv[i] * q : c1 * d[i] + c2 * dinv[i] * q;
-    d[i] = di;
-    eout[i] = ei + di;
+    if (MODE == 0) {
+        const float ei = e[i];
+        if (btag[i]) { out[i] = ei; return; }
+        const float q = r[i] - s;
+        const float di = first ? c2 * dinv[i] * q : c1 * d[i] + c2 * dinv[i] * q;
+        d[i] = di;
+        out[i] = ei + di;
+    } else {
+        out[i] = btag[i] ? 0.f : r[i] - s;
+    }
 }
 
-__global__ void __launch_bounds__(256) k_residual_o(int n, int k, const short *__restrict__ off,
-                                                    const float *__restrict__ A, const uint8_t *__restrict__ btag,
-                                                    const float *__restrict__ r, const float *__restrict__ e,
-                                                    float *__restrict__ q)
+template <int MODE>
+__global__ void __launch_bounds__(256) k_level_c1(int n, int ld, int k, const short *__restrict__ off,
+                                                  const float *__restrict__ A, const float *__restrict__ dinv,
+                                                  const uint8_t *__restrict__ btag, const float *__restrict__ r,
+                                                  const float *__restrict__ e, float *__restrict__ out,
+                                                  float *__restrict__ d, float c1, float c2, int first)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    if (btag[i]) { q[i] = 0.f; return; }
-    q[i] = r[i] - ell_row_dot_o(off, A, e, n, k, i, i);
+    if (btag[i]) {
+        out[i] = MODE == 0 ? e[i] : 0.f;
+        return;
+    }
+    level_row_out<MODE>(i, ell_row_dot_o(off, A, e, ld, k, i, i), dinv, btag, r, e, out, d, c1, c2, first);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_level_v4(int n, int ld, int k, const short *__restrict__ off,
+                                                  const float *__restrict__ A, const float *__restrict__ dinv,
+                                                  const uint8_t *__restrict__ btag, const float *__restrict__ r,
+                                                  const float *__restrict__ e, float *__restrict__ out,
+                                                  float *__restrict__ d, float c1, float c2, int first)
+{
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    if (i0 >= n) return;
+    float s[4] = {0.f, 0.f, 0.f, 0.f};
+    int j = 0;
+    for (; j + 4 <= k; j += 4) {
+        float a[4][4];
+        int c[4][4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const long o = (long)(j + q) * ld + i0;
+            const float4 av = __ldcs(reinterpret_cast<const float4 *>(A + o));
+            const uint2 ov = __ldcs(reinterpret_cast<const uint2 *>(off + o));
+            a[q][0] = av.x; a[q][1] = av.y; a[q][2] = av.z; a[q][3] = av.w;
+            c[q][0] = i0 + (int)(short)(ov.x & 0xffffu);
+            c[q][1] = i0 + 1 + (int)(short)(ov.x >> 16);
+            c[q][2] = i0 + 2 + (int)(short)(ov.y & 0xffffu);
+            c[q][3] = i0 + 3 + (int)(short)(ov.y >> 16);
+        }
+        // padding rows (i >= n) carry weight 0 and offset 0: clamp their gathers into the vector
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int v = 0; v < 4; v++) s[v] += a[q][v] * __ldg(e + min(c[q][v], n - 1));
+    }
+    for (; j < k; j++) {
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const long o = (long)j * ld + i0 + v;
+            s[v] += __ldcs(A + o) * __ldg(e + min(i0 + v + (int)__ldcs(off + o), n - 1));
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 4; v++)
+        if (i0 + v < n) level_row_out<MODE>(i0 + v, s[v], dinv, btag, r, e, out, d, c1, c2, first);
+}
+
+// rows from which a compact level runs k_level_v4 (below: k_level_c1)
+constexpr int kVecMinRows = 65536;
+
+template <int MODE>
+static void launch_compact(const SolveLevel<float> &L, const float *e, float *out, float c1, float c2, int first,
+                           cudaStream_t s)
+{
+    if (L.n >= kVecMinRows)
+        k_level_v4<MODE><<<blocks_for((L.n + 3) / 4, 256), 256, 0, s>>>(L.n, L.ld, L.k, L.off, L.A, L.dinv, L.btag,
+                                                                        L.r, e, out, L.d, c1, c2, first);
+    else
+        k_level_c1<MODE><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.ld, L.k, L.off, L.A, L.dinv, L.btag, L.r, e,
+                                                              out, L.d, c1, c2, first);
+    MGM_LAUNCHED();
 }
 
 __global__ void __launch_bounds__(256) k_restrict_o(int n, int k, const short *__restrict__ off,
@@ -209,7 +288,7 @@ __global__ void __launch_bounds__(256) k_prolong_o(int n, int k, const short *__
 // operator streams in while this tile's rows gather their neighbours.  A
 // thread then reads its row's stencil from shared memory and issues its
 // neighbour gathers back to back.  The products are summed in slot order, as
-// in k_cheb_o / k_residual_o, so the results are the same bits.
+// in k_level_v4, so the results are the same bits.
 //
 // Every mbarrier wait is bounded: on time-out the CTA sets *err, waits (again
 // bounded) for the copies it still has in flight, and stops.
@@ -278,7 +357,7 @@ __device__ __forceinline__ void tile_issue(unsigned char *st, uint64_t *bar, int
     bulk_g2s(st + L.o_off(), offt + t0, (unsigned)(k * kTileRows * sizeof(short)), bar);
 }
 
-// MODE 0: Chebyshev step (as k_cheb_o); MODE 1: residual (as k_residual_o).
+// MODE 0: Chebyshev step (as k_level_v4<0>); MODE 1: residual (as k_level_v4<1>).
 // Chunked variant for any k <= kTileMaxK: the row's stencil is read from the
 // stage while its gathers run, 8 at a time.
 template <int MODE>
@@ -568,15 +647,14 @@ static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, 
             if (L.At) {
                 launch_tiled<0>(L, L.e, L.e2, (float)c1, (float)c2, step == 0 ? 1 : 0, s);
             } else if (L.off) {
-                k_cheb_o<<<nb, 256, 0, s>>>(L.n, L.k, L.off, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d, (float)c1,
-                                            (float)c2, step == 0 ? 1 : 0);
+                launch_compact<0>(L, L.e, L.e2, (float)c1, (float)c2, step == 0 ? 1 : 0, s);
             } else {
-                k_cheb<T><<<nb, 256, 0, s>>>(L.n, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d, (T)c1,
+                k_cheb<T><<<nb, 256, 0, s>>>(L.n, L.ld, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d, (T)c1,
                                              (T)c2, step == 0 ? 1 : 0);
             }
         } else {
-            k_cheb<T><<<nb, 256, 0, s>>>(L.n, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d, (T)c1, (T)c2,
-                                         step == 0 ? 1 : 0);
+            k_cheb<T><<<nb, 256, 0, s>>>(L.n, L.ld, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d, (T)c1,
+                                         (T)c2, step == 0 ? 1 : 0);
         }
         MGM_LAUNCHED();
         if (prof) prof->mark(s);
@@ -604,15 +682,18 @@ static void vcycle_rec(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs,
     if constexpr (sizeof(T) == 4) {
         if (L.At) launch_tiled<1>(L, L.e, L.q, 0.f, 0.f, 0, s);
         else {
-            if (L.off) k_residual_o<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.off, L.A, L.btag, L.r, L.e, L.q);
-            else k_residual<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.idx, L.A, L.btag, L.r, L.e, L.q);
+            if (L.off)
+                launch_compact<1>(L, L.e, L.q, 0.f, 0.f, 0, s);
+            else
+                k_residual<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.ld, L.k, L.idx, L.A, L.btag, L.r, L.e,
+                                                                   L.q);
             MGM_LAUNCHED();
         }
         if (C.r_off) k_restrict_o<<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.kr, C.r_off, C.r_base, C.r_w, C.btag, L.q, C.r);
         else k_restrict<T><<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
         MGM_LAUNCHED();
     } else {
-        k_residual<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.idx, L.A, L.btag, L.r, L.e, L.q);
+        k_residual<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.ld, L.k, L.idx, L.A, L.btag, L.r, L.e, L.q);
         MGM_LAUNCHED();
         k_restrict<T><<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
         MGM_LAUNCHED();

@@ -53,7 +53,8 @@ void ref_multigrid(std::vector<RefLevel> &Ls, double w1, double w2, int num_rela
 template <class T>
 struct SolveLevel {
     int n, k, nb_list;            // rows, stencil width, number of boundary rows
-    const int *idx;               // ELL [k][n]
+    int ld;                       // leading dimension of idx, A and off (>= n; a multiple of 4 on FP32 levels)
+    const int *idx;               // ELL [k][ld]
     const T *A;                   // lap_Poison, row 0 replaced by the pin (A[0][0] = 1, rest 0)
     const T *dinv;                // 1 / diagonal
     const uint8_t *btag;
@@ -71,7 +72,7 @@ struct SolveLevel {
     const T *p_w;
     double lmax;                  // spectral radius estimate of D^-1 A on interior rows
     // compact indices (FP32 path only; each used when non-null): neighbours as
-    // int16 offsets c - i [k][n]; transfer gathers as int16 offsets from a
+    // int16 offsets c - i [k][ld]; transfer gathers as int16 offsets from a
     // per-row base node (restriction: rpts, prolongation: ppts)
     const short *off = nullptr;
     const short *r_off = nullptr;
