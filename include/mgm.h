@@ -50,6 +50,29 @@ MGM_API long long mgm_kernel_launches(void);
 MGM_API int mgm_version(void);
 
 /* ------------------------------------------------------------------ */
+/* Mesh files                                                          */
+/* ------------------------------------------------------------------ */
+typedef struct mgm_mesh mgm_mesh;
+/* read_PointStructure (header_files/mesh_functions.h:172-476): reads a Gmsh
+ * 2.2 ASCII mesh as one level's nodes in the state the reference's reader
+ * leaves them -- boundary tags and unnormalised normals accumulated from the
+ * boundary elements (2D: 2-node lines; 3D: 3-node triangles and 4-node
+ * quads), corner nodes (1-node points; in 3D also both ends of 2-node lines)
+ * counted and the first that many nodes dropped, d_avg from the bounding box
+ * and the element count.  The normals are summed on the calling thread's
+ * current device.  Unreadable or malformed files give MGM_ERR_ARG (the
+ * reference prints and exits). */
+MGM_API int mgm_mesh_read(const char *path, int dim, mgm_mesh **mesh);
+/* num_nodes (after the corner removal), num_boundary_nodes (corners
+ * subtracted, as the reference does), num_elem, d_avg; any may be NULL. */
+MGM_API int mgm_mesh_info(const mgm_mesh *mesh, int *num_nodes, int *num_boundary_nodes, int *num_elem,
+                          double *d_avg);
+/* Copies num_nodes entries into each non-NULL array. */
+MGM_API int mgm_mesh_get(const mgm_mesh *mesh, double *x, double *y, double *z, double *nx, double *ny, double *nz,
+                         unsigned char *boundary_tag, unsigned char *corner_tag);
+MGM_API void mgm_mesh_free(mgm_mesh *mesh);
+
+/* ------------------------------------------------------------------ */
 /* Stateless set-up operations: host arrays in, host arrays out.       */
 /* Each call uploads its inputs, runs its kernels and downloads the    */
 /* result (the reference's own call shape).                            */

@@ -1,6 +1,6 @@
 /*
  * mgm_reference.h -- drop-in replacement of the reference's C call surface
- * for the hot path (Multigrid_meshless header_files/*.h), backed by the
+ * for the hot path (the Multigrid_meshless header_files), backed by the
  * sm_100a kernels of libmgm.so.
  *
  * A program written against the reference includes this header instead of
@@ -131,6 +131,14 @@ MGM_API void AllocateMemoryFieldVariables(FieldVariables **field, PointStructure
 MGM_API void read_flow_parameters(char *filename);
 MGM_API void read_grid_filenames(PointStructure **myPointStruct, char *filename, short *num_levels);
 MGM_API void calculate_parameters(PointStructure *myPointStruct);
+/* mesh_functions.h:172-476: the Gmsh reader (mgm_mesh_read) into the level's
+ * arrays, corner nodes removed, num_boundary_nodes / num_elem / d_avg set. */
+MGM_API void read_PointStructure(PointStructure *myPointStruct);
+/* mesh_functions.h:914-928: per level read_PointStructure, find_cloud_index,
+ * rcm_reordering_with_boundarynodes, correct_normal_directions,
+ * calculate_avg_dx (poly_degree 3 on coarse levels, parameters.poly_degree on
+ * the finest), then create_prolongation_and_restriction_matrices. */
+MGM_API void read_complete_mesh_data(PointStructure *myPointStruct, short num_levels);
 /* kdtree_functions.h:113-175 */
 MGM_API void find_cloud_index(PointStructure *myPointStruct1);
 MGM_API int *find_nearest_point(PointStructure *myPointStruct1, PointStructure *myPointStruct2, int num_cloud_points);

@@ -48,6 +48,11 @@ SIGNATURES = {
     "mgm_transfer_weights": ([C.c_int, dp, dp, dp, u8p, ip, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                               C.c_int, dp, dp, dp, ip, dp], C.c_int),
     "mgm_spmv": ([C.c_int, C.c_int, dp, ip, dp, dp], C.c_int),
+    "mgm_mesh_read": ([C.c_char_p, C.c_int, C.POINTER(vp)], C.c_int),
+    "mgm_mesh_info": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)],
+                      C.c_int),
+    "mgm_mesh_get": ([vp, dp, dp, dp, dp, dp, dp, u8p, u8p], C.c_int),
+    "mgm_mesh_free": ([vp], None),
     "mgm_create": ([C.c_int, C.c_int, C.c_int], vp),
     "mgm_destroy": ([vp], None),
     "mgm_set_level": ([vp, C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, dp, dp, u8p, C.c_int, C.c_int], C.c_int),

@@ -10,6 +10,7 @@ Function names follow the reference (Multigrid_meshless header_files/*.h):
   create_derivative_matrices  rbf.h:401-421                -> derivative_weights()
   create_{restriction,prolongation}_matrix  mesh_functions.h:533-670 -> transfer_weights()
   multiply_sparse_matrix_vector_gpu  mat_lib.h:80-89       -> spmv()
+  read_PointStructure         mesh_functions.h:172-476     -> read_gmsh()
   fractional_step_explicit    fractional_step_solver.h:47-71 -> Multigrid.step()
 
 Arrays at this boundary use the reference's layout: node vectors of length n
@@ -122,6 +123,27 @@ def spmv(D, cloud, f):
     out = np.zeros(n)
     check(L.mgm_spmv(n, k, D, _i(cloud), _f(f), out))
     return out
+
+
+def read_gmsh(path, dim):
+    """read_PointStructure (mesh_functions.h:172-476): one level's nodes from a
+    Gmsh 2.2 ASCII file, as a clouds.Cloud (normals unnormalised, corner nodes
+    removed; meta holds num_elem, d_avg and the corner tags)."""
+    from .clouds import Cloud
+    L = load()
+    h = C.c_void_p()
+    check(L.mgm_mesh_read(str(path).encode(), int(dim), C.byref(h)))
+    try:
+        n, nb, ne, da = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        check(L.mgm_mesh_info(h, C.byref(n), C.byref(nb), C.byref(ne), C.byref(da)))
+        a = {nm: np.zeros(n.value) for nm in ("x", "y", "z", "nx", "ny", "nz")}
+        bt = np.zeros(n.value, np.uint8)
+        ct = np.zeros(n.value, np.uint8)
+        check(L.mgm_mesh_get(h, a["x"], a["y"], a["z"], a["nx"], a["ny"], a["nz"], bt, ct))
+    finally:
+        L.mgm_mesh_free(h)
+    return Cloud(a["x"], a["y"], a["z"], a["nx"], a["ny"], a["nz"], bt, nb.value, int(dim), da.value, kind="gmsh",
+                 meta={"num_elem": ne.value, "d_avg": da.value, "corner": ct, "path": str(path)})
 
 
 def kernel_launches() -> int:

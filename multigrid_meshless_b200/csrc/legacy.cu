@@ -156,6 +156,50 @@ void read_grid_filenames(PointStructure **ps, char *filename, short *num_levels)
     std::fclose(f);
 }
 
+// mesh_functions.h:172-476, through mgm_mesh_read (the same messages on stdout)
+void read_PointStructure(PointStructure *p)
+{
+    mgm_mesh *m = nullptr;
+    die_if(mgm_mesh_read(p->mesh_filename, parameters.dimension, &m), "read_PointStructure");
+    int n = 0, nb = 0, ne = 0;
+    double d_avg = 0;
+    die_if(mgm_mesh_info(m, &n, &nb, &ne, &d_avg), "read_PointStructure");
+    AllocateMemoryPointStructure(p, n);
+    std::vector<unsigned char> bt(n), ct(n);
+    die_if(mgm_mesh_get(m, p->x, p->y, p->z, p->x_normal, p->y_normal, p->z_normal, bt.data(), ct.data()),
+           "read_PointStructure");
+    mgm_mesh_free(m);
+    for (int i = 0; i < n; i++) {
+        p->boundary_tag[i] = bt[i] != 0;
+        p->corner_tag[i] = ct[i] != 0;
+        p->point_index[i] = i;
+    }
+    p->num_elem = ne;
+    p->d_avg = d_avg;
+    p->num_boundary_nodes = nb;
+    p->num_corners = 0;
+    std::printf("Average distance between nodes = %lf\n", d_avg);
+    std::printf("No of nodes = %d \nNo of elements = %d \n", n, ne);
+    std::printf("No of boundary nodes = %d \nNo of corner nodes = %d \n", nb, 0);
+}
+
+// mesh_functions.h:914-928
+void read_complete_mesh_data(PointStructure *ps, short num_levels)
+{
+    for (short l = 0; l < num_levels; l++) {
+        ps[l].poly_degree = 3;
+        ps[0].poly_degree = parameters.poly_degree;
+        std::printf("\nReading mesh data for level %d\n", l + 1);
+        calculate_parameters(&ps[l]);
+        read_PointStructure(&ps[l]);
+        find_cloud_index(&ps[l]);
+        rcm_reordering_with_boundarynodes(&ps[l]);
+        correct_normal_directions(&ps[l]);
+        calculate_avg_dx(&ps[l]);
+    }
+    create_prolongation_and_restriction_matrices(ps, num_levels);
+}
+
 // mesh_functions.h:131-170
 void calculate_parameters(PointStructure *p)
 {

@@ -167,4 +167,13 @@ void convert_d2f(const double *in, float *out, long n, cudaStream_t s);
 // bit-faithful ELL SpMV (mat_lib.h:80-89), cloud/W in ELL [k][n]
 void spmv_parity(int n, int k, const double *W, const int *idx, const double *f, double *out, cudaStream_t s);
 
+
+// kernel launch followed by the launch-error check
+template <class... P, class... A>
+inline void launch_k(void (*kern)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A... args)
+{
+    kern<<<grid, block, smem, s>>>(static_cast<P>(args)...);
+    MGM_LAUNCHED();
+}
+
 }  // namespace mgm

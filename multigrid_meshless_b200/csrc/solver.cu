@@ -37,6 +37,16 @@ __device__ __forceinline__ double block_sum_d(double v, double *sm)
 // ---------------------------------------------------------------------------
 // smoother
 // ---------------------------------------------------------------------------
+// Start of a smoothing pass from e = 0: interior rows 0, boundary rows their
+// exact solve r_i / a_ii (they couple only to interior nodes).
+template <class T>
+__global__ void __launch_bounds__(256) k_start_e(int n, const uint8_t *__restrict__ btag, const T *__restrict__ dinv,
+                                                 const T *__restrict__ r, T *__restrict__ e)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) e[i] = btag[i] ? r[i] * dinv[i] : T(0);
+}
+
 // Exact solve of the boundary rows, one warp per row.  A boundary row couples
 // only to itself and interior nodes, so rows can be updated in place.  The
 // rows are stored compactly (row-major [nbl][k]) so that a warp reads them
@@ -45,15 +55,11 @@ template <class T>
 __global__ void __launch_bounds__(256) k_bnd_exact(int nbl, const int *__restrict__ list, int k,
                                                    const int *__restrict__ bidx, const T *__restrict__ bA,
                                                    const T *__restrict__ dinv, const T *__restrict__ r,
-                                                   T *__restrict__ e, int zero_start)
+                                                   T *__restrict__ e)
 {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (w >= nbl) return;
     const int i = list[w];
-    if (zero_start) {
-        if (lane == 0) e[i] = r[i] * dinv[i];
-        return;
-    }
     T s = T(0);
     for (int j = lane; j < k; j += 32) s += bA[(long)w * k + j] * e[bidx[(long)w * k + j]];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
@@ -246,12 +252,11 @@ static void launch_compact(const SolveLevel<float> &L, const float *e, float *ou
                            cudaStream_t s)
 {
     if (L.n >= kVecMinRows)
-        k_level_v4<MODE><<<blocks_for((L.n + 3) / 4, 256), 256, 0, s>>>(L.n, L.ld, L.k, L.off, L.A, L.dinv, L.btag,
-                                                                        L.r, e, out, L.d, c1, c2, first);
+        launch_k(k_level_v4<MODE>, blocks_for((L.n + 3) / 4, 256), 256, 0, s, L.n, L.ld, L.k, L.off, L.A, L.dinv,
+                 L.btag, L.r, e, out, L.d, c1, c2, first);
     else
-        k_level_c1<MODE><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.ld, L.k, L.off, L.A, L.dinv, L.btag, L.r, e,
-                                                              out, L.d, c1, c2, first);
-    MGM_LAUNCHED();
+        launch_k(k_level_c1<MODE>, blocks_for(L.n, 256), 256, 0, s, L.n, L.ld, L.k, L.off, L.A, L.dinv, L.btag,
+                 L.r, e, out, L.d, c1, c2, first);
 }
 
 __global__ void __launch_bounds__(256) k_restrict_o(int n, int k, const short *__restrict__ off,
@@ -553,15 +558,14 @@ static void launch_tiled(const SolveLevel<float> &L, const float *e, float *out,
     if (L.k <= 32) {
         MGM_CUDA(cudaFuncSetAttribute(k_level_tiled_r<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(2 * tile_stage_bytes(32))));
-        k_level_tiled_r<MODE><<<tiled_grid(k_level_tiled_r<MODE>, L.n, smem), kTileRows, smem, s>>>(
-            L.n, L.k, L.offt, L.At, L.dinv, L.btag, L.r, e, out, L.d, c1, c2, first, L.tma_err);
+        launch_k(k_level_tiled_r<MODE>, tiled_grid(k_level_tiled_r<MODE>, L.n, smem), kTileRows, smem, s, L.n, L.k,
+                 L.offt, L.At, L.dinv, L.btag, L.r, e, out, L.d, c1, c2, first, L.tma_err);
     } else {
         MGM_CUDA(cudaFuncSetAttribute(k_level_tiled<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(2 * tile_stage_bytes(kTileMaxK))));
-        k_level_tiled<MODE><<<tiled_grid(k_level_tiled<MODE>, L.n, smem), kTileRows, smem, s>>>(
-            L.n, L.k, L.offt, L.At, L.dinv, L.btag, L.r, e, out, L.d, c1, c2, first, L.tma_err);
+        launch_k(k_level_tiled<MODE>, tiled_grid(k_level_tiled<MODE>, L.n, smem), kTileRows, smem, s, L.n, L.k,
+                 L.offt, L.At, L.dinv, L.btag, L.r, e, out, L.d, c1, c2, first, L.tma_err);
     }
-    MGM_LAUNCHED();
 }
 
 // e = inv * r, one warp per row of the dense coarsest inverse
@@ -626,13 +630,10 @@ static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, 
     const double th = 0.5 * (lM + lm), de = 0.5 * (lM - lm), sig = th / de;
     double rho = 1.0 / sig;
     const int nb = blocks_for(L.n, 256), nbb = blocks_for((long)L.nb_list * 32, 256);
-    k_bnd_exact<T><<<nbb, 256, 0, s>>>(L.nb_list, L.bnd_list, L.k, L.bnd_idx, L.bnd_A, L.dinv, L.r, L.e,
-                                       zero_start ? 1 : 0);
-    MGM_LAUNCHED();
-    if (zero_start) {
-        // interior entries of e must be zero before the first step reads them
-        // (done by the caller through a memset of e)
-    }
+    if (zero_start)
+        launch_k(k_start_e<T>, nb, 256, 0, s, L.n, L.btag, L.dinv, L.r, L.e);
+    else
+        launch_k(k_bnd_exact<T>, nbb, 256, 0, s, L.nb_list, L.bnd_list, L.k, L.bnd_idx, L.bnd_A, L.dinv, L.r, L.e);
     for (int step = 0; step < degree; step++) {
         double c1 = 0, c2;
         if (step == 0) c2 = 1.0 / th;
@@ -649,18 +650,16 @@ static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, 
             } else if (L.off) {
                 launch_compact<0>(L, L.e, L.e2, (float)c1, (float)c2, step == 0 ? 1 : 0, s);
             } else {
-                k_cheb<T><<<nb, 256, 0, s>>>(L.n, L.ld, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d, (T)c1,
-                                             (T)c2, step == 0 ? 1 : 0);
+                launch_k(k_cheb<T>, nb, 256, 0, s, L.n, L.ld, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d,
+                         (T)c1, (T)c2, step == 0 ? 1 : 0);
             }
         } else {
-            k_cheb<T><<<nb, 256, 0, s>>>(L.n, L.ld, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d, (T)c1,
-                                         (T)c2, step == 0 ? 1 : 0);
+            launch_k(k_cheb<T>, nb, 256, 0, s, L.n, L.ld, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d,
+                     (T)c1, (T)c2, step == 0 ? 1 : 0);
         }
-        MGM_LAUNCHED();
         if (prof) prof->mark(s);
         std::swap(L.e, L.e2);
-        k_bnd_exact<T><<<nbb, 256, 0, s>>>(L.nb_list, L.bnd_list, L.k, L.bnd_idx, L.bnd_A, L.dinv, L.r, L.e, 0);
-        MGM_LAUNCHED();
+        launch_k(k_bnd_exact<T>, nbb, 256, 0, s, L.nb_list, L.bnd_list, L.k, L.bnd_idx, L.bnd_A, L.dinv, L.r, L.e);
     }
 }
 
@@ -672,12 +671,10 @@ static void vcycle_rec(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs,
     SolveLevel<T> &L = Ls[l];
     const int nl = (int)Ls.size();
     if (l == nl - 1) {
-        k_dense_solve<T><<<blocks_for((long)L.n * 32, 256), 256, 0, s>>>(cs.n, cs.inv, L.r, L.e);
-        MGM_LAUNCHED();
+        launch_k(k_dense_solve<T>, blocks_for((long)L.n * 32, 256), 256, 0, s, cs.n, cs.inv, L.r, L.e);
         return;
     }
-    MGM_CUDA(cudaMemsetAsync(L.e, 0, sizeof(T) * L.n, s));
-    smooth(L, deg, ratio, true, s, lp);
+    smooth(L, deg, ratio, true, s, lp);  // from e = 0
     SolveLevel<T> &C = Ls[l + 1];
     if constexpr (sizeof(T) == 4) {
         if (L.At) launch_tiled<1>(L, L.e, L.q, 0.f, 0.f, 0, s);
@@ -685,29 +682,28 @@ static void vcycle_rec(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs,
             if (L.off)
                 launch_compact<1>(L, L.e, L.q, 0.f, 0.f, 0, s);
             else
-                k_residual<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.ld, L.k, L.idx, L.A, L.btag, L.r, L.e,
-                                                                   L.q);
-            MGM_LAUNCHED();
+                launch_k(k_residual<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.ld, L.k, L.idx, L.A, L.btag, L.r, L.e,
+                         L.q);
         }
-        if (C.r_off) k_restrict_o<<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.kr, C.r_off, C.r_base, C.r_w, C.btag, L.q, C.r);
-        else k_restrict<T><<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
-        MGM_LAUNCHED();
+        if (C.r_off)
+            launch_k(k_restrict_o, blocks_for(C.n, 256), 256, 0, s, C.n, C.kr, C.r_off, C.r_base, C.r_w, C.btag, L.q,
+                     C.r);
+        else
+            launch_k(k_restrict<T>, blocks_for(C.n, 256), 256, 0, s, C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
     } else {
-        k_residual<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.ld, L.k, L.idx, L.A, L.btag, L.r, L.e, L.q);
-        MGM_LAUNCHED();
-        k_restrict<T><<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
-        MGM_LAUNCHED();
+        launch_k(k_residual<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.ld, L.k, L.idx, L.A, L.btag, L.r, L.e, L.q);
+        launch_k(k_restrict<T>, blocks_for(C.n, 256), 256, 0, s, C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
     }
     vcycle_rec(Ls, cs, l + 1, deg, ratio, s, prof);
     bool poff = false;
     if constexpr (sizeof(T) == 4) poff = L.p_off != nullptr;
     if (poff) {
         if constexpr (sizeof(T) == 4)
-            k_prolong_o<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.kp, L.p_off, L.p_base, L.p_w, C.e, L.e);
+            launch_k(k_prolong_o, blocks_for(L.n, 256), 256, 0, s, L.n, L.kp, L.p_off, L.p_base, L.p_w,
+                     (const float *)C.e, L.e);
     } else {
-        k_prolong<T><<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.kp, L.p_idx, L.p_w, C.e, L.e);
+        launch_k(k_prolong<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.kp, L.p_idx, L.p_w, (const T *)C.e, L.e);
     }
-    MGM_LAUNCHED();
     smooth(L, deg, ratio, false, s, lp);
 }
 
@@ -723,8 +719,7 @@ void vcycle(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int cheb_d
 template <class T>
 const T *smooth_from_zero(SolveLevel<T> &L, int degree, double ratio, cudaStream_t s)
 {
-    MGM_CUDA(cudaMemsetAsync(L.e, 0, sizeof(T) * L.n, s));
-    smooth(L, degree, ratio, true, s, nullptr);
+    smooth(L, degree, ratio, true, s, nullptr);  // from e = 0
     return L.e;
 }
 template const double *smooth_from_zero<double>(SolveLevel<double> &, int, double, cudaStream_t);

@@ -20,6 +20,7 @@
  * bit, which the tests count.
  */
 #include <math.h>
+#include <stdio.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -1110,3 +1111,119 @@ ORC_EXPORT void orc_timple_mass(void *h) { timple_mass((orc_ctx *)h); }
 ORC_EXPORT void orc_timple_multigrid(void *h) { timple_multigrid((orc_ctx *)h); }
 ORC_EXPORT void orc_timple_update_velocity(void *h) { timple_update_velocity((orc_ctx *)h); }
 ORC_EXPORT void orc_timple_boundary_pressure(void *h) { timple_boundary_pressure((orc_ctx *)h); }
+
+/* ------------------------------------------------------------------------ */
+/* read_PointStructure (mesh_functions.h:172-476): Gmsh 2.2 ASCII reader.   */
+/* Nodes from $Nodes; boundary tags and unnormalised normals from the       */
+/* boundary elements (2D: 2-node lines, normal (-dy, dx) added to both      */
+/* nodes; 3D: 3-node triangles and 4-node quads, the cross product of the   */
+/* element's first two edges from node 1 added to every node), corner tags  */
+/* from 1-node points (and, in 3D, from both ends of 2-node lines); every   */
+/* element line holds three integers between its type and its nodes.  The   */
+/* first num_corners nodes are then dropped (Gmsh numbers the geometric     */
+/* points first).  d_avg = sqrt(Lx Ly / num_elem) in 2D, cbrt(Lx Ly Lz /    */
+/* num_elem) in 3D over the bounding box, min/max started at +-1e6.         */
+/* Returns the node count after the removal (-1: unreadable file); with     */
+/* cap >= that count the arrays are filled too.                             */
+/* ------------------------------------------------------------------------ */
+static int gm_seek(FILE *f, const char *word)
+{
+    char tok[64];
+    for (;;) {
+        if (fscanf(f, "%63s ", tok) != 1) return -1;
+        if (strcmp(tok, word) == 0) return 0;
+    }
+}
+
+ORC_EXPORT int orc_read_gmsh(const char *path, int dim, int cap, double *x, double *y, double *z,
+                             double *nx, double *ny, double *nz, unsigned char *btag, unsigned char *corner,
+                             int *nb, int *num_elem, double *d_avg)
+{
+    FILE *f = fopen(path, "r");
+    if (!f) return -1;
+    int nn = 0, ne = 0, id = 0;
+    if (gm_seek(f, "$Nodes") || fscanf(f, "%i ", &nn) != 1 || nn <= 0) { fclose(f); return -1; }
+    double *X = calloc((size_t)nn, sizeof(double)), *Y = calloc((size_t)nn, sizeof(double));
+    double *Z = calloc((size_t)nn, sizeof(double)), *NX = calloc((size_t)nn, sizeof(double));
+    double *NY = calloc((size_t)nn, sizeof(double)), *NZ = calloc((size_t)nn, sizeof(double));
+    unsigned char *BT = calloc((size_t)nn, 1), *CT = calloc((size_t)nn, 1);
+    double lo[3] = {1e6, 1e6, 1e6}, hi[3] = {-1e6, -1e6, -1e6};
+    int ok = 1;
+    for (int i = 0; i < nn && ok; i++) {
+        double v[3];
+        ok = fscanf(f, "%i ", &id) == 1 && fscanf(f, "%lf ", &v[0]) == 1 && fscanf(f, "%lf ", &v[1]) == 1 &&
+             fscanf(f, "%lf ", &v[2]) == 1;
+        X[i] = v[0]; Y[i] = v[1]; Z[i] = v[2];
+        for (int d = 0; d < 3; d++) {
+            if (v[d] < lo[d]) lo[d] = v[d];
+            if (v[d] > hi[d]) hi[d] = v[d];
+        }
+    }
+    if (ok) ok = gm_seek(f, "$Elements") == 0 && fscanf(f, "%i ", &ne) == 1;
+    for (int e = 0; e < ne && ok; e++) {
+        int type = 0, t[3], a = 0, b = 0, c = 0, q = 0;
+        ok = fscanf(f, "%i ", &id) == 1 && fscanf(f, "%i ", &type) == 1;
+        if (!ok) break;
+        const int two_d_line = dim == 2 && type == 1, tri = dim == 3 && type == 2, quad = dim == 3 && type == 3;
+        const int line3 = dim == 3 && type == 1, point = type == 15;
+        if (!(two_d_line || tri || quad || line3 || point)) {
+            if (fscanf(f, "%*[^\n]\n") == EOF) ok = 0;
+            continue;
+        }
+        ok = fscanf(f, "%i ", &t[0]) == 1 && fscanf(f, "%i ", &t[1]) == 1 && fscanf(f, "%i ", &t[2]) == 1;
+        if (!ok) break;
+        if (point) {
+            ok = fscanf(f, "%i ", &a) == 1 && a >= 1 && a <= nn;
+            if (ok) CT[a - 1] = 1;
+        } else if (line3) {
+            ok = fscanf(f, "%i ", &a) == 1 && fscanf(f, "%i ", &b) == 1 && a >= 1 && a <= nn && b >= 1 && b <= nn;
+            if (ok) { CT[a - 1] = 1; CT[b - 1] = 1; }
+        } else if (two_d_line) {
+            ok = fscanf(f, "%i ", &a) == 1 && fscanf(f, "%i ", &b) == 1 && a >= 1 && a <= nn && b >= 1 && b <= nn;
+            if (!ok) break;
+            a--; b--;
+            BT[a] = 1; BT[b] = 1;
+            const double dx = X[b] - X[a], dy = Y[b] - Y[a];
+            NX[a] += -dy; NY[a] += dx;
+            NX[b] += -dy; NY[b] += dx;
+        } else {
+            ok = fscanf(f, "%i ", &a) == 1 && fscanf(f, "%i ", &b) == 1 && fscanf(f, "%i ", &c) == 1 &&
+                 a >= 1 && a <= nn && b >= 1 && b <= nn && c >= 1 && c <= nn;
+            if (ok && quad) ok = fscanf(f, "%i ", &q) == 1 && q >= 1 && q <= nn;
+            if (!ok) break;
+            int nodes[4] = {a - 1, b - 1, c - 1, quad ? q - 1 : -1};
+            const int cnt = quad ? 4 : 3;
+            for (int m = 0; m < cnt; m++) BT[nodes[m]] = 1;
+            const int A = nodes[0], B = nodes[1], C = nodes[2];
+            const double dx = X[B] - X[A], dy = Y[B] - Y[A], dz = Z[B] - Z[A];
+            const double dx1 = X[C] - X[A], dy1 = Y[C] - Y[A], dz1 = Z[C] - Z[A];
+            const double cx = dy * dz1 - dz * dy1, cy = dz * dx1 - dx * dz1, cz = dx * dy1 - dy * dx1;
+            for (int m = 0; m < cnt; m++) NX[nodes[m]] += cx;
+            for (int m = 0; m < cnt; m++) NY[nodes[m]] += cy;
+            for (int m = 0; m < cnt; m++) NZ[nodes[m]] += cz;
+        }
+    }
+    fclose(f);
+    int n = -1;
+    if (ok) {
+        int nbnd = 0, ncorner = 0;
+        for (int i = 0; i < nn; i++) { nbnd += BT[i] != 0; ncorner += CT[i] != 0; }
+        n = nn - ncorner;
+        if (num_elem) *num_elem = ne;
+        if (nb) *nb = nbnd - ncorner;
+        if (d_avg) {
+            const double L0 = hi[0] - lo[0], L1 = hi[1] - lo[1], L2 = hi[2] - lo[2];
+            *d_avg = dim == 2 ? sqrt(L0 * L1 / ne) : cbrt(L0 * L1 * L2 / ne);
+        }
+        if (cap >= n) {
+            for (int i = 0; i < n; i++) {
+                const int s = i + ncorner;
+                x[i] = X[s]; y[i] = Y[s]; z[i] = Z[s];
+                nx[i] = NX[s]; ny[i] = NY[s]; nz[i] = NZ[s];
+                btag[i] = BT[s]; corner[i] = CT[s];
+            }
+        }
+    }
+    free(X); free(Y); free(Z); free(NX); free(NY); free(NZ); free(BT); free(CT);
+    return n;
+}

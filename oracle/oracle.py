@@ -24,6 +24,32 @@ ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
 
 
+# orc_read_gmsh / ref_read_mesh: path, dim, cap, x, y, z, nx, ny, nz, btag, corner, &nb, &num_elem, &d_avg
+_MESH_ARGS = [C.c_char_p, C.c_int, C.c_int] + [C.c_void_p] * 8 + [C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                                                   C.POINTER(C.c_double)]
+
+
+def read_mesh(path, dim, reference=False):
+    """read_PointStructure (mesh_functions.h:172-476) on a Gmsh file, by the
+    restatement (orc_read_gmsh) or, with reference=True, by the reference's
+    own reader (_ref/libref.so; the path must be shorter than 50 characters).
+    Returns a dict of the level's arrays and counts."""
+    fn = ref_lib().ref_read_mesh if reference else lib().orc_read_gmsh
+    nb, ne, da = C.c_int(), C.c_int(), C.c_double()
+    nulls = [None] * 8
+    n = fn(str(path).encode(), dim, 0, *nulls, C.byref(nb), C.byref(ne), C.byref(da))
+    if n < 0:
+        raise RuntimeError(f"cannot read {path}")
+    out = {nm: np.zeros(n) for nm in ("x", "y", "z", "nx", "ny", "nz")}
+    out["btag"] = np.zeros(n, np.uint8)
+    out["corner"] = np.zeros(n, np.uint8)
+    arrs = [out[k].ctypes.data_as(C.c_void_p) for k in ("x", "y", "z", "nx", "ny", "nz", "btag", "corner")]
+    n2 = fn(str(path).encode(), dim, n, *arrs, C.byref(nb), C.byref(ne), C.byref(da))
+    assert n2 == n
+    out.update(n=n, nb=nb.value, num_elem=ne.value, d_avg=da.value)
+    return out
+
+
 def lib(crpow: bool = False):
     """liboracle.so (libm pow, as the reference) or liboracle_crpow.so
     (correctly rounded powers, as the CUDA path)."""
@@ -71,6 +97,8 @@ def lib(crpow: bool = False):
         for nm in ("orc_timple_momentum", "orc_timple_mass", "orc_timple_multigrid", "orc_timple_update_velocity",
                    "orc_timple_boundary_pressure"):
             getattr(L, nm).argtypes = [C.c_void_p]
+        L.orc_read_gmsh.argtypes = _MESH_ARGS
+        L.orc_read_gmsh.restype = C.c_int
         _ORC[key] = L
     return _ORC[key]
 
@@ -107,6 +135,8 @@ def ref_lib(timple: bool = False):
         L.ref_field_get.argtypes = [C.c_int, C.c_int, dp]
         L.ref_field_set.argtypes = [C.c_int, C.c_int, dp]
         L.ref_spmv.argtypes = [C.c_int, C.c_int, dp, dp]
+        L.ref_read_mesh.argtypes = _MESH_ARGS
+        L.ref_read_mesh.restype = C.c_int
         if timple:
             L.ref_timple_params.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double]
             L.ref_timple_step.restype = C.c_double

@@ -17,6 +17,8 @@
  *   fractional_step_explicit & callees  fractional_step_solver.h:47-275
  *   time_implicit_solver & callees    timple_solver.h:40-410 (built with
  *                                     -DMGM_REF_TIMPLE into _ref/libref_timple.so)
+ *   read_PointStructure               mesh_functions.h:172-476 (the Gmsh reader;
+ *                                     ref_read_mesh)
  *
  * The level set-up mirrors read_complete_mesh_data (mesh_functions.h:914-928)
  * with the mesh reader replaced by arrays handed in by the caller (boundary
@@ -212,4 +214,30 @@ void ref_spmv(int lev, int op, const double *f, double *out)
     PointStructure *p = &g_ps[lev];
     double **D = op == 0 ? p->Dx : op == 1 ? p->Dy : op == 2 ? p->Dz : op == 3 ? p->lap : p->lap_Poison;
     multiply_sparse_matrix_vector_gpu(D, (double *)f, out, p->cloud_index, p->num_nodes, p->num_cloud_points);
+}
+
+/* read_PointStructure (mesh_functions.h:172-476) on a Gmsh file: returns the
+ * node count after corner removal; with cap >= that count the arrays are
+ * filled.  The path must be shorter than PointStructure.mesh_filename (50). */
+int ref_read_mesh(const char *path, int dim, int cap, double *x, double *y, double *z, double *nx, double *ny,
+                  double *nz, unsigned char *btag, unsigned char *corner, int *nb, int *num_elem, double *d_avg)
+{
+    PointStructure p;
+    memset(&p, 0, sizeof(p));
+    if (strlen(path) >= sizeof(p.mesh_filename)) return -1;
+    strcpy(p.mesh_filename, path);
+    parameters.dimension = (short)dim;
+    read_PointStructure(&p);
+    const int n = p.num_nodes;
+    *nb = p.num_boundary_nodes;
+    *num_elem = p.num_elem;
+    *d_avg = p.d_avg;
+    if (cap >= n) {
+        for (int i = 0; i < n; i++) {
+            x[i] = p.x[i]; y[i] = p.y[i]; z[i] = p.z[i];
+            nx[i] = p.x_normal[i]; ny[i] = p.y_normal[i]; nz[i] = p.z_normal[i];
+            btag[i] = p.boundary_tag[i]; corner[i] = p.corner_tag[i];
+        }
+    }
+    return n;
 }

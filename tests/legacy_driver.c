@@ -4,6 +4,12 @@
  * file), linked against libmgm.so through include/mgm_reference.h.
  *
  *   legacy_driver <input.bin> <output_dir> [timple]
+ *   legacy_driver --gmsh <flow_parameters.csv> <grid_filenames.csv> <output_dir>
+ *
+ * The --gmsh form is mg_NS_solver.c:17-45 as written: read_flow_parameters,
+ * read_grid_filenames, read_complete_mesh_data on Gmsh files (the reference's
+ * own reader semantics, mesh_functions.h:172-476, 914-928), then
+ * num_time_steps fractional steps on the lid-driven cavity.
  *
  * With "timple" the time loop is the reference main's default,
  * time_implicit_solver (timple_solver.h:40-70), on the Taylor-Couette
@@ -52,18 +58,44 @@ static void wr_rows_i(const char *dir, const char *name, int **rows, int n, int 
     free(flat);
 }
 
+static int read_bin(const char *path, PointStructure **out_ps, int *out_nsteps);
+static int run(PointStructure *ps, int nl, int nsteps, int timple, const char *out);
+
 int main(int argc, char **argv)
 {
     if (argc < 3) { fprintf(stderr, "usage: legacy_driver input.bin outdir [timple]\n"); return 1; }
-    const int timple = argc > 3 && strcmp(argv[3], "timple") == 0;
-    FILE *f = fopen(argv[1], "rb");
-    if (!f) { fprintf(stderr, "cannot open %s\n", argv[1]); return 1; }
-    const char *out = argv[2];
+    const int gmsh = argc >= 5 && strcmp(argv[1], "--gmsh") == 0;
+    const int timple = !gmsh && argc > 3 && strcmp(argv[3], "timple") == 0;
+    const char *out = gmsh ? argv[4] : argv[2];
+    PointStructure *ps = NULL;
+    int nl = 0, nsteps = 0;
+    if (gmsh) {
+        /* mg_NS_solver.c:21-45 */
+        short num_levels = 0;
+        read_flow_parameters(argv[2]);
+        read_grid_filenames(&ps, argv[3], &num_levels);
+        parameters.num_levels = num_levels;
+        read_complete_mesh_data(ps, num_levels);
+        nl = num_levels;
+        nsteps = parameters.num_time_steps;
+    } else {
+        nl = read_bin(argv[1], &ps, &nsteps);
+    }
+    for (int l = 0; l < nl; l++) create_derivative_matrices(&ps[l]);
+    return run(ps, nl, nsteps, timple, out);
+}
+
+/* nodes from input.bin, then the steps of read_complete_mesh_data after the reader */
+static int read_bin(const char *path, PointStructure **out_ps, int *out_nsteps)
+{
+    FILE *f = fopen(path, "rb");
+    if (!f) { fprintf(stderr, "cannot open %s\n", path); exit(1); }
     int hdr[9];
     double flow[3];
     rd(hdr, sizeof(int), 9, f);
     rd(flow, sizeof(double), 3, f);
-    const int nl = hdr[0], nsteps = hdr[5];
+    const int nl = hdr[0];
+    *out_nsteps = hdr[5];
     memset(&parameters, 0, sizeof(parameters));
     parameters.dimension = (short)hdr[1];
     parameters.phs_degree = (short)hdr[2];
@@ -113,8 +145,12 @@ int main(int argc, char **argv)
     }
     fclose(f);
     create_prolongation_and_restriction_matrices(ps, (short)nl);
-    for (int l = 0; l < nl; l++) create_derivative_matrices(&ps[l]);
+    *out_ps = ps;
+    return nl;
+}
 
+static int run(PointStructure *ps, int nl, int nsteps, int timple, const char *out)
+{
     /* mg_NS_solver.c:47-59 with the lid-driven cavity conditions (init_LDC.c)
      * or, for TIMPLE, the Taylor-Couette ones (init_TC.c:33-52) */
     FieldVariables *field;
