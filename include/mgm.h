@@ -259,6 +259,41 @@ MGM_API int mgm_timple_step(mgm_ctx *ctx, int mode, double *steady_err);
 #define MGM_TIMPLE_BOUNDARY_PRESSURE 4  /* update_boundary_pressure (:371-410) */
 MGM_API int mgm_timple_part(mgm_ctx *ctx, int part, int mode);
 
+/* The heat-conduction program (mg_heat_conduction.c:43-83 with
+ * header_files/heat_conduction.h:24-113 and init/init_heat_conduction.c:
+ * 14-67), 2D, on a context set up with MGM_SETUP_REFERENCE_TRANSFER.
+ * mgm_heat_init: initial_conditions, boundary_conditions and
+ * set_boundary_rhs for wave number k: level-0 source
+ * -8 pi^2 k^2 sin(2 pi k x) sin(2 pi k y) (pi written 3.14), every p and
+ * residual 0, coarse sources 0; the boundary nodes with x == 0 become
+ * Dirichlet rows (level 0's lap_Poison row = e_i, right-hand side 1 -- this
+ * changes level 0's lap_Poison, as the reference does), the other boundary
+ * nodes get the manufactured solution's normal derivative as right-hand side.
+ * mgm_heat_step: one pass of the program's time loop -- num_vcycles of its own
+ * V-cycles (omega, num_relax and num_vcycles of mgm_set_flow; sweeps in
+ * data-parallel order) -- and *steady_err = sum over level 0 of the squared
+ * change of p (the value the program compares with its steady-state
+ * tolerance; it prints sqrt(sum / n)).  p is MGM_FIELD_P of each level. */
+MGM_API int mgm_heat_init(mgm_ctx *ctx, int wave_number);
+MGM_API int mgm_heat_step(mgm_ctx *ctx, double *steady_err);
+
+/* Output and restart.
+ * mgm_write_solution: Solution.csv as mg_NS_solver.c:83-88 writes it --
+ * "%lf, %lf, %lf, %lf, %lf, %lf, %lf\n" of x, y, z, u, v, w and the pressure
+ * field (MGM_FIELD_P_OLD, the TIMPLE pressure the reference main writes, or
+ * MGM_FIELD_P), one line per level-0 node in the set-up's node order.
+ * mgm_checkpoint_save / _load: every field one time step hands to the next
+ * (each level's p, source and residual; level 0's velocities, their
+ * intermediate and old copies, dp/dn, grad p, the TIMPLE pressure) in one
+ * binary file, with the levels' sizes and a fingerprint of their coordinates
+ * and a checksum; a context loads only a checkpoint of matching levels
+ * (MGM_ERR_ARG otherwise), after mgm_setup (and after mgm_heat_init for the
+ * heat-conduction program).  A run continued from a checkpoint repeats the
+ * uninterrupted run bit for bit.  No counterpart in the reference. */
+MGM_API int mgm_write_solution(mgm_ctx *ctx, const char *path, int pressure_field);
+MGM_API int mgm_checkpoint_save(mgm_ctx *ctx, const char *path);
+MGM_API int mgm_checkpoint_load(mgm_ctx *ctx, const char *path);
+
 /* Poisson solve modes */
 #define MGM_MODE_REFERENCE 0   /* multigrid_Poisson_solver semantics, fixed num_vcycles (Jacobi-order sweeps) */
 #define MGM_MODE_FP64 1        /* convergent V-cycle preconditioned FGMRES, all FP64 */

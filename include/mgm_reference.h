@@ -139,6 +139,18 @@ MGM_API void read_PointStructure(PointStructure *myPointStruct);
  * calculate_avg_dx (poly_degree 3 on coarse levels, parameters.poly_degree on
  * the finest), then create_prolongation_and_restriction_matrices. */
 MGM_API void read_complete_mesh_data(PointStructure *myPointStruct, short num_levels);
+/* write_functions.h:29-201: text dumps of a level's host arrays, same formats
+ * and file names (write_processed_grid_data writes the six per-level files
+ * into the working directory). */
+MGM_API void write_normals(PointStructure *myPointStruct, char *filename);
+MGM_API void write_boundary_tags(PointStructure *myPointStruct, char *filename);
+MGM_API void write_corner_tags(PointStructure *myPointStruct, char *filename);
+MGM_API void write_coordinates(PointStructure *myPointStruct, char *filename);
+MGM_API void write_cloud_index(PointStructure *myPointStruct, char *filename);
+MGM_API void write_prolongation_and_restriction_points(PointStructure *myPointStruct, char *filename);
+MGM_API void write_test_files(double *f, double *fx, double *fy, double *fz, double *lapf, double *fxx, double *fyy,
+                              double *fzz, int num_nodes, char *folder1);
+MGM_API void write_processed_grid_data(PointStructure *myPointStruct, int level);
 /* kdtree_functions.h:113-175 */
 MGM_API void find_cloud_index(PointStructure *myPointStruct1);
 MGM_API int *find_nearest_point(PointStructure *myPointStruct1, PointStructure *myPointStruct2, int num_cloud_points);

@@ -48,6 +48,11 @@ SIGNATURES = {
     "mgm_transfer_weights": ([C.c_int, dp, dp, dp, u8p, ip, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                               C.c_int, dp, dp, dp, ip, dp], C.c_int),
     "mgm_spmv": ([C.c_int, C.c_int, dp, ip, dp, dp], C.c_int),
+    "mgm_write_solution": ([vp, C.c_char_p, C.c_int], C.c_int),
+    "mgm_checkpoint_save": ([vp, C.c_char_p], C.c_int),
+    "mgm_checkpoint_load": ([vp, C.c_char_p], C.c_int),
+    "mgm_heat_init": ([vp, C.c_int], C.c_int),
+    "mgm_heat_step": ([vp, C.POINTER(C.c_double)], C.c_int),
     "mgm_mesh_read": ([C.c_char_p, C.c_int, C.POINTER(vp)], C.c_int),
     "mgm_mesh_info": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)],
                       C.c_int),

@@ -239,6 +239,27 @@ class Multigrid:
     def set_timple(self, iter_timple=1, iter_momentum=1, facRe=1.0, facdt=1.0):
         check(self.L.mgm_set_timple(self.h, iter_timple, iter_momentum, facRe, facdt))
 
+    def write_solution(self, path, pressure="p_old"):
+        """Solution.csv in the format of mg_NS_solver.c:83-88 (x y z u v w pressure)."""
+        check(self.L.mgm_write_solution(self.h, str(path).encode(), _lib.FIELD[pressure]))
+
+    def checkpoint_save(self, path):
+        check(self.L.mgm_checkpoint_save(self.h, str(path).encode()))
+
+    def checkpoint_load(self, path):
+        check(self.L.mgm_checkpoint_load(self.h, str(path).encode()))
+
+    def heat_init(self, wave_number=1):
+        """The heat-conduction program's set-up (init_heat_conduction.c:14-67)."""
+        check(self.L.mgm_heat_init(self.h, int(wave_number)))
+
+    def heat_step(self):
+        """One pass of mg_heat_conduction.c's time loop; returns the sum of the
+        squared changes of level-0 p."""
+        e = C.c_double()
+        check(self.L.mgm_heat_step(self.h, C.byref(e)))
+        return e.value
+
     def timple_step(self, mode=_lib.MODE_REFERENCE):
         """time_implicit_solver (timple_solver.h:40-70); returns the steady-state error."""
         e = C.c_double()

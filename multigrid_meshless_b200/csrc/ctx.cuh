@@ -74,6 +74,9 @@ struct mgm_ctx {
     // and the previous-sweep copies of the momentum iterations
     DBuf<double> u_old, v_old, w_old, p_old, dpdx, dpdy, dpdz, tu, tv, tw;
     int iter_timple = 1, iter_momentum = 1;
+    // heat-conduction program (mgm_heat_init)
+    int heat_wave = 0;
+    bool heat_ready = false;
     double facRe = 1.0, facdt = 1.0;
     // solver controls and state
     double tol = 1e-8;

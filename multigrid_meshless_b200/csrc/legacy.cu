@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "../../include/mgm_reference.h"
@@ -154,6 +155,109 @@ void read_grid_filenames(PointStructure **ps, char *filename, short *num_levels)
             std::exit(1);
         }
     std::fclose(f);
+}
+
+// ---- write_functions.h:29-201: text dumps of a level (same formats) ----
+static std::FILE *open_or_exit(const char *filename)
+{
+    std::FILE *f = std::fopen(filename, "w");
+    if (!f) {
+        std::printf("Error: Unable to open the file %s\n", filename);
+        std::exit(1);
+    }
+    return f;
+}
+
+void write_normals(PointStructure *p, char *filename)
+{
+    std::printf("Writing normals to file %s\n", filename);
+    std::FILE *f = open_or_exit(filename);
+    for (int i = 0; i < p->num_nodes; i++)
+        std::fprintf(f, "%d %lf %lf %lf\n", i, p->x_normal[i], p->y_normal[i], p->z_normal[i]);
+    std::fclose(f);
+}
+
+void write_boundary_tags(PointStructure *p, char *filename)
+{
+    std::printf("Writing boundary tags to file %s\n", filename);
+    std::FILE *f = open_or_exit(filename);
+    for (int i = 0; i < p->num_nodes; i++) std::fprintf(f, "%d %d\n", i, (int)p->boundary_tag[i]);
+    std::fclose(f);
+}
+
+void write_corner_tags(PointStructure *p, char *filename)
+{
+    std::printf("Writing corner tags to file %s\n", filename);
+    std::FILE *f = open_or_exit(filename);
+    for (int i = 0; i < p->num_nodes; i++) std::fprintf(f, "%d %d\n", i, (int)p->corner_tag[i]);
+    std::fclose(f);
+}
+
+void write_coordinates(PointStructure *p, char *filename)
+{
+    std::printf("Writing coordinates to %s\n", filename);
+    std::FILE *f = open_or_exit(filename);
+    for (int i = 0; i < p->num_nodes; i++) std::fprintf(f, "%lf %lf %lf\n", p->x[i], p->y[i], p->z[i]);
+    std::fclose(f);
+}
+
+void write_cloud_index(PointStructure *p, char *filename)
+{
+    std::printf("Writing cloud index to %s\n", filename);
+    std::FILE *f = open_or_exit(filename);
+    for (int i = 0; i < p->num_nodes; i++) {
+        std::fprintf(f, "%d ", i);
+        for (int j = 0; j < p->num_cloud_points; j++) std::fprintf(f, "%d ", p->cloud_index[i][j]);
+        std::fprintf(f, "\n");
+    }
+    std::fclose(f);
+}
+
+void write_prolongation_and_restriction_points(PointStructure *p, char *filename)
+{
+    std::printf("Writing prolongation and restriction points to %s\n", filename);
+    std::FILE *f = open_or_exit(filename);
+    for (int i = 0; i < p->num_nodes; i++)
+        std::fprintf(f, "%d %d %d\n", i, p->prolongation_points[i], p->restriction_points[i]);
+    std::fclose(f);
+}
+
+// folder1 is a prefix (the reference concatenates it with the file names in a
+// 100-character buffer)
+void write_test_files(double *f, double *fx, double *fy, double *fz, double *lapf, double *fxx, double *fyy,
+                      double *fzz, int num_nodes, char *folder1)
+{
+    const char *names[8] = {"f.csv", "fx.csv", "fy.csv", "fz.csv", "lapf.csv", "fxx.csv", "fyy.csv", "fzz.csv"};
+    double *arrs[8] = {f, fx, fy, fz, lapf, fxx, fyy, fzz};
+    for (int t = 0; t < 8; t++) {
+        std::string path = std::string(folder1) + names[t];
+        std::FILE *o = std::fopen(path.c_str(), "w");
+        if (!o) {
+            std::printf("Error: Unable to open the file %s\n", path.c_str());
+            std::exit(1);
+        }
+        for (int i = 0; i < num_nodes; i++) std::fprintf(o, "%f\n", arrs[t][i]);
+        std::fclose(o);
+    }
+    std::printf("Files written\n");
+}
+
+void write_processed_grid_data(PointStructure *p, int level)
+{
+    char name[64];
+    std::snprintf(name, sizeof(name), "normals_%d.csv", level);
+    write_normals(p, name);
+    std::snprintf(name, sizeof(name), "boundary_tags_%d.csv", level);
+    write_boundary_tags(p, name);
+    std::snprintf(name, sizeof(name), "corner_tags_%d.csv", level);
+    write_corner_tags(p, name);
+    std::snprintf(name, sizeof(name), "coordinates_%d.csv", level);
+    write_coordinates(p, name);
+    std::snprintf(name, sizeof(name), "cloud_index_%d.csv", level);
+    write_cloud_index(p, name);
+    std::snprintf(name, sizeof(name), "prolongation_and_restriction_%d.csv", level);
+    write_prolongation_and_restriction_points(p, name);
+    std::printf("\n\n");
 }
 
 // mesh_functions.h:172-476, through mgm_mesh_read (the same messages on stdout)

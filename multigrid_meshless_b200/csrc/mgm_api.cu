@@ -527,7 +527,7 @@ void poisson(mgm_ctx *c, int mode, bool timple = false)
         MGM_REQUIRE(c->have_ref_transfer || c->nl == 1, "reference mode needs mgm_setup(..., MGM_SETUP_REFERENCE_TRANSFER)");
         auto R = ref_levels(c);
         const double w1 = (double)c->omega, w2 = (double)(1 - c->omega);
-        ref_multigrid(R, w1, w2, c->num_relax, c->num_vcycles, c->s, timple);
+        ref_multigrid(R, w1, w2, c->num_relax, c->num_vcycles, c->s, timple ? REF_TIMPLE : REF_FS);
         return;
     }
     // b = source with the pinned row's rhs 0 (boundary rows keep their (zero) source)
@@ -585,6 +585,15 @@ void alloc_solver_buffers(mgm_ctx *c)
 namespace mgm {
 // The Poisson solve of a step on L0.src -> L0.p (the TIMPLE step uses it for p').
 void poisson_solve(mgm_ctx *c, int mode, bool timple) { poisson(c, mode, timple); }
+// num_cycles reference-semantics V-cycles of one program's variant on every
+// level's p, src and res (the heat-conduction program drives its own cycle)
+void ref_cycles(mgm_ctx *c, RefVariant v, int num_cycles)
+{
+    MGM_REQUIRE(c->have_ref_transfer || c->nl == 1, "reference mode needs mgm_setup(..., MGM_SETUP_REFERENCE_TRANSFER)");
+    auto R = ref_levels(c);
+    const double w1 = (double)c->omega, w2 = (double)(1 - c->omega);
+    ref_multigrid(R, w1, w2, c->num_relax, num_cycles, c->s, v);
+}
 }  // namespace mgm
 
 // ===========================================================================

@@ -314,60 +314,73 @@ __global__ void k_zero_interior(int n, const uint8_t *__restrict__ btag, double 
     if (i < n && !btag[i]) p[i] = 0.0;
 }
 
-void ref_relaxation(const RefLevel &L, double w1, double w2, int num_relax, cudaStream_t s, bool timple)
+void ref_relaxation(const RefLevel &L, double w1, double w2, int num_relax, cudaStream_t s, RefVariant v)
 {
     const int nb = blocks_for(L.n, 256);
     for (int it = 0; it < num_relax; it++) {
         k_ref_sweep<<<nb, 256, 0, s>>>(L.n, L.k, L.idx, L.lapP, L.src, L.p, L.ptmp, w1, w2);
         MGM_LAUNCHED();
-        k_ref_shift_residual<<<nb, 256, 0, s>>>(L.n, L.k, L.idx, timple ? L.lapP : L.lap, L.src, L.ptmp, L.p, L.res,
-                                                timple ? L.btag : nullptr);
+        if (v == REF_HEAT) {
+            // heat_conduction.h:27-35: the sweep alone (no re-pin, no residual)
+            MGM_CUDA(cudaMemcpyAsync(L.p, L.ptmp, sizeof(double) * L.n, cudaMemcpyDeviceToDevice, s));
+            continue;
+        }
+        const bool t = v == REF_TIMPLE;
+        k_ref_shift_residual<<<nb, 256, 0, s>>>(L.n, L.k, L.idx, t ? L.lapP : L.lap, L.src, L.ptmp, L.p, L.res,
+                                                t ? L.btag : nullptr);
         MGM_LAUNCHED();
     }
 }
 
-void ref_residual_interior(const RefLevel &L, cudaStream_t s, bool timple)
+// the TIMPLE and heat residuals are the same: lap_Poison on interior rows, 0 on
+// boundary rows (timple_solver.h:285-301, heat_conduction.h:100-113)
+void ref_residual_interior(const RefLevel &L, cudaStream_t s, RefVariant v)
 {
-    k_ref_residual_interior<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.idx, timple ? L.lapP : L.lap, L.btag,
-                                                                 L.src, L.p, L.res, timple ? 1 : 0);
+    const bool t = v != REF_FS;
+    k_ref_residual_interior<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, L.k, L.idx, t ? L.lapP : L.lap, L.btag,
+                                                                 L.src, L.p, L.res, t ? 1 : 0);
     MGM_LAUNCHED();
 }
 
-void ref_restrict(const RefLevel &F, const RefLevel &C, cudaStream_t s, bool timple)
+// the TIMPLE and heat restrictions write every coarse row (timple_solver.h:303-317,
+// heat_conduction.h:57-75)
+void ref_restrict(const RefLevel &F, const RefLevel &C, cudaStream_t s, RefVariant v)
 {
     k_ref_transfer<<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, F.k, C.r_idx, C.restr, C.btag, F.res, C.src, 0,
-                                                        timple ? 1 : 0);
+                                                        v != REF_FS ? 1 : 0);
     MGM_LAUNCHED();
 }
 
-void ref_prolongate(const RefLevel &F, const RefLevel &C, cudaStream_t s, bool timple)
+void ref_prolongate(const RefLevel &F, const RefLevel &C, cudaStream_t s, RefVariant v)
 {
     k_ref_transfer<<<blocks_for(F.n, 256), 256, 0, s>>>(F.n, C.k, F.p_idx, F.prol, F.btag, C.p, F.p, 1, 0);
     MGM_LAUNCHED();
-    if (timple) {
+    if (v == REF_TIMPLE) {
         // every coarse correction reset (timple_solver.h:333-338)
         MGM_CUDA(cudaMemsetAsync(C.p, 0, sizeof(double) * C.n, s));
     } else {
+        // coarse interior corrections reset (fractional_step_solver.h:228-233, heat_conduction.h:92-97)
         k_zero_interior<<<blocks_for(C.n, 256), 256, 0, s>>>(C.n, C.btag, C.p);
         MGM_LAUNCHED();
     }
 }
 
-// multigrid_Poisson_solver (fractional_step_solver.h:150-166; the TIMPLE
-// variant timple_solver.h:203-220 has the same cycle over its own routines)
+// multigrid_Poisson_solver (fractional_step_solver.h:150-166); the TIMPLE
+// variant (timple_solver.h:203-220) and the heat-conduction program's cycle
+// (mg_heat_conduction.c:57-71) have the same shape over their own routines
 void ref_multigrid(std::vector<RefLevel> &Ls, double w1, double w2, int num_relax, int num_vcycles, cudaStream_t s,
-                   bool timple)
+                   RefVariant v)
 {
     const int nl = (int)Ls.size();
     for (int cyc = 0; cyc < num_vcycles; cyc++) {
         for (int l = 0; l < nl; l++) {
-            ref_relaxation(Ls[l], w1, w2, num_relax, s, timple);
-            ref_residual_interior(Ls[l], s, timple);
-            if (l != nl - 1) ref_restrict(Ls[l], Ls[l + 1], s, timple);
+            ref_relaxation(Ls[l], w1, w2, num_relax, s, v);
+            ref_residual_interior(Ls[l], s, v);
+            if (l != nl - 1) ref_restrict(Ls[l], Ls[l + 1], s, v);
         }
         for (int l = nl - 1; l > 0; l--) {
-            ref_prolongate(Ls[l - 1], Ls[l], s, timple);
-            if (l != 1) ref_relaxation(Ls[l - 1], w1, w2, num_relax, s, timple);
+            ref_prolongate(Ls[l - 1], Ls[l], s, v);
+            if (l != 1) ref_relaxation(Ls[l - 1], w1, w2, num_relax, s, v);
         }
     }
 }

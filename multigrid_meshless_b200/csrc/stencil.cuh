@@ -38,13 +38,17 @@ struct RefLevel {
     const double *prol;
 };
 
-// timple: the TIMPLE solver's variants (timple_solver.h:203-339)
-void ref_relaxation(const RefLevel &L, double w1, double w2, int num_relax, cudaStream_t s, bool timple = false);
-void ref_residual_interior(const RefLevel &L, cudaStream_t s, bool timple = false);
-void ref_restrict(const RefLevel &F, const RefLevel &C, cudaStream_t s, bool timple = false);
-void ref_prolongate(const RefLevel &F, const RefLevel &C, cudaStream_t s, bool timple = false);
+// Which program's multigrid routines: the fractional step's
+// (fractional_step_solver.h:150-246), the TIMPLE solver's
+// (timple_solver.h:203-339) or the heat-conduction program's
+// (heat_conduction.h:24-113).
+enum RefVariant : int { REF_FS = 0, REF_TIMPLE = 1, REF_HEAT = 2 };
+void ref_relaxation(const RefLevel &L, double w1, double w2, int num_relax, cudaStream_t s, RefVariant v = REF_FS);
+void ref_residual_interior(const RefLevel &L, cudaStream_t s, RefVariant v = REF_FS);
+void ref_restrict(const RefLevel &F, const RefLevel &C, cudaStream_t s, RefVariant v = REF_FS);
+void ref_prolongate(const RefLevel &F, const RefLevel &C, cudaStream_t s, RefVariant v = REF_FS);
 void ref_multigrid(std::vector<RefLevel> &Ls, double w1, double w2, int num_relax, int num_vcycles, cudaStream_t s,
-                   bool timple = false);
+                   RefVariant v = REF_FS);
 
 // ---------------------------------------------------------------------------
 // convergent solver (solver.cu)

@@ -573,6 +573,7 @@ typedef struct {
     int n, k, dim;
     const int *cloud;
     const unsigned char *btag;
+    const double *x, *y, *z;   /* set by orc_ctx_coords (the heat program's sources need them) */
     const double *nx, *ny, *nz;
     const double *Dx, *Dy, *Dz, *lap, *lapP;
     /* transfer data of this level */
@@ -1226,4 +1227,138 @@ ORC_EXPORT int orc_read_gmsh(const char *path, int dim, int cap, double *x, doub
     }
     free(X); free(Y); free(Z); free(NX); free(NY); free(NZ); free(BT); free(CT);
     return n;
+}
+
+/* ------------------------------------------------------------------------ */
+/* The heat-conduction program (mg_heat_conduction.c:43-83 with             */
+/* heat_conduction.h:24-113 and init/init_heat_conduction.c:14-67): a      */
+/* manufactured Poisson problem with Dirichlet rows (boundary nodes at      */
+/* x == 0) and Neumann rows (the other boundary nodes) solved by the       */
+/* program's own V-cycle.  jacobi = 0: in-place sweeps (the C build);      */
+/* jacobi = 1: every node from the previous sweep's values (the GPU).      */
+/* ------------------------------------------------------------------------ */
+ORC_EXPORT void orc_ctx_coords(void *h, int l, const double *x, const double *y, const double *z)
+{
+    orc_ctx *c = (orc_ctx *)h;
+    c->L[l].x = x; c->L[l].y = y; c->L[l].z = z;
+}
+
+/* relaxation (heat_conduction.h:24-48): SOR over every row with lap_Poison,
+ * nothing else (no re-pin, no residual) */
+static void heat_relaxation(const orc_level *L, double *p, const double *source, float omega, int num_relax,
+                            int jacobi, double *scratch)
+{
+    int n = L->n, k = L->k;
+    for (int it = 0; it < num_relax; it++) {
+        const double *pin = p;
+        if (jacobi) { memcpy(scratch, p, sizeof(double) * (size_t)n); pin = scratch; }
+        for (int i = 0; i < n; i++) {
+            double sum = 0.0;
+            for (int j = 1; j < k; j++) sum += L->lapP[(size_t)i * k + j] * pin[L->cloud[(size_t)i * k + j]];
+            p[i] = omega * ((source[i] - sum) / L->lapP[(size_t)i * k]) + (1 - omega) * pin[i];
+        }
+    }
+}
+
+/* calculate_residuals (heat_conduction.h:100-113): lap_Poison, boundary rows 0 */
+static void heat_residuals(const orc_level *L, const double *p, const double *source, double *res)
+{
+    int n = L->n, k = L->k;
+    for (int i = 0; i < n; i++) {
+        res[i] = 0.0;
+        if (L->btag[i]) continue;
+        double sum = 0;
+        for (int j = 0; j < k; j++) sum += L->lapP[(size_t)i * k + j] * p[L->cloud[(size_t)i * k + j]];
+        res[i] = source[i] - sum;
+    }
+}
+
+/* restrict_residuals (heat_conduction.h:50-69): every coarse row written, boundary rows 0 */
+static void heat_restrict(const orc_level *F, const orc_level *C, const double *res_f, double *source_c)
+{
+    for (int i = 0; i < C->n; i++) {
+        double r = 0.0;
+        if (!C->btag[i]) {
+            int ir = C->rpts[i];
+            for (int j = 0; j < F->k; j++) r += C->restr[(size_t)i * F->k + j] * res_f[F->cloud[(size_t)ir * F->k + j]];
+        }
+        source_c[i] = r;
+    }
+}
+
+/* the cycle of mg_heat_conduction.c:58-71 (prolongate_corrections,
+ * heat_conduction.h:71-98, is the fractional step's) */
+static void heat_cycle(orc_ctx *c)
+{
+    const int nl = c->nl;
+    for (int l = 0; l < nl; l++) {
+        heat_relaxation(&c->L[l], c->p[l], c->source[l], c->omega, c->num_relax, c->jacobi, c->scratch);
+        heat_residuals(&c->L[l], c->p[l], c->source[l], c->res[l]);
+        if (l != nl - 1) heat_restrict(&c->L[l], &c->L[l + 1], c->res[l], c->source[l + 1]);
+    }
+    for (int l = nl - 1; l > 0; l--) {
+        prolongate(&c->L[l - 1], &c->L[l], c->p[l - 1], c->p[l]);
+        if (l != 1) heat_relaxation(&c->L[l - 1], c->p[l - 1], c->source[l - 1], c->omega, c->num_relax, c->jacobi,
+                                    c->scratch);
+    }
+}
+
+/* initial_conditions + boundary_conditions (init_heat_conduction.c:14-49):
+ * res = p = 0 everywhere, level-0 source -8 pi^2 k^2 sin(2 pi k x) sin(2 pi k y)
+ * with pi written 3.14, coarse sources 0 */
+ORC_EXPORT void orc_heat_init(void *h, int wave)
+{
+    orc_ctx *c = (orc_ctx *)h;
+    const int k = wave;
+    for (int l = 0; l < c->nl; l++) {
+        const orc_level *L = &c->L[l];
+        for (int i = 0; i < L->n; i++) {
+            c->res[l][i] = 0.0;
+            c->source[l][i] = l == 0 ? -8 * 3.14 * 3.14 * k * k * sin(2 * 3.14 * k * c->L[0].x[i]) *
+                                           sin(2 * 3.14 * k * c->L[0].y[i])
+                                     : 0.0;
+            c->p[l][i] = 0.0;
+        }
+    }
+}
+
+/* set_boundary_rhs (init_heat_conduction.c:51-65), level 0: boundary nodes at
+ * x == 0 become Dirichlet rows (lap_Poison row = e_i, source 1), the others
+ * get the manufactured solution's normal derivative as their source */
+ORC_EXPORT void orc_heat_boundary_rhs(void *h, int wave)
+{
+    orc_ctx *c = (orc_ctx *)h;
+    orc_level *L = &c->L[0];
+    const int k = wave, kk = L->k;
+    double *lapP = (double *)L->lapP;
+    for (int i = 0; i < L->n; i++) {
+        if (!L->btag[i]) continue;
+        const double x = L->x[i], y = L->y[i];
+        if (x == 0) {
+            c->source[0][i] = 1.0;
+            for (int j = 0; j < kk; j++) lapP[(size_t)i * kk + j] = 0.0;
+            lapP[(size_t)i * kk] = 1.0;
+        } else {
+            c->source[0][i] = 2 * 3.14 * k * (sin(2 * 3.14 * k * x) * cos(2 * 3.14 * k * y) * L->ny[i] +
+                                              cos(2 * 3.14 * k * x) * sin(2 * 3.14 * k * y) * L->nx[i]);
+        }
+    }
+}
+
+/* one time step of mg_heat_conduction.c:47-77: num_vcycles cycles, each after
+ * set_boundary_rhs; returns the sum over level 0 of (p_before - p_after)^2 */
+ORC_EXPORT double orc_heat_step(void *h, int wave)
+{
+    orc_ctx *c = (orc_ctx *)h;
+    const int n = c->L[0].n;
+    double *temp = (double *)malloc(sizeof(double) * (size_t)n);
+    memcpy(temp, c->p[0], sizeof(double) * (size_t)n);
+    for (int cyc = 0; cyc < c->num_vcycles; cyc++) {
+        orc_heat_boundary_rhs(h, wave);
+        heat_cycle(c);
+    }
+    double e = 0.0;
+    for (int i = 0; i < n; i++) e += (temp[i] - c->p[0][i]) * (temp[i] - c->p[0][i]);
+    free(temp);
+    return e;
 }

@@ -99,20 +99,29 @@ def lib(crpow: bool = False):
             getattr(L, nm).argtypes = [C.c_void_p]
         L.orc_read_gmsh.argtypes = _MESH_ARGS
         L.orc_read_gmsh.restype = C.c_int
+        L.orc_ctx_coords.argtypes = [C.c_void_p, C.c_int, dp, dp, dp]
+        for nm in ("orc_heat_init", "orc_heat_boundary_rhs", "orc_heat_step"):
+            getattr(L, nm).argtypes = [C.c_void_p, C.c_int]
+        L.orc_heat_step.restype = C.c_double
         _ORC[key] = L
     return _ORC[key]
 
 
-def ref_available(timple: bool = False) -> bool:
-    return os.path.exists(os.path.join(HERE, "_ref", "libref_timple.so" if timple else "libref.so"))
+def _ref_name(timple, heat):
+    return "libref_heat.so" if heat else ("libref_timple.so" if timple else "libref.so")
 
 
-def ref_lib(timple: bool = False):
-    """_ref/libref.so (fractional-step build) or _ref/libref_timple.so (the
-    reference's TIMPLE solver); each is its own library with its own globals."""
-    key = "timple" if timple else "fs"
+def ref_available(timple: bool = False, heat: bool = False) -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", _ref_name(timple, heat)))
+
+
+def ref_lib(timple: bool = False, heat: bool = False):
+    """_ref/libref.so (fractional-step build), _ref/libref_timple.so (the
+    reference's TIMPLE solver) or _ref/libref_heat.so (the heat-conduction
+    program's routines); each is its own library with its own globals."""
+    key = "heat" if heat else ("timple" if timple else "fs")
     if key not in _REF:
-        path = os.path.join(HERE, "_ref", "libref_timple.so" if timple else "libref.so")
+        path = os.path.join(HERE, "_ref", _ref_name(timple, heat))
         if not os.path.exists(path):
             raise RuntimeError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
         L = C.CDLL(path)
@@ -129,7 +138,8 @@ def ref_lib(timple: bool = False):
         L.ref_get_geometry.argtypes = [C.c_int, dp, dp, dp, dp, dp, dp, u8p, ip]
         L.ref_get_ops.argtypes = [C.c_int, dp, dp, dp, dp, dp]
         L.ref_get_transfer.argtypes = [C.c_int, ip, ip, C.c_void_p, C.c_void_p]
-        L.ref_bc.argtypes = [C.c_int]
+        if not heat:
+            L.ref_bc.argtypes = [C.c_int]
         L.ref_dt.restype = C.c_double
         L.ref_set_dt.argtypes = [C.c_double]
         L.ref_field_get.argtypes = [C.c_int, C.c_int, dp]
@@ -137,7 +147,11 @@ def ref_lib(timple: bool = False):
         L.ref_spmv.argtypes = [C.c_int, C.c_int, dp, dp]
         L.ref_read_mesh.argtypes = _MESH_ARGS
         L.ref_read_mesh.restype = C.c_int
-        if timple:
+        if heat:
+            L.ref_heat_init.argtypes = [C.c_int]
+            L.ref_heat_step.argtypes = [C.c_int]
+            L.ref_heat_step.restype = C.c_double
+        elif timple:
             L.ref_timple_params.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double]
             L.ref_timple_step.restype = C.c_double
         else:
@@ -184,11 +198,11 @@ def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
-def ref_pipeline(clouds, ks, polys, phs=3, with_weights=True, search_scale=0.3, timple=False):
+def ref_pipeline(clouds, ks, polys, phs=3, with_weights=True, search_scale=0.3, timple=False, heat=False):
     """Runs read_complete_mesh_data's steps (minus the file reader) and
     create_derivative_matrices through the reference's own code (in the
-    TIMPLE build when timple)."""
-    R = ref_lib(timple)
+    TIMPLE or heat-conduction build when asked)."""
+    R = ref_lib(timple, heat)
     nl = len(clouds)
     dim = clouds[0].dim
     R.ref_begin(dim, phs, nl)
@@ -361,6 +375,33 @@ class TimpleSolver(OracleSolver):
 
     def step(self):
         return self.O.orc_timple_step(self.h)
+
+
+class HeatSolver(OracleSolver):
+    """The heat-conduction program (mg_heat_conduction.c:43-83 with
+    heat_conduction.h:24-113, init/init_heat_conduction.c:14-67) on restated
+    levels: self.p[l], self.source[l] as the program leaves them; level 0's
+    lap_Poison is a private copy (set_boundary_rhs turns its x == 0 boundary
+    rows into Dirichlet rows)."""
+
+    def __init__(self, levels, omega, num_relax, num_vcycles, wave=1, jacobi=True):
+        import dataclasses
+        lv = list(levels)
+        lv[0] = dataclasses.replace(levels[0], lapP=np.array(levels[0].lapP, dtype=np.float64, copy=True))
+        super().__init__(lv, 100.0, 0.5, omega, num_relax, num_vcycles, jacobi=jacobi, dt=1.0)
+        self.wave = wave
+        for l, L in enumerate(lv):
+            xyz = [np.ascontiguousarray(a, np.float64) for a in (L.x, L.y, L.z)]
+            self.keep += xyz
+            self.O.orc_ctx_coords(self.h, l, *xyz)
+        self.lapP0 = self.keep[9]    # level 0's lap_Poison as the context holds it
+        self.O.orc_heat_init(self.h, wave)
+
+    def boundary_rhs(self):
+        self.O.orc_heat_boundary_rhs(self.h, self.wave)
+
+    def step(self):
+        return self.O.orc_heat_step(self.h, self.wave)
 
 
 def lid_bc(L, f):

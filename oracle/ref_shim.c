@@ -19,6 +19,9 @@
  *                                     -DMGM_REF_TIMPLE into _ref/libref_timple.so)
  *   read_PointStructure               mesh_functions.h:172-476 (the Gmsh reader;
  *                                     ref_read_mesh)
+ *   the heat-conduction program's routines  heat_conduction.h:24-113 and
+ *                                     init/init_heat_conduction.c:14-67 (built
+ *                                     with -DMGM_REF_HEAT into _ref/libref_heat.so)
  *
  * The level set-up mirrors read_complete_mesh_data (mesh_functions.h:914-928)
  * with the mesh reader replaced by arrays handed in by the caller (boundary
@@ -28,6 +31,12 @@
  */
 #include <stdio.h>
 #include <string.h>
+#if defined(MGM_REF_HEAT)
+/* _ref/libref_heat.so: the same handle over the heat-conduction program's
+ * routines (heat_conduction.h:24-113, init/init_heat_conduction.c:14-67) */
+#include "header_files/heat_conduction.h"
+#include "init/init_heat_conduction.c"
+#else
 #ifdef MGM_REF_TIMPLE
 /* _ref/libref_timple.so: the same handle over the reference's time-implicit
  * (TIMPLE) solver, timple_solver.h:40-410, the default of mg_NS_solver.c */
@@ -42,6 +51,7 @@
 #include "init/init_TC.c"
 #undef initial_conditions
 #undef boundary_conditions
+#endif
 
 static PointStructure *g_ps = NULL;
 static FieldVariables *g_field = NULL;
@@ -153,6 +163,7 @@ void ref_get_transfer(int lev, int *rpts, int *ppts, double *restr, double *prol
 /* ---- fields and the fractional step ---------------------------------- */
 void ref_fields_alloc(void) { AllocateMemoryFieldVariables(&g_field, g_ps, g_levels); }
 
+#ifndef MGM_REF_HEAT
 /* kind 0: lid-driven cavity (init_LDC.c), kind 1: Taylor-Couette (init_TC.c).
  * Applied to level 0 only, as mg_NS_solver.c:49-50 does. */
 void ref_bc(int kind)
@@ -160,6 +171,7 @@ void ref_bc(int kind)
     if (kind == 0) { initial_conditions(g_ps, g_field, 1); boundary_conditions(g_ps, g_field, 1); }
     else { tc_initial_conditions(g_ps, g_field, 1); tc_boundary_conditions(g_ps, g_field, 1); }
 }
+#endif
 
 double ref_dt(void) { parameters.dt = calculate_dt(&g_ps[0]); return parameters.dt; }
 void ref_set_dt(double dt) { parameters.dt = dt; }
@@ -180,7 +192,39 @@ static double *field_ptr(int lev, int which)
 void ref_field_get(int lev, int which, double *out) { memcpy(out, field_ptr(lev, which), sizeof(double) * g_ps[lev].num_nodes); }
 void ref_field_set(int lev, int which, const double *in) { memcpy(field_ptr(lev, which), in, sizeof(double) * g_ps[lev].num_nodes); }
 
-#ifdef MGM_REF_TIMPLE
+#if defined(MGM_REF_HEAT)
+/* mg_heat_conduction.c:47-48: initial and boundary conditions of wave number k */
+void ref_heat_init(int wave)
+{
+    initial_conditions(g_ps, g_field, g_levels, wave);
+    boundary_conditions(g_ps, g_field, g_levels, wave);
+}
+/* one pass of the time loop of mg_heat_conduction.c:55-77 (the program's own
+ * V-cycle after set_boundary_rhs, num_vcycles times); returns its
+ * steady_state_error, the sum of squared changes of p on level 0 */
+double ref_heat_step(int wave)
+{
+    const int n = g_ps[0].num_nodes, nl = g_levels;
+    double *temp = (double *)malloc(sizeof(double) * (size_t)n);
+    for (int i = 0; i < n; i++) temp[i] = g_field[0].p[i];
+    for (int icycle = 0; icycle < parameters.num_vcycles; icycle++) {
+        set_boundary_rhs(&g_ps[0], g_field, nl, wave);
+        for (int ilev = 0; ilev < nl; ilev++) {
+            relaxation(&g_ps[ilev], &g_field[ilev]);
+            calculate_residuals(&g_ps[ilev], &g_field[ilev]);
+            if (ilev != nl - 1) restrict_residuals(&g_ps[ilev], &g_ps[ilev + 1], &g_field[ilev], &g_field[ilev + 1]);
+        }
+        for (int ilev = nl - 1; ilev > 0; ilev--) {
+            prolongate_corrections(&g_ps[ilev - 1], &g_ps[ilev], &g_field[ilev - 1], &g_field[ilev]);
+            if (ilev != 1) relaxation(&g_ps[ilev - 1], &g_field[ilev - 1]);
+        }
+    }
+    double e = 0.0;
+    for (int i = 0; i < n; i++) e += (temp[i] - g_field[0].p[i]) * (temp[i] - g_field[0].p[i]);
+    free(temp);
+    return e;
+}
+#elif defined(MGM_REF_TIMPLE)
 /* TIMPLE parameters (read_flow_parameters, mesh_functions.h:82-91).  The
  * reference never sets FieldVariables.rho, which update_boundary_pressure
  * (timple_solver.h:365) reads; it is defined here as parameters.rho. */
@@ -204,7 +248,9 @@ void ref_mass_residual(void) { calculate_mass_residual(&g_ps[0], &g_field[0]); }
 void ref_boundary_dpdn(void) { calculate_boundary_dpdn(&g_ps[0], &g_field[0]); }
 void ref_update_velocity(void) { update_velocity(&g_ps[0], &g_field[0]); }
 #endif
+#ifndef MGM_REF_HEAT
 void ref_multigrid(void) { multigrid_Poisson_solver(g_ps, g_field); }
+#endif
 void ref_relaxation(int lev) { relaxation(&g_ps[lev], &g_field[lev]); }
 void ref_residuals(int lev) { calculate_residuals(&g_ps[lev], &g_field[lev]); }
 void ref_restrict(int lev) { restrict_residuals(&g_ps[lev], &g_ps[lev + 1], &g_field[lev], &g_field[lev + 1]); }
@@ -240,4 +286,13 @@ int ref_read_mesh(const char *path, int dim, int cap, double *x, double *y, doub
         }
     }
     return n;
+}
+
+/* write_processed_grid_data (write_functions.h:186-201) of a level into the
+ * working directory, and write_test_files (:124-184) with prefix `folder` */
+void ref_write_grid(int lev) { write_processed_grid_data(&g_ps[lev], lev); }
+void ref_write_test_files(double *f, double *fx, double *fy, double *fz, double *lapf, double *fxx, double *fyy,
+                          double *fzz, int n, char *folder)
+{
+    write_test_files(f, fx, fy, fz, lapf, fxx, fyy, fzz, n, folder);
 }
