@@ -250,6 +250,11 @@ MGM_API int mgm_apply_bc(mgm_ctx *ctx, int kind);
  * :203-339); MGM_MODE_FP64 / MGM_MODE_FP32_IR = the convergent pinned solve. */
 MGM_API int mgm_set_timple(mgm_ctx *ctx, int iter_timple, int iter_momentum, double facRe, double facdt);
 MGM_API int mgm_timple_step(mgm_ctx *ctx, int mode, double *steady_err);
+/* nsteps TIMPLE steps timed with CUDA events on the context's stream:
+ * step_ms (all steps), vcycles (p' V-cycles over all steps), the last
+ * steady-state error; any output may be NULL. */
+MGM_API int mgm_timple_run(mgm_ctx *ctx, int mode, int nsteps, double *step_ms, long long *vcycles,
+                           double *steady_err);
 /* One part of a TIMPLE iteration, for callers that drive the loop themselves
  * (the reference's callees): */
 #define MGM_TIMPLE_MOMENTUM 0           /* calculate_intermediate_velocity_implicit (:72-175) */

@@ -51,6 +51,8 @@ SIGNATURES = {
     "mgm_write_solution": ([vp, C.c_char_p, C.c_int], C.c_int),
     "mgm_checkpoint_save": ([vp, C.c_char_p], C.c_int),
     "mgm_checkpoint_load": ([vp, C.c_char_p], C.c_int),
+    "mgm_timple_run": ([vp, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                        C.POINTER(C.c_double)], C.c_int),
     "mgm_heat_init": ([vp, C.c_int], C.c_int),
     "mgm_heat_step": ([vp, C.POINTER(C.c_double)], C.c_int),
     "mgm_mesh_read": ([C.c_char_p, C.c_int, C.POINTER(vp)], C.c_int),

@@ -249,6 +249,12 @@ class Multigrid:
     def checkpoint_load(self, path):
         check(self.L.mgm_checkpoint_load(self.h, str(path).encode()))
 
+    def timple_run(self, mode, nsteps):
+        """nsteps TIMPLE steps timed on the device: (step_ms, p' V-cycles, steady_err)."""
+        sm, vc, e = C.c_double(), C.c_longlong(), C.c_double()
+        check(self.L.mgm_timple_run(self.h, mode, nsteps, C.byref(sm), C.byref(vc), C.byref(e)))
+        return sm.value, vc.value, e.value
+
     def heat_init(self, wave_number=1):
         """The heat-conduction program's set-up (init_heat_conduction.c:14-67)."""
         check(self.L.mgm_heat_init(self.h, int(wave_number)))

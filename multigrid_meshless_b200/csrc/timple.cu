@@ -325,6 +325,7 @@ double timple_step(mgm_ctx *c, int mode)
         timple_momentum(c);
         timple_mass(c);
         poisson_solve(c, mode, true);  // the pressure-correction equation, on p' (L.p)
+        c->vcycles_acc += mode == MGM_MODE_REFERENCE ? c->num_vcycles : c->last_iters;
         timple_update(c);
         timple_boundary_pressure(c);
     }
@@ -395,6 +396,38 @@ int mgm_timple_part(mgm_ctx *c, int part, int mode)
         MGM_CUDA(cudaSetDevice(c->device));
         MGM_REQUIRE(c->setup_done && c->dt > 0, "mgm_timple_part: call mgm_setup and mgm_set_flow first");
         timple_part(c, part, mode);
+    });
+}
+
+int mgm_timple_run(mgm_ctx *c, int mode, int nsteps, double *step_ms, long long *vcycles, double *steady_err)
+{
+    return tguard([&] {
+        MGM_REQUIRE(c != nullptr, "null context");
+        MGM_CUDA(cudaSetDevice(c->device));
+        MGM_REQUIRE(c->setup_done && c->dt > 0, "mgm_timple_run: call mgm_setup and mgm_set_flow first");
+        MGM_REQUIRE(nsteps >= 0, "mgm_timple_run: nsteps < 0");
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        MGM_CUDA(cudaEventCreate(&ev[0]));
+        MGM_CUDA(cudaEventCreate(&ev[1]));
+        try {
+            c->vcycles_acc = 0;
+            double e = 0;
+            MGM_CUDA(cudaEventRecord(ev[0], c->s));
+            for (int t = 0; t < nsteps; t++) e = timple_step(c, mode);
+            MGM_CUDA(cudaEventRecord(ev[1], c->s));
+            MGM_CUDA(cudaEventSynchronize(ev[1]));
+            float ms = 0;
+            MGM_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+            if (step_ms) *step_ms = ms;
+            if (vcycles) *vcycles = c->vcycles_acc;
+            if (steady_err) *steady_err = e;
+        } catch (...) {
+            cudaEventDestroy(ev[0]);
+            cudaEventDestroy(ev[1]);
+            throw;
+        }
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
     });
 }
 

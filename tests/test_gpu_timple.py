@@ -101,3 +101,22 @@ def test_convergent_timple_matches_direct_solve(annulus, mode):
     for nm in ("u_new", "v_new", "dpdn"):
         assert np.array_equal(mg.get_field(nm), S.f[nm]), nm
     assert np.array_equal(mg.get_field("p_old"), S.p_old)
+
+
+def test_timple_run_matches_single_steps(annulus):
+    """mgm_timple_run (device-timed steps) leaves the same fields as the same
+    number of mgm_timple_step calls."""
+    mg = annulus
+    out = []
+    for run in (True, False):
+        _fresh(mg, 100.0, 1.0, 2, 3)
+        mg.set_timple(2, 2, 1.0, 1.0)
+        if run:
+            ms, vc, e = mg.timple_run(mgm.MODE_REFERENCE, 3)
+            assert ms > 0 and vc == 3 * 2 * 3
+        else:
+            for _ in range(3):
+                e = mg.timple_step(mgm.MODE_REFERENCE)
+        out.append((e, mg.get_field("u_new"), mg.get_field("p_old")))
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
