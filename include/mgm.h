@@ -152,6 +152,18 @@ MGM_API int mgm_transfer_weights(int nt, const double *tx, const double *ty, con
  * (bit-identical to the reference's C build). */
 MGM_API int mgm_spmv(int n, int k, const double *D, const int *cloud, const double *f, double *out);
 
+/* matrixInverse_Gauss_Jordan (header_files/mat_lib.h:423-491) of one dense
+ * row-major order x order matrix on the GPU: one bubble pass on column 0,
+ * elimination without pivoting, rows scaled last, every operation rounded
+ * separately (the same bits as the reference's C build).  order <= 1024. */
+MGM_API int mgm_gauss_jordan(int order, const double *A, double *inverse);
+
+/* create_laplacian_for_Poisson (header_files/rbf.h:382-399): lapP = lap on
+ * interior rows, Dx nx + Dy ny (+ Dz nz in 3D) on boundary rows; [n][k]. */
+MGM_API int mgm_laplacian_for_poisson(int n, int k, int dim, const double *Dx, const double *Dy, const double *Dz,
+                                      const double *lap, const double *nx, const double *ny, const double *nz,
+                                      const unsigned char *btag, double *lapP);
+
 /* ------------------------------------------------------------------ */
 /* Device-resident solver context (copyin_*_to_gpu + the time loop)    */
 /* ------------------------------------------------------------------ */
@@ -318,6 +330,16 @@ MGM_API int mgm_set_solver(mgm_ctx *ctx, double rel_tol, int max_iters, int cheb
  * from the row's nearest node, wherever the reordered bandwidth allows) or
  * 32-bit (enable = 0).  Results are identical either way. */
 MGM_API int mgm_use_compact(mgm_ctx *ctx, int enable);
+/* One routine of the fractional step's reference-semantics multigrid on the
+ * levels' p, source and residual (sweeps in data-parallel order):
+ * relaxation (fractional_step_solver.h:168-196) or calculate_residuals
+ * (:236-246) on `level`; restrict_residuals (:198-212) from `level` into
+ * level + 1; prolongate_corrections (:214-234) from level + 1 into `level`. */
+#define MGM_REF_RELAXATION 0
+#define MGM_REF_RESIDUALS 1
+#define MGM_REF_RESTRICT 2
+#define MGM_REF_PROLONGATE 3
+MGM_API int mgm_ref_routine(mgm_ctx *ctx, int level, int routine);
 /* Replay each V-cycle from a captured CUDA graph (default on) or launch its
  * kernels one by one (enable = 0).  Results are identical either way. */
 MGM_API int mgm_use_graphs(mgm_ctx *ctx, int enable);

@@ -164,6 +164,16 @@ MGM_API void create_prolongation_and_restriction_matrices(PointStructure *myPoin
 /* rbf.h:32-40, 401-421 */
 MGM_API double calculate_phs_rbf(double *pt1, double *pt2, int phs, int dimension);
 MGM_API void create_derivative_matrices(PointStructure *myPointStruct);
+/* rbf.h:274-380: one operator each (Dx, Dy, Dz, lap) into the level's rows
+ * (allocated here when NULL); rbf.h:382-399: lap_Poison from lap, Dx, Dy,
+ * (Dz) and the normals */
+MGM_API void create_full_gradx_matrix(PointStructure *myPointStruct);
+MGM_API void create_full_grady_matrix(PointStructure *myPointStruct);
+MGM_API void create_full_gradz_matrix(PointStructure *myPointStruct);
+MGM_API void create_full_laplacian_matrix(PointStructure *myPointStruct);
+MGM_API void create_laplacian_for_Poisson(PointStructure *myPointStruct);
+/* mat_lib.h:423-491 (order <= 1024), on the GPU; `inverse` rows allocated by the caller */
+MGM_API void matrixInverse_Gauss_Jordan(double **matrix1, double **inverse, int order);
 /* mat_lib.h:80-89 */
 MGM_API void multiply_sparse_matrix_vector_gpu(double **D_coeff, double *f, double *dfdx, int **cloud, int n_rows_D,
                                                int n_cols_D);
@@ -179,12 +189,25 @@ MGM_API void calculate_intermediate_velocity(PointStructure *myPointStruct, Fiel
 MGM_API void calculate_mass_residual(PointStructure *myPointStruct, FieldVariables *field);
 MGM_API void calculate_boundary_dpdn(PointStructure *myPointStruct, FieldVariables *field);
 MGM_API void multigrid_Poisson_solver(PointStructure *myPointStruct, FieldVariables *field);
+/* fractional_step_solver.h:168-246: the multigrid's routines, on the device
+ * levels of copyin_essentials_to_gpu (myPointStruct must point into that
+ * array; restrict/prolongate take consecutive levels), sweeps in
+ * data-parallel order; the device holds the fields, and the host arrays each
+ * routine changes (p and res; the coarse source; both levels' p) are
+ * refreshed after it runs. */
+MGM_API void relaxation(PointStructure *myPointStruct, FieldVariables *field);
+MGM_API void calculate_residuals(PointStructure *myPointStruct, FieldVariables *field);
+MGM_API void restrict_residuals(PointStructure *myPointStruct_f, PointStructure *myPointStruct_c,
+                                FieldVariables *field_f, FieldVariables *field_c);
+MGM_API void prolongate_corrections(PointStructure *myPointStruct_f, PointStructure *myPointStruct_c,
+                                    FieldVariables *field_f, FieldVariables *field_c);
 MGM_API void update_velocity(PointStructure *myPointStruct, FieldVariables *field);
 
 /* timple_solver.h:40-70, 72-201, 341-410 (the default solver of mg_NS_solver.c).
  * time_implicit_solver runs the TIMPLE variants of the multigrid routines
  * (timple_solver.h:203-339) internally; the exported multigrid_Poisson_solver,
- * relaxation, ... above are the fractional step's.  Momentum sweeps run in
+ * relaxation, calculate_residuals, restrict_residuals and
+ * prolongate_corrections above are the fractional step's.  Momentum sweeps run in
  * data-parallel order. */
 MGM_API double time_implicit_solver(PointStructure *myPointStruct, FieldVariables *field);
 MGM_API void calculate_intermediate_velocity_implicit(PointStructure *myPointStruct, FieldVariables *field);

@@ -53,6 +53,9 @@ SIGNATURES = {
     "mgm_checkpoint_load": ([vp, C.c_char_p], C.c_int),
     "mgm_timple_run": ([vp, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                         C.POINTER(C.c_double)], C.c_int),
+    "mgm_gauss_jordan": ([C.c_int, dp, dp], C.c_int),
+    "mgm_laplacian_for_poisson": ([C.c_int, C.c_int, C.c_int, dp, dp, vp, dp, dp, dp, vp, u8p, dp], C.c_int),
+    "mgm_ref_routine": ([vp, C.c_int, C.c_int], C.c_int),
     "mgm_heat_init": ([vp, C.c_int], C.c_int),
     "mgm_heat_step": ([vp, C.POINTER(C.c_double)], C.c_int),
     "mgm_mesh_read": ([C.c_char_p, C.c_int, C.POINTER(vp)], C.c_int),

@@ -18,6 +18,7 @@ namespace {
 
 mgm_ctx *g_ctx = nullptr;
 int g_levels = 0;
+PointStructure *g_ps = nullptr;  // the level array handed to copyin_essentials_to_gpu
 int g_mode = MGM_MODE_REFERENCE;
 
 void die_if(int status, const char *what)
@@ -442,6 +443,55 @@ void create_derivative_matrices(PointStructure *p)
     p->lap_Poison = unpack_rows(lapP, n, k);
 }
 
+// create_full_gradx/grady/gradz/laplacian_matrix (rbf.h:274-380): one operator
+// of the level into its (caller-allocated, or here allocated) rows
+static void full_operator(PointStructure *p, int which, const char *fn)
+{
+    require_no_corners(p, fn);
+    const int n = p->num_nodes, k = p->num_cloud_points, dim = parameters.dimension;
+    if (which == 2 && dim != 3) return;
+    std::vector<int> cl = pack_rows(p->cloud_index, n, k);
+    std::vector<unsigned char> bt = tags(p->boundary_tag, n);
+    std::vector<double> op[5];
+    for (int t = 0; t < 5; t++) op[t].resize(t == 2 && dim != 3 ? 0 : (size_t)n * k);
+    die_if(mgm_derivative_weights(n, k, dim, parameters.phs_degree, p->poly_degree, p->x, p->y, p->z, p->x_normal,
+                                  p->y_normal, p->z_normal, bt.data(), cl.data(), op[0].data(), op[1].data(),
+                                  dim == 3 ? op[2].data() : nullptr, op[3].data(), op[4].data()),
+           fn);
+    double ***dst[4] = {&p->Dx, &p->Dy, &p->Dz, &p->lap};
+    if (!*dst[which]) *dst[which] = unpack_rows(op[which], n, k);
+    else
+        for (int i = 0; i < n; i++) std::memcpy((*dst[which])[i], &op[which][(size_t)i * k], sizeof(double) * k);
+}
+void create_full_gradx_matrix(PointStructure *p) { full_operator(p, 0, "create_full_gradx_matrix"); }
+void create_full_grady_matrix(PointStructure *p) { full_operator(p, 1, "create_full_grady_matrix"); }
+void create_full_gradz_matrix(PointStructure *p) { full_operator(p, 2, "create_full_gradz_matrix"); }
+void create_full_laplacian_matrix(PointStructure *p) { full_operator(p, 3, "create_full_laplacian_matrix"); }
+
+// rbf.h:382-399, from the level's Dx, Dy, (Dz), lap and normals
+void create_laplacian_for_Poisson(PointStructure *p)
+{
+    const int n = p->num_nodes, k = p->num_cloud_points, dim = parameters.dimension;
+    std::vector<unsigned char> bt = tags(p->boundary_tag, n);
+    std::vector<double> Dx = pack_rows(p->Dx, n, k), Dy = pack_rows(p->Dy, n, k), lap = pack_rows(p->lap, n, k),
+                        Dz, out((size_t)n * k);
+    if (dim == 3) Dz = pack_rows(p->Dz, n, k);
+    die_if(mgm_laplacian_for_poisson(n, k, dim, Dx.data(), Dy.data(), dim == 3 ? Dz.data() : nullptr, lap.data(),
+                                     p->x_normal, p->y_normal, p->z_normal, bt.data(), out.data()),
+           "create_laplacian_for_Poisson");
+    if (!p->lap_Poison) p->lap_Poison = unpack_rows(out, n, k);
+    else
+        for (int i = 0; i < n; i++) std::memcpy(p->lap_Poison[i], &out[(size_t)i * k], sizeof(double) * k);
+}
+
+// mat_lib.h:423-491 on the GPU; inverse rows allocated by the caller
+void matrixInverse_Gauss_Jordan(double **matrix1, double **inverse, int order)
+{
+    std::vector<double> a = pack_rows(matrix1, order, order), inv((size_t)order * order);
+    die_if(mgm_gauss_jordan(order, a.data(), inv.data()), "matrixInverse_Gauss_Jordan");
+    for (int i = 0; i < order; i++) std::memcpy(inverse[i], &inv[(size_t)i * order], sizeof(double) * order);
+}
+
 void multiply_sparse_matrix_vector_gpu(double **D, double *f, double *dfdx, int **cloud, int n, int k)
 {
     std::vector<double> W = pack_rows(D, n, k);
@@ -472,6 +522,7 @@ void copyin_essentials_to_gpu(PointStructure *ps)
 {
     if (g_ctx) mgm_destroy(g_ctx);
     g_levels = parameters.num_levels;
+    g_ps = ps;
     g_ctx = mgm_create(parameters.dimension, parameters.phs_degree, g_levels);
     if (!g_ctx) { std::printf("Error: copyin_essentials_to_gpu: %s\n", mgm_last_error()); std::exit(1); }
     for (int l = 0; l < g_levels; l++) {
@@ -527,6 +578,53 @@ static void need_ctx(const char *fn)
     if (!g_ctx) { std::printf("Error: %s before copyin_essentials_to_gpu\n", fn); std::exit(1); }
 }
 
+// the level index of a PointStructure of the array handed to copyin_essentials_to_gpu
+static int level_of(const PointStructure *p, const char *fn)
+{
+    need_ctx(fn);
+    const long l = p - g_ps;
+    if (!g_ps || l < 0 || l >= g_levels) {
+        std::printf("Error: %s: not a level of the structure passed to copyin_essentials_to_gpu\n", fn);
+        std::exit(1);
+    }
+    return (int)l;
+}
+
+// fractional_step_solver.h:168-246: one multigrid routine on the device levels
+// (data-parallel sweep order); the host arrays it changes are refreshed after
+void relaxation(PointStructure *p, FieldVariables *f)
+{
+    const int l = level_of(p, "relaxation");
+    die_if(mgm_ref_routine(g_ctx, l, MGM_REF_RELAXATION), "relaxation");
+    die_if(mgm_get_field(g_ctx, l, MGM_FIELD_P, f->p), "relaxation");
+    die_if(mgm_get_field(g_ctx, l, MGM_FIELD_RES, f->res), "relaxation");
+}
+
+void calculate_residuals(PointStructure *p, FieldVariables *f)
+{
+    const int l = level_of(p, "calculate_residuals");
+    die_if(mgm_ref_routine(g_ctx, l, MGM_REF_RESIDUALS), "calculate_residuals");
+    die_if(mgm_get_field(g_ctx, l, MGM_FIELD_RES, f->res), "calculate_residuals");
+}
+
+void restrict_residuals(PointStructure *pf, PointStructure *pc, FieldVariables *ff, FieldVariables *fc)
+{
+    (void)ff;
+    const int l = level_of(pf, "restrict_residuals");
+    if (pc != pf + 1) { std::printf("Error: restrict_residuals: levels not consecutive\n"); std::exit(1); }
+    die_if(mgm_ref_routine(g_ctx, l, MGM_REF_RESTRICT), "restrict_residuals");
+    die_if(mgm_get_field(g_ctx, l + 1, MGM_FIELD_SOURCE, fc->source), "restrict_residuals");
+}
+
+void prolongate_corrections(PointStructure *pf, PointStructure *pc, FieldVariables *ff, FieldVariables *fc)
+{
+    const int l = level_of(pf, "prolongate_corrections");
+    if (pc != pf + 1) { std::printf("Error: prolongate_corrections: levels not consecutive\n"); std::exit(1); }
+    die_if(mgm_ref_routine(g_ctx, l, MGM_REF_PROLONGATE), "prolongate_corrections");
+    die_if(mgm_get_field(g_ctx, l, MGM_FIELD_P, ff->p), "prolongate_corrections");
+    die_if(mgm_get_field(g_ctx, l + 1, MGM_FIELD_P, fc->p), "prolongate_corrections");
+}
+
 void calculate_intermediate_velocity(PointStructure *p, FieldVariables *f)
 {
     (void)p;
@@ -562,7 +660,11 @@ void update_velocity(PointStructure *p, FieldVariables *f)
     double mass = 0;
     die_if(mgm_update_velocity(g_ctx, &mass), "update_velocity");
     std::printf("Mass residual: %e\n", mass);
-    (void)p; (void)f;
+    // the host view of the corrected velocities (the reference's managed memory)
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_U, f->u), "update_velocity");
+    die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_V, f->v), "update_velocity");
+    if (parameters.dimension == 3) die_if(mgm_get_field(g_ctx, 0, MGM_FIELD_W, f->w), "update_velocity");
+    (void)p;
 }
 
 // fractional_step_solver.h:47-71

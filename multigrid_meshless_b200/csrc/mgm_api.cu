@@ -1337,6 +1337,28 @@ int mgm_set_solver(mgm_ctx *c, double rel_tol, int max_iters, int cheb_degree, d
     });
 }
 
+int mgm_ref_routine(mgm_ctx *c, int level, int routine)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done, "mgm_ref_routine: not ready");
+        MGM_REQUIRE(c->have_ref_transfer || c->nl == 1,
+                    "mgm_ref_routine: needs mgm_setup(..., MGM_SETUP_REFERENCE_TRANSFER) or mgm_load_transfer");
+        const bool pair = routine == MGM_REF_RESTRICT || routine == MGM_REF_PROLONGATE;
+        MGM_REQUIRE(level >= 0 && level < c->nl - (pair ? 1 : 0), "mgm_ref_routine: level out of range");
+        auto R = ref_levels(c);
+        const double w1 = (double)c->omega, w2 = (double)(1 - c->omega);
+        switch (routine) {
+        case MGM_REF_RELAXATION: ref_relaxation(R[level], w1, w2, c->num_relax, c->s); break;
+        case MGM_REF_RESIDUALS: ref_residual_interior(R[level], c->s); break;
+        case MGM_REF_RESTRICT: ref_restrict(R[level], R[level + 1], c->s); break;
+        case MGM_REF_PROLONGATE: ref_prolongate(R[level], R[level + 1], c->s); break;
+        default: throw Error{MGM_ERR_ARG, "mgm_ref_routine: unknown routine"};
+        }
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+    });
+}
+
 int mgm_use_compact(mgm_ctx *c, int enable)
 {
     return guard([&] {

@@ -1362,3 +1362,13 @@ ORC_EXPORT double orc_heat_step(void *h, int wave)
     free(temp);
     return e;
 }
+
+/* matrixInverse_Gauss_Jordan (mat_lib.h:423-491) of one row-major N x N matrix */
+ORC_EXPORT void orc_gauss_jordan(int N, const double *A, double *Ainv)
+{
+    double *aug = (double *)malloc(sizeof(double) * (size_t)N * 2 * N);
+    double **rows = (double **)malloc(sizeof(double *) * (size_t)N);
+    gauss_jordan(N, A, Ainv, aug, rows);
+    free(aug);
+    free(rows);
+}

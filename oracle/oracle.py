@@ -100,6 +100,7 @@ def lib(crpow: bool = False):
         L.orc_read_gmsh.argtypes = _MESH_ARGS
         L.orc_read_gmsh.restype = C.c_int
         L.orc_ctx_coords.argtypes = [C.c_void_p, C.c_int, dp, dp, dp]
+        L.orc_gauss_jordan.argtypes = [C.c_int, dp, dp]
         for nm in ("orc_heat_init", "orc_heat_boundary_rhs", "orc_heat_step"):
             getattr(L, nm).argtypes = [C.c_void_p, C.c_int]
         L.orc_heat_step.restype = C.c_double
@@ -145,6 +146,7 @@ def ref_lib(timple: bool = False, heat: bool = False):
         L.ref_field_get.argtypes = [C.c_int, C.c_int, dp]
         L.ref_field_set.argtypes = [C.c_int, C.c_int, dp]
         L.ref_spmv.argtypes = [C.c_int, C.c_int, dp, dp]
+        L.ref_gauss_jordan.argtypes = [C.c_int, dp, dp]
         L.ref_read_mesh.argtypes = _MESH_ARGS
         L.ref_read_mesh.restype = C.c_int
         if heat:
@@ -402,6 +404,24 @@ class HeatSolver(OracleSolver):
 
     def step(self):
         return self.O.orc_heat_step(self.h, self.wave)
+
+
+def phs_system(n_pts, poly, seed=0, phs=3, dim=2):
+    """A PHS + polynomial saddle-point matrix (create_A_matrix_from_cloud_indices,
+    rbf.h:42-77) of a seeded point cloud, row-major, for the dense-inverse tests."""
+    rng = np.random.default_rng(seed)
+    p = rng.uniform(-1, 1, (n_pts, dim)) * 0.05
+    p[0] = 0.0
+    ex = [(i, j) for i in range(poly + 1) for j in range(poly + 1 - i)]
+    N = n_pts + len(ex)
+    A = np.zeros((N, N))
+    r = np.sqrt(((p[:, None, :] - p[None, :, :]) ** 2).sum(-1))
+    A[:n_pts, :n_pts] = r ** phs
+    for t, (a, b) in enumerate(ex):
+        v = (p[:, 0] - p[0, 0]) ** a * (p[:, 1] - p[0, 1]) ** b
+        A[:n_pts, n_pts + t] = v
+        A[n_pts + t, :n_pts] = v
+    return A
 
 
 def lid_bc(L, f):

@@ -296,3 +296,22 @@ void ref_write_test_files(double *f, double *fx, double *fy, double *fz, double 
 {
     write_test_files(f, fx, fy, fz, lapf, fxx, fyy, fzz, n, folder);
 }
+
+/* matrixInverse_Gauss_Jordan (mat_lib.h:423-491) on a row-major N x N matrix */
+void ref_gauss_jordan(int N, const double *A, double *Ainv)
+{
+    double **a = (double **)malloc(sizeof(double *) * (size_t)N), **b = (double **)malloc(sizeof(double *) * (size_t)N);
+    for (int i = 0; i < N; i++) {
+        a[i] = (double *)malloc(sizeof(double) * (size_t)N);
+        b[i] = (double *)malloc(sizeof(double) * (size_t)N);
+        for (int j = 0; j < N; j++) a[i][j] = A[(size_t)i * N + j];
+    }
+    matrixInverse_Gauss_Jordan(a, b, N);
+    for (int i = 0; i < N; i++) {
+        for (int j = 0; j < N; j++) Ainv[(size_t)i * N + j] = b[i][j];
+        free(a[i]);
+        free(b[i]);
+    }
+    free(a);
+    free(b);
+}

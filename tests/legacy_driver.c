@@ -3,7 +3,7 @@
  * (the flow of mg_NS_solver.c:17-103 with the mesh reader replaced by a node
  * file), linked against libmgm.so through include/mgm_reference.h.
  *
- *   legacy_driver <input.bin> <output_dir> [timple]
+ *   legacy_driver <input.bin> <output_dir> [timple|routines]
  *   legacy_driver --gmsh <flow_parameters.csv> <grid_filenames.csv> <output_dir>
  *
  * The --gmsh form is mg_NS_solver.c:17-45 as written: read_flow_parameters,
@@ -15,6 +15,11 @@
  * time_implicit_solver (timple_solver.h:40-70), on the Taylor-Couette
  * conditions of init_TC.c (iter_timple = iter_momentum = 2, facRe = facdt = 1);
  * otherwise fractional_step_explicit on the lid-driven cavity (init_LDC.c).
+ * With "routines" the operators come from create_full_gradx/grady/gradz/
+ * laplacian_matrix and create_laplacian_for_Poisson, and each step calls the
+ * fractional step's parts and multigrid routines one by one (the cycle of
+ * multigrid_Poisson_solver, fractional_step_solver.h:150-166, written out);
+ * it also writes the inverse of a small matrix by matrixInverse_Gauss_Jordan.
  *
  * input.bin: int32 nl, dim, phs, poly, multiplier, nsteps, num_vcycles,
  *            num_relax, mode; double Re, courant, omega; per level: int32 n,
@@ -59,13 +64,15 @@ static void wr_rows_i(const char *dir, const char *name, int **rows, int n, int 
 }
 
 static int read_bin(const char *path, PointStructure **out_ps, int *out_nsteps);
-static int run(PointStructure *ps, int nl, int nsteps, int timple, const char *out);
+static int run(PointStructure *ps, int nl, int nsteps, int kind, const char *out);
+static void step_by_routines(PointStructure *ps, FieldVariables *field, int nl);
 
 int main(int argc, char **argv)
 {
-    if (argc < 3) { fprintf(stderr, "usage: legacy_driver input.bin outdir [timple]\n"); return 1; }
+    if (argc < 3) { fprintf(stderr, "usage: legacy_driver input.bin outdir [timple|routines]\n"); return 1; }
     const int gmsh = argc >= 5 && strcmp(argv[1], "--gmsh") == 0;
     const int timple = !gmsh && argc > 3 && strcmp(argv[3], "timple") == 0;
+    const int routines = !gmsh && argc > 3 && strcmp(argv[3], "routines") == 0;
     const char *out = gmsh ? argv[4] : argv[2];
     PointStructure *ps = NULL;
     int nl = 0, nsteps = 0;
@@ -81,8 +88,47 @@ int main(int argc, char **argv)
     } else {
         nl = read_bin(argv[1], &ps, &nsteps);
     }
-    for (int l = 0; l < nl; l++) create_derivative_matrices(&ps[l]);
-    return run(ps, nl, nsteps, timple, out);
+    for (int l = 0; l < nl; l++) {
+        if (!routines) {
+            create_derivative_matrices(&ps[l]);
+            continue;
+        }
+        create_full_gradx_matrix(&ps[l]);
+        create_full_grady_matrix(&ps[l]);
+        if (parameters.dimension == 3) create_full_gradz_matrix(&ps[l]);
+        create_full_laplacian_matrix(&ps[l]);
+        create_laplacian_for_Poisson(&ps[l]);
+    }
+    if (routines) {
+        /* a 5 x 5 matrix with a zero first pivot */
+        double a[5][5] = {{0, 2, 1, 0, 3}, {2, 0, 4, 1, 0}, {1, 4, 0, 2, 1}, {0, 1, 2, 5, 1}, {3, 0, 1, 1, 6}};
+        double *ar[5], *br[5], inv[25];
+        for (int i = 0; i < 5; i++) { ar[i] = a[i]; br[i] = inv + 5 * i; }
+        matrixInverse_Gauss_Jordan(ar, br, 5);
+        wr(out, "gj_inverse", inv, sizeof(inv));
+    }
+    return run(ps, nl, nsteps, timple ? 1 : (routines ? 2 : 0), out);
+}
+
+/* fractional_step_explicit (fractional_step_solver.h:47-71) through its parts,
+ * the multigrid written out with the per-level routines */
+static void step_by_routines(PointStructure *ps, FieldVariables *field, int nl)
+{
+    calculate_intermediate_velocity(&ps[0], &field[0]);
+    calculate_mass_residual(&ps[0], &field[0]);
+    calculate_boundary_dpdn(&ps[0], &field[0]);
+    for (int cyc = 0; cyc < parameters.num_vcycles; cyc++) {
+        for (int l = 0; l < nl; l++) {
+            relaxation(&ps[l], &field[l]);
+            calculate_residuals(&ps[l], &field[l]);
+            if (l != nl - 1) restrict_residuals(&ps[l], &ps[l + 1], &field[l], &field[l + 1]);
+        }
+        for (int l = nl - 1; l > 0; l--) {
+            prolongate_corrections(&ps[l - 1], &ps[l], &field[l - 1], &field[l]);
+            if (l != 1) relaxation(&ps[l - 1], &field[l - 1]);
+        }
+    }
+    update_velocity(&ps[0], &field[0]);
 }
 
 /* nodes from input.bin, then the steps of read_complete_mesh_data after the reader */
@@ -149,8 +195,10 @@ static int read_bin(const char *path, PointStructure **out_ps, int *out_nsteps)
     return nl;
 }
 
-static int run(PointStructure *ps, int nl, int nsteps, int timple, const char *out)
+/* kind 0: fractional_step_explicit, 1: time_implicit_solver, 2: the step by routines */
+static int run(PointStructure *ps, int nl, int nsteps, int kind, const char *out)
 {
+    const int timple = kind == 1;
     /* mg_NS_solver.c:47-59 with the lid-driven cavity conditions (init_LDC.c)
      * or, for TIMPLE, the Taylor-Couette ones (init_TC.c:33-52) */
     FieldVariables *field;
@@ -178,7 +226,14 @@ static int run(PointStructure *ps, int nl, int nsteps, int timple, const char *o
     copyin_parameters_to_gpu();
 
     double *errs = malloc(sizeof(double) * (nsteps > 0 ? nsteps : 1));
-    for (int s = 0; s < nsteps; s++) errs[s] = timple ? time_implicit_solver(ps, field) : fractional_step_explicit(ps, field);
+    for (int s = 0; s < nsteps; s++) {
+        if (kind == 2) {
+            step_by_routines(ps, field, nl);
+            errs[s] = 0;
+        } else {
+            errs[s] = timple ? time_implicit_solver(ps, field) : fractional_step_explicit(ps, field);
+        }
+    }
 
     for (int l = 0; l < nl; l++) {
         PointStructure *p = &ps[l];

@@ -134,3 +134,39 @@ def test_reference_call_surface_timple(require_gpu, tmp_path):
     for nm in ("u_new", "v_new"):
         assert np.array_equal(_read(out, nm, np.float64), S.f[nm]), nm
     assert np.array_equal(_read(out, "p_old", np.float64), S.p_old)
+
+
+def test_reference_routines_one_by_one(require_gpu, tmp_path):
+    """A C program that builds the operators with create_full_gradx/grady/
+    laplacian_matrix + create_laplacian_for_Poisson and runs each step through
+    calculate_intermediate_velocity ... update_velocity with the multigrid
+    written out (relaxation, calculate_residuals, restrict_residuals,
+    prolongate_corrections per level) gets the bits of create_derivative_matrices
+    + fractional_step_explicit; and its matrixInverse_Gauss_Jordan matches the
+    restatement."""
+    exe = _compile(str(tmp_path))
+    cl = clouds.cavity_hierarchy(40, 3, seed=21)
+    k = 20
+    inp = str(tmp_path / "in.bin")
+    _write_input(inp, cl, 3, 2, 2, 2, 3, 0, 100.0, 0.5, 1.2)
+    outs = {}
+    for mode in ("default", "routines"):
+        out = str(tmp_path / mode)
+        os.makedirs(out)
+        args = [exe, inp, out] + ([mode] if mode == "routines" else [])
+        r = subprocess.run(args, capture_output=True, text=True)
+        assert r.returncode == 0, r.stdout + r.stderr
+        outs[mode] = out
+    for l, c in enumerate(cl):
+        for nm in ("Dx", "Dy", "lap", "lapP"):
+            a = _read(outs["default"], f"l{l}_{nm}", np.float64)
+            b = _read(outs["routines"], f"l{l}_{nm}", np.float64)
+            assert np.array_equal(a, b), (l, nm)
+    for nm in ("u", "v", "p"):
+        a, b = _read(outs["default"], nm, np.float64), _read(outs["routines"], nm, np.float64)
+        assert np.array_equal(a, b), nm
+        assert np.abs(a).max() > 0
+    A = np.array([[0, 2, 1, 0, 3], [2, 0, 4, 1, 0], [1, 4, 0, 2, 1], [0, 1, 2, 5, 1], [3, 0, 1, 1, 6]], np.float64)
+    want = np.zeros(25)
+    O.lib().orc_gauss_jordan(5, np.ascontiguousarray(A), want)
+    assert np.array_equal(_read(outs["routines"], "gj_inverse", np.float64), want)

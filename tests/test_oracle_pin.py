@@ -108,3 +108,20 @@ def test_tie_free_clouds():
         t_raw = Ol.orc_count_ties(n, c.nb, c.x, c.y, c.z, 20, cl)
         assert t_raw == 0
         assert t >= 0
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build not present")
+def test_gauss_jordan_restatement_matches_reference():
+    """matrixInverse_Gauss_Jordan (mat_lib.h:423-491): the restatement and the
+    reference's own function give the same bits on PHS saddle-point systems
+    (zero first pivot, so the bubble pass matters) and on random matrices."""
+    rng = np.random.default_rng(5)
+    cases = [O.phs_system(m, poly, seed=m + poly) for m, poly in ((20, 3), (30, 4), (12, 2))]
+    cases += [rng.standard_normal((n, n)) + n * np.eye(n) for n in (1, 7, 64)]
+    for A in cases:
+        A = np.ascontiguousarray(A)
+        n = A.shape[0]
+        want, got = np.zeros(n * n), np.zeros(n * n)
+        O.ref_lib().ref_gauss_jordan(n, A, want)
+        O.lib().orc_gauss_jordan(n, A, got)
+        assert np.array_equal(got, want), n
