@@ -153,3 +153,32 @@ def test_reference_main_on_gmsh_files(require_gpu, tmp_path):
     assert np.array_equal(rd("u", np.float64), S.f["u"])
     assert np.array_equal(rd("v", np.float64), S.f["v"])
     assert np.array_equal(rd("p", np.float64), S.p[0])
+
+
+def test_gmsh_cube_hierarchy_setup(require_gpu, tmp_path):
+    """Two 3D levels read from Gmsh cube meshes (triangle and quad faces; edge
+    lines make their nodes corners, which the reader drops): clouds, order,
+    normals and every operator bit for bit against the oracle pipeline on the
+    restatement's reading, and a convergent FP32-in-FP64 step on top."""
+    paths = []
+    for l, m in enumerate((10, 6)):
+        p = os.path.join(str(tmp_path), f"cu{l}.msh")
+        meshgen.cube3d(p, m, seed=30 + l, quads_on_top=(l == 0))
+        paths.append(p)
+    k, poly = 30, 2
+    mg = api.Multigrid([api.read_gmsh(p, 3) for p in paths], [k] * 2, [poly] * 2, reference_transfer=True)
+    try:
+        P = O.orc_pipeline([_cloud(O.read_mesh(p, 3), 3) for p in paths], [k] * 2, [poly] * 2, crpow=True)
+        levels = O.levels_from_device(mg)
+        for l, L in enumerate(P):
+            for nm in ("cloud", "x", "y", "z", "nx", "ny", "nz", "btag"):
+                assert np.array_equal(getattr(levels[l], nm), getattr(L, nm)), (l, nm)
+            for nm in ("Dx", "Dy", "Dz", "lap", "lapP"):
+                assert np.array_equal(getattr(levels[l], nm), getattr(L, nm)), (l, nm)
+        mg.set_flow(Re=400.0, courant=0.3)
+        mg.set_solver(rel_tol=1e-8, max_iters=80)
+        mg.apply_bc(mgm.BC_LID)
+        mg.step(mgm.MODE_FP32_IR)
+        assert mg.last_solve()[1] < 1e-8
+    finally:
+        mg.close()
