@@ -11,6 +11,10 @@ Function names follow the reference (Multigrid_meshless header_files/*.h):
   create_{restriction,prolongation}_matrix  mesh_functions.h:533-670 -> transfer_weights()
   multiply_sparse_matrix_vector_gpu  mat_lib.h:80-89       -> spmv()
   read_PointStructure         mesh_functions.h:172-476     -> read_gmsh()
+  matrixInverse_Gauss_Jordan  mat_lib.h:423-491            -> gauss_jordan()
+  create_laplacian_for_Poisson  rbf.h:382-399              -> laplacian_for_poisson()
+  relaxation / calculate_residuals / restrict_residuals / prolongate_corrections
+                              fractional_step_solver.h:168-246 -> Multigrid.ref_routine()
   fractional_step_explicit    fractional_step_solver.h:47-71 -> Multigrid.step()
 
 Arrays at this boundary use the reference's layout: node vectors of length n
@@ -122,6 +126,29 @@ def spmv(D, cloud, f):
     n, k = D.shape
     out = np.zeros(n)
     check(L.mgm_spmv(n, k, D, _i(cloud), _f(f), out))
+    return out
+
+
+def gauss_jordan(A):
+    """matrixInverse_Gauss_Jordan (mat_lib.h:423-491) of a square matrix on the GPU."""
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    n = A.shape[0]
+    inv = np.zeros((n, n))
+    check(load().mgm_gauss_jordan(n, A, inv))
+    return inv
+
+
+def laplacian_for_poisson(Dx, Dy, Dz, lap, nx, ny, nz, btag):
+    """create_laplacian_for_Poisson (rbf.h:382-399): lap on interior rows, the
+    normal derivative on boundary rows ([n][k] arrays; Dz, nz None in 2D)."""
+    Dx = _f(Dx)
+    n, k = Dx.shape
+    dim = 2 if Dz is None else 3
+    Dz = None if Dz is None else _f(Dz)
+    nz = None if nz is None else _f(nz)
+    out = np.zeros((n, k))
+    check(load().mgm_laplacian_for_poisson(n, k, dim, Dx, _f(Dy), ptr(Dz), _f(lap), _f(nx), _f(ny), ptr(nz),
+                                           _u8(btag), out))
     return out
 
 
@@ -248,6 +275,14 @@ class Multigrid:
 
     def checkpoint_load(self, path):
         check(self.L.mgm_checkpoint_load(self.h, str(path).encode()))
+
+    REF_ROUTINES = {"relaxation": 0, "residuals": 1, "restrict": 2, "prolongate": 3}
+
+    def ref_routine(self, level, routine):
+        """One routine of the fractional step's reference-semantics multigrid:
+        relaxation / residuals on `level`, restrict from `level` into level+1,
+        prolongate from level+1 into `level` (fractional_step_solver.h:168-246)."""
+        check(self.L.mgm_ref_routine(self.h, int(level), self.REF_ROUTINES[routine]))
 
     def timple_run(self, mode, nsteps):
         """nsteps TIMPLE steps timed on the device: (step_ms, p' V-cycles, steady_err)."""
