@@ -245,7 +245,9 @@ MGM_API int mgm_set_field(mgm_ctx *ctx, int lev, int which, const double *values
 MGM_API int mgm_get_field(mgm_ctx *ctx, int lev, int which, double *values);
 
 /* Boundary/initial conditions on level 0: MGM_BC_LID (init/init_LDC.c:16-44)
- * or MGM_BC_TAYLOR_COUETTE (init/init_TC.c:17-54).  Fields are zeroed first. */
+ * or MGM_BC_TAYLOR_COUETTE (init/init_TC.c:17-54).  Every field of every
+ * level (velocities and their copies, pressures, p', sources, residuals,
+ * gradients) is zeroed first, as the reference's fields start. */
 #define MGM_BC_LID 0
 #define MGM_BC_TAYLOR_COUETTE 1
 MGM_API int mgm_apply_bc(mgm_ctx *ctx, int kind);

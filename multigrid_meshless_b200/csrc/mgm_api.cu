@@ -1312,8 +1312,15 @@ int mgm_apply_bc(mgm_ctx *c, int kind)
         MGM_REQUIRE(c->setup_done, "mgm_apply_bc: call mgm_setup first");
         MGM_REQUIRE(kind == MGM_BC_LID || kind == MGM_BC_TAYLOR_COUETTE, "mgm_apply_bc: unknown kind");
         cudaStream_t s = c->s;
-        for (DBuf<double> *b : {&c->u, &c->v, &c->w, &c->u_new, &c->v_new, &c->w_new}) b->zero(s);
-        c->L[0].p.zero(s);
+        // every field starts from zero, as the reference's calloc'd fields do
+        for (DBuf<double> *b : {&c->u, &c->v, &c->w, &c->u_new, &c->v_new, &c->w_new, &c->u_old, &c->v_old,
+                                &c->w_old, &c->dpdn, &c->dpdx, &c->dpdy, &c->dpdz, &c->p_old})
+            b->zero(s);
+        for (int l = 0; l < c->nl; l++) {
+            c->L[l].p.zero(s);
+            c->L[l].src.zero(s);
+            c->L[l].res.zero(s);
+        }
         Level &L = c->L[0];
         k_bc<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, kind, L.x.p, L.y.p, c->u.p, c->v.p, c->u_new.p, c->v_new.p);
         MGM_LAUNCHED();

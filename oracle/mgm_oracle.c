@@ -829,10 +829,21 @@ typedef struct {
     double *p_old;
     int iter_timple, iter_momentum;
     double facRe, facdt;
+    const int *color;   /* jacobi == 2: the momentum sweeps' colours (orc_ctx_timple_colors) */
+    int ncolors;
     double *su, *sv, *sw;  /* previous-sweep copies (Jacobi order) */
 } orc_timple;
 
 static orc_timple g_timple;
+
+/* the colours of the momentum sweeps in colour order (jacobi == 2); borrowed */
+ORC_EXPORT void orc_ctx_timple_colors(void *h, const int *color, int ncolors)
+{
+    orc_ctx *c = (orc_ctx *)h;
+    c->jacobi = 2;
+    g_timple.color = color;
+    g_timple.ncolors = ncolors;
+}
 
 ORC_EXPORT void orc_ctx_timple(void *h, double *p_old, int iter_timple, int iter_momentum, double facRe, double facdt)
 {
@@ -863,13 +874,18 @@ static void timple_momentum(orc_ctx *c)
     if (dim == 3) orc_spmv(n, k, L->Dz, L->cloud, t->p_old, f->dpdz);
     for (int it = 0; it < t->iter_momentum; it++) {
         const double *uin = f->u_new, *vin = f->v_new, *win = f->w_new;
-        if (c->jacobi) {
+        if (c->jacobi == 1) {
             memcpy(t->su, f->u_new, sizeof(double) * (size_t)n); uin = t->su;
             memcpy(t->sv, f->v_new, sizeof(double) * (size_t)n); vin = t->sv;
             if (dim == 3) { memcpy(t->sw, f->w_new, sizeof(double) * (size_t)n); win = t->sw; }
         }
+        /* jacobi == 2: in place, colour by colour (no two nodes of a colour in
+         * each other's clouds, so a colour's nodes may go in any order) */
+        const int passes = c->jacobi == 2 ? t->ncolors : 1;
+        for (int pass = 0; pass < passes; pass++)
         for (int i = 0; i < n; i++) {
             if (L->btag[i]) continue;
+            if (c->jacobi == 2 && t->color[i] != pass) continue;
             const size_t r = (size_t)i * k;
             const double *comp_in[3] = {uin, vin, win};
             double *comp_out[3] = {f->u_new, f->v_new, f->w_new};
