@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--sample-m", type=int, default=128, help="cavity size of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start measurement")
+    ap.add_argument("--no-half", action="store_true", help="skip the FP16-operator measurement")
     ap.add_argument("--learn-episodes", type=int, default=12, help="training episodes (Re ~ U[100, 1000])")
     ap.add_argument("--learn-iters", type=int, default=400, help="Adam iterations of the GPU training")
     ap.add_argument("--workload", choices=["cavity", "annulus", "cube", "shell-batch"], default="cavity",
@@ -361,6 +362,31 @@ def run_ours(a, rank, world, local_rank):
     barrier()
     ms = max_over_ranks(ms)
 
+    # the same steps with the FP16 operator (D^-1 A) in the FP32 V-cycle
+    # (mgm_use_half_operator); reported beside the headline, not as it
+    half = None
+    if not a.no_half:
+        mg.use_half_operator(True)
+        arm(fast, min(a.warmup, 2))
+        barrier()
+        mg.sync()
+        h0 = mg.profile_read()
+        half_ms, half_pms, half_vc, half_err = arm(fast, a.steps)
+        h1 = mg.profile_read()
+        barrier()
+        half_ms = max_over_ranks(half_ms)
+        mg.use_half_operator(False)
+        h_launch = h1[1] - h0[1]
+        h_avg_s = ((h1[0] - h0[0]) / 1e3) / max(h_launch, 1)
+        half = {"steps_per_s": a.steps * world / (half_ms / 1e3), "ms_per_step": half_ms / a.steps,
+                "poisson_ms": half_pms / a.steps, "vcycles_per_step": half_vc / a.steps,
+                "steady_err_last": half_err,
+                "level0_smoother": {"kernel": "k_level_h4<0> (FP16 D^-1 A + int16 offsets, one 16-byte load "
+                                              "per slot per 4 rows)",
+                                    "bytes_per_launch": h1[2], "launches": h_launch,
+                                    "avg_launch_us": h_avg_s * 1e6,
+                                    "achieved_gbs": h1[2] / h_avg_s / 1e9 if h_launch else None}}
+
     # end to end through the public API with page-locked host buffers:
     # per step H2D of u, v and D2H of u, v, p (the reference's `update host(field[0])`)
     bufs = [api.PinnedArray(n) for _ in range(5)]
@@ -421,6 +447,7 @@ def run_ours(a, rank, world, local_rank):
             "plain_fp64": {"steps_per_s": a.steps * world / (plain_ms / 1e3), "ms_per_step": plain_ms / a.steps,
                            "poisson_ms": plain_pms / a.steps, "vcycles_per_step": plain_vc / a.steps},
             "learned_warm_start": learned,
+            "half_operator": half,
             "headline_arm": ("FP32 V-cycle inside FP64 FGMRES without the learned warm start (the faster arm: "
                              "the measured learned arm is in learned_warm_start)"),
             "e2e": {"value": steps_total / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": 2 * 8 * n,

@@ -350,6 +350,18 @@ MGM_API int mgm_use_graphs(mgm_ctx *ctx, int enable);
  * or read it with plain vector loads, four rows per thread (enable = 0, the
  * default, faster on B200).  Same results either way. */
 MGM_API int mgm_use_tiled(mgm_ctx *ctx, int enable);
+/* MGM_MODE_FP32_IR with a half-precision operator (enable = 1; default 0):
+ * on levels of at least 65,536 rows the V-cycle's smoother and residual read
+ * D^-1 A in FP16 packed with the int16 neighbour offsets (4 bytes per stencil
+ * slot instead of 6), each row applied in difference form about its node so
+ * that the row keeps its FP32 row sum; all sums stay FP32 and the FGMRES
+ * refinement around the V-cycle stays FP64, so a solve still ends at the
+ * relative residual set by mgm_set_solver.  A level whose scaled weights
+ * leave FP16's range keeps its FP32 operator.  Results differ in rounding
+ * from enable = 0 (a different preconditioner); the tile-streamed kernels of
+ * mgm_use_tiled take precedence where enabled.  No counterpart in the
+ * reference (its solver is FP64 throughout). */
+MGM_API int mgm_use_half_operator(mgm_ctx *ctx, int enable);
 /* Statistics of the last Poisson solve: outer iterations (V-cycles) and the
  * true relative residual ||b - A p|| / ||b|| over rows != 0 (FP64). */
 MGM_API int mgm_last_solve(mgm_ctx *ctx, int *iters, double *rel_res);

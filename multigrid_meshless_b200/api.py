@@ -313,6 +313,10 @@ class Multigrid:
     def use_tiled(self, enable=True):
         check(self.L.mgm_use_tiled(self.h, 1 if enable else 0))
 
+    def use_half_operator(self, enable=True):
+        """FP32_IR V-cycle on the FP16 operator D^-1 A (large levels); no reference counterpart."""
+        check(self.L.mgm_use_half_operator(self.h, 1 if enable else 0))
+
     def use_graphs(self, enable=True):
         check(self.L.mgm_use_graphs(self.h, 1 if enable else 0))
 

@@ -45,6 +45,11 @@ struct Level {
     DBuf<float> A32t;
     DBuf<short> off16t;
     int ldt = 0;
+    // FP16 operator for the half-operator V-cycle (levels of kVecMinRows rows
+    // or more): D^-1 A (row sum in the diagonal slot) packed with off16 per 4
+    // rows and slot, [k][ld4 / 4]
+    DBuf<uint4> W16;
+    bool h_ok = false;
     // reference-mode state
     DBuf<double> p, ptmp, src, res;
     // solver work vectors
@@ -92,6 +97,7 @@ struct mgm_ctx {
     double last_learned_alpha = 0;    // step length the last solve took along the learned direction
     int warm_smooth_steps = 3;        // Chebyshev steps that clean the learned direction
     bool use_tma = false;             // tile-streamed level kernels where a level has them (else 4 rows per thread)
+    bool half_operator = false;       // FP32 V-cycle reads the FP16 operator where built
     DBuf<int> tma_err;                // set by a tile-streamed kernel whose bounded wait ran out
     double *h_pinned = nullptr;
     SmootherProfile prof;

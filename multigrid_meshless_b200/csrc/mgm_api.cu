@@ -139,6 +139,49 @@ __global__ void __launch_bounds__(128) k_sort_slots(int n, int k, int ld, const 
     for (int j = 0; j < k; j++) { sidx[(long)j * ld + i] = c[j]; A32[(long)j * ld + i] = a[j]; }
 }
 
+// FP16 operator of the half-operator V-cycle (k_level_h4).  Interior row i's
+// weights are scaled by 1 / A_ii (D^-1 A: unit diagonal, off-diagonal weights
+// of order one) and rounded to FP16; the diagonal slot (offset 0) holds the
+// row sum of the scaled weights instead, which k_level_h4 uses to apply the
+// row in difference form.  Packed per 4 rows and stencil slot with the int16
+// offsets as {w_i, w_i+1 | w_i+2, w_i+3 | o_i, o_i+1 | o_i+2, o_i+3}; boundary
+// and padding rows (which the level kernels do not use) get zero weights.  A
+// value outside FP16's finite range sets *overflow.  One thread per 4 rows.
+__global__ void k_pack_half(int n, int k, int ld4, const float *__restrict__ A32, const short *__restrict__ off16,
+                            const float *__restrict__ dinv, const uint8_t *__restrict__ btag, uint4 *__restrict__ W,
+                            int *__restrict__ overflow)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int q4 = ld4 >> 2;
+    if (t >= q4) return;
+    bool live[4];
+    float di[4];
+    double rs[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int v = 0; v < 4; v++) {
+        const int i = 4 * t + v;
+        live[v] = i < n && !btag[i];
+        di[v] = live[v] ? dinv[i] : 0.f;
+    }
+    for (int j = 0; j < k; j++)
+        for (int v = 0; v < 4; v++)
+            if (live[v]) rs[v] += (double)(A32[(long)j * ld4 + 4 * t + v] * di[v]);
+    for (int j = 0; j < k; j++) {
+        unsigned h[4], o[4];
+        for (int v = 0; v < 4; v++) {
+            const long e = (long)j * ld4 + 4 * t + v;
+            float w = 0.f;
+            if (live[v]) {
+                w = off16[e] == 0 ? (float)rs[v] : A32[e] * di[v];
+                if (!(fabsf(w) <= 65504.f)) atomicExch(overflow, 1);
+            }
+            h[v] = __half_as_ushort(__float2half_rn(w));
+            o[v] = (unsigned short)off16[e];
+        }
+        W[(long)j * q4 + t] =
+            make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), o[0] | (o[1] << 16), o[2] | (o[3] << 16));
+    }
+}
+
 // tile-major copy of an ELL array [k][ldin]: out[(t*k + j)*kTileRows + r] = in[j][t*kTileRows + r], zero past row n
 template <class T>
 __global__ void k_tile_major(int n, int k, int ld, int ldin, const T *__restrict__ in, T *__restrict__ out)
@@ -255,6 +298,7 @@ std::vector<SolveLevel<float>> solve_levels<float>(mgm_ctx *c)
             if (c->use_tma && L.ldt > 0) {
                 S.At = L.A32t.p; S.offt = L.off16t.p; S.ldt = L.ldt; S.tma_err = c->tma_err.p;
             }
+            if (c->half_operator && L.h_ok) S.W16 = L.W16.p;
         }
         out.push_back(S);
     }
@@ -1008,6 +1052,22 @@ void prepare_solver(mgm_ctx *c)
             MGM_LAUNCHED();
             L.ldt = ld;
         }
+        // FP16 operator for the large levels
+        L.W16.release();
+        L.h_ok = false;
+        if (L.off_ok && L.n >= kVecMinRows) {
+            DBuf<int> ovf(1);
+            ovf.zero(s);
+            L.W16.alloc((size_t)L.k * (L.ld4 / 4));
+            k_pack_half<<<blocks_for(L.ld4 / 4, 256), 256, 0, s>>>(L.n, L.k, L.ld4, L.A32.p, L.off16.p, L.dinv32.p,
+                                                                  L.btag.p, L.W16.p, ovf.p);
+            MGM_LAUNCHED();
+            int h_ovf = 0;
+            ovf.download(&h_ovf, 1, s);
+            MGM_CUDA(cudaStreamSynchronize(s));
+            L.h_ok = h_ovf == 0;
+            if (!L.h_ok) L.W16.release();
+        }
         for (DBuf<double> *b : {&L.p, &L.ptmp, &L.src, &L.res, &L.r64, &L.e64, &L.e64b, &L.d64, &L.q64}) { b->alloc(L.n); b->zero(s); }
         for (DBuf<float> *b : {&L.r32, &L.e32, &L.e32b, &L.d32, &L.q32}) { b->alloc(L.n); b->zero(s); }
     }
@@ -1386,6 +1446,16 @@ int mgm_use_tiled(mgm_ctx *c, int enable)
     });
 }
 
+int mgm_use_half_operator(mgm_ctx *c, int enable)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+        drop_graphs(c);
+        c->half_operator = enable != 0;
+    });
+}
+
 int mgm_use_graphs(mgm_ctx *c, int enable)
 {
     return guard([&] {
@@ -1569,10 +1639,14 @@ int mgm_profile_read(mgm_ctx *c, double *ms_total, long long *launches, long lon
         if (launches) *launches = c->prof.launches;
         if (bytes_per_launch) {
             // level-0 Chebyshev step of MGM_MODE_FP32_IR, each array counted once:
-            // per slot the weight and the index; per node r, dinv, e read, e' written,
-            // d written, d read by all but the first step of a smoothing pass, btag
+            // per slot the weight and the index (FP32 + int16, FP16 + int16 on the
+            // half-precision operator, FP32 + int32 on the plain layout); per node
+            // r, dinv, e read, e' written, d written, d read by all but the first
+            // step of a smoothing pass, btag
             const Level &L = c->L[0];
-            const double slot = (c->compact && L.off_ok) ? 6.0 : 8.0;
+            const bool compact = c->compact && L.off_ok;
+            const bool half = compact && c->half_operator && L.h_ok && !(c->use_tma && L.ldt > 0);
+            const double slot = half ? 4.0 : compact ? 6.0 : 8.0;
             const double dread = 4.0 * (c->cheb_deg - 1) / (double)c->cheb_deg;
             *bytes_per_launch = (long long)((double)L.n * (L.k * slot + 4 * 5 + 1 + dread));
         }

@@ -244,14 +244,99 @@ __global__ void __launch_bounds__(256) k_level_v4(int n, int ld, int k, const sh
         if (i0 + v < n) level_row_out<MODE>(i0 + v, s[v], dinv, btag, r, e, out, d, c1, c2, first);
 }
 
-// rows from which a compact level runs k_level_v4 (below: k_level_c1)
-constexpr int kVecMinRows = 65536;
+// k_level_h4: k_level_v4 on the FP16 operator W ~ D^-1 A.  One 16-byte load
+// per stencil slot brings the four rows' weights (FP16) and offsets (int16):
+// 4 bytes per slot instead of 6.  The off-diagonal weights enter in
+// difference form, s = sum_{j != i} w_ij (e_j - e_i) + rho_i e_i, where the
+// diagonal slot (offset 0) holds rho_i, the row sum of D^-1 A: the rows then
+// keep their sums (a Laplacian row maps constants to ~0) whatever the FP16
+// rounding of the single weights, which would otherwise perturb the smooth
+// modes by (rounding error) x (condition number).  Sums in FP32, in slot
+// order.  MODE 0: d = c1 d + c2 (D^-1 r - s), e' = e + d on interior rows;
+// MODE 1: q = r - s / D^-1 on interior rows, 0 on boundary rows.
+template <int MODE>
+__device__ __forceinline__ void level_row_out_h(int i, float s, const float *__restrict__ dinv,
+                                                const uint8_t *__restrict__ btag, const float *__restrict__ r,
+                                                float ei, float *__restrict__ out, float *__restrict__ d, float c1,
+                                                float c2, int first)
+{
+    if (MODE == 0) {
+        if (btag[i]) { out[i] = ei; return; }
+        const float q = dinv[i] * r[i] - s;
+        const float di = first ? c2 * q : c1 * d[i] + c2 * q;
+        d[i] = di;
+        out[i] = ei + di;
+    } else {
+        out[i] = btag[i] ? 0.f : r[i] - s / dinv[i];
+    }
+}
+
+__device__ __forceinline__ float h16(unsigned bits) { return __half2float(__ushort_as_half((unsigned short)bits)); }
+
+template <int MODE>
+__global__ void __launch_bounds__(256, 5) k_level_h4(int n, int ld, int k, const uint4 *__restrict__ W,
+                                                  const float *__restrict__ dinv, const uint8_t *__restrict__ btag,
+                                                  const float *__restrict__ r, const float *__restrict__ e,
+                                                  float *__restrict__ out, float *__restrict__ d, float c1, float c2,
+                                                  int first)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i0 = t * 4;
+    if (i0 >= n) return;
+    const long q4 = ld >> 2;
+    float s[4] = {0.f, 0.f, 0.f, 0.f}, ws[4] = {0.f, 0.f, 0.f, 0.f};
+    int j = 0;
+    for (; j + 4 <= k; j += 4) {
+        uint4 w[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) w[q] = __ldcs(W + (long)(j + q) * q4 + t);
+        float a[4][4];
+        int o[4][4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            a[q][0] = h16(w[q].x & 0xffffu); a[q][1] = h16(w[q].x >> 16);
+            a[q][2] = h16(w[q].y & 0xffffu); a[q][3] = h16(w[q].y >> 16);
+            o[q][0] = (int)(short)(w[q].z & 0xffffu); o[q][1] = (int)(short)(w[q].z >> 16);
+            o[q][2] = (int)(short)(w[q].w & 0xffffu); o[q][3] = (int)(short)(w[q].w >> 16);
+        }
+        // padding rows (i >= n) carry weight 0 and offset 0: clamp their gathers into the vector
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                s[v] += a[q][v] * __ldg(e + min(i0 + v + o[q][v], n - 1));
+                ws[v] += o[q][v] != 0 ? a[q][v] : 0.f;
+            }
+    }
+    for (; j < k; j++) {
+        const uint4 w = __ldcs(W + (long)j * q4 + t);
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const unsigned hw = (v < 2 ? w.x : w.y) >> (16 * (v & 1)), ow = (v < 2 ? w.z : w.w) >> (16 * (v & 1));
+            const float a = h16(hw & 0xffffu);
+            const int o = (int)(short)(ow & 0xffffu);
+            s[v] += a * __ldg(e + min(i0 + v + o, n - 1));
+            ws[v] += o != 0 ? a : 0.f;
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        const int i = i0 + v;
+        if (i < n) {
+            const float ei = e[i];
+            level_row_out_h<MODE>(i, s[v] - ws[v] * ei, dinv, btag, r, ei, out, d, c1, c2, first);
+        }
+    }
+}
 
 template <int MODE>
 static void launch_compact(const SolveLevel<float> &L, const float *e, float *out, float c1, float c2, int first,
                            cudaStream_t s)
 {
-    if (L.n >= kVecMinRows)
+    if (L.W16)
+        launch_k(k_level_h4<MODE>, blocks_for((L.n + 3) / 4, 256), 256, 0, s, L.n, L.ld, L.k, L.W16, L.dinv, L.btag,
+                 L.r, e, out, L.d, c1, c2, first);
+    else if (L.n >= kVecMinRows)
         launch_k(k_level_v4<MODE>, blocks_for((L.n + 3) / 4, 256), 256, 0, s, L.n, L.ld, L.k, L.off, L.A, L.dinv,
                  L.btag, L.r, e, out, L.d, c1, c2, first);
     else

@@ -88,7 +88,15 @@ struct SolveLevel {
     const short *offt = nullptr;
     int ldt = 0;
     int *tma_err = nullptr;
+    // FP16 copy of the compact operator (FP32 path, large levels; used when
+    // non-null): D^-1 A with the row sum in the diagonal slot, packed per 4
+    // rows and stencil slot as one uint4 {4 FP16 weights, 4 int16 offsets}, [k][ld / 4]
+    const uint4 *W16 = nullptr;
 };
+
+// rows from which a compact level runs the four-rows-per-thread kernels
+// (below: one row per thread); the FP16 operator is built from here too
+constexpr int kVecMinRows = 65536;
 
 // rows per tile of the tile-streamed level kernels
 constexpr int kTileRows = 256;

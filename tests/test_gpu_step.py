@@ -180,6 +180,52 @@ def test_tiled_levels_match_plain_loads(require_gpu):
 
 
 
+def test_half_operator_solves_to_tolerance(require_gpu):
+    """MGM_MODE_FP32_IR with the FP16 operator (D^-1 A packed with the int16
+    offsets) on the levels of >= 65,536 rows and FP16 prolongation weights
+    into them: a different preconditioner, so different bits from the FP32
+    operator, but the FP64 refinement still ends at the 1e-8 relative
+    residual, with at most two more V-cycles, and the pressure matches an
+    FP64 direct solve; graph replay and eager launches give the same bits,
+    and NS steps on it match the FP32-operator steps."""
+    cl = clouds.cavity_hierarchy(300, 4, seed=8)
+    mg = api.Multigrid(cl, [30] * 4, [4] * 4)
+    try:
+        assert mg.n(0) >= 65536 > mg.n(1)
+        mg.set_solver(rel_tol=1e-8, max_iters=80)
+        g = mg.geometry(0)
+        ops = mg.operators(0)
+        b = _smooth_rhs(g, 4)
+        p32, it32, rr32 = mg.solve_poisson(b, mode=mgm.MODE_FP32_IR)
+        mg.use_half_operator(True)
+        ph, ith, rrh = mg.solve_poisson(b, mode=mgm.MODE_FP32_IR)
+        mg.use_graphs(False)
+        pe, ite, _ = mg.solve_poisson(b, mode=mgm.MODE_FP32_IR)
+        mg.use_graphs(True)
+        assert rr32 < 1e-8 and rrh < 1e-8
+        assert ith <= it32 + 2, (ith, it32)
+        assert not np.array_equal(ph, p32)           # the FP16 operator was read
+        assert ite == ith and np.array_equal(pe, ph)
+        assert O.rel_residual(ops["lapP"], g["cloud"], b, ph) < 2e-8
+        want = O.pinned_poisson_direct(ops["lapP"], g["cloud"], b)
+        assert np.linalg.norm(ph - want) / np.linalg.norm(want) < P_TOL
+        # fractional steps from rest, FP16 operator against FP32 operator
+        runs = []
+        for half in (False, True):
+            mg.use_half_operator(half)
+            mg.set_flow(Re=100.0, courant=0.5)
+            mg.apply_bc(mgm.BC_LID)
+            for _ in range(3):
+                mg.step(mgm.MODE_FP32_IR)
+            runs.append((mg.get_field("u"), mg.get_field("p")))
+        (u0, p0), (u1, p1) = runs
+        assert np.all(np.isfinite(u1)) and np.all(np.isfinite(p1))
+        assert np.linalg.norm(u1 - u0) / np.linalg.norm(u0) < P_TOL
+        assert np.linalg.norm(p1 - p0) / np.linalg.norm(p0) < 1e-5
+    finally:
+        mg.close()
+
+
 def test_ref_routines_one_by_one_match_the_cycle(cavity):
     """The fractional step's multigrid written out with Multigrid.ref_routine
     (relaxation, residuals, restrict, prolongate per level) gives the bits of
