@@ -45,9 +45,10 @@ struct Level {
     DBuf<float> A32t;
     DBuf<short> off16t;
     int ldt = 0;
-    // FP16 operator for the half-operator V-cycle (levels of kVecMinRows rows
-    // or more): D^-1 A (row sum in the diagonal slot) packed with off16 per 4
-    // rows and slot, [k][ld4 / 4]
+    // FP16 operator of the half-operator V-cycle (levels of kVecMinRows rows
+    // or more): D^-1 A (row sum in the diagonal slot) packed with the offsets,
+    // four interleaved rows per uint4, [k][ldi / 4]
+    int ldi = 0;
     DBuf<uint4> W16;
     bool h_ok = false;
     // reference-mode state

@@ -143,39 +143,45 @@ __global__ void __launch_bounds__(128) k_sort_slots(int n, int k, int ld, const 
 // weights are scaled by 1 / A_ii (D^-1 A: unit diagonal, off-diagonal weights
 // of order one) and rounded to FP16; the diagonal slot (offset 0) holds the
 // row sum of the scaled weights instead, which k_level_h4 uses to apply the
-// row in difference form.  Packed per 4 rows and stencil slot with the int16
-// offsets as {w_i, w_i+1 | w_i+2, w_i+3 | o_i, o_i+1 | o_i+2, o_i+3}; boundary
-// and padding rows (which the level kernels do not use) get zero weights.  A
-// value outside FP16's finite range sets *overflow.  One thread per 4 rows.
-__global__ void k_pack_half(int n, int k, int ld4, const float *__restrict__ A32, const short *__restrict__ off16,
-                            const float *__restrict__ dinv, const uint8_t *__restrict__ btag, uint4 *__restrict__ W,
-                            int *__restrict__ overflow)
+// row in difference form.  One uint4 per stencil slot j and thread t (rows
+// 128 g + 32 v + lane, g = t / 32, lane = t % 32, v = 0..3):
+// {w_0, w_1 | w_2, w_3 | o_0, o_1 | o_2, o_3}, [k][ldi / 4];
+// boundary and padding rows (which the level kernels do not use) get zero
+// weights.  A value outside FP16's finite range sets *overflow.
+__global__ void k_pack_half(int n, int k, int ld4, int ldi, const float *__restrict__ A32,
+                            const short *__restrict__ off16, const float *__restrict__ dinv,
+                            const uint8_t *__restrict__ btag, uint4 *__restrict__ W, int *__restrict__ overflow)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int q4 = ld4 >> 2;
+    const int q4 = ldi >> 2;
     if (t >= q4) return;
+    const int ib = (t >> 5) * 128 + (t & 31);
     bool live[4];
     float di[4];
     double rs[4] = {0.0, 0.0, 0.0, 0.0};
     for (int v = 0; v < 4; v++) {
-        const int i = 4 * t + v;
+        const int i = ib + 32 * v;
         live[v] = i < n && !btag[i];
         di[v] = live[v] ? dinv[i] : 0.f;
     }
     for (int j = 0; j < k; j++)
         for (int v = 0; v < 4; v++)
-            if (live[v]) rs[v] += (double)(A32[(long)j * ld4 + 4 * t + v] * di[v]);
+            if (live[v]) rs[v] += (double)(A32[(long)j * ld4 + ib + 32 * v] * di[v]);
     for (int j = 0; j < k; j++) {
         unsigned h[4], o[4];
         for (int v = 0; v < 4; v++) {
-            const long e = (long)j * ld4 + 4 * t + v;
+            const int i = ib + 32 * v;
             float w = 0.f;
-            if (live[v]) {
-                w = off16[e] == 0 ? (float)rs[v] : A32[e] * di[v];
-                if (!(fabsf(w) <= 65504.f)) atomicExch(overflow, 1);
+            o[v] = 0;
+            if (i < n) {
+                const long e = (long)j * ld4 + i;
+                o[v] = (unsigned short)off16[e];
+                if (live[v]) {
+                    w = off16[e] == 0 ? (float)rs[v] : A32[e] * di[v];
+                    if (!(fabsf(w) <= 65504.f)) atomicExch(overflow, 1);
+                }
             }
             h[v] = __half_as_ushort(__float2half_rn(w));
-            o[v] = (unsigned short)off16[e];
         }
         W[(long)j * q4 + t] =
             make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), o[0] | (o[1] << 16), o[2] | (o[3] << 16));
@@ -298,7 +304,7 @@ std::vector<SolveLevel<float>> solve_levels<float>(mgm_ctx *c)
             if (c->use_tma && L.ldt > 0) {
                 S.At = L.A32t.p; S.offt = L.off16t.p; S.ldt = L.ldt; S.tma_err = c->tma_err.p;
             }
-            if (c->half_operator && L.h_ok) S.W16 = L.W16.p;
+            if (c->half_operator && L.h_ok) { S.W16 = L.W16.p; S.ldi = L.ldi; }
         }
         out.push_back(S);
     }
@@ -1054,18 +1060,21 @@ void prepare_solver(mgm_ctx *c)
         }
         // FP16 operator for the large levels
         L.W16.release();
+        L.ldi = 0;
         L.h_ok = false;
         if (L.off_ok && L.n >= kVecMinRows) {
+            const int ldi = (L.n + 127) / 128 * 128;
             DBuf<int> ovf(1);
             ovf.zero(s);
-            L.W16.alloc((size_t)L.k * (L.ld4 / 4));
-            k_pack_half<<<blocks_for(L.ld4 / 4, 256), 256, 0, s>>>(L.n, L.k, L.ld4, L.A32.p, L.off16.p, L.dinv32.p,
-                                                                  L.btag.p, L.W16.p, ovf.p);
+            L.W16.alloc((size_t)L.k * (ldi / 4));
+            k_pack_half<<<blocks_for(ldi / 4, 256), 256, 0, s>>>(L.n, L.k, L.ld4, ldi, L.A32.p, L.off16.p,
+                                                                L.dinv32.p, L.btag.p, L.W16.p, ovf.p);
             MGM_LAUNCHED();
             int h_ovf = 0;
             ovf.download(&h_ovf, 1, s);
             MGM_CUDA(cudaStreamSynchronize(s));
             L.h_ok = h_ovf == 0;
+            L.ldi = ldi;
             if (!L.h_ok) L.W16.release();
         }
         for (DBuf<double> *b : {&L.p, &L.ptmp, &L.src, &L.res, &L.r64, &L.e64, &L.e64b, &L.d64, &L.q64}) { b->alloc(L.n); b->zero(s); }

@@ -244,8 +244,13 @@ __global__ void __launch_bounds__(256) k_level_v4(int n, int ld, int k, const sh
         if (i0 + v < n) level_row_out<MODE>(i0 + v, s[v], dinv, btag, r, e, out, d, c1, c2, first);
 }
 
-// k_level_h4: k_level_v4 on the FP16 operator W ~ D^-1 A.  One 16-byte load
-// per stencil slot brings the four rows' weights (FP16) and offsets (int16):
+// k_level_h4: k_level_v4 on the FP16 operator W ~ D^-1 A, four rows per
+// thread interleaved: lane t of warp g holds rows 128 g + t + 32 v (v =
+// 0..3), so that a warp's gathers for one slot and row set v come from 32
+// consecutive rows and its per-row loads and stores are coalesced (measured
+// 8% faster than consecutive rows here; k_level_v4 measured 4% slower with
+// it).  One 16-byte load per stencil slot brings the four rows' weights
+// (FP16) and offsets (int16):
 // 4 bytes per slot instead of 6.  The off-diagonal weights enter in
 // difference form, s = sum_{j != i} w_ij (e_j - e_i) + rho_i e_i, where the
 // diagonal slot (offset 0) holds rho_i, the row sum of D^-1 A: the rows then
@@ -281,8 +286,8 @@ __global__ void __launch_bounds__(256, 5) k_level_h4(int n, int ld, int k, const
                                                   int first)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i0 = t * 4;
-    if (i0 >= n) return;
+    const int ib = (t >> 5) * 128 + (t & 31);   // rows ib + 32 v, v = 0..3
+    if (ib >= n) return;
     const long q4 = ld >> 2;
     float s[4] = {0.f, 0.f, 0.f, 0.f}, ws[4] = {0.f, 0.f, 0.f, 0.f};
     int j = 0;
@@ -304,7 +309,7 @@ __global__ void __launch_bounds__(256, 5) k_level_h4(int n, int ld, int k, const
         for (int q = 0; q < 4; q++)
 #pragma unroll
             for (int v = 0; v < 4; v++) {
-                s[v] += a[q][v] * __ldg(e + min(i0 + v + o[q][v], n - 1));
+                s[v] += a[q][v] * __ldg(e + min(ib + 32 * v + o[q][v], n - 1));
                 ws[v] += o[q][v] != 0 ? a[q][v] : 0.f;
             }
     }
@@ -315,13 +320,13 @@ __global__ void __launch_bounds__(256, 5) k_level_h4(int n, int ld, int k, const
             const unsigned hw = (v < 2 ? w.x : w.y) >> (16 * (v & 1)), ow = (v < 2 ? w.z : w.w) >> (16 * (v & 1));
             const float a = h16(hw & 0xffffu);
             const int o = (int)(short)(ow & 0xffffu);
-            s[v] += a * __ldg(e + min(i0 + v + o, n - 1));
+            s[v] += a * __ldg(e + min(ib + 32 * v + o, n - 1));
             ws[v] += o != 0 ? a : 0.f;
         }
     }
 #pragma unroll
     for (int v = 0; v < 4; v++) {
-        const int i = i0 + v;
+        const int i = ib + 32 * v;
         if (i < n) {
             const float ei = e[i];
             level_row_out_h<MODE>(i, s[v] - ws[v] * ei, dinv, btag, r, ei, out, d, c1, c2, first);
@@ -334,7 +339,7 @@ static void launch_compact(const SolveLevel<float> &L, const float *e, float *ou
                            cudaStream_t s)
 {
     if (L.W16)
-        launch_k(k_level_h4<MODE>, blocks_for((L.n + 3) / 4, 256), 256, 0, s, L.n, L.ld, L.k, L.W16, L.dinv, L.btag,
+        launch_k(k_level_h4<MODE>, blocks_for(L.ldi / 4, 256), 256, 0, s, L.n, L.ldi, L.k, L.W16, L.dinv, L.btag,
                  L.r, e, out, L.d, c1, c2, first);
     else if (L.n >= kVecMinRows)
         launch_k(k_level_v4<MODE>, blocks_for((L.n + 3) / 4, 256), 256, 0, s, L.n, L.ld, L.k, L.off, L.A, L.dinv,

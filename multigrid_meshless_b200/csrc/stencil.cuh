@@ -88,10 +88,13 @@ struct SolveLevel {
     const short *offt = nullptr;
     int ldt = 0;
     int *tma_err = nullptr;
-    // FP16 copy of the compact operator (FP32 path, large levels; used when
-    // non-null): D^-1 A with the row sum in the diagonal slot, packed per 4
-    // rows and stencil slot as one uint4 {4 FP16 weights, 4 int16 offsets}, [k][ld / 4]
+    // FP16 copy of the compact operator (levels of at least kVecMinRows rows;
+    // used when non-null): D^-1 A with the row sum in the diagonal slot, one
+    // uint4 {4 FP16 weights, 4 int16 offsets} per slot and thread, the
+    // thread's rows interleaved (128 g + 32 v + lane), [k][ldi / 4] with ldi
+    // the rows rounded up to a multiple of 128
     const uint4 *W16 = nullptr;
+    int ldi = 0;
 };
 
 // rows from which a compact level runs the four-rows-per-thread kernels
