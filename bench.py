@@ -167,6 +167,11 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
+            # nvidia-smi takes a moment to start: wait (at most 5 s) for its first
+            # sample, so that a short timed region is still sampled
+            t_end = time.time() + 5.0
+            while time.time() < t_end and self.proc.poll() is None and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
 
@@ -382,7 +387,7 @@ def run_ours(a, rank, world, local_rank):
                 "poisson_ms": half_pms / a.steps, "vcycles_per_step": half_vc / a.steps,
                 "steady_err_last": half_err,
                 "level0_smoother": {"kernel": "k_level_h4<0> (FP16 D^-1 A + int16 offsets, one 16-byte load "
-                                              "per slot per 4 rows)",
+                                              "per slot per 4 interleaved rows, rows in difference form)",
                                     "bytes_per_launch": h1[2], "launches": h_launch,
                                     "avg_launch_us": h_avg_s * 1e6,
                                     "achieved_gbs": h1[2] / h_avg_s / 1e9 if h_launch else None}}

@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(256) k_level_c1(int n, int ld, int k, const sh
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(256) k_level_v4(int n, int ld, int k, const short *__restrict__ off,
+__global__ void __launch_bounds__(256, 4) k_level_v4(int n, int ld, int k, const short *__restrict__ off,
                                                   const float *__restrict__ A, const float *__restrict__ dinv,
                                                   const uint8_t *__restrict__ btag, const float *__restrict__ r,
                                                   const float *__restrict__ e, float *__restrict__ out,
@@ -279,7 +279,7 @@ __device__ __forceinline__ void level_row_out_h(int i, float s, const float *__r
 __device__ __forceinline__ float h16(unsigned bits) { return __half2float(__ushort_as_half((unsigned short)bits)); }
 
 template <int MODE>
-__global__ void __launch_bounds__(256, 5) k_level_h4(int n, int ld, int k, const uint4 *__restrict__ W,
+__global__ void __launch_bounds__(256, 4) k_level_h4(int n, int ld, int k, const uint4 *__restrict__ W,
                                                   const float *__restrict__ dinv, const uint8_t *__restrict__ btag,
                                                   const float *__restrict__ r, const float *__restrict__ e,
                                                   float *__restrict__ out, float *__restrict__ d, float c1, float c2,
