@@ -76,3 +76,13 @@ def test_bfs_rejects_out_of_range_index():
 def test_spmv_rejects_bad_index():
     with pytest.raises(_lib.MgmError):
         api.spmv(np.ones((3, 2)), np.array([[0, 1], [1, 2], [2, 3]], np.int32), np.ones(3))
+
+
+@pytest.mark.parametrize("name", ["mgm_use_half_operator", "mgm_use_tiled", "mgm_use_graphs", "mgm_use_compact"])
+def test_solver_switches_reject_null_context(name):
+    """The V-cycle switches check their context on the host: a null context
+    is MGM_ERR_ARG with a message, before any CUDA call."""
+    L = _lib.load()
+    rc = getattr(L, name)(None, 1)
+    assert rc == _lib.MGM_ERR_ARG
+    assert b"null context" in L.mgm_last_error()
