@@ -362,6 +362,20 @@ MGM_API int mgm_use_tiled(mgm_ctx *ctx, int enable);
  * mgm_use_tiled take precedence where enabled.  No counterpart in the
  * reference (its solver is FP64 throughout). */
 MGM_API int mgm_use_half_operator(mgm_ctx *ctx, int enable);
+/* MGM_MODE_FP64 / MGM_MODE_FP32_IR with compatible right-hand sides
+ * (enable = 1; default 0).  lap_Poison (Laplacian interior rows, Neumann
+ * boundary rows) is singular; the pinned solve (row 0 replaced by p[0] = 0)
+ * otherwise puts the part of the source along the left null vector z into
+ * row 0, a pressure spike at node 0 that a converged solve resolves and the
+ * reference's non-converging cycles never do.  Enabled, each solve projects
+ * the source to b - alpha w (w: 1 on interior rows, alpha = z.b / z.w) and
+ * returns the pinned solution of that consistent system, which satisfies
+ * every row of lap_Poison: p_b - alpha p_w, with alpha from the residuals of
+ * the unpinned row-0 equation and p_w (the pinned solution for w) computed
+ * once per set-up, here when the context is set up, else at the next solve.
+ * Applies to the fractional step, the TIMPLE p' solve and
+ * mgm_solve_poisson.  No counterpart in the reference. */
+MGM_API int mgm_set_compatible_rhs(mgm_ctx *ctx, int enable);
 /* Statistics of the last Poisson solve: outer iterations (V-cycles) and the
  * true relative residual ||b - A p|| / ||b|| over rows != 0 (FP64). */
 MGM_API int mgm_last_solve(mgm_ctx *ctx, int *iters, double *rel_res);

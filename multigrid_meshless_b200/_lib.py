@@ -88,6 +88,7 @@ SIGNATURES = {
     "mgm_use_compact": ([vp, C.c_int], C.c_int),
     "mgm_use_tiled": ([vp, C.c_int], C.c_int),
     "mgm_use_half_operator": ([vp, C.c_int], C.c_int),
+    "mgm_set_compatible_rhs": ([vp, C.c_int], C.c_int),
     "mgm_set_timple": ([vp, C.c_int, C.c_int, C.c_double, C.c_double], C.c_int),
     "mgm_timple_step": ([vp, C.c_int, C.POINTER(C.c_double)], C.c_int),
     "mgm_timple_part": ([vp, C.c_int, C.c_int], C.c_int),

@@ -313,6 +313,11 @@ class Multigrid:
     def use_tiled(self, enable=True):
         check(self.L.mgm_use_tiled(self.h, 1 if enable else 0))
 
+    def set_compatible_rhs(self, enable=True):
+        """Project every Poisson source onto the consistent subspace of the
+        singular lap_Poison before the pinned solve; no reference counterpart."""
+        check(self.L.mgm_set_compatible_rhs(self.h, 1 if enable else 0))
+
     def use_half_operator(self, enable=True):
         """FP32_IR V-cycle on the FP16 operator D^-1 A (large levels); no reference counterpart."""
         check(self.L.mgm_use_half_operator(self.h, 1 if enable else 0))

@@ -99,6 +99,11 @@ struct mgm_ctx {
     int warm_smooth_steps = 3;        // Chebyshev steps that clean the learned direction
     bool use_tma = false;             // tile-streamed level kernels where a level has them (else 4 rows per thread)
     bool half_operator = false;       // FP32 V-cycle reads the FP16 operator where built
+    // compatible right-hand sides (mgm_set_compatible_rhs): the pinned solution
+    // for the interior indicator and {rho0(w), rho0(b)} on the device
+    bool compat = false, compat_ready = false;
+    DBuf<double> compat_pw, compat_s;
+    bool warm_suspended = false;      // no learned warm start in the solve for p_w
     DBuf<int> tma_err;                // set by a tile-streamed kernel whose bounded wait ran out
     double *h_pinned = nullptr;
     SmootherProfile prof;

@@ -98,6 +98,41 @@ __global__ void k_bc(int n, int kind, const double *x, const double *y, double *
 
 __global__ void k_zero_pinned(double *b) { b[0] = 0.0; }
 
+// Compatible right-hand sides.  lap_Poison (interior Laplacian rows, Neumann
+// boundary rows) is singular with a left null vector z; the pinned solve
+// (row 0 replaced by p[0] = 0) puts the part of b along z into row 0, where
+// it shows as the residual of the unpinned row-0 equation,
+// rho0(x) = x[0] - (lap_Poison p)[0] = z.x / z[0].  Projecting b to
+// b - alpha w (w: 1 on interior rows) with alpha = z.b / z.w = rho0(b) / rho0(w)
+// makes the system consistent; by linearity its pinned solution is
+// p_b - alpha p_w, p_w the pinned solution for w.
+
+// w: 1 on interior rows, 0 on boundary rows
+__global__ void k_interior_indicator(int n, const uint8_t *__restrict__ btag, double *__restrict__ w)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) w[i] = btag[i] ? 0.0 : 1.0;
+}
+
+// *out = x[0] - sum_j lapP[j][0] p[idx[j][0]] (ELL [k][n]), one warp
+__global__ void k_row0_residual(int n, int k, const int *__restrict__ idx, const double *__restrict__ lapP,
+                                const double *__restrict__ x, const double *__restrict__ p, double *__restrict__ out)
+{
+    const int lane = threadIdx.x;
+    double v = 0.0;
+    for (int j = lane; j < k; j += 32) v += lapP[(long)j * n] * p[idx[(long)j * n]];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) *out = x[0] - v;
+}
+
+// p -= (rho0(b) / rho0(w)) p_w with s = {rho0(w), rho0(b)}
+__global__ void k_compat_apply(int n, const double *__restrict__ s, const double *__restrict__ pw,
+                               double *__restrict__ p)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] -= (s[1] / s[0]) * pw[i];
+}
+
 // int16 offsets of a gather index from a per-row base node (base = nullptr: the row itself)
 // ELL [k][ld] int16 offsets gidx - base (base: per-row node, or the row itself);
 // padding rows (n <= i < ld) get offset 0
@@ -570,6 +605,49 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
                                           std::to_string(relres) + " after " + std::to_string(total_it) + " V-cycles)"};
 }
 
+// p_w and rho0(w) of the compatible right-hand sides, after every set-up
+void ensure_compat(mgm_ctx *c)
+{
+    if (c->compat_ready) return;
+    Level &L0 = c->L[0];
+    const int n = L0.n;
+    cudaStream_t s = c->s;
+    c->compat_pw.alloc(n);
+    c->compat_s.alloc(2);
+    DBuf<double> w(n);
+    k_interior_indicator<<<blocks_for(n, 256), 256, 0, s>>>(n, L0.btag.p, w.p);
+    MGM_LAUNCHED();
+    copy_out<double>(n, w.p, c->bvec.p, s);
+    k_zero_pinned<<<1, 1, 0, s>>>(c->bvec.p);
+    MGM_LAUNCHED();
+    c->compat_pw.zero(s);
+    // p_w carries the pin's singular response to an incompatible source, so
+    // its FP64 residual floors near the solver tolerance on fine levels; it
+    // enters every solution scaled by alpha (the source's incompatible
+    // fraction, ~1e-4 of |b|), so a relative residual of 1e-6 adds ~1e-10 |b|
+    const double tol = c->tol;
+    c->tol = std::max(tol, 1e-6);
+    c->warm_suspended = true;
+    try {
+        fgmres<double>(c, c->bvec.p, c->compat_pw.p);
+    } catch (...) {
+        c->tol = tol;
+        c->warm_suspended = false;
+        throw;
+    }
+    c->tol = tol;
+    c->warm_suspended = false;
+    k_row0_residual<<<1, 32, 0, s>>>(n, L0.k, L0.idx.p, L0.lapP.p, w.p, c->compat_pw.p, c->compat_s.p);
+    MGM_LAUNCHED();
+    double rw = 0.0;
+    c->compat_s.download(&rw, 1, s);
+    MGM_CUDA(cudaStreamSynchronize(s));
+    MGM_REQUIRE(std::isfinite(rw) && rw != 0.0,
+                "compatible right-hand sides: the row-0 residual of the interior indicator is zero or not finite");
+    c->last_iters = 0;
+    c->compat_ready = true;
+}
+
 void poisson(mgm_ctx *c, int mode, bool timple = false)
 {
     Level &L0 = c->L[0];
@@ -580,13 +658,20 @@ void poisson(mgm_ctx *c, int mode, bool timple = false)
         ref_multigrid(R, w1, w2, c->num_relax, c->num_vcycles, c->s, timple ? REF_TIMPLE : REF_FS);
         return;
     }
+    if (mode != MGM_MODE_FP64 && mode != MGM_MODE_FP32_IR) throw Error{MGM_ERR_ARG, "unknown Poisson mode"};
+    if (c->compat) ensure_compat(c);
     // b = source with the pinned row's rhs 0 (boundary rows keep their (zero) source)
     copy_out<double>(L0.n, L0.src.p, c->bvec.p, c->s);
     k_zero_pinned<<<1, 1, 0, c->s>>>(c->bvec.p);
     MGM_LAUNCHED();
     if (mode == MGM_MODE_FP64) fgmres<double>(c, c->bvec.p, L0.p.p);
-    else if (mode == MGM_MODE_FP32_IR) fgmres<float>(c, c->bvec.p, L0.p.p);
-    else throw Error{MGM_ERR_ARG, "unknown Poisson mode"};
+    else fgmres<float>(c, c->bvec.p, L0.p.p);
+    if (c->compat) {
+        k_row0_residual<<<1, 32, 0, c->s>>>(L0.n, L0.k, L0.idx.p, L0.lapP.p, L0.src.p, L0.p.p, c->compat_s.p + 1);
+        MGM_LAUNCHED();
+        k_compat_apply<<<blocks_for(L0.n, 256), 256, 0, c->s>>>(L0.n, c->compat_s.p, c->compat_pw.p, L0.p.p);
+        MGM_LAUNCHED();
+    }
 }
 
 void ensure_events(mgm_ctx *c)
@@ -989,6 +1074,7 @@ void prepare_solver(mgm_ctx *c)
 {
     cudaStream_t s = c->s;
     drop_graphs(c);
+    c->compat_ready = false;
     for (int l = 0; l < c->nl; l++) {
         Level &L = c->L[l];
         const size_t nk = (size_t)L.n * L.k;
@@ -1452,6 +1538,15 @@ int mgm_use_tiled(mgm_ctx *c, int enable)
         MGM_CUDA(cudaStreamSynchronize(c->s));
         drop_graphs(c);
         c->use_tma = enable != 0;
+    });
+}
+
+int mgm_set_compatible_rhs(mgm_ctx *c, int enable)
+{
+    return guard([&] {
+        check_ctx(c);
+        c->compat = enable != 0;
+        if (c->compat && c->setup_done) ensure_compat(c);
     });
 }
 

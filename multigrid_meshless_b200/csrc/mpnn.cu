@@ -697,7 +697,7 @@ __global__ void k_to_T(int n, const float *y, T *out)
     if (i < n) out[i] = (T)y[i];
 }
 
-bool warm_start_enabled(mgm_ctx *c) { return c->mpnn && c->mpnn->ready && c->mpnn->warm; }
+bool warm_start_enabled(mgm_ctx *c) { return c->mpnn && c->mpnn->ready && c->mpnn->warm && !c->warm_suspended; }
 
 template <class T>
 void warm_direction(mgm_ctx *c, const double *b, const double *p, T *out, cudaStream_t s)

@@ -467,6 +467,25 @@ def pinned_poisson_direct(lapP, cloud, b):
     return spla.spsolve(A.tocsc(), bb)
 
 
+def compatible_pinned_direct(lapP, cloud, btag, b):
+    """FP64 direct solve of lap_Poison p = b - alpha w, pinned p[0] = 0, where
+    w is 1 on interior rows and alpha = z.b / z.w with z the left null vector
+    of the singular lap_Poison (z = A_pinned^-T (e_0 - row 0 of lap_Poison)):
+    the answer of the solve modes with compatible right-hand sides."""
+    import scipy.sparse.linalg as spla
+    n = lapP.shape[0]
+    lu = spla.splu(pinned_operator(lapP, cloud).tocsc())
+    row0 = np.zeros(n)
+    np.add.at(row0, np.asarray(cloud[0], np.int64), lapP[0])
+    e0 = np.zeros(n)
+    e0[0] = 1.0
+    z = lu.solve(e0 - row0, trans="T")
+    w = (np.asarray(btag) == 0).astype(np.float64)
+    bb = np.array(b, dtype=np.float64) - (z @ b) / (z @ w) * w
+    bb[0] = 0.0
+    return lu.solve(bb)
+
+
 def rel_residual(lapP, cloud, b, p):
     A = pinned_operator(lapP, cloud)
     bb = np.array(b, dtype=np.float64)

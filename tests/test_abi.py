@@ -78,7 +78,8 @@ def test_spmv_rejects_bad_index():
         api.spmv(np.ones((3, 2)), np.array([[0, 1], [1, 2], [2, 3]], np.int32), np.ones(3))
 
 
-@pytest.mark.parametrize("name", ["mgm_use_half_operator", "mgm_use_tiled", "mgm_use_graphs", "mgm_use_compact"])
+@pytest.mark.parametrize("name", ["mgm_use_half_operator", "mgm_set_compatible_rhs", "mgm_use_tiled", "mgm_use_graphs",
+                                  "mgm_use_compact"])
 def test_solver_switches_reject_null_context(name):
     """The V-cycle switches check their context on the host: a null context
     is MGM_ERR_ARG with a message, before any CUDA call."""
