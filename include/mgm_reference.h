@@ -220,6 +220,11 @@ MGM_API void update_boundary_pressure(PointStructure *myPointStruct, FieldVariab
  * reference's fixed V-cycles; MGM_MODE_FP64 / MGM_MODE_FP32_IR: the
  * convergent solve to parameters.poisson_solver_tolerance). */
 MGM_API void mgm_reference_set_poisson_mode(int mode);
+/* No counterpart in the reference: mgm_set_compatible_rhs for the convergent
+ * modes of mgm_reference_set_poisson_mode (the Poisson source projected along
+ * lap_Poison's left null vector before the pinned solve); taken over by
+ * copyin_essentials_to_gpu, and applied at once to a context already there. */
+MGM_API void mgm_reference_set_compatible_rhs(int enable);
 
 #ifdef __cplusplus
 }

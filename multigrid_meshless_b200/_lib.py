@@ -101,6 +101,7 @@ SIGNATURES = {
     "mgm_solve_poisson": ([vp, C.c_int, dp, dp, C.POINTER(C.c_int), C.POINTER(C.c_double)], C.c_int),
     "mgm_sync": ([vp], C.c_int),
     "mgm_reference_set_poisson_mode": ([C.c_int], None),
+    "mgm_reference_set_compatible_rhs": ([C.c_int], None),
     "mgm_mpnn_init": ([vp, C.c_ulonglong, C.c_int], C.c_int),
     "mgm_mpnn_num_params": ([], C.c_int),
     "mgm_mpnn_params": ([vp, vp, vp], C.c_int),

@@ -20,6 +20,7 @@ mgm_ctx *g_ctx = nullptr;
 int g_levels = 0;
 PointStructure *g_ps = nullptr;  // the level array handed to copyin_essentials_to_gpu
 int g_mode = MGM_MODE_REFERENCE;
+int g_compat = 0;  // mgm_reference_set_compatible_rhs
 
 void die_if(int status, const char *what)
 {
@@ -76,6 +77,12 @@ void require_no_corners(const PointStructure *p, const char *fn)
 extern "C" {
 
 void mgm_reference_set_poisson_mode(int mode) { g_mode = mode; }
+
+void mgm_reference_set_compatible_rhs(int enable)
+{
+    g_compat = enable != 0;
+    if (g_ctx) die_if(mgm_set_compatible_rhs(g_ctx, g_compat), "mgm_reference_set_compatible_rhs");
+}
 
 // structures.h:114-126
 void AllocateMemoryPointStructure(PointStructure *p, int nodes)
@@ -552,6 +559,7 @@ void copyin_essentials_to_gpu(PointStructure *ps)
     die_if(mgm_set_solver(g_ctx, parameters.poisson_solver_tolerance > 0 ? parameters.poisson_solver_tolerance : 1e-8,
                           100, 4, 10.0),
            "copyin_essentials_to_gpu");
+    if (g_compat) die_if(mgm_set_compatible_rhs(g_ctx, 1), "copyin_essentials_to_gpu");
 }
 
 // openACC_functions.h:67-90: level-0 fields (the coarse levels start at zero, as allocated)

@@ -87,3 +87,11 @@ def test_solver_switches_reject_null_context(name):
     rc = getattr(L, name)(None, 1)
     assert rc == _lib.MGM_ERR_ARG
     assert b"null context" in L.mgm_last_error()
+
+
+def test_reference_compatible_rhs_switch_without_context():
+    """Before copyin_essentials_to_gpu there is no context: the legacy switch
+    only records the setting (no CUDA call, no exit)."""
+    L = _lib.load()
+    L.mgm_reference_set_compatible_rhs(1)
+    L.mgm_reference_set_compatible_rhs(0)
