@@ -215,18 +215,16 @@ def measured_peak():
         return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
 
 
+# DRAM bytes per launch of the level-0 FP32 smoother step (k_level_v4<0>) from
+# one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, one launch) of
+# level 0 of the 1M-node cavity; the summary with its command is committed
+# under profiles/.  Scaled by node count in the bench line's `traffic`.
+NCU_L0_SMOOTHER_DRAM_BYTES = 200_700_000
+NCU_L0_SMOOTHER_NODES = 999_996
+
+
 def ncu_traffic():
-    """DRAM bytes per launch of the level-0 smoother from the committed ncu summary
-    (profiles/k_level_v4_cavity1m.md), to be scaled by node count."""
-    import re
-    path = os.path.join(ROOT, "profiles", "k_level_v4_cavity1m.md")
-    try:
-        txt = open(path).read()
-        b = re.search(r"dram_bytes_per_launch:\s*(\d+)", txt)
-        nn = re.search(r"nodes:\s*(\d+)", txt)
-        return {"dram_bytes_per_launch": float(b.group(1)), "nodes": float(nn.group(1))}
-    except Exception:
-        return None
+    return {"dram_bytes_per_launch": float(NCU_L0_SMOOTHER_DRAM_BYTES), "nodes": float(NCU_L0_SMOOTHER_NODES)}
 
 
 # ---------------------------------------------------------------------------

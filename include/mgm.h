@@ -121,8 +121,11 @@ MGM_API int mgm_avg_dx(int n, int k, int dim, const double *x, const double *y, 
  * array of MGM_NOALLOC_MAX_NODES doubles (16 MiB) that every GPU loading this
  * library keeps until exit.  n above that limit is rejected with MGM_ERR_ARG.
  * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  Calls share the array: calls that
- * overlap on the GPU race. */
+ * first call before any stream capture.  `stream` must belong to the device
+ * that is current at the call (the address looked up is that device's).  The
+ * address is kept for the life of the process, so cudaDeviceReset after the
+ * first call is not supported.  Calls share the array: calls that overlap on
+ * the GPU race. */
 #define MGM_NOALLOC_MAX_NODES 2097152
 MGM_API int mgm_avg_dx_noalloc(int n, int k, int dim, const double *d_x, const double *d_y, const double *d_z,
                                const unsigned char *d_btag, const int *d_cloud, double *d_avg, void *stream);
@@ -373,6 +376,9 @@ MGM_API int mgm_use_half_operator(mgm_ctx *ctx, int enable);
  * every row of lap_Poison: p_b - alpha p_w, with alpha from the residuals of
  * the unpinned row-0 equation and p_w (the pinned solution for w) computed
  * once per set-up, here when the context is set up, else at the next solve.
+ * The residual that mgm_last_solve and mgm_solve_poisson report is that of
+ * the pinned solve for b, before the projection p_b - alpha p_w is applied
+ * (p_w itself is solved to max(rel_tol, 1e-6)).
  * Applies to the fractional step, the TIMPLE p' solve and
  * mgm_solve_poisson.  No counterpart in the reference. */
 MGM_API int mgm_set_compatible_rhs(mgm_ctx *ctx, int enable);

@@ -33,6 +33,9 @@ double *g_scratch_addr[kMaxDevices] = {nullptr};
 
 // The device address of g_spacing_scratch on the current device, looked up
 // once per device (the host-side name of the array is not a device address).
+// The address is kept for the life of the process: a cudaDeviceReset after
+// the first call would leave it stale, which the header states is not
+// supported.  The caller's stream must belong to the current device.
 double *scratch_for_current_device()
 {
     int dev = 0;

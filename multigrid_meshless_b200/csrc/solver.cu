@@ -492,7 +492,12 @@ __global__ void __launch_bounds__(kTileRows) k_level_tiled(int n, int k, const s
         if (!ok_flag) {
             if (tid == 0) {
                 atomicOr(err, 1);
-                // the other stage may still have a copy in flight
+                // Best effort before the CTA exits: give the timed-out stage's
+                // copies one more bounded spell, then wait (bounded) for the
+                // other stage's, so that normally no bulk copy still writes
+                // into this CTA's shared memory after it has returned.  The
+                // host turns the error flag into MGM_ERR_TIMEOUT.
+                mbar_wait_bounded(&bar[st], parity);
                 const int o = st ^ 1;
                 if (pending & (1u << o)) mbar_wait_bounded(&bar[o], (unsigned)(((it + 1) >> 1) & 1));
             }
@@ -580,6 +585,12 @@ __global__ void __launch_bounds__(kTileRows, 2) k_level_tiled_r(int n, int k, co
         if (!ok_flag) {
             if (tid == 0) {
                 atomicOr(err, 1);
+                // Best effort before the CTA exits: give the timed-out stage's
+                // copies one more bounded spell, then wait (bounded) for the
+                // other stage's, so that normally no bulk copy still writes
+                // into this CTA's shared memory after it has returned.  The
+                // host turns the error flag into MGM_ERR_TIMEOUT.
+                mbar_wait_bounded(&bar[st], parity);
                 const int o = st ^ 1;
                 if (pending & (1u << o)) mbar_wait_bounded(&bar[o], (unsigned)(((it + 1) >> 1) & 1));
             }

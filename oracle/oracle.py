@@ -124,7 +124,7 @@ def ref_lib(timple: bool = False, heat: bool = False):
     if key not in _REF:
         path = os.path.join(HERE, "_ref", _ref_name(timple, heat))
         if not os.path.exists(path):
-            raise RuntimeError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
+            raise RuntimeError(f"{path} missing: run `make -C oracle ref REF=<reference tree>` where the reference tree exists")
         L = C.CDLL(path)
         L.ref_begin.argtypes = [C.c_int, C.c_int, C.c_int]
         L.ref_set_flow.argtypes = [C.c_double, C.c_double, C.c_float, C.c_int, C.c_int]

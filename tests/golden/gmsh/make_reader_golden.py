@@ -1,6 +1,6 @@
 """Regenerates reader.npz in this folder from the REFERENCE's own mesh reader.
 
-    make -C oracle            # builds oracle/_ref/libref.so from the reference sources
+    make -C oracle REF=<reference tree>   # builds oracle/_ref/libref.so from the reference sources
     python tests/golden/gmsh/make_reader_golden.py
 
 The synthetic Gmsh meshes of tests/test_gmsh_oracle.py (written by

@@ -1,6 +1,6 @@
 """Regenerates the golden fixtures in this folder from the REFERENCE's own code.
 
-    make -C oracle            # builds oracle/_ref/libref.so from the reference sources
+    make -C oracle REF=<reference tree>   # builds oracle/_ref/libref.so from the reference sources
     python tests/golden/make_golden.py
 
 Each fixture runs the reference's set-up pipeline (find_cloud_index,
