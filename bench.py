@@ -11,8 +11,9 @@ Poisson solve to 1e-8, velocity correction) through the C ABI.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 --impl reference times the reference's own C implementation of the step
-(oracle/_ref/libref.so, compiled from the reference sources) on the host
-cores, on a bounded sample of the same construction, scaled to 1M nodes.
+(oracle/_ref/libref.so, compiled from the reference sources; serial C, one
+core) on the full 1M-node workload, its set-up built untimed by the
+restatement (bit-identical to the reference's set-up) on all host cores.
 Under torchrun each rank runs an independent replica on its own GPU
 ("replicas only": the path has no exchange step); rank 0 prints the line.
 """
@@ -81,68 +82,133 @@ def workload(a):
 
 
 # ---------------------------------------------------------------------------
-# CPU: the reference's own fractional step on a bounded sample
+# CPU: the reference's own fractional step
 # ---------------------------------------------------------------------------
-def reference_sample(a, steps, warmup):
-    """Times fractional_step_explicit of the reference build (or, if it was
-    not built, the oracle restatement) on a cavity of a.sample-m nodes per side
-    with the same stencil/polynomial settings; returns per-step seconds."""
+class _QuietStdout:
+    """The reference prints its parameters and a line per step: send fd 1 to
+    /dev/null while it runs."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.devnull = os.open(os.devnull, os.O_WRONLY)
+        self.saved = os.dup(1)
+        os.dup2(self.devnull, 1)
+        return self
+
+    def __exit__(self, *exc):
+        os.dup2(self.saved, 1)
+        os.close(self.devnull)
+        os.close(self.saved)
+        return False
+
+
+def _ref_steps(R, O, levels, a, steps, warmup, opt):
+    """warmup + timed steps of the reference's fractional_step_explicit on
+    levels already handed to it, in episodes of a.episode steps from rest
+    (initial_conditions + boundary_conditions of init_LDC.c re-applied,
+    untimed), with the reference's own V-cycle settings: 10 V-cycles of 3 SOR
+    sweeps, omega 1.0 (its V-cycle never reaches 1e-8)."""
+    R.ref_set_flow(a.courant, a.Re, 1.0, 10, 3)
+    R.ref_fields_alloc()
+    R.ref_bc(0)
+    R.ref_dt()
+    done = 0
+    secs = 0.0
+    for phase, count in (("warmup", warmup), ("timed", steps)):
+        for _ in range(count):
+            if done % a.episode == 0:
+                R.ref_bc(0)
+            t0 = time.perf_counter()
+            R.ref_step()
+            if phase == "timed":
+                secs += time.perf_counter() - t0
+            done += 1
+    return secs / max(steps, 1)
+
+
+def reference_full(a, steps, warmup):
+    """The reference's own fractional_step_explicit at the full workload (the
+    1M-node cavity of our arm, same seed, k, polynomial degree and levels):
+    the set-up is built untimed by the restatement (oracle/mgm_oracle.c,
+    libm powers, OpenMP over rows), whose clouds, reorder, normals, spacing,
+    operators and transfer weights are pinned bit for bit to the reference's
+    own set-up, and handed to the reference's structures (oracle/ref_shim.c);
+    then K steps of the reference's code (oracle/_ref/libref.so, gcc -O2,
+    serial C: one core) are timed.  Without the reference build, the
+    restatement's own step (in-place sweeps, as the C build runs them) is
+    timed instead (kind "port")."""
+    from multigrid_meshless_b200 import clouds, replicas
+    from oracle import oracle as O
+    cl = clouds.cavity_hierarchy(a.m, a.levels, seed=replicas.replica_seed(1, 0))
+    ks, polys = [a.k] * a.levels, [a.poly] * a.levels
+    t0 = time.perf_counter()
+    levels = O.orc_pipeline(cl, ks, polys, reference_rows=True)
+    setup_s = time.perf_counter() - t0
+    with _QuietStdout():
+        if O.ref_available():
+            kind = "reference"
+            R = O.ref_load_levels(levels)
+            per = _ref_steps(R, O, levels, a, steps, warmup, "O2")
+        else:
+            kind = "port"
+            S = O.OracleSolver(levels, a.Re, a.courant, 1.0, 3, 10, jacobi=False)
+            for _ in range(warmup):
+                S.step()
+            t1 = time.perf_counter()
+            for _ in range(steps):
+                S.step()
+            per = (time.perf_counter() - t1) / max(steps, 1)
+    return {"kind": kind, "sec_per_step": per, "nodes": cl[0].n, "levels": a.levels, "setup_s": setup_s,
+            "setup_threads": os.cpu_count()}
+
+
+def reference_sample(a, steps, warmup, opt="O2"):
+    """The reference's own fractional_step_explicit (its own set-up, then
+    timed steps) on a cavity of a.sample-m nodes per side with the workload's
+    stencil size, polynomial degree and the same construction, 3 levels; the
+    -O0 build is the reference compiled as its README documents."""
     from multigrid_meshless_b200 import clouds
     from oracle import oracle as O
     nl = 3
     cl = clouds.cavity_hierarchy(a.sample_m, nl, seed=1)
-    n = cl[0].n
     ks, polys = [a.k] * nl, [a.poly] * nl
-    devnull = os.open(os.devnull, os.O_WRONLY)
-    saved = os.dup(1)
-    os.dup2(devnull, 1)  # the reference prints its parameters and a line per step
-    try:
-        return _reference_sample(a, steps, warmup, cl, n, nl, ks, polys, O)
-    finally:
-        os.dup2(saved, 1)
-        os.close(devnull)
-        os.close(saved)
-
-
-def _reference_sample(a, steps, warmup, cl, n, nl, ks, polys, O):
     t0 = time.perf_counter()
-    if O.ref_available():
-        kind = "reference"
-        levels = O.ref_pipeline(cl, ks, polys, with_weights=True)
-        R = O.ref_lib()
-        R.ref_set_flow(a.courant, a.Re, 1.0, 10, 3)
-        R.ref_fields_alloc()
-        R.ref_bc(0)
-        R.ref_dt()
-        setup_s = time.perf_counter() - t0
-        step = R.ref_step
-    else:
-        kind = "port"
-        levels = O.orc_pipeline(cl, ks, polys)
-        S = O.OracleSolver(levels, a.Re, a.courant, 1.0, 3, 10, jacobi=False)
-        O.lid_bc(levels[0], S.f)
-        setup_s = time.perf_counter() - t0
-        step = S.step
-    for _ in range(warmup):
-        step()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        step()
-    per = (time.perf_counter() - t0) / max(steps, 1)
-    return {"kind": kind, "sec_per_step": per, "nodes": n, "levels": nl, "setup_s": setup_s}
+    with _QuietStdout():
+        if O.ref_available(opt=opt):
+            kind = "reference"
+            levels = O.ref_pipeline(cl, ks, polys, with_weights=True, opt=opt)
+            R = O.ref_lib(opt=opt)
+            setup_s = time.perf_counter() - t0
+            per = _ref_steps(R, O, levels, a, steps, warmup, opt)
+        else:
+            kind = "port"
+            levels = O.orc_pipeline(cl, ks, polys)
+            setup_s = time.perf_counter() - t0
+            S = O.OracleSolver(levels, a.Re, a.courant, 1.0, 3, 10, jacobi=False)
+            for _ in range(warmup):
+                S.step()
+            t1 = time.perf_counter()
+            for _ in range(steps):
+                S.step()
+            per = (time.perf_counter() - t1) / max(steps, 1)
+    return {"kind": kind, "sec_per_step": per, "nodes": cl[0].n, "levels": nl, "setup_s": setup_s, "opt": opt}
 
 
 def cpu_baseline_entry(a, s, full_nodes):
+    """A bounded sample scaled to the metric's unit: the sample's steps/s
+    times (sample nodes / workload nodes), the step's work being linear in
+    the node count at fixed k and V-cycle count."""
     val = (1.0 / s["sec_per_step"]) * (s["nodes"] / full_nodes)
     return {
         "value": val,
         "unit": "steps/s",
         "cores": 1,
         "kind": s["kind"],
-        "sample": (f"fractional_step_explicit of the reference C code on a {a.sample_m}x{a.sample_m} cavity "
-                   f"({s['nodes']} nodes, {s['levels']} levels, k={a.k}, poly {a.poly}, its fixed 10 V-cycles x 3 "
-                   f"SOR sweeps, omega 1.0 -- it never reaches 1e-8), steps/s scaled by node count to "
-                   f"{full_nodes} nodes; reference set-up of the sample took {s['setup_s']:.1f} s"),
+        "sample": (f"fractional_step_explicit of the reference C code (gcc -{s['opt']}, one core) on a "
+                   f"{a.sample_m}x{a.sample_m} cavity of the same construction ({s['nodes']} nodes, {s['levels']} "
+                   f"levels, k={a.k}, poly {a.poly}) with its own V-cycle (10 V-cycles x 3 SOR sweeps, omega 1.0; "
+                   f"it never reaches 1e-8); {s['sec_per_step'] * 1e3:.1f} ms per sample step, scaled by node count "
+                   f"to {full_nodes} nodes; the reference's own set-up of the sample took {s['setup_s']:.1f} s"),
     }
 
 
@@ -468,7 +534,15 @@ def run_ours(a, rank, world, local_rank):
         }
         if world == 1 and not a.no_cpu_baseline:
             s = reference_sample(a, steps=3, warmup=1)
-            line["cpu_baseline"] = cpu_baseline_entry(a, s, n)
+            cb = cpu_baseline_entry(a, s, n)
+            # the same sample through the reference compiled as its README
+            # documents (-O0), beside the -O2 figure
+            s0 = reference_sample(a, steps=2, warmup=0, opt="O0")
+            cb["variants"] = {"reference_gcc_O2_1core": cb["value"],
+                              "reference_gcc_O0_1core": cpu_baseline_entry(a, s0, n)["value"],
+                              "note": ("the reference's OpenACC builds (nvc -acc multicore / GPU) are unavailable on "
+                                       "this box (no nvc); its C code is serial")}
+            line["cpu_baseline"] = cb
     mg.close()
     if dist is not None:
         dist.barrier()
@@ -648,12 +722,15 @@ def run_batch(a):
 
 
 def run_reference(a, rank):
+    """The reference arm: the reference's own fractional step at the full
+    workload (reference_full), one JSON line on rank 0; other ranks exit."""
     if rank != 0:
         return None
-    full_nodes = a.m * a.m - 4
-    s = reference_sample(a, steps=max(a.steps, 1), warmup=a.warmup)
-    cb = cpu_baseline_entry(a, s, full_nodes)
-    val = cb["value"]
+    s = reference_full(a, steps=max(a.steps, 1), warmup=a.warmup)
+    val = 1.0 / s["sec_per_step"]
+    cfg = workload(a)
+    cfg["reference_solver"] = ("the reference's own multigrid_Poisson_solver: a fixed 10 V-cycles of 3 SOR sweeps "
+                               "(omega 1.0) per step; it has no tolerance test and never reaches 1e-8")
     return {
         "impl": "reference",
         "metric": METRIC,
@@ -668,9 +745,17 @@ def run_reference(a, rank):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded jittered cloud, no mesh files)",
-        "config": workload(a),
-        "cpu_baseline": cb,
+        "config": cfg,
+        "cpu_baseline": {
+            "value": val, "unit": "steps/s", "cores": 1, "kind": s["kind"],
+            "sample": (f"fractional_step_explicit of the reference C code (gcc -O2, serial: one core) on the full "
+                       f"workload ({s['nodes']} nodes, {s['levels']} levels), {a.steps} timed steps after "
+                       f"{a.warmup} warm-up steps, in episodes of {a.episode} from rest; the set-up was built untimed "
+                       f"by the restatement (bit-identical to the reference's own set-up) in {s['setup_s']:.1f} s "
+                       f"on {s['setup_threads']} threads and handed to the reference's structures"),
+        },
         "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "setup_s": s["setup_s"],
     }
 
 

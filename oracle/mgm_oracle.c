@@ -175,20 +175,26 @@ ORC_EXPORT void orc_knn_cloud(int n, int nb, const double *x, const double *y, c
     for (int i = 0; i < n; i++) interior[i] = btag[i] ? 0 : 1;
     grid_build(&gall, n, x, y, z, NULL, dim);
     grid_build(&gint, n, x, y, z, interior, dim);
-    double *bd = (double *)malloc(sizeof(double) * (size_t)k);
-    int *bi = (int *)malloc(sizeof(int) * (size_t)k);
-    for (int i = 0; i < n; i++) {
-        int *row = cloud + (size_t)i * k;
-        if (i >= nb) {
-            grid_topk(&gall, x, y, z, x[i], y[i], z[i], k, bd, bi);
-            for (int j = 0; j < k; j++) row[j] = bi[j];
-        } else {
-            grid_topk(&gint, x, y, z, x[i], y[i], z[i], k, bd, bi);
-            row[0] = i;
-            for (int j = 1; j < k; j++) row[j] = bi[j - 1];
+    /* rows are independent: OpenMP threads share the grids, each its own scratch */
+#pragma omp parallel
+    {
+        double *bd = (double *)malloc(sizeof(double) * (size_t)k);
+        int *bi = (int *)malloc(sizeof(int) * (size_t)k);
+#pragma omp for schedule(dynamic, 1024)
+        for (int i = 0; i < n; i++) {
+            int *row = cloud + (size_t)i * k;
+            if (i >= nb) {
+                grid_topk(&gall, x, y, z, x[i], y[i], z[i], k, bd, bi);
+                for (int j = 0; j < k; j++) row[j] = bi[j];
+            } else {
+                grid_topk(&gint, x, y, z, x[i], y[i], z[i], k, bd, bi);
+                row[0] = i;
+                for (int j = 1; j < k; j++) row[j] = bi[j - 1];
+            }
         }
+        free(bd); free(bi);
     }
-    free(bd); free(bi); free(interior);
+    free(interior);
     grid_free(&gall); grid_free(&gint);
 }
 
@@ -215,8 +221,9 @@ ORC_EXPORT void orc_nearest(int n1, const double *x1, const double *y1, const do
 {
     grid_t g;
     grid_build(&g, n2, x2, y2, z2, NULL, dim);
-    double bd[1]; int bi[1];
+#pragma omp parallel for schedule(dynamic, 1024)
     for (int i = 0; i < n1; i++) {
+        double bd[1]; int bi[1];
         grid_topk(&g, x2, y2, z2, x1[i], y1[i], z1[i], 1, bd, bi);
         out[i] = bi[0];
     }
@@ -473,12 +480,16 @@ ORC_EXPORT void orc_derivative_weights(int n, int k, int dim, int phs, int poly_
     short px[64], py[64], pz[64];
     int np = orc_monomials(dim, poly_degree, px, py, pz);
     int N = k + np;
+    int nops = dim == 3 ? 4 : 3;
+    /* rows are independent: each OpenMP thread solves its rows with its own scratch */
+#pragma omp parallel
+    {
     double *A = (double *)malloc(sizeof(double) * (size_t)N * N);
     double *Ai = (double *)malloc(sizeof(double) * (size_t)N * N);
     double *aug = (double *)malloc(sizeof(double) * (size_t)N * 2 * N);
     double **rows = (double **)malloc(sizeof(double *) * (size_t)N);
     double *L = (double *)malloc(sizeof(double) * (size_t)N);
-    int nops = dim == 3 ? 4 : 3;
+#pragma omp for schedule(dynamic, 64)
     for (int i = 0; i < n; i++) {
         const int *cl = cloud + (size_t)i * k;
         build_A(k, np, dim, phs, cl, x, y, z, px, py, pz, A);
@@ -503,6 +514,7 @@ ORC_EXPORT void orc_derivative_weights(int n, int k, int dim, int phs, int poly_
         }
     }
     free(A); free(Ai); free(aug); free(rows); free(L);
+    }
 }
 
 /* create_restriction_matrix / create_prolongation_matrix (mesh_functions.h:533-670):
@@ -520,12 +532,16 @@ ORC_EXPORT void orc_transfer_weights(int nt, const double *tx, const double *ty,
     short px[64], py[64], pz[64];
     int np = orc_monomials(dim, poly_degree_src, px, py, pz);
     int m = ks, N = ks + np;
+    memset(W, 0, sizeof(double) * (size_t)nt * ks);
+    /* rows are independent: each OpenMP thread solves its rows with its own scratch */
+#pragma omp parallel
+    {
     double *A = (double *)malloc(sizeof(double) * (size_t)N * N);
     double *Ai = (double *)malloc(sizeof(double) * (size_t)N * N);
     double *aug = (double *)malloc(sizeof(double) * (size_t)N * 2 * N);
     double **rows = (double **)malloc(sizeof(double *) * (size_t)N);
     double *tmp = (double *)malloc(sizeof(double) * (size_t)N);
-    memset(W, 0, sizeof(double) * (size_t)nt * ks);
+#pragma omp for schedule(dynamic, 64)
     for (int i = 0; i < nt; i++) {
         if (only_interior ? (tbtag[i] != 0) : (i < rows_from)) continue;
         int ip = src_pt[i];
@@ -547,6 +563,7 @@ ORC_EXPORT void orc_transfer_weights(int nt, const double *tx, const double *ty,
         }
     }
     free(A); free(Ai); free(aug); free(rows); free(tmp);
+    }
 }
 
 /* ------------------------------------------------------------------------ */

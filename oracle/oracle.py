@@ -108,21 +108,27 @@ def lib(crpow: bool = False):
     return _ORC[key]
 
 
-def _ref_name(timple, heat):
+def _ref_name(timple, heat, opt="O2"):
+    if opt == "O0":
+        return "libref_O0.so"
     return "libref_heat.so" if heat else ("libref_timple.so" if timple else "libref.so")
 
 
-def ref_available(timple: bool = False, heat: bool = False) -> bool:
-    return os.path.exists(os.path.join(HERE, "_ref", _ref_name(timple, heat)))
+def ref_available(timple: bool = False, heat: bool = False, opt: str = "O2") -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", _ref_name(timple, heat, opt)))
 
 
-def ref_lib(timple: bool = False, heat: bool = False):
+def ref_lib(timple: bool = False, heat: bool = False, opt: str = "O2"):
     """_ref/libref.so (fractional-step build), _ref/libref_timple.so (the
     reference's TIMPLE solver) or _ref/libref_heat.so (the heat-conduction
-    program's routines); each is its own library with its own globals."""
+    program's routines); each is its own library with its own globals.
+    opt="O0": _ref/libref_O0.so, the fractional-step build compiled without
+    optimisation, as the reference's README compiles it."""
     key = "heat" if heat else ("timple" if timple else "fs")
+    if opt == "O0":
+        key = "fs_O0"
     if key not in _REF:
-        path = os.path.join(HERE, "_ref", _ref_name(timple, heat))
+        path = os.path.join(HERE, "_ref", _ref_name(timple, heat, opt))
         if not os.path.exists(path):
             raise RuntimeError(f"{path} missing: run `make -C oracle ref REF=<reference tree>` where the reference tree exists")
         L = C.CDLL(path)
@@ -139,6 +145,8 @@ def ref_lib(timple: bool = False, heat: bool = False):
         L.ref_get_geometry.argtypes = [C.c_int, dp, dp, dp, dp, dp, dp, u8p, ip]
         L.ref_get_ops.argtypes = [C.c_int, dp, dp, dp, dp, dp]
         L.ref_get_transfer.argtypes = [C.c_int, ip, ip, C.c_void_p, C.c_void_p]
+        L.ref_load_ops.argtypes = [C.c_int, ip, dp, dp, C.c_void_p, dp, dp]
+        L.ref_load_transfer.argtypes = [C.c_int, ip, ip, C.c_void_p, C.c_void_p]
         if not heat:
             L.ref_bc.argtypes = [C.c_int]
         L.ref_dt.restype = C.c_double
@@ -200,11 +208,11 @@ def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
-def ref_pipeline(clouds, ks, polys, phs=3, with_weights=True, search_scale=0.3, timple=False, heat=False):
+def ref_pipeline(clouds, ks, polys, phs=3, with_weights=True, search_scale=0.3, timple=False, heat=False, opt="O2"):
     """Runs read_complete_mesh_data's steps (minus the file reader) and
     create_derivative_matrices through the reference's own code (in the
     TIMPLE or heat-conduction build when asked)."""
-    R = ref_lib(timple, heat)
+    R = ref_lib(timple, heat, opt)
     nl = len(clouds)
     dim = clouds[0].dim
     R.ref_begin(dim, phs, nl)
@@ -246,6 +254,31 @@ def ref_pipeline(clouds, ks, polys, phs=3, with_weights=True, search_scale=0.3, 
             L.restr = restr.reshape(n, out[l - 1].k) if restr is not None else None
             L.prol = prol.reshape(n, out[l + 1].k) if prol is not None else None
     return out
+
+
+def ref_load_levels(levels, phs=3, timple=False):
+    """Hands levels set up elsewhere (geometry after the reorder, clouds,
+    operators, transfer points and weights -- e.g. orc_pipeline's, which are
+    pinned bit for bit to the reference's own set-up) to the reference's
+    structures, so that its own step routines run on them without repeating
+    the set-up.  Returns the reference library handle."""
+    R = ref_lib(timple)
+    nl = len(levels)
+    dim = levels[0].dim
+    R.ref_begin(dim, phs, nl)
+    for l, L in enumerate(levels):
+        R.ref_set_level(l, L.n, L.nb, _f64(L.x), _f64(L.y), _f64(L.z), _f64(L.nx), _f64(L.ny), _f64(L.nz),
+                        np.ascontiguousarray(L.btag, np.uint8), L.poly, L.k, L.d_avg)
+    for l, L in enumerate(levels):
+        dz = _f64(L.Dz.ravel()) if L.Dz is not None else None
+        R.ref_load_ops(l, np.ascontiguousarray(L.cloud.ravel(), np.int32), _f64(L.Dx.ravel()), _f64(L.Dy.ravel()),
+                       dz.ctypes.data if dz is not None else None, _f64(L.lap.ravel()), _f64(L.lapP.ravel()))
+        restr = _f64(L.restr.ravel()) if l > 0 else None
+        prol = _f64(L.prol.ravel()) if l < nl - 1 else None
+        R.ref_load_transfer(l, np.ascontiguousarray(L.rpts, np.int32), np.ascontiguousarray(L.ppts, np.int32),
+                            restr.ctypes.data if restr is not None else None,
+                            prol.ctypes.data if prol is not None else None)
+    return R
 
 
 def orc_level_setup(c, k, crpow=False):

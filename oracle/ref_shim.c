@@ -160,6 +160,66 @@ void ref_get_transfer(int lev, int *rpts, int *ppts, double *restr, double *prol
     }
 }
 
+/* Hands a level's clouds and derivative operators (row-major [n][k], built
+ * elsewhere -- e.g. by the restatement, whose set-up is pinned bit for bit to
+ * find_cloud_index + create_derivative_matrices) to the reference's
+ * structures, allocated row by row as kdtree_functions.h:115-118 and
+ * rbf.h:401-421 allocate them.  Dz is read only when dim == 3. */
+void ref_load_ops(int lev, const int *cloud, const double *Dx, const double *Dy, const double *Dz, const double *lap,
+                  const double *lapP)
+{
+    PointStructure *p = &g_ps[lev];
+    const int n = p->num_nodes, k = p->num_cloud_points;
+    const int d3 = parameters.dimension == 3;
+    p->cloud_index = (int **)malloc(sizeof(int *) * (size_t)n);
+    for (int i = 0; i < n; i++) {
+        p->cloud_index[i] = (int *)malloc(sizeof(int) * (size_t)k);
+        memcpy(p->cloud_index[i], cloud + (size_t)i * k, sizeof(int) * (size_t)k);
+    }
+    /* one matrix after the other, rows consecutively, in create_derivative_matrices' order */
+    double ***ops[5] = {&p->Dx, &p->Dy, &p->lap, &p->Dz, &p->lap_Poison};
+    const double *src[5] = {Dx, Dy, lap, Dz, lapP};
+    for (int o = 0; o < 5; o++) {
+        if (o == 3 && !d3) { p->Dz = NULL; continue; }
+        double **m = (double **)malloc(sizeof(double *) * (size_t)n);
+        for (int i = 0; i < n; i++) {
+            m[i] = (double *)malloc(sizeof(double) * (size_t)k);
+            memcpy(m[i], src[o] + (size_t)i * k, sizeof(double) * (size_t)k);
+        }
+        *ops[o] = m;
+    }
+}
+
+/* The transfer data of a level, as create_prolongation_and_restriction_matrices
+ * (mesh_functions.h:874-893) leaves it: restriction / prolongation points [n],
+ * restr_mat [n][k of the finer level] (levels > 0), prol_mat [n][k of the
+ * coarser level] (all but the coarsest), allocated row by row. */
+void ref_load_transfer(int lev, const int *rpts, const int *ppts, const double *restr, const double *prol)
+{
+    PointStructure *p = &g_ps[lev];
+    const int n = p->num_nodes;
+    p->restriction_points = (int *)malloc(sizeof(int) * (size_t)n);
+    p->prolongation_points = (int *)malloc(sizeof(int) * (size_t)n);
+    memcpy(p->restriction_points, rpts, sizeof(int) * (size_t)n);
+    memcpy(p->prolongation_points, ppts, sizeof(int) * (size_t)n);
+    if (lev > 0 && restr) {
+        const int kf = g_ps[lev - 1].num_cloud_points;
+        p->restr_mat = (double **)malloc(sizeof(double *) * (size_t)n);
+        for (int i = 0; i < n; i++) {
+            p->restr_mat[i] = (double *)malloc(sizeof(double) * (size_t)kf);
+            memcpy(p->restr_mat[i], restr + (size_t)i * kf, sizeof(double) * (size_t)kf);
+        }
+    }
+    if (lev < g_levels - 1 && prol) {
+        const int kc = g_ps[lev + 1].num_cloud_points;
+        p->prol_mat = (double **)malloc(sizeof(double *) * (size_t)n);
+        for (int i = 0; i < n; i++) {
+            p->prol_mat[i] = (double *)malloc(sizeof(double) * (size_t)kc);
+            memcpy(p->prol_mat[i], prol + (size_t)i * kc, sizeof(double) * (size_t)kc);
+        }
+    }
+}
+
 /* ---- fields and the fractional step ---------------------------------- */
 void ref_fields_alloc(void) { AllocateMemoryFieldVariables(&g_field, g_ps, g_levels); }
 

@@ -125,3 +125,36 @@ def test_gauss_jordan_restatement_matches_reference():
         O.ref_lib().ref_gauss_jordan(n, A, want)
         O.lib().orc_gauss_jordan(n, A, got)
         assert np.array_equal(got, want), n
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build not present")
+def test_reference_steps_on_restated_setup_are_its_own():
+    """The bench's reference arm builds the set-up with the restatement
+    (OpenMP over rows) and hands it to the reference's structures
+    (ref_load_levels).  Three fractional_step_explicit calls on that hand-over
+    give the bits of the same calls after the reference's own set-up."""
+    cl = clouds.cavity_hierarchy(40, 3, seed=2)
+    ks, polys = [20] * 3, [3] * 3
+    out = []
+    for handed_over in (False, True):
+        if handed_over:
+            R = O.ref_load_levels(O.orc_pipeline(cl, ks, polys))
+        else:
+            O.ref_pipeline(cl, ks, polys)
+            R = O.ref_lib()
+        R.ref_set_flow(0.5, 100.0, 1.0, 4, 2)
+        R.ref_fields_alloc()
+        R.ref_bc(0)
+        R.ref_dt()
+        for _ in range(3):
+            R.ref_step()
+        n = cl[0].n
+        fields = {}
+        for nm in ("u", "v", "p", "source"):
+            a = np.zeros(n)
+            R.ref_field_get(0, O.FIELD[nm], a)
+            fields[nm] = a
+        out.append(fields)
+    for nm in out[0]:
+        assert np.array_equal(out[0][nm], out[1][nm]), nm
+    assert np.abs(out[0]["u"]).max() == 1.0
