@@ -294,6 +294,59 @@ def ncu_traffic():
 
 
 # ---------------------------------------------------------------------------
+# step-level roofline: algorithmic bytes of every kernel of a fractional step
+# ---------------------------------------------------------------------------
+def step_bytes(sizes, dim, deg, fp32, vcycles, cycles, solves, steps):
+    """Compulsory HBM bytes of `steps` fractional steps whose Poisson solves
+    took `vcycles` Arnoldi steps (V-cycles) over `cycles` restart-cycle starts
+    and `solves` solves: every array a kernel reads or writes counted once per
+    launch, gathered vectors once per element.  sizes: [(n, nb, k)] per level.
+    Per V-cycle and level l above the coarsest: a start kernel (r, dinv, btag
+    in; e out), deg Chebyshev steps and deg boundary-row solves before the
+    coarse correction, the residual, the restriction into l+1, the
+    prolongation from l+1, one boundary-row solve and deg Chebyshev steps with
+    their boundary-row solves after it; at the coarsest level the dense
+    inverse.  The FGMRES in FP64: per Arnoldi step j the V-cycle's input and
+    output copies, w = A z_j, the Gram-Schmidt passes over V_0..V_{j+1}
+    (re-orthogonalisation passes not counted), the normalisation; per restart
+    start the true residual and V_0's scaling, per cycle the update
+    p += Z y; per step momentum, divergence, correction and the solve's
+    right-hand-side copy."""
+    s = 4 if fp32 else 8            # V-cycle vector bytes
+    slot = 6 if fp32 else 12        # weight + index per stencil slot (FP32 + int16 / FP64 + int32)
+    n0, _, k0 = sizes[0]
+    vc = 0.0
+    L = len(sizes)
+    for l in range(L - 1):
+        n, nb, k = sizes[l]
+        nc, _, kc = sizes[l + 1]
+        cheb = n * (k * slot + 5 * s + 1 + (s * (deg - 1) / deg))   # e, r, dinv in; e', d out; d in; btag
+        resid = n * (k * slot + 3 * s + 1)
+        bnd = nb * (k * (s + 4) + 3 * s)
+        start = n * (3 * s + 1)
+        restrict = nc * (k * slot + 4 + s) + n * s                  # rows of l+1 gather l's residual
+        prolong = n * (kc * slot + 4 + 2 * s) + nc * s
+        vc += start + 2 * deg * cheb + (2 * deg + 1) * bnd + resid + restrict + prolong
+    nc = sizes[-1][0]
+    vc += nc * nc * s + 2 * nc * s
+    per_vcycles = vcycles * vc
+    # FGMRES (FP64 vectors, pinned FP64 operator with int32 indices)
+    j_per_cycle = vcycles / max(cycles - solves, 1)  # Arnoldi steps per working cycle (each solve ends on a check)
+    krylov = 0.0
+    J = int(round(j_per_cycle))
+    per_cycle_arnoldi = 0.0
+    for j in range(max(J, 1)):
+        per_cycle_arnoldi += (8 + s) * n0 + 2 * s * n0 + n0 * (12 * k0 + 8 + s) \
+            + (j + 2) * 8 * n0 + (j + 3) * 8 * n0 + 16 * n0
+    krylov += per_cycle_arnoldi * (vcycles / max(J, 1))
+    krylov += cycles * (n0 * (12 * k0 + 24) + 16 * n0)            # true residual, V_0 scaling
+    krylov += (cycles - solves) * (J * s * n0 + 16 * n0)          # p += Z y
+    ops = 3 if dim == 2 else 4
+    step = n0 * (ops * k0 * 8 + 4 * k0 + 8 * 8) + 2 * n0 * (2 * k0 * 8 + 4 * k0 + 5 * 8) + 16 * n0
+    return per_vcycles + krylov + steps * step
+
+
+# ---------------------------------------------------------------------------
 # learned warm start: trained on the GPU on plain-solver episodes, evaluated on
 # held-out episodes with and without it
 # ---------------------------------------------------------------------------
@@ -393,20 +446,39 @@ def run_ours(a, rank, world, local_rank):
 
     fast = mgm.MODE_FP32_IR
 
+    counts = {}
+
     def arm(mode, steps):
         """steps fractional steps in episodes from rest; device time of the steps only"""
         tot = [0.0, 0.0, 0, 0.0]
+        cnt = [0, 0, 0]
         done = 0
         while done < steps:
             m_ = min(a.episode, steps - done)
             mg.apply_bc(mgm.BC_LID)
             ms_, pms_, vc_, err_ = mg.run_steps(mode, m_)
             tot[0] += ms_; tot[1] += pms_; tot[2] += vc_; tot[3] = err_
+            for i, v in enumerate(mg.solve_counters()):
+                cnt[i] += v
             done += m_
+        counts[mode] = cnt
         return tot
 
-    # warm-up (captures the V-cycle graphs), then the plain FP64 arm
-    mg.profile_smoother(True)
+    def smoother_pass(steps):
+        """CUDA events around every level-0 smoother launch, recorded inside
+        the V-cycle graphs of a host-driven pass of the same steps (event
+        nodes cannot sit in the step graph's conditional bodies): total ms,
+        launches, algorithmic bytes per launch"""
+        mg.profile_smoother(True)
+        arm(fast, 1)  # captures the V-cycle graphs with their event nodes
+        mg.sync()
+        s0 = mg.profile_read()
+        arm(fast, steps)
+        s1 = mg.profile_read()
+        mg.profile_smoother(False)
+        return s1[0] - s0[0], s1[1] - s0[1], s1[2]
+
+    # warm-up (captures the step graphs), then the plain FP64 arm
     arm(fast, a.warmup)
     arm(mgm.MODE_FP64, min(a.warmup, 2))
     barrier()
@@ -414,22 +486,31 @@ def run_ours(a, rank, world, local_rank):
     plain_ms, plain_pms, plain_vc, _ = arm(mgm.MODE_FP64, a.steps)
     plain_ms = max_over_ranks(plain_ms)
 
-    # headline: FP32-in-FP64 refinement, device-timed on the library's stream,
-    # with CUDA events around every level-0 smoother launch (inside the graph)
+    # headline: FP32-in-FP64 refinement, each step one graph launch (the
+    # solve's loops as conditional nodes), device-timed on the library's stream
     barrier()
     mg.sync()
-    mg.profile_read()
-    sm0 = mg.profile_read()
     clocks = ClockSampler(local_rank)
     clocks.start()
     l0 = api.kernel_launches()
     ms, pms, vc, err = arm(fast, a.steps)
     launches = api.kernel_launches() - l0
     ck = clocks.stop()
-    sm1 = mg.profile_read()
-    sm_ms, sm_launch, sm_bytes = sm1[0] - sm0[0], sm1[1] - sm0[1], sm1[2]
     barrier()
     ms = max_over_ranks(ms)
+    head_counts = list(counts[fast])
+
+    # the same steps with the solve's loops driven from the host (one read of
+    # the loop flags per Arnoldi step, V-cycle graphs): what the one-graph step saves
+    mg.use_step_graph(False)
+    arm(fast, min(a.warmup, 2))
+    mg.sync()
+    hd_ms, hd_pms, hd_vc, _ = arm(fast, a.steps)
+    mg.use_step_graph(True)
+    hd_ms = max_over_ranks(hd_ms)
+
+    # the dominant kernel's launches, timed by events (roofline)
+    sm_ms, sm_launch, sm_bytes = smoother_pass(a.steps)
 
     # the same steps with the FP16 operator (D^-1 A) in the FP32 V-cycle
     # (mgm_use_half_operator); reported beside the headline, not as it
@@ -439,22 +520,20 @@ def run_ours(a, rank, world, local_rank):
         arm(fast, min(a.warmup, 2))
         barrier()
         mg.sync()
-        h0 = mg.profile_read()
         half_ms, half_pms, half_vc, half_err = arm(fast, a.steps)
-        h1 = mg.profile_read()
         barrier()
         half_ms = max_over_ranks(half_ms)
+        h_ms, h_launch, h_bytes = smoother_pass(min(a.steps, a.episode))
         mg.use_half_operator(False)
-        h_launch = h1[1] - h0[1]
-        h_avg_s = ((h1[0] - h0[0]) / 1e3) / max(h_launch, 1)
+        h_avg_s = (h_ms / 1e3) / max(h_launch, 1)
         half = {"steps_per_s": a.steps * world / (half_ms / 1e3), "ms_per_step": half_ms / a.steps,
                 "poisson_ms": half_pms / a.steps, "vcycles_per_step": half_vc / a.steps,
                 "steady_err_last": half_err,
                 "level0_smoother": {"kernel": "k_level_h4<0> (FP16 D^-1 A + int16 offsets, one 16-byte load "
                                               "per slot per 4 interleaved rows, rows in difference form)",
-                                    "bytes_per_launch": h1[2], "launches": h_launch,
+                                    "bytes_per_launch": h_bytes, "launches": h_launch,
                                     "avg_launch_us": h_avg_s * 1e6,
-                                    "achieved_gbs": h1[2] / h_avg_s / 1e9 if h_launch else None}}
+                                    "achieved_gbs": h_bytes / h_avg_s / 1e9 if h_launch else None}}
 
     # end to end through the public API with page-locked host buffers:
     # per step H2D of u, v and D2H of u, v, p (the reference's `update host(field[0])`)
@@ -492,6 +571,14 @@ def run_ours(a, rank, world, local_rank):
         peak, peak_src = measured_peak()
         avg_launch_s = (sm_ms / 1e3) / max(sm_launch, 1)
         achieved = sm_bytes / avg_launch_s / 1e9 if sm_launch else None
+        sizes = [tuple(mg.sizes[l][:3]) for l in range(mg.nl)]
+        sb = step_bytes(sizes, 2, a.cheb_degree, True, *head_counts, a.steps)
+        step_roof = {"bytes_per_step": sb / a.steps, "achieved": sb / (ms / 1e3) / 1e9, "unit": "GB/s",
+                     "frac": sb / (ms / 1e3) / 1e9 / peak,
+                     "vcycles": head_counts[0], "restart_cycle_starts": head_counts[1], "solves": head_counts[2],
+                     "model": ("compulsory bytes of every kernel of the step (step_bytes in bench.py): V-cycle "
+                               "levels, FP64 FGMRES, momentum/divergence/correction; re-orthogonalisation "
+                               "passes not counted")}
         tr = ncu_traffic()
         traffic = None
         if tr and tr.get("nodes"):
@@ -515,6 +602,11 @@ def run_ours(a, rank, world, local_rank):
             "steady_err_last": err,
             "plain_fp64": {"steps_per_s": a.steps * world / (plain_ms / 1e3), "ms_per_step": plain_ms / a.steps,
                            "poisson_ms": plain_pms / a.steps, "vcycles_per_step": plain_vc / a.steps},
+            "host_driven_fp32": {"ms_per_step": hd_ms / a.steps, "poisson_ms": hd_pms / a.steps,
+                                 "vcycles_per_step": hd_vc / a.steps,
+                                 "note": ("the same steps with the solve's loops driven from the host (one read of "
+                                          "the loop flags per Arnoldi step, each V-cycle a graph replay); the "
+                                          "headline runs each step as one graph launch")},
             "learned_warm_start": learned,
             "half_operator": half,
             "headline_arm": ("FP32 V-cycle inside FP64 FGMRES without the learned warm start (the faster arm: "
@@ -527,7 +619,10 @@ def run_ours(a, rank, world, local_rank):
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "bytes_per_launch": sm_bytes, "launches": sm_launch,
-                         "avg_launch_us": avg_launch_s * 1e6, "peak_source": peak_src},
+                         "avg_launch_us": avg_launch_s * 1e6, "peak_source": peak_src,
+                         "timing": ("CUDA events around every level-0 smoother launch, recorded inside the V-cycle "
+                                    "graphs of a host-driven pass of the same steps after the timed region"),
+                         "step": step_roof},
             "clocks": ck,
             "gpu_launches": launches,
             "setup_s": setup_s,
@@ -605,15 +700,21 @@ def run_other(a):
     arm(mgm.MODE_FP32_IR, a.warmup)
     arm(mgm.MODE_FP64, min(a.warmup, 2))
     pl = arm(mgm.MODE_FP64, a.steps)
-    mg.profile_smoother(True)
-    sm0 = mg.profile_read()
     clocks = ClockSampler(0)
     clocks.start()
     l0 = api.kernel_launches()
     ms, pms, vc, err = arm(mgm.MODE_FP32_IR, a.steps)
     launches = api.kernel_launches() - l0
     ck = clocks.stop()
+    # the level-0 smoother's launches timed by CUDA events in the V-cycle
+    # graphs of a host-driven pass of the same steps (roofline)
+    mg.profile_smoother(True)
+    arm(mgm.MODE_FP32_IR, 1)
+    mg.sync()
+    sm0 = mg.profile_read()
+    arm(mgm.MODE_FP32_IR, a.steps)
     sm1 = mg.profile_read()
+    mg.profile_smoother(False)
     sm_ms, sm_launch, sm_bytes = sm1[0] - sm0[0], sm1[1] - sm0[1], sm1[2]
     peak, peak_src = measured_peak()
     avg = (sm_ms / 1e3) / max(sm_launch, 1)

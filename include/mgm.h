@@ -218,6 +218,23 @@ MGM_API int mgm_get_operators(mgm_ctx *ctx, int lev, double *Dx, double *Dy, dou
 /* restriction_points / prolongation_points and the reference-semantics
  * restr_mat ([n][k of level lev-1]) / prol_mat ([n][k of level lev+1]). */
 MGM_API int mgm_get_transfer(mgm_ctx *ctx, int lev, int *rpts, int *ppts, double *restr, double *prol);
+/* The convergent solver's transfer weights of a level (no counterpart in the
+ * reference): restriction into the level from level lev-1, built with
+ * create_restriction_matrix's interpolation (mesh_functions.h:533-600) for
+ * every non-boundary row ([n][k of level lev-1], boundary rows 0), and
+ * prolongation into the level from level lev+1, built with
+ * create_prolongation_matrix's interpolation (:602-670) for every row
+ * ([n][k of level lev+1]).  Either pointer may be NULL. */
+MGM_API int mgm_get_solver_transfer(mgm_ctx *ctx, int lev, double *restr, double *prol);
+/* The FP32 V-cycle's compact copies of a level as the level kernels read
+ * them, decoded (no counterpart in the reference).  which = 0: the pinned
+ * operator with each row's slots sorted by neighbour index, [n][k]; 1: the
+ * restriction into the level, [n][k of level lev-1]; 2: the prolongation
+ * into the level, [n][k of level lev+1].  idx[i][j] is the gathered node:
+ * rebuilt from the int16 offset (row i, restriction / prolongation point of
+ * row i) where the level holds the offsets (*compact = 1), else the stored
+ * 32-bit index (*compact = 0); w[i][j] the FP32 weight. */
+MGM_API int mgm_get_compact(mgm_ctx *ctx, int lev, int which, int *idx, float *w, int *compact);
 
 /* Flow parameters (read_flow_parameters, mesh_functions.h:37-100: rho = 1,
  * mu = rho/Re, nu = mu/rho).  dt <= 0 computes calculate_dt
@@ -345,9 +362,32 @@ MGM_API int mgm_use_compact(mgm_ctx *ctx, int enable);
 #define MGM_REF_RESTRICT 2
 #define MGM_REF_PROLONGATE 3
 MGM_API int mgm_ref_routine(mgm_ctx *ctx, int level, int routine);
-/* Replay each V-cycle from a captured CUDA graph (default on) or launch its
- * kernels one by one (enable = 0).  Results are identical either way. */
+/* Replay captured CUDA graphs (default on) or launch every kernel one by one
+ * (enable = 0).  With graphs on, mgm_step, mgm_run_steps, mgm_step_host and
+ * the learned-start data collection run each fractional step in the FP64 /
+ * FP32-IR modes as ONE graph launch (mgm_use_step_graph), and the other
+ * solves replay each V-cycle from a captured graph.  Results are identical
+ * either way. */
 MGM_API int mgm_use_graphs(mgm_ctx *ctx, int enable);
+/* With graphs on: the whole fractional step as one captured graph (enable =
+ * 1, default) -- momentum, divergence, the Poisson solve with its restart and
+ * Arnoldi loops as conditional WHILE nodes whose conditions device kernels
+ * set, the velocity correction -- so that a step makes no host round trip;
+ * or (enable = 0) the solve's loops driven from the host, which reads the
+ * loop flags of the device-resident iteration state once per Arnoldi step
+ * and replays each V-cycle from its graph.  The same kernels run in the same
+ * order: results are identical.  The step graph is recaptured when dt, the
+ * learned warm start or compatible right-hand sides change, and dropped by
+ * every solver setting.  Profiling (mgm_profile_smoother) uses the
+ * host-driven form, whose V-cycle graphs carry the timing events.  No
+ * counterpart in the reference (fractional_step_solver.h:47-71 is one host
+ * function). */
+MGM_API int mgm_use_step_graph(mgm_ctx *ctx, int enable);
+/* Counters of the Poisson solves of the last mgm_run_steps / mgm_step call
+ * (read from the device-resident iteration state): Arnoldi steps (V-cycles),
+ * restart-cycle starts (each computes a true residual), solves.  Any pointer
+ * may be NULL.  No counterpart in the reference. */
+MGM_API int mgm_solve_counters(mgm_ctx *ctx, long long *vcycles, long long *cycles, long long *solves);
 /* FP32 compact path: on levels of at least 65,536 rows, stream the operator
  * tile by tile into shared memory with bulk asynchronous copies (enable = 1),
  * or read it with plain vector loads, four rows per thread (enable = 0, the

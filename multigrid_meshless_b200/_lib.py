@@ -77,6 +77,8 @@ SIGNATURES = {
     "mgm_get_geometry": ([vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
     "mgm_get_operators": ([vp, C.c_int, vp, vp, vp, vp, vp], C.c_int),
     "mgm_get_transfer": ([vp, C.c_int, vp, vp, vp, vp], C.c_int),
+    "mgm_get_solver_transfer": ([vp, C.c_int, vp, vp], C.c_int),
+    "mgm_get_compact": ([vp, C.c_int, C.c_int, vp, vp, vp], C.c_int),
     "mgm_set_flow": ([vp, C.c_double, C.c_double, C.c_float, C.c_int, C.c_int, C.c_double], C.c_int),
     "mgm_get_dt": ([vp, C.POINTER(C.c_double)], C.c_int),
     "mgm_set_field": ([vp, C.c_int, C.c_int, dp], C.c_int),
@@ -85,6 +87,8 @@ SIGNATURES = {
     "mgm_step": ([vp, C.c_int, C.POINTER(C.c_double)], C.c_int),
     "mgm_set_solver": ([vp, C.c_double, C.c_int, C.c_int, C.c_double], C.c_int),
     "mgm_use_graphs": ([vp, C.c_int], C.c_int),
+    "mgm_use_step_graph": ([vp, C.c_int], C.c_int),
+    "mgm_solve_counters": ([vp, vp, vp, vp], C.c_int),
     "mgm_use_compact": ([vp, C.c_int], C.c_int),
     "mgm_use_tiled": ([vp, C.c_int], C.c_int),
     "mgm_use_half_operator": ([vp, C.c_int], C.c_int),

@@ -250,6 +250,29 @@ class Multigrid:
         check(self.L.mgm_get_transfer(self.h, l, ptr(rp), ptr(pp), ptr(restr), ptr(prol)))
         return {"rpts": rp, "ppts": pp, "restr": restr, "prol": prol}
 
+    def solver_transfer(self, l):
+        """The convergent solver's restriction into level l (interior rows,
+        [n][k of l-1]) and prolongation into level l (all rows, [n][k of l+1])."""
+        n = self.sizes[l][0]
+        restr = np.zeros((n, self.sizes[l - 1][2])) if l > 0 else None
+        prol = np.zeros((n, self.sizes[l + 1][2])) if l < self.nl - 1 else None
+        check(self.L.mgm_get_solver_transfer(self.h, l, ptr(restr), ptr(prol)))
+        return {"restr": restr, "prol": prol}
+
+    def compact(self, l, which):
+        """The FP32 V-cycle's copy of level l's operator (which="op"), the
+        restriction into it ("restr") or the prolongation into it ("prol"),
+        decoded as the level kernels read it: (idx [n][k], w [n][k] float32,
+        True where the gathers come from int16 offsets)."""
+        code = {"op": 0, "restr": 1, "prol": 2}[which]
+        n = self.sizes[l][0]
+        k = self.sizes[l][2] if code == 0 else self.sizes[l - 1 if code == 1 else l + 1][2]
+        idx = np.zeros((n, k), np.int32)
+        w = np.zeros((n, k), np.float32)
+        flag = C.c_int()
+        check(self.L.mgm_get_compact(self.h, l, code, ptr(idx), ptr(w), C.byref(flag)))
+        return idx, w, bool(flag.value)
+
     def set_flow(self, Re, courant, omega=1.0, num_relax=3, num_vcycles=10, dt=0.0):
         check(self.L.mgm_set_flow(self.h, Re, courant, omega, num_relax, num_vcycles, dt))
         d = C.c_double()
@@ -324,6 +347,15 @@ class Multigrid:
 
     def use_graphs(self, enable=True):
         check(self.L.mgm_use_graphs(self.h, 1 if enable else 0))
+
+    def solve_counters(self):
+        """(V-cycles, restart-cycle starts, solves) of the last run_steps / step."""
+        v, c, n = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        check(self.L.mgm_solve_counters(self.h, C.byref(v), C.byref(c), C.byref(n)))
+        return v.value, c.value, n.value
+
+    def use_step_graph(self, enable=True):
+        check(self.L.mgm_use_step_graph(self.h, 1 if enable else 0))
 
     def apply_bc(self, kind=_lib.BC_LID):
         check(self.L.mgm_apply_bc(self.h, kind))

@@ -117,9 +117,28 @@ struct mgm_ctx {
         long long kernels = 0;      // kernel nodes in the graph
     } vg[2];
     bool use_graphs = true;
+    // The device-resident state of the outer FGMRES (krylov.cuh), a pinned
+    // host copy of its head, and the side streams that capture the bodies of
+    // the solve's conditional WHILE nodes.
+    DBuf<FgState> fg;
+    FgState *h_fg = nullptr;
+    cudaStream_t s_body[2] = {nullptr, nullptr};
+    // A whole fractional step captured as one graph, [0] FP64, [1] FP32-IR:
+    // momentum, divergence, the Poisson solve with its loops as conditional
+    // nodes, the velocity correction and the steady-state error read-back.
+    // Kernel nodes per replay = top + outer * restart cycles + inner * V-cycles.
+    struct StepGraph {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t x = nullptr;
+        bool warm = false, compat = false;
+        double dt = 0;
+        long long k_top = 0, k_outer = 0, k_inner = 0;
+    } sg[2];
+    bool step_graphs = true;  // mgm_step / mgm_run_steps replay the step graph (when not profiling)
     bool compact = true;    // FP32 V-cycle on compact storage
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     double poisson_ms_acc = 0;
     long long vcycles_acc = 0;
+    long long ref_vcycles_acc = 0;    // reference-mode V-cycles of the running batch of steps
 };
 

@@ -236,6 +236,20 @@ __global__ void k_tile_major(int n, int k, int ld, int ldin, const T *__restrict
     out[e] = row < n ? in[(long)j * ldin + row] : T(0);
 }
 
+// decoded compact copy, row-major out: idx[i][j] = base_i + off[j][i] (base_i:
+// the row itself, or base[i]) where off is given, else gidx[j][i]; w[i][j] = W[j][i]
+__global__ void k_decode_compact(int n, int k, int ld, const short *__restrict__ off, const int *__restrict__ base,
+                                 const int *__restrict__ gidx, const float *__restrict__ W, int *__restrict__ idx,
+                                 float *__restrict__ w)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)n * k) return;
+    const int i = (int)(t / k), j = (int)(t % k);
+    const long e = (long)j * ld + i;
+    idx[t] = off ? (base ? base[i] : i) + (int)off[e] : gidx[e];
+    w[t] = W[e];
+}
+
 // compact copies of the boundary rows of the pinned operator: out[w][j] = A[j][list[w]]
 __global__ void k_gather_rows(int nbl, const int *__restrict__ list, int n, int k, const int *__restrict__ idx,
                               const double *__restrict__ A, int *__restrict__ bidx, double *__restrict__ bA64,
@@ -385,8 +399,11 @@ void destroy_mpnn(mgm_ctx *c);
 
 namespace {
 
+void drop_step_graphs(mgm_ctx *c);
+
 void drop_graphs(mgm_ctx *c)
 {
+    drop_step_graphs(c);
     for (auto &g : c->vg) {
         if (g.x) cudaGraphExecDestroy(g.x);
         if (g.g) cudaGraphDestroy(g.g);
@@ -449,144 +466,221 @@ const T *run_vcycle(mgm_ctx *c, std::vector<SolveLevel<T>> &levels, const Coarse
     return (const T *)G.out;
 }
 
-// Flexible GMRES(m) in FP64 right-preconditioned by one V-cycle in precision T.
-// Solves A p = b (pinned level-0 operator); p is the initial guess.
+// ---------------------------------------------------------------------------
+// Flexible GMRES(m) in FP64 right-preconditioned by one V-cycle in precision
+// T.  Solves A p = b (pinned level-0 operator); p is the initial guess.
+//
+// Every scalar of the iteration lives on the device (FgState) and is updated
+// by small kernels, so the same kernel sequence runs in two forms:
+//  * host loops: after each restart cycle's start and each Arnoldi step the
+//    host reads the loop flags (go_outer, go_inner) of the state's head;
+//  * captured: the two loops become WHILE conditional nodes whose conditions
+//    the same kernels set on the device (cudaGraphSetConditional), so the
+//    whole solve (and the whole fractional step around it) is one graph
+//    with no host round trip.
+// Both forms launch the same kernels in the same order and give the same bits.
+// ---------------------------------------------------------------------------
+constexpr int kMaxRestarts = 4;
+
 template <class T>
-void fgmres(mgm_ctx *c, const double *b, double *p)
+struct FgRun {
+    mgm_ctx *c;
+    std::vector<SolveLevel<T>> levels;
+    CoarseSolve<T> cs;
+    T *Z;
+    double *V;
+    long ld;
+    int n, k, nbres;
+    FgState *st;
+    const double *b;
+    double *p;
+};
+
+// the flags of the state's head, read by the host loops
+const FgState &read_fg_head(mgm_ctx *c)
+{
+    MGM_CUDA(cudaMemcpyAsync(c->h_fg, c->fg.p, kFgHead, cudaMemcpyDeviceToHost, c->s));
+    MGM_CUDA(cudaStreamSynchronize(c->s));
+    return *c->h_fg;
+}
+
+// Adds a WHILE conditional node at the current capture position of stream s
+// and returns its body graph.  create: a new handle *h on the graph s
+// captures into, its condition reset to `dflt` at every launch of the graph;
+// else *h is an existing handle of that graph.
+cudaGraph_t add_while_node(cudaStream_t s, bool create, unsigned dflt, cudaGraphConditionalHandle *h)
+{
+    cudaStreamCaptureStatus cst;
+    unsigned long long id = 0;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    MGM_CUDA(cudaStreamGetCaptureInfo(s, &cst, &id, &g, &deps, &ndeps));
+    MGM_REQUIRE(cst == cudaStreamCaptureStatusActive && g, "add_while_node: stream is not capturing");
+    if (create) MGM_CUDA(cudaGraphConditionalHandleCreate(h, g, dflt, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = *h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    MGM_CUDA(cudaGraphAddNode(&node, g, deps, ndeps, &np));
+    MGM_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    return np.conditional.phGraph_out[0];
+}
+
+// captures body(bs) into a conditional node's body graph on side stream bs
+template <class F>
+void capture_body(cudaGraph_t body, cudaStream_t bs, F &&fn)
+{
+    MGM_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    try {
+        fn();
+    } catch (...) {
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(bs, &junk);
+        throw;
+    }
+    cudaGraph_t out = nullptr;
+    MGM_CUDA(cudaStreamEndCapture(bs, &out));
+}
+
+// one Arnoldi step: z_j = M v_j (V-cycle), w = A z_j, classical Gram-Schmidt
+// (projections and |w|^2 in one pass, the update with the norm of the result
+// in a second, a re-orthogonalisation pass only when the first cancelled more
+// than 1 - 1/sqrt(2) of |w|: the Daniel-Gragg-Kaufman-Stewart test), the
+// Givens update and the convergence test
+template <class T>
+void arnoldi_step(FgRun<T> &R, cudaStream_t s, FgHandles hd, bool captured)
+{
+    mgm_ctx *c = R.c;
+    Level &L0 = c->L[0];
+    fg_load<T>(R.n, R.V, R.ld, R.st, R.levels[0].r, s);
+    const T *z;
+    if (captured) {
+        vcycle<T>(R.levels, R.cs, c->cheb_deg, c->cheb_ratio, s, nullptr);
+        z = R.levels[0].e;
+    } else {
+        z = run_vcycle<T>(c, R.levels, R.cs);
+    }
+    fg_store<T>(R.n, z, R.Z, R.ld, R.st, s);
+    fg_apply<T>(R.n, R.k, L0.idx.p, L0.A64.p, R.Z, R.ld, R.st, R.V, s);
+    fg_gram_schmidt(R.n, R.V, R.ld, R.st, 0, c->kpart.p, s);
+    fg_dgks(R.st, s);
+    fg_gram_schmidt(R.n, R.V, R.ld, R.st, 1, c->kpart.p, s);
+    fg_scale_w(R.n, R.V, R.ld, R.st, s);
+    fg_arnoldi_end(R.st, hd, s);
+    if (!captured && c->prof.on) {
+        auto &G = c->vg[sizeof(T) == 4 ? 1 : 0];
+        if (c->use_graphs && G.x && G.prof) c->prof.harvest_graph(G.ev_first, G.ev_pairs);
+        else c->prof.harvest();
+    }
+}
+
+// one restart cycle: r = b - A p into V_0, the cycle's start (norms,
+// convergence test, g = beta e_0), the Arnoldi steps, y = H^-1 g, p += Z y
+template <class T>
+void restart_cycle(FgRun<T> &R, cudaStream_t s, FgHandles hd, bool captured, long long *k_inner)
+{
+    mgm_ctx *c = R.c;
+    Level &L0 = c->L[0];
+    resid64(R.n, R.k, L0.idx.p, L0.A64.p, R.b, R.p, R.V, c->kpart.p, s);
+    fg_begin(R.st, c->kpart.p, R.nbres, hd, s);
+    fg_scale0(R.n, R.V, R.st, s);
+    if (captured) {
+        // the inner handle exists already: fg_begin above sets it
+        cudaGraph_t body = add_while_node(s, false, 0, &hd.inner);
+        cudaStream_t bs = c->s_body[1];
+        const long long before = g_launches;
+        capture_body(body, bs, [&] { arnoldi_step<T>(R, bs, hd, true); });
+        if (k_inner) *k_inner = g_launches - before;
+        g_launches = before;
+    } else {
+        while (read_fg_head(c).go_inner) arnoldi_step<T>(R, s, hd, false);
+    }
+    fg_solve_y(R.st, hd, s);
+    fg_combine<T>(R.n, R.Z, R.ld, R.st, R.p, s);
+}
+
+// The learned warm start.  The network's increment d carries BF16-level
+// grid-scale noise that the Laplacian amplifies, so it is first cleaned by
+// Chebyshev smoothing of A e = b - A (p + d) on the fine level (d <- d + e),
+// then p += alpha d with alpha minimising |b - A (p + alpha d)|_2 (never worse
+// than p).  The FGMRES then runs unchanged to the tolerance.  Every scalar
+// stays on the device.
+template <class T>
+void warm_start(FgRun<T> &R, cudaStream_t s)
+{
+    mgm_ctx *c = R.c;
+    Level &L0 = c->L[0];
+    const int n = R.n, k = R.k;
+    const long ld = R.ld;
+    double *d = c->wdir.p, *r0 = R.V, *Ad = c->wv.p, *pd = R.V + ld;
+    warm_direction<double>(c, R.b, R.p, d, s);
+    if (c->warm_smooth_steps > 0) {
+        copy_out<double>(n, R.p, pd, s);
+        set_scalar(c->kscal.p, 1.0, s);
+        combine<double>(n, 1, d, ld, c->kscal.p, pd, s);                 // pd = p + d
+        resid64(n, k, L0.idx.p, L0.A64.p, R.b, pd, r0, c->kpart.p, s);   // r0 = b - A (p + d)
+        copy_convert<T>(n, r0, R.levels[0].r, s);
+        const T *e = smooth_from_zero<T>(R.levels[0], c->warm_smooth_steps, c->cheb_ratio, s);
+        combine<T>(n, 1, e, ld, c->kscal.p, d, s);                      // d += e
+    }
+    resid64(n, k, L0.idx.p, L0.A64.p, R.b, R.p, r0, c->kpart.p, s);
+    apply64<double>(n, k, L0.idx.p, L0.A64.p, d, Ad, s);
+    multidot(n, 1, r0, ld, Ad, c->kpart.p, c->kscal.p, s);
+    multidot(n, 1, Ad, ld, Ad, c->kpart.p, c->kscal.p + 1, s);
+    fg_alpha(R.st, c->kscal.p, s);
+    combine<double>(n, 1, d, ld, c->kscal.p, R.p, s);
+}
+
+// Enqueues the solve on c->s.  captured: c->s is capturing a graph and the
+// loops become conditional nodes (kernel counts of the loop bodies into
+// k_outer / k_inner); else host loops, and the result is checked here.
+template <class T>
+void fgmres(mgm_ctx *c, const double *b, double *p, bool captured = false, long long *k_outer = nullptr,
+            long long *k_inner = nullptr)
 {
     cudaStream_t s = c->s;
     Level &L0 = c->L[0];
-    const int n = L0.n, k = L0.k;
+    FgRun<T> R;
+    R.c = c;
+    R.n = L0.n;
+    R.k = L0.k;
+    R.ld = L0.n;
+    R.nbres = blocks_for(L0.n, 256);
+    R.levels = solve_levels<T>(c);
+    R.cs.n = c->L[c->nl - 1].n;
+    if constexpr (sizeof(T) == 8) R.cs.inv = (const T *)c->cinv64.p; else R.cs.inv = (const T *)c->cinv32.p;
+    R.Z = sizeof(T) == 8 ? (T *)c->Z64.p : (T *)c->Z32.p;
+    R.V = c->V.p;
+    R.st = c->fg.p;
+    R.b = b;
+    R.p = p;
     const int m = std::min(c->max_iters, kMaxKrylov);
-    const long ld = n;
-    auto levels = solve_levels<T>(c);
-    CoarseSolve<T> cs;
-    cs.n = c->L[c->nl - 1].n;
-    if constexpr (sizeof(T) == 8) cs.inv = (const T *)c->cinv64.p; else cs.inv = (const T *)c->cinv32.p;
-    T *Z = sizeof(T) == 8 ? (T *)c->Z64.p : (T *)c->Z32.p;
-    double *V = c->V.p, *w = c->wv.p;
-    const int nbres = blocks_for(n, 256);
-    double *hp = c->h_pinned;  // pinned host scratch [2*kMaxKrylov+8]
-    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs_(m), sn_(m), g(m + 1);
-    int total_it = 0;
-    c->vcycles_in_solve = 0;
-    double bnorm = 0, relres = 1;
-    const int max_restarts = 4;
-    if (warm_start_enabled(c)) {
-        // learned warm start.  The network's increment d carries BF16-level
-        // grid-scale noise that the Laplacian amplifies, so it is first cleaned
-        // by Chebyshev smoothing of A e = b - A (p + d) on the fine level
-        // (d <- d + e), then p += alpha d with alpha minimising
-        // |b - A (p + alpha d)|_2 (never worse than p).  The FGMRES below then
-        // runs unchanged to the tolerance.
-        double *d = c->wdir.p, *r0 = V, *Ad = w, *pd = V + ld;
-        warm_direction<double>(c, b, p, d, s);
-        if (c->warm_smooth_steps > 0) {
-            copy_out<double>(n, p, pd, s);
-            hp[0] = 1.0;
-            MGM_CUDA(cudaMemcpyAsync(c->kscal.p, hp, sizeof(double), cudaMemcpyHostToDevice, s));
-            combine<double>(n, 1, d, ld, c->kscal.p, pd, s);                 // pd = p + d
-            resid64(n, k, L0.idx.p, L0.A64.p, b, pd, r0, c->kpart.p, s);     // r0 = b - A (p + d)
-            copy_convert<T>(n, r0, levels[0].r, s);
-            const T *e = smooth_from_zero<T>(levels[0], c->warm_smooth_steps, c->cheb_ratio, s);
-            combine<T>(n, 1, e, ld, c->kscal.p, d, s);                      // d += e
-        }
-        resid64(n, k, L0.idx.p, L0.A64.p, b, p, r0, c->kpart.p, s);
-        apply64<double>(n, k, L0.idx.p, L0.A64.p, d, Ad, s);
-        multidot(n, 1, r0, ld, Ad, c->kpart.p, c->kscal.p, s);
-        multidot(n, 1, Ad, ld, Ad, c->kpart.p, c->kscal.p + 1, s);
-        MGM_CUDA(cudaMemcpyAsync(hp, c->kscal.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
-        MGM_CUDA(cudaStreamSynchronize(s));
-        const double alpha = hp[1] > 0 && std::isfinite(hp[0] / hp[1]) ? hp[0] / hp[1] : 0.0;
-        c->last_learned_alpha = alpha;
-        hp[0] = alpha;
-        MGM_CUDA(cudaMemcpyAsync(c->kscal.p, hp, sizeof(double), cudaMemcpyHostToDevice, s));
-        combine<double>(n, 1, d, ld, c->kscal.p, p, s);
+    fg_init(R.st, m, c->max_iters * (kMaxRestarts + 1), kMaxRestarts, c->tol, s);
+    if (warm_start_enabled(c)) warm_start<T>(R, s);
+    FgHandles hd;
+    if (captured) {
+        hd.use = 1;
+        cudaGraph_t body = add_while_node(s, true, 1, &hd.outer);
+        // the inner node lives in the outer body: its handle belongs to that graph
+        MGM_CUDA(cudaGraphConditionalHandleCreate(&hd.inner, body, 0, 0));
+        cudaStream_t bs = c->s_body[0];
+        const long long before = g_launches;
+        long long kin = 0;
+        capture_body(body, bs, [&] { restart_cycle<T>(R, bs, hd, true, &kin); });
+        if (k_outer) *k_outer = g_launches - before;
+        if (k_inner) *k_inner = kin;
+        g_launches = before;
+        fg_final(R.st, s);
+        return;
     }
-    for (int restart = 0; restart <= max_restarts; restart++) {
-        // r0 = b - A p  -> V_0 (unnormalised), norms
-        resid64(n, k, L0.idx.p, L0.A64.p, b, p, V, c->kpart.p, s);
-        MGM_CUDA(cudaMemcpyAsync(hp, c->kpart.p, sizeof(double) * 2 * nbres, cudaMemcpyDeviceToHost, s));
-        MGM_CUDA(cudaStreamSynchronize(s));
-        double rr = 0, bb = 0;
-        for (int t = 0; t < nbres; t++) { rr += hp[2 * t]; bb += hp[2 * t + 1]; }
-        bnorm = sqrt(bb);
-        const double beta = sqrt(rr);
-        relres = bnorm > 0 ? beta / bnorm : 0.0;
-        if (!std::isfinite(relres)) throw Error{MGM_ERR_DIVERGED, "Poisson solve: non-finite residual"};
-        if (bnorm == 0 || relres < c->tol || total_it >= c->max_iters * (max_restarts + 1)) break;
-        hp[0] = beta;
-        MGM_CUDA(cudaMemcpyAsync(c->kscal.p, hp, sizeof(double), cudaMemcpyHostToDevice, s));
-        scale_by(n, V, V, c->kscal.p, 0, s);
-        std::fill(g.begin(), g.end(), 0.0);
-        g[0] = beta;
-        int j_done = 0;
-        for (int j = 0; j < m; j++) {
-            {
-                copy_convert<T>(n, V + j * ld, levels[0].r, s);
-                const T *zout = run_vcycle<T>(c, levels, cs);
-                copy_out<T>(n, zout, Z + j * ld, s);
-                c->vcycles_in_solve++;
-            }
-            // w = A z_j, written into the slot of V_{j+1}; classical Gram-Schmidt:
-            // the projections and |w|^2 in one pass, the update with the norm of
-            // the result in a second, and a re-orthogonalisation only when the
-            // first pass cancelled more than 1 - 1/sqrt(2) of |w| (the
-            // Daniel-Gragg-Kaufman-Stewart test)
-            double *wn = V + (j + 1) * ld;
-            double *h2 = c->kscal.p + kMaxKrylov + 2, *nrm = c->kscal.p + 2 * kMaxKrylov + 4;
-            apply64<T>(n, k, L0.idx.p, L0.A64.p, Z + j * ld, wn, s);
-            multidot(n, j + 2, V, ld, wn, c->kpart.p, c->kscal.p, s);
-            orth_norm(n, j + 1, V, ld, c->kscal.p, wn, c->kpart.p, nrm, s);
-            MGM_CUDA(cudaMemcpyAsync(hp, c->kscal.p, sizeof(double) * (2 * kMaxKrylov + 5), cudaMemcpyDeviceToHost, s));
-            MGM_CUDA(cudaStreamSynchronize(s));
-            for (int i = 0; i <= j; i++) hp[kMaxKrylov + 2 + i] = 0.0;
-            if (hp[2 * kMaxKrylov + 4] < 0.5 * hp[j + 1]) {
-                multidot(n, j + 1, V, ld, wn, c->kpart.p, h2, s);
-                orth_norm(n, j + 1, V, ld, h2, wn, c->kpart.p, nrm, s);
-                MGM_CUDA(cudaMemcpyAsync(hp + kMaxKrylov + 2, h2, sizeof(double) * (kMaxKrylov + 3),
-                                         cudaMemcpyDeviceToHost, s));
-                MGM_CUDA(cudaStreamSynchronize(s));
-            }
-            scale_by(n, wn, wn, nrm, 1, s);
-            if (c->prof.on) {
-                auto &G = c->vg[sizeof(T) == 4 ? 1 : 0];
-                if (c->use_graphs && G.x && G.prof) c->prof.harvest_graph(G.ev_first, G.ev_pairs);
-                else c->prof.harvest();
-            }
-            double *col = &H[(size_t)j * (m + 1)];
-            for (int i = 0; i <= j; i++) col[i] = hp[i] + hp[kMaxKrylov + 2 + i];
-            col[j + 1] = sqrt(std::max(hp[2 * kMaxKrylov + 4], 0.0));
-            for (int i = 0; i < j; i++) {
-                const double t0 = cs_[i] * col[i] + sn_[i] * col[i + 1];
-                col[i + 1] = -sn_[i] * col[i] + cs_[i] * col[i + 1];
-                col[i] = t0;
-            }
-            const double a = col[j], bb2 = col[j + 1];
-            const double rden = std::hypot(a, bb2);
-            cs_[j] = rden > 0 ? a / rden : 1.0;
-            sn_[j] = rden > 0 ? bb2 / rden : 0.0;
-            col[j] = rden;
-            col[j + 1] = 0;
-            g[j + 1] = -sn_[j] * g[j];
-            g[j] = cs_[j] * g[j];
-            total_it++;
-            j_done = j + 1;
-            const double est = fabs(g[j + 1]) / bnorm;
-            if (!std::isfinite(est)) throw Error{MGM_ERR_DIVERGED, "Poisson solve: non-finite Krylov residual"};
-            if (est < c->tol) break;
-        }
-        // y = H^-1 g (upper triangular), p += Z y
-        std::vector<double> y(j_done);
-        for (int i = j_done - 1; i >= 0; i--) {
-            double sacc = g[i];
-            for (int q = i + 1; q < j_done; q++) sacc -= H[(size_t)q * (m + 1) + i] * y[q];
-            y[i] = sacc / H[(size_t)i * (m + 1) + i];
-        }
-        for (int i = 0; i < j_done; i++) hp[i] = y[i];
-        MGM_CUDA(cudaMemcpyAsync(c->kscal.p, hp, sizeof(double) * j_done, cudaMemcpyHostToDevice, s));
-        combine<T>(n, j_done, Z, ld, c->kscal.p, p, s);
-    }
+    do {
+        restart_cycle<T>(R, s, hd, false, nullptr);
+    } while (read_fg_head(c).go_outer);
+    fg_final(R.st, s);
+    const FgState &h = read_fg_head(c);
     if constexpr (sizeof(T) == 4) {
         if (c->tma_err.p) {
             int h_err = 0;
@@ -598,11 +692,14 @@ void fgmres(mgm_ctx *c, const double *b, double *p)
             }
         }
     }
-    c->last_iters = (int)c->vcycles_in_solve;  // V-cycles (learned directions are not V-cycles)
-    c->last_relres = relres;
-    if (!(relres < c->tol) && bnorm > 0)
+    c->last_iters = h.vcycles;  // V-cycles (learned directions are not V-cycles)
+    c->last_relres = h.relres;
+    c->last_learned_alpha = h.alpha;
+    if (h.status == FG_NONFINITE) throw Error{MGM_ERR_DIVERGED, "Poisson solve: non-finite residual"};
+    if (h.status == FG_NOT_CONVERGED)
         throw Error{MGM_ERR_DIVERGED, "Poisson solve did not reach the tolerance (rel. residual " +
-                                          std::to_string(relres) + " after " + std::to_string(total_it) + " V-cycles)"};
+                                          std::to_string(h.relres) + " after " + std::to_string(h.total_it) +
+                                          " V-cycles)"};
 }
 
 // p_w and rho0(w) of the compatible right-hand sides, after every set-up
@@ -648,7 +745,11 @@ void ensure_compat(mgm_ctx *c)
     c->compat_ready = true;
 }
 
-void poisson(mgm_ctx *c, int mode, bool timple = false)
+// The Poisson solve of a step on L0.src -> L0.p.  captured: enqueued into a
+// graph being captured on c->s (the loops as conditional nodes, kernel counts
+// of the loop bodies into k_outer / k_inner).
+void poisson(mgm_ctx *c, int mode, bool timple = false, bool captured = false, long long *k_outer = nullptr,
+             long long *k_inner = nullptr)
 {
     Level &L0 = c->L[0];
     if (mode == MGM_MODE_REFERENCE) {
@@ -659,13 +760,14 @@ void poisson(mgm_ctx *c, int mode, bool timple = false)
         return;
     }
     if (mode != MGM_MODE_FP64 && mode != MGM_MODE_FP32_IR) throw Error{MGM_ERR_ARG, "unknown Poisson mode"};
+    if (c->compat) MGM_REQUIRE(c->compat_ready || !captured, "poisson: compatible right-hand sides not prepared");
     if (c->compat) ensure_compat(c);
     // b = source with the pinned row's rhs 0 (boundary rows keep their (zero) source)
     copy_out<double>(L0.n, L0.src.p, c->bvec.p, c->s);
     k_zero_pinned<<<1, 1, 0, c->s>>>(c->bvec.p);
     MGM_LAUNCHED();
-    if (mode == MGM_MODE_FP64) fgmres<double>(c, c->bvec.p, L0.p.p);
-    else fgmres<float>(c, c->bvec.p, L0.p.p);
+    if (mode == MGM_MODE_FP64) fgmres<double>(c, c->bvec.p, L0.p.p, captured, k_outer, k_inner);
+    else fgmres<float>(c, c->bvec.p, L0.p.p, captured, k_outer, k_inner);
     if (c->compat) {
         k_row0_residual<<<1, 32, 0, c->s>>>(L0.n, L0.k, L0.idx.p, L0.lapP.p, L0.src.p, L0.p.p, c->compat_s.p + 1);
         MGM_LAUNCHED();
@@ -680,24 +782,130 @@ void ensure_events(mgm_ctx *c)
         if (!e) MGM_CUDA(cudaEventCreate(&e));
 }
 
-// one fractional step (fractional_step_explicit) with the Poisson solve timed by events
-double step_timed(mgm_ctx *c, int mode)
+// The kernels of one fractional step (fractional_step_explicit) on c->s:
+// momentum, divergence, the Poisson solve between two device time marks,
+// the velocity correction and its steady-state error, and the error's copy
+// into c->h_pinned[0].
+void step_kernels(mgm_ctx *c, int mode, bool captured, long long *k_outer = nullptr, long long *k_inner = nullptr)
 {
-    ensure_events(c);
     StepArgs a = step_args(c);
     launch_momentum(a, c->dim, c->s);
     launch_divergence(a, c->dim, c->s);
-    MGM_CUDA(cudaEventRecord(c->ev[2], c->s));
-    poisson(c, mode);
-    MGM_CUDA(cudaEventRecord(c->ev[3], c->s));
+    fg_time_mark(c->fg.p, 0, c->s);
+    poisson(c, mode, false, captured, k_outer, k_inner);
+    fg_time_mark(c->fg.p, 1, c->s);
     launch_correct(a, c->dim, c->partial.p, c->scal.p, c->s);
     MGM_CUDA(cudaMemcpyAsync(c->h_pinned, c->scal.p, sizeof(double), cudaMemcpyDeviceToHost, c->s));
+}
+
+void drop_step_graphs(mgm_ctx *c)
+{
+    for (auto &g : c->sg) {
+        if (g.x) cudaGraphExecDestroy(g.x);
+        if (g.g) cudaGraphDestroy(g.g);
+        g = mgm_ctx::StepGraph();
+    }
+}
+
+bool step_graph_usable(mgm_ctx *c, int mode)
+{
+    return c->use_graphs && c->step_graphs && !c->prof.on && (mode == MGM_MODE_FP64 || mode == MGM_MODE_FP32_IR);
+}
+
+// The step graph of `mode`, captured on first use and whenever the settings
+// it bakes in (dt through the kernels' arguments, the learned warm start,
+// compatible right-hand sides) changed; solver settings drop it (drop_graphs).
+mgm_ctx::StepGraph &step_graph(mgm_ctx *c, int mode)
+{
+    auto &G = c->sg[mode == MGM_MODE_FP32_IR ? 1 : 0];
+    const bool warm = warm_start_enabled(c);
+    if (G.x && (G.warm != warm || G.compat != c->compat || G.dt != c->dt)) {
+        cudaGraphExecDestroy(G.x);
+        cudaGraphDestroy(G.g);
+        G = mgm_ctx::StepGraph();
+    }
+    if (G.x) return G;
+    if (c->compat) ensure_compat(c);
     MGM_CUDA(cudaStreamSynchronize(c->s));
-    float pm = 0;
-    MGM_CUDA(cudaEventElapsedTime(&pm, c->ev[2], c->ev[3]));
-    c->poisson_ms_acc += pm;
-    c->vcycles_acc += mode == MGM_MODE_REFERENCE ? (long long)c->num_vcycles : c->last_iters;
+    const long long before = g_launches;
+    long long ko = 0, ki = 0;
+    MGM_CUDA(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
+    try {
+        step_kernels(c, mode, true, &ko, &ki);
+    } catch (...) {
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(c->s, &junk);
+        if (junk) cudaGraphDestroy(junk);
+        g_launches = before;
+        throw;
+    }
+    MGM_CUDA(cudaStreamEndCapture(c->s, &G.g));
+    MGM_CUDA(cudaGraphInstantiate(&G.x, G.g, 0));
+    G.k_top = g_launches - before;
+    G.k_outer = ko;
+    G.k_inner = ki;
+    g_launches = before;
+    G.warm = warm;
+    G.compat = c->compat;
+    G.dt = c->dt;
+    return G;
+}
+
+// Launches nsteps fractional steps: replays of the step graph (no host
+// synchronisation inside or between them) or, in reference mode, with
+// profiling or with step graphs off, the host-driven step.  Returns the
+// steady-state error of the last step; the Poisson time and V-cycles of the
+// steps accumulate on the device (c->fg totals, cleared by the caller).
+double run_steps_device(mgm_ctx *c, int mode, int nsteps)
+{
+    if (step_graph_usable(c, mode)) {
+        auto &G = step_graph(c, mode);
+        for (int t = 0; t < nsteps; t++) MGM_CUDA(cudaGraphLaunch(G.x, c->s));
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+        const FgState &h = read_fg_head(c);
+        g_launches += (long long)nsteps * G.k_top + h.cycles_total * G.k_outer + h.vcycles_total * G.k_inner;
+        if (c->tma_err.p) {
+            int h_err = 0;
+            c->tma_err.download(&h_err, 1, c->s);
+            MGM_CUDA(cudaStreamSynchronize(c->s));
+            if (h_err) {
+                c->tma_err.zero(c->s);
+                throw Error{MGM_ERR_TIMEOUT, "Poisson solve: a tile-streamed level kernel timed out waiting for its copies"};
+            }
+        }
+        if (h.err_any & 1) throw Error{MGM_ERR_DIVERGED, "Poisson solve: non-finite residual"};
+        if (h.err_any & 2) throw Error{MGM_ERR_DIVERGED, "Poisson solve did not reach the tolerance"};
+        c->last_iters = h.vcycles;
+        c->last_relres = h.relres;
+        c->last_learned_alpha = h.alpha;
+        return c->h_pinned[0];
+    }
+    for (int t = 0; t < nsteps; t++) {
+        step_kernels(c, mode, false);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+        if (mode == MGM_MODE_REFERENCE) c->ref_vcycles_acc += c->num_vcycles;
+    }
     return c->h_pinned[0];
+}
+
+// p_w of the compatible right-hand sides before a run of steps (so that its
+// own solve is not counted in the steps' V-cycles)
+void prepare_steps(mgm_ctx *c, int mode)
+{
+    if (c->compat && (mode == MGM_MODE_FP64 || mode == MGM_MODE_FP32_IR)) ensure_compat(c);
+}
+
+// one fractional step; Poisson time and V-cycles added to the context's counters
+double step_timed(mgm_ctx *c, int mode)
+{
+    prepare_steps(c, mode);
+    fg_clear_totals(c->fg.p, c->s);
+    c->ref_vcycles_acc = 0;
+    const double e = run_steps_device(c, mode, 1);
+    const FgState &h = read_fg_head(c);
+    c->poisson_ms_acc += h.t_ns * 1e-6;
+    c->vcycles_acc += mode == MGM_MODE_REFERENCE ? c->ref_vcycles_acc : h.vcycles_total;
+    return e;
 }
 
 void alloc_solver_buffers(mgm_ctx *c)
@@ -712,6 +920,11 @@ void alloc_solver_buffers(mgm_ctx *c)
     c->bvec.alloc(n);
     c->kpart.alloc((size_t)std::max(2 * blocks_for(n, 256), (kMaxKrylov + 1) * dot_blocks(n)) + 16);
     c->kscal.alloc(3 * kMaxKrylov + 16);
+    if (!c->fg.p) {
+        c->fg.alloc(1);
+        c->fg.zero(c->s);
+    }
+    if (!c->h_fg) MGM_CUDA(cudaMallocHost(&c->h_fg, sizeof(FgState)));
     if (!c->h_pinned) MGM_CUDA(cudaMallocHost(&c->h_pinned, sizeof(double) * (3 * kMaxKrylov + 16 + 2 * 65536)));
 }
 
@@ -949,6 +1162,7 @@ mgm_ctx *mgm_create(int dim, int phs_degree, int num_levels)
         cc->dim = dim; cc->phs = phs_degree; cc->nl = num_levels;
         cc->L.resize(num_levels);
         MGM_CUDA(cudaStreamCreateWithFlags(&cc->s, cudaStreamNonBlocking));
+        for (auto &bs : cc->s_body) MGM_CUDA(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
         c = cc.release();
     });
     return st == MGM_OK ? c : nullptr;
@@ -960,9 +1174,12 @@ void mgm_destroy(mgm_ctx *c)
     cudaSetDevice(c->device);
     if (c->s) cudaStreamSynchronize(c->s);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
+    if (c->h_fg) cudaFreeHost(c->h_fg);
     drop_graphs(c);
     destroy_mpnn(c);
     c->L.clear();
+    for (auto &bs : c->s_body)
+        if (bs) cudaStreamDestroy(bs);
     if (c->s) cudaStreamDestroy(c->s);
     delete c;
 }
@@ -1385,6 +1602,66 @@ int mgm_get_transfer(mgm_ctx *c, int lev, int *rpts, int *ppts, double *restr, d
     });
 }
 
+int mgm_get_solver_transfer(mgm_ctx *c, int lev, double *restr, double *prol)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(lev >= 0 && lev < c->nl && c->setup_done, "mgm_get_solver_transfer: not set up");
+        Level &L = c->L[lev];
+        cudaStream_t s = c->s;
+        if (restr && lev > 0) {
+            const int kf = c->L[lev - 1].k;
+            DBuf<double> tmp((size_t)L.n * kf);
+            transpose_ell_to_rowmajor_d(L.s_r_w64.p, tmp.p, L.n, kf, s);
+            tmp.download(restr, (size_t)L.n * kf, s);
+            MGM_CUDA(cudaStreamSynchronize(s));
+        }
+        if (prol && lev < c->nl - 1) {
+            const int kc = c->L[lev + 1].k;
+            DBuf<double> tmp((size_t)L.n * kc);
+            transpose_ell_to_rowmajor_d(L.s_p_w64.p, tmp.p, L.n, kc, s);
+            tmp.download(prol, (size_t)L.n * kc, s);
+            MGM_CUDA(cudaStreamSynchronize(s));
+        }
+    });
+}
+
+int mgm_get_compact(mgm_ctx *c, int lev, int which, int *idx, float *w, int *compact)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(lev >= 0 && lev < c->nl && c->setup_done, "mgm_get_compact: not set up");
+        MGM_REQUIRE(which >= 0 && which <= 2, "mgm_get_compact: which must be 0, 1 or 2");
+        MGM_REQUIRE(idx && w, "mgm_get_compact: null output");
+        MGM_REQUIRE(which != 1 || lev > 0, "mgm_get_compact: level 0 has no restriction into it");
+        MGM_REQUIRE(which != 2 || lev < c->nl - 1, "mgm_get_compact: the coarsest level has no prolongation into it");
+        Level &L = c->L[lev];
+        cudaStream_t s = c->s;
+        int k = L.k, ld = L.ld4;
+        const short *off = nullptr;
+        const int *base = nullptr, *gidx = nullptr;
+        const float *W = nullptr;
+        if (which == 0) {
+            off = L.off_ok ? L.off16.p : nullptr; gidx = L.sidx.p; W = L.A32.p;
+        } else if (which == 1) {
+            k = c->L[lev - 1].k; ld = L.n;
+            off = L.r_off_ok ? L.r_off16.p : nullptr; base = L.rpts.p; gidx = L.s_r_idx.p; W = L.s_r_w32.p;
+        } else {
+            k = c->L[lev + 1].k; ld = L.n;
+            off = L.p_off_ok ? L.p_off16.p : nullptr; base = L.ppts.p; gidx = L.s_p_idx.p; W = L.s_p_w32.p;
+        }
+        const size_t nk = (size_t)L.n * k;
+        DBuf<int> di(nk);
+        DBuf<float> dw(nk);
+        k_decode_compact<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, k, ld, off, base, gidx, W, di.p, dw.p);
+        MGM_LAUNCHED();
+        di.download(idx, nk, s);
+        dw.download(w, nk, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+        if (compact) *compact = off ? 1 : 0;
+    });
+}
+
 int mgm_set_flow(mgm_ctx *c, double Re, double courant, float omega, int num_relax, int num_vcycles, double dt)
 {
     return guard([&] {
@@ -1570,6 +1847,28 @@ int mgm_use_graphs(mgm_ctx *c, int enable)
     });
 }
 
+int mgm_use_step_graph(mgm_ctx *c, int enable)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+        drop_step_graphs(c);
+        c->step_graphs = enable != 0;
+    });
+}
+
+int mgm_solve_counters(mgm_ctx *c, long long *vcycles, long long *cycles, long long *solves)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done && c->fg.p, "mgm_solve_counters: not set up");
+        const FgState &h = read_fg_head(c);
+        if (vcycles) *vcycles = h.vcycles_total;
+        if (cycles) *cycles = h.cycles_total;
+        if (solves) *solves = h.solves_total;
+    });
+}
+
 int mgm_set_warm_smoothing(mgm_ctx *c, int steps)
 {
     return guard([&] {
@@ -1671,18 +1970,20 @@ int mgm_run_steps(mgm_ctx *c, int mode, int nsteps, double *step_ms, double *poi
         MGM_REQUIRE(c->setup_done && c->dt > 0, "mgm_run_steps: call mgm_setup and mgm_set_flow first");
         MGM_REQUIRE(nsteps >= 0, "mgm_run_steps: nsteps < 0");
         ensure_events(c);
-        c->poisson_ms_acc = 0;
-        c->vcycles_acc = 0;
-        double e = 0;
+        prepare_steps(c, mode);
+        if (step_graph_usable(c, mode)) step_graph(c, mode);  // captured before the timed region
+        fg_clear_totals(c->fg.p, c->s);
+        c->ref_vcycles_acc = 0;
         MGM_CUDA(cudaEventRecord(c->ev[0], c->s));
-        for (int t = 0; t < nsteps; t++) e = step_timed(c, mode);
+        const double e = run_steps_device(c, mode, nsteps);
         MGM_CUDA(cudaEventRecord(c->ev[1], c->s));
         MGM_CUDA(cudaEventSynchronize(c->ev[1]));
         float ms = 0;
         MGM_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+        const FgState &h = read_fg_head(c);
         if (step_ms) *step_ms = ms;
-        if (poisson_ms) *poisson_ms = c->poisson_ms_acc;
-        if (vcycles) *vcycles = c->vcycles_acc;
+        if (poisson_ms) *poisson_ms = h.t_ns * 1e-6;
+        if (vcycles) *vcycles = mode == MGM_MODE_REFERENCE ? c->ref_vcycles_acc : h.vcycles_total;
         if (steady_err) *steady_err = e;
     });
 }

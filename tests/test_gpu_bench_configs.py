@@ -1,0 +1,275 @@
+"""Parity at the configurations the benchmarks run, not only on small clouds.
+
+* C1 exactly as configured (2D cavity 128^2, 3 levels, k = 20, PHS 3 + poly 3,
+  Re 100, Courant 0.5, SOR omega 1.2, num_relax 3, 10 V-cycles): the whole
+  set-up against the restatement (clouds, breadth-first order, normals,
+  spacing, restriction/prolongation points bit for bit; derivative and
+  transfer weights bit for bit against the correctly-rounded-power build and
+  within 1e-10 of each row's largest weight against the libm build, which is
+  the reference's own arithmetic); 200 reference-semantics fractional steps
+  bit for bit (Jacobi sweep order), including the steps after the
+  reference's own V-cycle has made them non-finite; ten steps of the
+  FP32-in-FP64 solve against the restated step with an FP64 direct solve.
+* The 1M-node cavity of bench.py, the 1M-node Taylor-Couette annulus and the
+  128^3 cube: on every level the clouds, breadth-first order, normals,
+  spacing and nearest points of the whole level bit for bit; the derivative
+  weights and the solver's transfer weights on a seeded sample of at least
+  20,000 rows per level (every row of smaller levels), boundary rows and the
+  rows with the widest 16-bit neighbour offsets included; the FP32
+  V-cycle's compact copies (int16 offsets) decoded back to the neighbours and
+  weights they stand for, on every row.
+* Ten fractional steps on a 250k-node cavity with the FP32-in-FP64 solve
+  against the restated step whose Poisson solve is an FP64 direct solve:
+  pressure and velocity within 1e-6 relative L2 after every step.
+
+Reference functions: kdtree_functions.h:61-151, 153-175;
+mesh_functions.h:478-527, 533-670, 774-872, 895-910; rbf.h:274-421;
+fractional_step_solver.h:47-275.
+"""
+import numpy as np
+import pytest
+
+import multigrid_meshless_b200 as mgm
+from multigrid_meshless_b200 import api, clouds
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+W_TOL = 1e-10      # weights against the libm build, relative to each row's largest weight
+P_TOL = 1e-6       # pressure and velocity, relative L2
+SAMPLE = 20000     # rows per level checked against the per-row weight solves
+
+
+def _rowrel(a, b):
+    den = np.maximum(np.abs(a).max(1), 1e-300)
+    return float((np.abs(a - b).max(1) / den).max())
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+# ---------------------------------------------------------------------------
+# C1 as configured
+# ---------------------------------------------------------------------------
+C1_KS, C1_POLYS = [20] * 3, [3] * 3
+
+
+@pytest.fixture(scope="module")
+def c1(require_gpu):
+    cl = clouds.cavity_hierarchy(128, 3, seed=1)
+    mg = api.Multigrid(cl, C1_KS, C1_POLYS, reference_transfer=True)
+    yield cl, mg
+    mg.close()
+
+
+def test_c1_setup_against_restatement(c1):
+    cl, mg = c1
+    assert mg.n(0) == 16380
+    for crpow in (True, False):
+        ref = O.orc_pipeline(cl, C1_KS, C1_POLYS, reference_rows=True, crpow=crpow)
+        for l, R in enumerate(ref):
+            g = mg.geometry(l)
+            if crpow:
+                for nm in ("x", "y", "z", "nx", "ny", "nz", "btag", "cloud"):
+                    assert np.array_equal(g[nm], getattr(R, nm)), (l, nm)
+                assert g["d_avg"] == R.d_avg, l
+                tr = mg.transfer(l)
+                assert np.array_equal(tr["rpts"], R.rpts) and np.array_equal(tr["ppts"], R.ppts), l
+            ops = mg.operators(l)
+            for nm in ("Dx", "Dy", "lap", "lapP"):
+                if crpow:
+                    assert np.array_equal(ops[nm], getattr(R, nm)), (l, nm)
+                else:
+                    assert _rowrel(getattr(R, nm), ops[nm]) < W_TOL, (l, nm)
+            tr = mg.transfer(l)
+            for nm in ("restr", "prol"):
+                want = getattr(R, nm)
+                if want is None:
+                    continue
+                if crpow:
+                    assert np.array_equal(tr[nm], want), (l, nm)
+                else:
+                    rows = np.abs(want).max(1) > 0
+                    assert _rowrel(want[rows], tr[nm][rows]) < W_TOL, (l, nm)
+
+
+def test_c1_reference_steps_bit_exact(c1):
+    """200 steps of the reference's fractional step with its own V-cycle
+    (omega 1.2, 3 sweeps, 10 V-cycles): the reference's V-cycle diverges at
+    omega 1.2, and the comparison continues bit for bit (NaN where both are
+    NaN) through every step."""
+    cl, mg = c1
+    levels = O.levels_from_device(mg)
+    dt = mg.set_flow(Re=100.0, courant=0.5, omega=1.2, num_relax=3, num_vcycles=10)
+    S = O.OracleSolver(levels, 100.0, 0.5, 1.2, 3, 10, jacobi=True)
+    assert S.dt == dt
+    mg.apply_bc(mgm.BC_LID)
+    O.lid_bc(levels[0], S.f)
+    finite_steps = 0
+    for s in range(200):
+        mg.step(mgm.MODE_REFERENCE)
+        S.step()
+        for nm in ("u", "v"):
+            assert np.array_equal(mg.get_field(nm), S.f[nm], equal_nan=True), (s, nm)
+        p = mg.get_field("p")
+        assert np.array_equal(p, S.p[0], equal_nan=True), (s, "p")
+        if np.all(np.isfinite(p)):
+            finite_steps += 1
+    assert finite_steps >= 1
+
+
+def test_c1_fp32_ir_steps_match_direct_solve_steps(c1):
+    cl, mg = c1
+    levels = O.levels_from_device(mg)
+    mg.set_flow(Re=100.0, courant=0.5)
+    mg.set_solver(rel_tol=1e-10, max_iters=100)
+    S = O.OracleSolver(levels, 100.0, 0.5, 1.0, 1, 1, jacobi=True)
+    solve = O.pinned_lu(levels[0].lapP, levels[0].cloud)
+    mg.apply_bc(mgm.BC_LID)
+    O.lid_bc(levels[0], S.f)
+    for s in range(10):
+        mg.step(mgm.MODE_FP32_IR)
+        S.O.orc_intermediate_velocity(S.h)
+        S.O.orc_mass_residual(S.h)
+        S.p[0][:] = solve(S.source[0])
+        S.O.orc_update_velocity(S.h)
+        for nm in ("u", "v"):
+            assert _rel(mg.get_field(nm), S.f[nm]) < P_TOL, (s, nm)
+        assert _rel(mg.get_field("p"), S.p[0]) < P_TOL, (s, "p")
+
+
+# ---------------------------------------------------------------------------
+# the large benchmark configurations
+# ---------------------------------------------------------------------------
+LARGE = {
+    # name: (hierarchy, k per level, poly per level)
+    "cavity_1m": (lambda: clouds.cavity_hierarchy(1000, 6, seed=1), 30, 4),
+    "annulus_1m": (lambda: clouds.annulus_hierarchy(clouds.annulus_h_for_nodes(1_000_000), 6, seed=1), 30, 4),
+    "cube_128": (lambda: clouds.cube_hierarchy(128, 4, seed=1), 35, 2),
+}
+
+
+def _sample_rows(n, btag, compact_idx, seed):
+    """At least SAMPLE rows (all rows of smaller levels): up to 2,000 boundary
+    rows, the 500 rows whose compact-operator neighbours lie farthest from
+    the row index, and seeded uniform rows."""
+    if n <= SAMPLE:
+        return np.arange(n)
+    rng = np.random.default_rng(seed)
+    bnd = np.flatnonzero(btag)
+    pick = [rng.choice(bnd, min(2000, bnd.size), replace=False)] if bnd.size else []
+    span = np.abs(compact_idx - np.arange(n)[:, None]).max(1)
+    pick.append(np.argsort(span)[-500:])
+    pick.append(rng.choice(n, SAMPLE, replace=False))
+    return np.unique(np.concatenate(pick)).astype(np.int64)
+
+
+@pytest.mark.parametrize("name", list(LARGE))
+def test_large_config_setup(require_gpu, name):
+    build, k, poly = LARGE[name]
+    cl = build()
+    nl = len(cl)
+    dim = cl[0].dim
+    mg = api.Multigrid(cl, [k] * nl, [poly] * nl)
+    try:
+        geo = []
+        for l in range(nl):
+            # the whole level: kNN -> breadth-first reorder -> normals -> spacing
+            ref = O.orc_level_setup(cl[l], k)
+            g = mg.geometry(l)
+            for nm in ("x", "y", "z", "nx", "ny", "nz", "btag", "cloud"):
+                assert np.array_equal(g[nm], ref[nm]), (name, l, nm)
+            assert g["d_avg"] == ref["d_avg"], (name, l)
+            assert O.lib().orc_count_ties(cl[l].n, cl[l].nb, ref["x"], ref["y"], ref["z"], k,
+                                          np.ascontiguousarray(ref["cloud"].ravel())) == 0, (name, l)
+            geo.append(g)
+        for l in range(nl):
+            G = geo[l]
+            n = G["x"].shape[0]
+            tr = mg.transfer(l)
+            # nearest points of the whole level (find_nearest_point)
+            for key, other in (("ppts", geo[min(l + 1, nl - 1)]), ("rpts", geo[max(l - 1, 0)])):
+                want = np.zeros(n, np.int32)
+                O.lib().orc_nearest(n, G["x"], G["y"], G["z"], other["x"].shape[0], other["x"], other["y"],
+                                    other["z"], dim, want)
+                assert np.array_equal(tr[key], want), (name, l, key)
+            # the FP32 V-cycle's compact operator: every row's neighbours and weights
+            idx, w32, compact = mg.compact(l, "op")
+            assert compact, (name, l, "int16 offsets not in use")
+            ops = mg.operators(l)
+            order = np.argsort(G["cloud"], axis=1, kind="stable")
+            want_idx = np.take_along_axis(G["cloud"], order, 1)
+            want_w = np.take_along_axis(ops["lapP"], order, 1).astype(np.float32)
+            assert np.array_equal(idx[1:], want_idx[1:]), (name, l)
+            assert np.array_equal(w32[1:], want_w[1:]), (name, l)
+            # derivative weights on the sample, against the per-row oracle solves
+            S = _sample_rows(n, G["btag"], idx, seed=100 + l)
+            assert S.size >= min(n, SAMPLE)
+            sub = {nm: np.ascontiguousarray(G[nm][S]) for nm in ("nx", "ny", "nz", "btag")}
+            cl_s = np.ascontiguousarray(G["cloud"][S].ravel())
+            names = ("Dx", "Dy", "Dz", "lap", "lapP")
+            for crpow in (True, False):
+                want = [np.zeros(S.size * k) for _ in range(5)]
+                O.lib(crpow).orc_derivative_weights(S.size, k, dim, 3, poly, G["x"], G["y"], G["z"], sub["nx"],
+                                                    sub["ny"], sub["nz"], sub["btag"], cl_s, *want)
+                for nm, wv in zip(names, want):
+                    if nm == "Dz" and dim != 3:
+                        continue
+                    got = ops[nm][S]
+                    wv = wv.reshape(S.size, k)
+                    if crpow:
+                        assert np.array_equal(got, wv), (name, l, nm)
+                    else:
+                        assert _rowrel(wv, got) < W_TOL, (name, l, nm)
+            # the solver's transfer weights on the sample (restriction: interior
+            # rows; prolongation: every row), and their compact copies
+            st = mg.solver_transfer(l)
+            for kind, src_l, pts_key, only_int in (("restr", l - 1, "rpts", 1), ("prol", l + 1, "ppts", 0)):
+                if not (0 <= src_l < nl):
+                    continue
+                Sg = geo[src_l]
+                ks = Sg["cloud"].shape[1]
+                pts = tr[pts_key]
+                cidx, cw, ccompact = mg.compact(l, kind)
+                assert ccompact, (name, l, kind, "int16 offsets not in use")
+                live = (G["btag"] == 0) if only_int else np.ones(n, bool)
+                assert np.array_equal(cidx[live], Sg["cloud"][pts][live]), (name, l, kind)
+                assert np.array_equal(cw, st[kind].astype(np.float32)), (name, l, kind)
+                want = np.zeros(S.size * ks)
+                O.lib(True).orc_transfer_weights(S.size, np.ascontiguousarray(G["x"][S]),
+                                                 np.ascontiguousarray(G["y"][S]), np.ascontiguousarray(G["z"][S]),
+                                                 sub["btag"], np.ascontiguousarray(pts[S]), 0, only_int,
+                                                 Sg["x"].shape[0], ks, dim, 3, poly, Sg["x"], Sg["y"], Sg["z"],
+                                                 np.ascontiguousarray(Sg["cloud"].ravel()), want)
+                assert np.array_equal(st[kind][S], want.reshape(S.size, ks)), (name, l, kind)
+    finally:
+        mg.close()
+
+
+# ---------------------------------------------------------------------------
+# ten converged steps at 250k nodes
+# ---------------------------------------------------------------------------
+def test_fp32_ir_steps_at_250k_match_direct_solve_steps(require_gpu):
+    cl = clouds.cavity_hierarchy(500, 5, seed=11)
+    mg = api.Multigrid(cl, [30] * 5, [4] * 5)
+    try:
+        assert mg.n(0) >= 250_000 - 4
+        levels = O.levels_from_device(mg)
+        mg.set_flow(Re=100.0, courant=0.5)
+        mg.set_solver(rel_tol=1e-10, max_iters=100)
+        S = O.OracleSolver(levels, 100.0, 0.5, 1.0, 1, 1, jacobi=True)
+        solve = O.pinned_lu(levels[0].lapP, levels[0].cloud)
+        mg.apply_bc(mgm.BC_LID)
+        O.lid_bc(levels[0], S.f)
+        for s in range(10):
+            mg.step(mgm.MODE_FP32_IR)
+            S.O.orc_intermediate_velocity(S.h)
+            S.O.orc_mass_residual(S.h)
+            S.p[0][:] = solve(S.source[0])
+            S.O.orc_update_velocity(S.h)
+            for nm in ("u", "v"):
+                assert _rel(mg.get_field(nm), S.f[nm]) < P_TOL, (s, nm)
+            assert _rel(mg.get_field("p"), S.p[0]) < P_TOL, (s, "p")
+    finally:
+        mg.close()

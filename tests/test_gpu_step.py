@@ -257,3 +257,53 @@ def test_ref_routines_one_by_one_match_the_cycle(cavity):
     for l in range(mg.nl):
         assert np.array_equal(out[0][l], out[1][l]), l
     assert np.abs(out[0][0]).max() > 0
+
+
+def test_step_graph_matches_host_driven_steps(cavity):
+    """A fractional step as ONE graph launch (the solve's restart and Arnoldi
+    loops as conditional WHILE nodes set by device kernels) gives the bits of
+    the host-driven solve (host reads the loop flags, V-cycle graphs) and of
+    fully eager launches: fields after every step, V-cycle counts, steady
+    error; through mgm_run_steps and mgm_step."""
+    mg = cavity
+    mg.set_flow(Re=100.0, courant=0.5)
+    mg.set_solver(rel_tol=1e-8, max_iters=80)
+    try:
+        for mode in (mgm.MODE_FP64, mgm.MODE_FP32_IR):
+            runs = []
+            for graphs, step_graph in ((True, True), (True, False), (False, False)):
+                mg.use_graphs(graphs)
+                mg.use_step_graph(step_graph)
+                mg.apply_bc(mgm.BC_LID)
+                out = []
+                for rep in range(2):  # second replay of the same step graph
+                    _, _, vc, err = mg.run_steps(mode, 2)
+                    out += [vc, err, mg.get_field("u"), mg.get_field("v"), mg.get_field("p")]
+                out += [mg.step(mode), mg.last_solve()[0], mg.get_field("p")]
+                runs.append(out)
+            for r in runs[1:]:
+                assert len(r) == len(runs[0])
+                for a, b in zip(r, runs[0]):
+                    if isinstance(a, np.ndarray):
+                        assert np.array_equal(a, b)
+                    else:
+                        assert a == b
+            assert runs[0][0] > 0
+    finally:
+        mg.use_graphs(True)
+        mg.use_step_graph(True)
+
+
+def test_step_graph_reports_unconverged_solve(cavity):
+    """A tolerance the iteration budget cannot reach: the captured loops stop
+    at the budget (two Arnoldi steps per cycle, five cycles) and the host
+    raises the solver's error after the graph launch."""
+    mg = cavity
+    mg.set_flow(Re=100.0, courant=0.5)
+    mg.set_solver(rel_tol=1e-15, max_iters=2)
+    try:
+        mg.apply_bc(mgm.BC_LID)
+        with pytest.raises(Exception, match="tolerance"):
+            mg.run_steps(mgm.MODE_FP32_IR, 1)
+    finally:
+        mg.set_solver(rel_tol=1e-8, max_iters=80)
