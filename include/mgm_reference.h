@@ -23,7 +23,17 @@
 #ifndef MGM_REFERENCE_H
 #define MGM_REFERENCE_H
 
+/* The reference's structures.h guard: its init files (init/init_TC.c:7,
+ * init/init_LDC.c:7) include "../header_files/structures.h", whose contents
+ * this header replaces; with the guard defined that include adds nothing. */
+#define STRUCTURES_H
+
+#include <math.h>
 #include <stdbool.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
 
 #include "mgm.h"
 
@@ -127,6 +137,18 @@ typedef struct FieldVariables {
 /* structures.h:114-172 */
 MGM_API void AllocateMemoryPointStructure(PointStructure *myPointStruct, int nodes);
 MGM_API void AllocateMemoryFieldVariables(FieldVariables **field, PointStructure *myPointStruct, int num_levels);
+/* structures.h:174-226: frees the levels' host arrays and jagged rows (rows
+ * absent on a level are skipped, where the reference's version frees
+ * unallocated restr_mat / prol_mat rows) and the device context when these
+ * levels are the ones copyin_essentials_to_gpu took; free_field frees every
+ * member array. */
+MGM_API void free_PointStructure(PointStructure *myPointStruct, int num_levels);
+MGM_API void free_field(FieldVariables *field, int num_levels);
+/* general_functions.h:44-192: the derivative self-test (mg_NS_solver.c:40-43):
+ * per level, the RMS error over interior nodes of Dx, Dy, (Dz), lap applied
+ * on the GPU to sin(2*3.14*x) sin(2*3.14*y) (sin(2*3.14*z)) against its exact
+ * derivatives, printed in the reference's format. */
+MGM_API void test_derivatives(PointStructure *myPointStruct, short num_levels, short domain_dimension);
 /* mesh_functions.h:37-129, 131-170 */
 MGM_API void read_flow_parameters(char *filename);
 MGM_API void read_grid_filenames(PointStructure **myPointStruct, char *filename, short *num_levels);

@@ -776,4 +776,130 @@ double time_implicit_solver(PointStructure *ps, FieldVariables *field)
     return err;
 }
 
+// ---------------------------------------------------------------------------
+// general_functions.h:44-192: the derivative self-test of mg_NS_solver.c:40-43
+// (parameters.test > 0).  The manufactured solution and its exact
+// derivatives are evaluated on the host with libm, as the reference does
+// (pi written 3.14, wave number 1); the operators are applied on the GPU
+// (mgm_spmv: the same row sums in the same order as the reference's
+// multiply_sparse_matrix_vector); the RMS error over interior nodes is
+// summed on the host in node order and printed in the reference's format.
+// ---------------------------------------------------------------------------
+static double l2_interior(const PointStructure *p, const double *A, const double *B)
+{
+    double r = 0.0;
+    for (int i = 0; i < p->num_nodes; i++)
+        if (p->boundary_tag[i] == 0) {
+            const double d = A[i] - B[i];
+            r += d * d;
+        }
+    return std::sqrt(r / p->num_nodes);
+}
+
+static void apply_op(PointStructure *p, double **D, const double *f, double *out, const char *fn)
+{
+    const int n = p->num_nodes, k = p->num_cloud_points;
+    if (!D || !p->cloud_index) { std::printf("Error: %s: operators not built\n", fn); std::exit(1); }
+    std::vector<double> flat = pack_rows(D, n, k);
+    std::vector<int> cl = pack_rows(p->cloud_index, n, k);
+    die_if(mgm_spmv(n, k, flat.data(), cl.data(), f, out), fn);
+}
+
+void test_derivatives(PointStructure *ps, short num_levels, short domain_dimension)
+{
+    for (int ii = 0; ii < num_levels; ii++) {
+        std::printf("Testing level %d\n", ii);
+        PointStructure *p = &ps[ii];
+        const int n = p->num_nodes;
+        const int k = 1;  // wave number
+        const bool d3 = domain_dimension > 2;
+        std::vector<double> F(n), Fx(n), Fy(n), Fz(n), lapF(n), f(n), fx(n), fy(n), fz(n), lapf(n);
+        for (int i = 0; i < n; i++) {
+            const double x = p->x[i], y = p->y[i], z = p->z[i];
+            if (d3) {
+                F[i] = sin(2 * 3.14 * k * x) * sin(2 * 3.14 * k * y) * sin(2 * 3.14 * k * z);
+                Fx[i] = 2 * 3.14 * k * cos(2 * 3.14 * k * x) * sin(2 * 3.14 * k * y) * sin(2 * 3.14 * k * z);
+                Fy[i] = 2 * 3.14 * k * sin(2 * 3.14 * k * x) * cos(2 * 3.14 * k * y) * sin(2 * 3.14 * k * z);
+                Fz[i] = 2 * 3.14 * k * sin(2 * 3.14 * k * x) * sin(2 * 3.14 * k * y) * cos(2 * 3.14 * k * z);
+                lapF[i] = -12 * 3.14 * 3.14 * k * k * sin(2 * 3.14 * k * x) * sin(2 * 3.14 * k * y) *
+                          sin(2 * 3.14 * k * z);
+            } else {
+                F[i] = sin(2 * 3.14 * k * x) * sin(2 * 3.14 * k * y);
+                Fx[i] = 2 * 3.14 * k * cos(2 * 3.14 * k * x) * sin(2 * 3.14 * k * y);
+                Fy[i] = 2 * 3.14 * k * sin(2 * 3.14 * k * x) * cos(2 * 3.14 * k * y);
+                lapF[i] = -8 * 3.14 * 3.14 * k * k * sin(2 * 3.14 * k * x) * sin(2 * 3.14 * k * y);
+            }
+        }
+        // the reference overwrites f's derivative slots with the operators applied to f
+        f = F;
+        apply_op(p, p->Dx, f.data(), fx.data(), "test_derivatives");
+        apply_op(p, p->Dy, f.data(), fy.data(), "test_derivatives");
+        if (d3) apply_op(p, p->Dz, f.data(), fz.data(), "test_derivatives");
+        apply_op(p, p->lap, f.data(), lapf.data(), "test_derivatives");
+        const double ef = l2_interior(p, F.data(), f.data()), ex = l2_interior(p, Fx.data(), fx.data()),
+                     ey = l2_interior(p, Fy.data(), fy.data()), el = l2_interior(p, lapF.data(), lapf.data());
+        if (d3) {
+            const double ez = l2_interior(p, Fz.data(), fz.data());
+            std::printf("L2 error in f, fx, fy, fz, lapf:\n%lf %lf %lf %lf %lf\n", ef, ex, ey, ez, el);
+        } else {
+            std::printf("L2 error in f, fx, fy, lapf:\n%lf %lf %lf %lf\n", ef, ex, ey, el);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// structures.h:174-226.  Frees what this library allocated for the levels
+// (host arrays and jagged rows; a row array absent on a level, such as
+// restr_mat on the finest or prol_mat on the coarsest, is skipped instead of
+// being freed row by row as the reference's version does) and releases the
+// device context when these are the levels copyin_essentials_to_gpu took.
+// ---------------------------------------------------------------------------
+static void free_rows(void **rows, int n)
+{
+    if (!rows) return;
+    for (int i = 0; i < n; i++) std::free(rows[i]);
+    std::free(rows);
+}
+
+void free_PointStructure(PointStructure *ps, int num_levels)
+{
+    if (!ps) return;
+    if (ps == g_ps && g_ctx) {
+        mgm_destroy(g_ctx);
+        g_ctx = nullptr;
+        g_ps = nullptr;
+        g_levels = 0;
+    }
+    for (int l = 0; l < num_levels; l++) {
+        PointStructure *p = &ps[l];
+        const int n = p->num_nodes;
+        void *flat[] = {p->x, p->y, p->z, p->point_index, p->x_normal, p->y_normal, p->z_normal, p->boundary_tag,
+                        p->corner_tag, p->pow_x, p->pow_y, p->pow_z, p->prolongation_points, p->restriction_points};
+        for (void *a : flat) std::free(a);
+        free_rows((void **)p->cloud_index, n);
+        free_rows((void **)p->Dx, n);
+        free_rows((void **)p->Dy, n);
+        free_rows((void **)p->Dz, n);
+        free_rows((void **)p->lap, n);
+        free_rows((void **)p->lap_Poison, n);
+        free_rows((void **)p->restr_mat, n);
+        free_rows((void **)p->prol_mat, n);
+    }
+    std::free(ps);
+}
+
+// structures.h:212-226: every member array (the reference's version frees
+// only eleven of them)
+void free_field(FieldVariables *field, int num_levels)
+{
+    if (!field) return;
+    for (int l = 0; l < num_levels; l++) {
+        FieldVariables *f = &field[l];
+        double *arrs[] = {f->u, f->v, f->w, f->p, f->u_new, f->v_new, f->w_new, f->u_old, f->v_old, f->w_old,
+                          f->p_old, f->pprime, f->res, f->source, f->T, f->dpdn, f->dpdx, f->dpdy, f->dpdz};
+        for (double *a : arrs) std::free(a);
+    }
+    std::free(field);
+}
+
 }  // extern "C"
