@@ -28,6 +28,7 @@ struct Level {
     // row's slots sorted by neighbour index, [k][ld4] (rows padded to a
     // multiple of 4 with zero weights), indices in sidx
     DBuf<double> A64, dinv64;
+    DBuf<double> A64s;  // FP64 copy in the sorted slot order of A32, [k][ld4] (compact FP64 V-cycle)
     DBuf<float> A32, dinv32;
     DBuf<int> sidx;
     int ld4 = 0;

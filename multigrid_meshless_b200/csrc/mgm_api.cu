@@ -151,27 +151,37 @@ __global__ void k_make_offsets(int n, int ld, int k, const int *__restrict__ gid
 // The FP32 solver operator with each row's slots sorted by neighbour index
 // (consecutive rows then gather from nearby addresses in the same slot), [k][ld]
 // with ld >= n a multiple of 4; padding rows get weight 0 and index 0.
+// The same sort gives the FP64 copy of the compact FP64 V-cycle (A64s, the
+// level's slot order permuted the same way).
 __global__ void __launch_bounds__(128) k_sort_slots(int n, int k, int ld, const int *__restrict__ idx,
                                                     const double *__restrict__ A64, int *__restrict__ sidx,
-                                                    float *__restrict__ A32)
+                                                    float *__restrict__ A32, double *__restrict__ A64s)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ld) return;
     if (i >= n) {
-        for (int j = 0; j < k; j++) { sidx[(long)j * ld + i] = 0; A32[(long)j * ld + i] = 0.f; }
+        for (int j = 0; j < k; j++) {
+            sidx[(long)j * ld + i] = 0;
+            A32[(long)j * ld + i] = 0.f;
+            A64s[(long)j * ld + i] = 0.0;
+        }
         return;
     }
     int c[kMaxK];
-    float a[kMaxK];
+    short src[kMaxK];
     for (int j = 0; j < k; j++) {
         const int cj = idx[(long)j * n + i];
-        const float aj = (float)A64[(long)j * n + i];
         int p = j;
-        while (p > 0 && c[p - 1] > cj) { c[p] = c[p - 1]; a[p] = a[p - 1]; p--; }
+        while (p > 0 && c[p - 1] > cj) { c[p] = c[p - 1]; src[p] = src[p - 1]; p--; }
         c[p] = cj;
-        a[p] = aj;
+        src[p] = (short)j;
     }
-    for (int j = 0; j < k; j++) { sidx[(long)j * ld + i] = c[j]; A32[(long)j * ld + i] = a[j]; }
+    for (int j = 0; j < k; j++) {
+        const double a = A64[(long)src[j] * n + i];
+        sidx[(long)j * ld + i] = c[j];
+        A32[(long)j * ld + i] = (float)a;
+        A64s[(long)j * ld + i] = a;
+    }
 }
 
 // FP16 operator of the half-operator V-cycle (k_level_h4).  Interior row i's
@@ -327,6 +337,13 @@ std::vector<SolveLevel<double>> solve_levels<double>(mgm_ctx *c)
         S.kr = l > 0 ? c->L[l - 1].k : 0; S.r_idx = L.s_r_idx.p; S.r_w = L.s_r_w64.p;
         S.kp = l < c->nl - 1 ? c->L[l + 1].k : 0; S.p_idx = L.s_p_idx.p; S.p_w = L.s_p_w64.p;
         S.lmax = L.lmax;
+        if (c->compact) {
+            // the FP32 path's layout with FP64 weights: slots sorted by
+            // neighbour, int16 offsets, four rows per thread on large levels
+            if (L.off_ok) { S.ld = L.ld4; S.idx = L.sidx.p; S.A = L.A64s.p; S.off = L.off16.p; }
+            S.r_off = L.r_off_ok ? L.r_off16.p : nullptr; S.r_base = L.rpts.p;
+            S.p_off = L.p_off_ok ? L.p_off16.p : nullptr; S.p_base = L.ppts.p;
+        }
         out.push_back(S);
     }
     return out;
@@ -1297,11 +1314,13 @@ void prepare_solver(mgm_ctx *c)
         const size_t nk = (size_t)L.n * L.k;
         L.ld4 = (L.n + 3) & ~3;
         const size_t nk4 = (size_t)L.ld4 * L.k;
-        L.A64.alloc(nk); L.A32.alloc(nk4); L.sidx.alloc(nk4); L.dinv64.alloc(L.n); L.dinv32.alloc(L.n);
+        L.A64.alloc(nk); L.A32.alloc(nk4); L.A64s.alloc(nk4); L.sidx.alloc(nk4); L.dinv64.alloc(L.n);
+        L.dinv32.alloc(L.n);
         k_pin_operator<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.lapP.p, L.A64.p, L.dinv64.p,
                                                                L.dinv32.p);
         MGM_LAUNCHED();
-        k_sort_slots<<<blocks_for(L.ld4, 128), 128, 0, s>>>(L.n, L.k, L.ld4, L.idx.p, L.A64.p, L.sidx.p, L.A32.p);
+        k_sort_slots<<<blocks_for(L.ld4, 128), 128, 0, s>>>(L.n, L.k, L.ld4, L.idx.p, L.A64.p, L.sidx.p, L.A32.p,
+                                                            L.A64s.p);
         MGM_LAUNCHED();
         std::vector<uint8_t> hb(L.n);
         L.btag.download(hb.data(), L.n, s);
@@ -1383,10 +1402,16 @@ void prepare_solver(mgm_ctx *c)
         for (DBuf<double> *b : {&L.p, &L.ptmp, &L.src, &L.res, &L.r64, &L.e64, &L.e64b, &L.d64, &L.q64}) { b->alloc(L.n); b->zero(s); }
         for (DBuf<float> *b : {&L.r32, &L.e32, &L.e32b, &L.d32, &L.q32}) { b->alloc(L.n); b->zero(s); }
     }
-    for (int l = 0; l < c->nl - 1; l++) {
-        auto lv = solve_levels<double>(c);
-        estimate_lmax<double>(lv[l], s);
-        c->L[l].lmax = lv[l].lmax;
+    {
+        // the power iteration reads the operator in the level's own slot order
+        const bool compact = c->compact;
+        c->compact = false;
+        for (int l = 0; l < c->nl - 1; l++) {
+            auto lv = solve_levels<double>(c);
+            estimate_lmax<double>(lv[l], s);
+            c->L[l].lmax = lv[l].lmax;
+        }
+        c->compact = compact;
     }
     Level &Lc = c->L[c->nl - 1];
     MGM_REQUIRE(Lc.n <= 8192, "mgm_setup: coarsest level too large for the dense solve (use more levels)");

@@ -129,15 +129,15 @@ __global__ void __launch_bounds__(256) k_prolong(int n, int k, const int *__rest
 // compact FP32 path: FP32 weights, neighbours stored as int16 offsets c - base
 // (6 bytes per stencil slot instead of 8)
 // ---------------------------------------------------------------------------
-template <class X>
-__device__ __forceinline__ float ell_row_dot_o(const short *__restrict__ off, const float *__restrict__ A,
-                                               const X *__restrict__ x, long n, int k, long i, int base)
+template <class T, class X>
+__device__ __forceinline__ T ell_row_dot_o(const short *__restrict__ off, const T *__restrict__ A,
+                                           const X *__restrict__ x, long n, int k, long i, int base)
 {
-    float s = 0.f;
+    T s = T(0);
     int j = 0;
     for (; j + 8 <= k; j += 8) {
         int c[8];
-        float a[8];
+        T a[8];
 #pragma unroll
         for (int q = 0; q < 8; q++) {
             const long o = (long)(j + q) * n + i;
@@ -145,82 +145,96 @@ __device__ __forceinline__ float ell_row_dot_o(const short *__restrict__ off, co
             a[q] = __ldg(A + o);
         }
 #pragma unroll
-        for (int q = 0; q < 8; q++) s += a[q] * (float)__ldg(x + c[q]);
+        for (int q = 0; q < 8; q++) s += a[q] * (T)__ldg(x + c[q]);
     }
     for (; j < k; j++) {
         const long o = (long)j * n + i;
-        s += A[o] * (float)x[base + (int)off[o]];
+        s += A[o] * (T)x[base + (int)off[o]];
     }
     return s;
 }
 
-// Compact level kernels (FP32 weights, int16 offsets, ELL [k][ld]).
+// Compact level kernels (FP32 or FP64 weights, int16 offsets, ELL [k][ld],
+// each row's slots sorted by neighbour index).
 //
 // k_level_v4: four consecutive rows per thread; the weights and offsets of
-// rows i0..i0+3 come in as one 16-byte and one 8-byte load per stencil slot
-// (ld a multiple of 4; streamed past L1 with evict-first loads), so a thread
-// has 8 operator loads and 16 gathers in flight per 4 slots.  For the large
-// levels, which are bandwidth-bound.
+// rows i0..i0+3 come in as one 16-byte (FP32; two for FP64) and one 8-byte
+// load per stencil slot (ld a multiple of 4; streamed past L1 with
+// evict-first loads), so a thread has 8 operator loads and 16 gathers in
+// flight per 4 slots.  For the large levels, which are bandwidth-bound.
 // k_level_c1: one row per thread, for the small levels, which are latency-
 // bound and need the threads more than the wide loads.
-// Each row's sum runs in slot order in both, as in every other FP32 level
-// kernel, so all of them give the same bits.  MODE 0: Chebyshev step
-// q = r - A e, d = c1 d + c2 D^-1 q, e' = e + d on interior rows (boundary
-// rows copy e); MODE 1: residual q = r - A e on interior rows, 0 on boundary rows.
-template <int MODE>
-__device__ __forceinline__ void level_row_out(int i, float s, const float *__restrict__ dinv,
-                                              const uint8_t *__restrict__ btag, const float *__restrict__ r,
-                                              const float *__restrict__ e, float *__restrict__ out,
-                                              float *__restrict__ d, float c1, float c2, int first)
+// Each row's sum runs in slot order in both, as in every other level kernel
+// of the same precision, so all of them give the same bits.  MODE 0:
+// Chebyshev step q = r - A e, d = c1 d + c2 D^-1 q, e' = e + d on interior
+// rows (boundary rows copy e); MODE 1: residual q = r - A e on interior rows,
+// 0 on boundary rows.
+template <int MODE, class T>
+__device__ __forceinline__ void level_row_out(int i, T s, const T *__restrict__ dinv,
+                                              const uint8_t *__restrict__ btag, const T *__restrict__ r,
+                                              const T *__restrict__ e, T *__restrict__ out,
+                                              T *__restrict__ d, T c1, T c2, int first)
 {
     if (MODE == 0) {
-        const float ei = e[i];
+        const T ei = e[i];
         if (btag[i]) { out[i] = ei; return; }
-        const float q = r[i] - s;
-        const float di = first ? c2 * dinv[i] * q : c1 * d[i] + c2 * dinv[i] * q;
+        const T q = r[i] - s;
+        const T di = first ? c2 * dinv[i] * q : c1 * d[i] + c2 * dinv[i] * q;
         d[i] = di;
         out[i] = ei + di;
     } else {
-        out[i] = btag[i] ? 0.f : r[i] - s;
+        out[i] = btag[i] ? T(0) : r[i] - s;
     }
 }
 
-template <int MODE>
+template <int MODE, class T>
 __global__ void __launch_bounds__(256) k_level_c1(int n, int ld, int k, const short *__restrict__ off,
-                                                  const float *__restrict__ A, const float *__restrict__ dinv,
-                                                  const uint8_t *__restrict__ btag, const float *__restrict__ r,
-                                                  const float *__restrict__ e, float *__restrict__ out,
-                                                  float *__restrict__ d, float c1, float c2, int first)
+                                                  const T *__restrict__ A, const T *__restrict__ dinv,
+                                                  const uint8_t *__restrict__ btag, const T *__restrict__ r,
+                                                  const T *__restrict__ e, T *__restrict__ out,
+                                                  T *__restrict__ d, T c1, T c2, int first)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (btag[i]) {
-        out[i] = MODE == 0 ? e[i] : 0.f;
+        out[i] = MODE == 0 ? e[i] : T(0);
         return;
     }
-    level_row_out<MODE>(i, ell_row_dot_o(off, A, e, ld, k, i, i), dinv, btag, r, e, out, d, c1, c2, first);
+    level_row_out<MODE, T>(i, ell_row_dot_o(off, A, e, ld, k, i, i), dinv, btag, r, e, out, d, c1, c2, first);
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(256, 4) k_level_v4(int n, int ld, int k, const short *__restrict__ off,
-                                                  const float *__restrict__ A, const float *__restrict__ dinv,
-                                                  const uint8_t *__restrict__ btag, const float *__restrict__ r,
-                                                  const float *__restrict__ e, float *__restrict__ out,
-                                                  float *__restrict__ d, float c1, float c2, int first)
+// the four weights of rows i0..i0+3 in slot o (evict-first)
+__device__ __forceinline__ void load4(const float *A, long o, float (&a)[4])
+{
+    const float4 v = __ldcs(reinterpret_cast<const float4 *>(A + o));
+    a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
+}
+__device__ __forceinline__ void load4(const double *A, long o, double (&a)[4])
+{
+    const double2 v0 = __ldcs(reinterpret_cast<const double2 *>(A + o));
+    const double2 v1 = __ldcs(reinterpret_cast<const double2 *>(A + o + 2));
+    a[0] = v0.x; a[1] = v0.y; a[2] = v1.x; a[3] = v1.y;
+}
+
+// FP32: 4 CTAs of 256 per SM (64 registers); FP64: 3 (twice the weight registers)
+template <int MODE, class T>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) k_level_v4(
+    int n, int ld, int k, const short *__restrict__ off, const T *__restrict__ A, const T *__restrict__ dinv,
+    const uint8_t *__restrict__ btag, const T *__restrict__ r, const T *__restrict__ e, T *__restrict__ out,
+    T *__restrict__ d, T c1, T c2, int first)
 {
     const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
     if (i0 >= n) return;
-    float s[4] = {0.f, 0.f, 0.f, 0.f};
+    T s[4] = {T(0), T(0), T(0), T(0)};
     int j = 0;
     for (; j + 4 <= k; j += 4) {
-        float a[4][4];
+        T a[4][4];
         int c[4][4];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const long o = (long)(j + q) * ld + i0;
-            const float4 av = __ldcs(reinterpret_cast<const float4 *>(A + o));
+            load4(A, o, a[q]);
             const uint2 ov = __ldcs(reinterpret_cast<const uint2 *>(off + o));
-            a[q][0] = av.x; a[q][1] = av.y; a[q][2] = av.z; a[q][3] = av.w;
             c[q][0] = i0 + (int)(short)(ov.x & 0xffffu);
             c[q][1] = i0 + 1 + (int)(short)(ov.x >> 16);
             c[q][2] = i0 + 2 + (int)(short)(ov.y & 0xffffu);
@@ -241,7 +255,7 @@ __global__ void __launch_bounds__(256, 4) k_level_v4(int n, int ld, int k, const
     }
 #pragma unroll
     for (int v = 0; v < 4; v++)
-        if (i0 + v < n) level_row_out<MODE>(i0 + v, s[v], dinv, btag, r, e, out, d, c1, c2, first);
+        if (i0 + v < n) level_row_out<MODE, T>(i0 + v, s[v], dinv, btag, r, e, out, d, c1, c2, first);
 }
 
 // k_level_h4: k_level_v4 on the FP16 operator W ~ D^-1 A, four rows per
@@ -334,37 +348,42 @@ __global__ void __launch_bounds__(256, 4) k_level_h4(int n, int ld, int k, const
     }
 }
 
-template <int MODE>
-static void launch_compact(const SolveLevel<float> &L, const float *e, float *out, float c1, float c2, int first,
-                           cudaStream_t s)
+template <int MODE, class T>
+static void launch_compact(const SolveLevel<T> &L, const T *e, T *out, T c1, T c2, int first, cudaStream_t s)
 {
-    if (L.W16)
-        launch_k(k_level_h4<MODE>, blocks_for(L.ldi / 4, 256), 256, 0, s, L.n, L.ldi, L.k, L.W16, L.dinv, L.btag,
-                 L.r, e, out, L.d, c1, c2, first);
-    else if (L.n >= kVecMinRows)
-        launch_k(k_level_v4<MODE>, blocks_for((L.n + 3) / 4, 256), 256, 0, s, L.n, L.ld, L.k, L.off, L.A, L.dinv,
+    if constexpr (sizeof(T) == 4) {
+        if (L.W16) {
+            launch_k(k_level_h4<MODE>, blocks_for(L.ldi / 4, 256), 256, 0, s, L.n, L.ldi, L.k, L.W16, L.dinv, L.btag,
+                     L.r, e, out, L.d, c1, c2, first);
+            return;
+        }
+    }
+    if (L.n >= kVecMinRows)
+        launch_k(k_level_v4<MODE, T>, blocks_for((L.n + 3) / 4, 256), 256, 0, s, L.n, L.ld, L.k, L.off, L.A, L.dinv,
                  L.btag, L.r, e, out, L.d, c1, c2, first);
     else
-        launch_k(k_level_c1<MODE>, blocks_for(L.n, 256), 256, 0, s, L.n, L.ld, L.k, L.off, L.A, L.dinv, L.btag,
+        launch_k(k_level_c1<MODE, T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.ld, L.k, L.off, L.A, L.dinv, L.btag,
                  L.r, e, out, L.d, c1, c2, first);
 }
 
+template <class T>
 __global__ void __launch_bounds__(256) k_restrict_o(int n, int k, const short *__restrict__ off,
-                                                    const int *__restrict__ base, const float *__restrict__ rw,
-                                                    const uint8_t *__restrict__ btag, const float *__restrict__ qf,
-                                                    float *__restrict__ rc)
+                                                    const int *__restrict__ base, const T *__restrict__ rw,
+                                                    const uint8_t *__restrict__ btag, const T *__restrict__ qf,
+                                                    T *__restrict__ rc)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    if (btag[i] || i == 0) { rc[i] = 0.f; return; }
+    if (btag[i] || i == 0) { rc[i] = T(0); return; }
     rc[i] = ell_row_dot_o(off, rw, qf, n, k, i, base[i]);
 }
 
+template <class T>
 __global__ void __launch_bounds__(256) k_prolong_o(int n, int k, const short *__restrict__ off,
-                                                   const int *__restrict__ base, const float *__restrict__ pw,
-                                                   const float *__restrict__ ec, float *__restrict__ ef)
+                                                   const int *__restrict__ base, const T *__restrict__ pw,
+                                                   const T *__restrict__ ec, T *__restrict__ ef)
 {
-    __shared__ float shift;
+    __shared__ T shift;
     if (threadIdx.x == 0) shift = ell_row_dot_o(off, pw, ec, n, k, 0, base[0]);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -745,15 +764,16 @@ static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, 
             rho = rn;
         }
         if (prof) prof->mark(s);
+        bool done = false;
         if constexpr (sizeof(T) == 4) {
             if (L.At) {
                 launch_tiled<0>(L, L.e, L.e2, (float)c1, (float)c2, step == 0 ? 1 : 0, s);
-            } else if (L.off) {
-                launch_compact<0>(L, L.e, L.e2, (float)c1, (float)c2, step == 0 ? 1 : 0, s);
-            } else {
-                launch_k(k_cheb<T>, nb, 256, 0, s, L.n, L.ld, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d,
-                         (T)c1, (T)c2, step == 0 ? 1 : 0);
+                done = true;
             }
+        }
+        if (done) {
+        } else if (L.off) {
+            launch_compact<0, T>(L, L.e, L.e2, (T)c1, (T)c2, step == 0 ? 1 : 0, s);
         } else {
             launch_k(k_cheb<T>, nb, 256, 0, s, L.n, L.ld, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d,
                      (T)c1, (T)c2, step == 0 ? 1 : 0);
@@ -777,31 +797,28 @@ static void vcycle_rec(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs,
     }
     smooth(L, deg, ratio, true, s, lp);  // from e = 0
     SolveLevel<T> &C = Ls[l + 1];
+    bool tiled = false;
     if constexpr (sizeof(T) == 4) {
-        if (L.At) launch_tiled<1>(L, L.e, L.q, 0.f, 0.f, 0, s);
-        else {
-            if (L.off)
-                launch_compact<1>(L, L.e, L.q, 0.f, 0.f, 0, s);
-            else
-                launch_k(k_residual<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.ld, L.k, L.idx, L.A, L.btag, L.r, L.e,
-                         L.q);
+        if (L.At) {
+            launch_tiled<1>(L, L.e, L.q, 0.f, 0.f, 0, s);
+            tiled = true;
         }
-        if (C.r_off)
-            launch_k(k_restrict_o, blocks_for(C.n, 256), 256, 0, s, C.n, C.kr, C.r_off, C.r_base, C.r_w, C.btag, L.q,
-                     C.r);
-        else
-            launch_k(k_restrict<T>, blocks_for(C.n, 256), 256, 0, s, C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
+    }
+    if (tiled) {
+    } else if (L.off) {
+        launch_compact<1, T>(L, L.e, L.q, T(0), T(0), 0, s);
     } else {
         launch_k(k_residual<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.ld, L.k, L.idx, L.A, L.btag, L.r, L.e, L.q);
-        launch_k(k_restrict<T>, blocks_for(C.n, 256), 256, 0, s, C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
     }
+    if (C.r_off)
+        launch_k(k_restrict_o<T>, blocks_for(C.n, 256), 256, 0, s, C.n, C.kr, C.r_off, C.r_base, C.r_w, C.btag, L.q,
+                 C.r);
+    else
+        launch_k(k_restrict<T>, blocks_for(C.n, 256), 256, 0, s, C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
     vcycle_rec(Ls, cs, l + 1, deg, ratio, s, prof);
-    bool poff = false;
-    if constexpr (sizeof(T) == 4) poff = L.p_off != nullptr;
-    if (poff) {
-        if constexpr (sizeof(T) == 4)
-            launch_k(k_prolong_o, blocks_for(L.n, 256), 256, 0, s, L.n, L.kp, L.p_off, L.p_base, L.p_w,
-                     (const float *)C.e, L.e);
+    if (L.p_off) {
+        launch_k(k_prolong_o<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.kp, L.p_off, L.p_base, L.p_w,
+                 (const T *)C.e, L.e);
     } else {
         launch_k(k_prolong<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.kp, L.p_idx, L.p_w, (const T *)C.e, L.e);
     }

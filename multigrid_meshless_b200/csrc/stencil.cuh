@@ -75,7 +75,8 @@ struct SolveLevel {
     const int *p_idx;
     const T *p_w;
     double lmax;                  // spectral radius estimate of D^-1 A on interior rows
-    // compact indices (FP32 path only; each used when non-null): neighbours as
+    // compact indices (each used when non-null; A then holds each row's slots
+    // sorted by neighbour index, [k][ld], ld a multiple of 4): neighbours as
     // int16 offsets c - i [k][ld]; transfer gathers as int16 offsets from a
     // per-row base node (restriction: rpts, prolongation: ppts)
     const short *off = nullptr;
