@@ -466,22 +466,40 @@ MGM_API int mgm_profile_read(mgm_ctx *ctx, double *ms_total, long long *launches
 /* ------------------------------------------------------------------ */
 /* Learned warm start (no counterpart in the reference)                */
 /* ------------------------------------------------------------------ */
+/* The initial guess of each fractional step's Poisson solve (FP64 and
+ * FP32-IR modes).  By default (flags 0) the solve starts from the previous
+ * step's pressure, as the reference's p does.  MGM_GUESS_EXTRAPOLATE adds the
+ * direction p_prev - p_prev2 (the last pressure increment; none right after
+ * mgm_apply_bc), MGM_GUESS_LEARNED the network's predicted increment
+ * (mgm_set_warm_start); the solve starts from p_prev + sum_i c_i d_i with
+ * the coefficients that minimise the FP64 residual |b - A p|_2 (a minimal-
+ * residual step over the directions: never a larger starting residual than
+ * p_prev), then iterates to the same tolerance.  Guesses apply to mgm_step,
+ * mgm_run_steps, mgm_step_host and mgm_mpnn_collect; they need max_iters >= 4
+ * (the directions are staged in the Krylov basis).  No counterpart in the
+ * reference. */
+#define MGM_GUESS_EXTRAPOLATE 1
+#define MGM_GUESS_LEARNED 2
+MGM_API int mgm_set_initial_guess(mgm_ctx *ctx, int flags);
 /* A 4-layer message-passing network (hidden width 64, BF16 weights and
  * activations, FP32 accumulation) on the level-0 stencil graph predicts the
- * pressure increment of a Poisson solve from (b, previous p, coordinates).
- * With the warm start on, each solve first steps along the prediction with
- * the length that minimises the FP64 residual; the V-cycle-preconditioned
- * FGMRES then runs to the same tolerance as without it.
- * mgm_mpnn_init allocates it (seeded weights) and a dataset ring of
- * dataset_capacity samples; mgm_mpnn_collect runs time steps with a solver
- * mode and records (b, p_prev, p_new - p_prev); mgm_mpnn_train runs Adam on a
+ * pressure increment of a Poisson solve from (b, previous p, the last
+ * increment p_prev - p_prev2, coordinates).  With the warm start on
+ * (mgm_set_warm_start: the MGM_GUESS_LEARNED bit of mgm_set_initial_guess)
+ * each step's solve starts from the minimal-residual combination of the
+ * prediction (and, with MGM_GUESS_EXTRAPOLATE, the last increment); the
+ * V-cycle-preconditioned FGMRES then runs to the same tolerance as without
+ * it.  mgm_mpnn_init allocates it (seeded weights) and a dataset ring of
+ * dataset_capacity samples (4 n floats each); mgm_mpnn_collect runs time
+ * steps with a solver mode and records (b, p_prev, p_prev - p_prev2,
+ * p_new - p_prev), each normalised by its RMS; mgm_mpnn_train runs Adam on a
  * range of samples (losses[it] per iteration, may be NULL); mgm_mpnn_eval
  * returns the mean loss on a range.  Params: mgm_mpnn_num_params() floats. */
 MGM_API int mgm_mpnn_init(mgm_ctx *ctx, unsigned long long seed, int dataset_capacity);
 MGM_API int mgm_mpnn_num_params(void);
 MGM_API int mgm_mpnn_params(mgm_ctx *ctx, float *get, const float *set);
-MGM_API int mgm_mpnn_loss_grad(mgm_ctx *ctx, const float *b_hat, const float *p_hat, const float *target,
-                               double *loss, float *grads, float *prediction);
+MGM_API int mgm_mpnn_loss_grad(mgm_ctx *ctx, const float *b_hat, const float *p_hat, const float *dp_hat,
+                               const float *target, double *loss, float *grads, float *prediction);
 MGM_API int mgm_mpnn_collect(mgm_ctx *ctx, int mode, int nsteps);
 MGM_API int mgm_mpnn_dataset_size(mgm_ctx *ctx, int *count);
 MGM_API int mgm_mpnn_train(mgm_ctx *ctx, int first, int count, int iters, float lr, unsigned long long seed,
@@ -493,8 +511,8 @@ MGM_API int mgm_mpnn_eval(mgm_ctx *ctx, int first, int count, double *mean_loss)
 MGM_API int mgm_mpnn_set_loss(mgm_ctx *ctx, float w_mse, float w_res);
 MGM_API int mgm_set_warm_start(mgm_ctx *ctx, int enable);
 /* Fine-level Chebyshev steps applied to the learned direction before the
- * minimal-residual step (default 3; 0 = use the raw prediction), and the step
- * length the last solve took along it. */
+ * minimal-residual step (default 3; 0 = use the raw prediction), and the
+ * coefficient the last step's solve took along it. */
 MGM_API int mgm_set_warm_smoothing(mgm_ctx *ctx, int steps);
 MGM_API int mgm_last_learned_alpha(mgm_ctx *ctx, double *alpha);
 

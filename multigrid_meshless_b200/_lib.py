@@ -22,6 +22,7 @@ vp = C.c_void_p
 # status codes (include/mgm.h)
 MGM_OK, MGM_ERR_CUDA, MGM_ERR_ARG, MGM_ERR_DIVERGED, MGM_ERR_TIMEOUT, MGM_ERR_NOMEM, MGM_ERR_STATE = range(7)
 MODE_REFERENCE, MODE_FP64, MODE_FP32_IR = 0, 1, 2
+GUESS_EXTRAPOLATE, GUESS_LEARNED = 1, 2
 NOALLOC_MAX_NODES = 2097152  # MGM_NOALLOC_MAX_NODES
 BC_LID, BC_TAYLOR_COUETTE = 0, 1
 SETUP_REFERENCE_TRANSFER = 1
@@ -89,6 +90,7 @@ SIGNATURES = {
     "mgm_use_graphs": ([vp, C.c_int], C.c_int),
     "mgm_use_step_graph": ([vp, C.c_int], C.c_int),
     "mgm_solve_counters": ([vp, vp, vp, vp], C.c_int),
+    "mgm_set_initial_guess": ([vp, C.c_int], C.c_int),
     "mgm_use_compact": ([vp, C.c_int], C.c_int),
     "mgm_use_tiled": ([vp, C.c_int], C.c_int),
     "mgm_use_half_operator": ([vp, C.c_int], C.c_int),
@@ -109,7 +111,7 @@ SIGNATURES = {
     "mgm_mpnn_init": ([vp, C.c_ulonglong, C.c_int], C.c_int),
     "mgm_mpnn_num_params": ([], C.c_int),
     "mgm_mpnn_params": ([vp, vp, vp], C.c_int),
-    "mgm_mpnn_loss_grad": ([vp, vp, vp, vp, C.POINTER(C.c_double), vp, vp], C.c_int),
+    "mgm_mpnn_loss_grad": ([vp, vp, vp, vp, vp, C.POINTER(C.c_double), vp, vp], C.c_int),
     "mgm_mpnn_collect": ([vp, C.c_int, C.c_int], C.c_int),
     "mgm_mpnn_dataset_size": ([vp, C.POINTER(C.c_int)], C.c_int),
     "mgm_mpnn_train": ([vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_ulonglong, vp], C.c_int),

@@ -354,6 +354,10 @@ class Multigrid:
         check(self.L.mgm_solve_counters(self.h, C.byref(v), C.byref(c), C.byref(n)))
         return v.value, c.value, n.value
 
+    def set_initial_guess(self, flags):
+        """MGM_GUESS_* flags of the steps' Poisson solves (0: previous pressure)."""
+        check(self.L.mgm_set_initial_guess(self.h, int(flags)))
+
     def use_step_graph(self, enable=True):
         check(self.L.mgm_use_step_graph(self.h, 1 if enable else 0))
 

@@ -98,6 +98,12 @@ struct mgm_ctx {
     long long vcycles_in_solve = 0;   // V-cycles of the last solve
     double last_learned_alpha = 0;    // step length the last solve took along the learned direction
     int warm_smooth_steps = 3;        // Chebyshev steps that clean the learned direction
+    int guess_flags = 0;              // MGM_GUESS_* of the steps' solves
+    // pressure history of the fractional steps: p at the start of the running
+    // step's solve, the previous one (p_prev2 of the next step) and whether
+    // that one exists (device flag, cleared by mgm_apply_bc)
+    DBuf<double> p_start, p_hist;
+    DBuf<int> hist_ok;
     bool use_tma = false;             // tile-streamed level kernels where a level has them (else 4 rows per thread)
     bool half_operator = false;       // FP32 V-cycle reads the FP16 operator where built
     // compatible right-hand sides (mgm_set_compatible_rhs): the pinned solution
@@ -131,7 +137,8 @@ struct mgm_ctx {
     struct StepGraph {
         cudaGraph_t g = nullptr;
         cudaGraphExec_t x = nullptr;
-        bool warm = false, compat = false;
+        int guess = 0;
+        bool compat = false;
         double dt = 0;
         long long k_top = 0, k_outer = 0, k_inner = 0;
     } sg[2];

@@ -514,12 +514,32 @@ __global__ void k_fg_final(FgState *st)
     }
 }
 
-__global__ void k_fg_alpha(FgState *st, double *s2)
+__global__ void k_fg_guess(FgState *st, double *ks, int nd)
 {
-    const double q = s2[0] / s2[1];
-    const double alpha = s2[1] > 0 && isfinite(q) ? q : 0.0;
-    st->alpha = alpha;
-    s2[0] = alpha;
+    const double g0 = ks[0], G00 = ks[2];
+    double c0 = 0.0, c1 = 0.0;
+    auto one = [](double g, double G) {
+        const double q = g / G;
+        return G > 0 && isfinite(q) ? q : 0.0;
+    };
+    if (nd == 1) {
+        c0 = one(g0, G00);
+    } else {
+        const double g1 = ks[1], G01 = ks[4], G11 = ks[5];
+        const double det = G00 * G11 - G01 * G01;
+        if (!(G00 > 0)) {
+            c1 = one(g1, G11);
+        } else if (!(G11 > 0) || !(det > 1e-12 * G00 * G11)) {
+            c0 = one(g0, G00);
+        } else {
+            c0 = (G11 * g0 - G01 * g1) / det;
+            c1 = (G00 * g1 - G01 * g0) / det;
+            if (!isfinite(c0) || !isfinite(c1)) { c0 = one(g0, G00); c1 = 0.0; }
+        }
+    }
+    ks[6] = c0;
+    ks[7] = c1;
+    st->alpha = nd == 1 ? c0 : c1;
 }
 
 __global__ void k_set_scalar(double *dst, double v) { *dst = v; }
@@ -621,9 +641,9 @@ void fg_final(FgState *st, cudaStream_t s)
     k_fg_final<<<1, 1, 0, s>>>(st);
     MGM_LAUNCHED();
 }
-void fg_alpha(FgState *st, double *s2, cudaStream_t s)
+void fg_guess_coefficients(FgState *st, double *ks, int nd, cudaStream_t s)
 {
-    k_fg_alpha<<<1, 1, 0, s>>>(st, s2);
+    k_fg_guess<<<1, 1, 0, s>>>(st, ks, nd);
     MGM_LAUNCHED();
 }
 void set_scalar(double *dst, double v, cudaStream_t s)

@@ -97,8 +97,11 @@ void fg_solve_y(FgState *st, FgHandles hd, cudaStream_t s);
 template <class T>
 void fg_combine(int n, const T *Z, long ld, const FgState *st, double *x, cudaStream_t s);
 void fg_final(FgState *st, cudaStream_t s);
-// learned warm start: alpha = <r0, Ad> / <Ad, Ad> (0 when not finite) into st->alpha and s[0]
-void fg_alpha(FgState *st, double *s2, cudaStream_t s);
+// initial guess: coefficients c minimising |r0 - sum_i c_i AD_i|_2 over nd (1 or
+// 2) directions from ks[i] = AD_i . r0, ks[2 + i] = AD_i . AD_0, ks[4 + i] =
+// AD_i . AD_1, into ks[6 + i]; a zero or collinear direction is dropped; the
+// coefficient of the last direction into st->alpha
+void fg_guess_coefficients(FgState *st, double *ks, int nd, cudaStream_t s);
 void set_scalar(double *dst, double v, cudaStream_t s);
 
 }  // namespace mgm

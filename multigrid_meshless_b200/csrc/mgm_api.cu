@@ -133,6 +133,16 @@ __global__ void k_compat_apply(int n, const double *__restrict__ s, const double
     if (i < n) p[i] -= (s[1] / s[0]) * pw[i];
 }
 
+// D = p - p_hist when the history holds a previous pressure, else 0
+__global__ void k_history_direction(int n, const double *__restrict__ p, const double *__restrict__ ph,
+                                    const int *__restrict__ ok, double *__restrict__ d)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) d[i] = *ok ? p[i] - ph[i] : 0.0;
+}
+
+__global__ void k_set_flag(int *flag, int v) { *flag = v; }
+
 // int16 offsets of a gather index from a per-row base node (base = nullptr: the row itself)
 // ELL [k][ld] int16 offsets gidx - base (base: per-row node, or the row itself);
 // padding rows (n <= i < ld) get offset 0
@@ -410,7 +420,7 @@ std::vector<RefLevel> ref_levels(mgm_ctx *c)
 namespace mgm {
 bool warm_start_enabled(mgm_ctx *c);
 template <class T>
-void warm_direction(mgm_ctx *c, const double *b, const double *p, T *out, cudaStream_t s);
+void warm_direction(mgm_ctx *c, const double *b, const double *p, const double *dp, T *out, cudaStream_t s);
 void destroy_mpnn(mgm_ctx *c);
 }  // namespace mgm
 
@@ -619,44 +629,58 @@ void restart_cycle(FgRun<T> &R, cudaStream_t s, FgHandles hd, bool captured, lon
     fg_combine<T>(R.n, R.Z, R.ld, R.st, R.p, s);
 }
 
-// The learned warm start.  The network's increment d carries BF16-level
-// grid-scale noise that the Laplacian amplifies, so it is first cleaned by
-// Chebyshev smoothing of A e = b - A (p + d) on the fine level (d <- d + e),
-// then p += alpha d with alpha minimising |b - A (p + alpha d)|_2 (never worse
-// than p).  The FGMRES then runs unchanged to the tolerance.  Every scalar
-// stays on the device.
+// The initial guess of a step's solve (mgm_set_initial_guess).  Directions,
+// staged in the Krylov basis: D0 = p - p_hist, the last pressure increment
+// (zero when there is no history), and with the learned guess D1 = the
+// network's predicted increment.  The network's output carries BF16-level
+// grid-scale noise that the Laplacian amplifies, so D1 is first cleaned by
+// Chebyshev smoothing of A e = b - A (p + D1) on the fine level (D1 += e).
+// Then p += D c with c minimising |b - A (p + D c)|_2 (normal equations of
+// the 1 or 2 columns A D; a zero or collinear column is dropped), which is
+// never worse than p itself; the FGMRES then runs unchanged to the
+// tolerance.  Every scalar stays on the device.
 template <class T>
-void warm_start(FgRun<T> &R, cudaStream_t s)
+void initial_guess(FgRun<T> &R, bool learned, cudaStream_t s)
 {
     mgm_ctx *c = R.c;
     Level &L0 = c->L[0];
     const int n = R.n, k = R.k;
     const long ld = R.ld;
-    double *d = c->wdir.p, *r0 = R.V, *Ad = c->wv.p, *pd = R.V + ld;
-    warm_direction<double>(c, R.b, R.p, d, s);
-    if (c->warm_smooth_steps > 0) {
-        copy_out<double>(n, R.p, pd, s);
-        set_scalar(c->kscal.p, 1.0, s);
-        combine<double>(n, 1, d, ld, c->kscal.p, pd, s);                 // pd = p + d
-        resid64(n, k, L0.idx.p, L0.A64.p, R.b, pd, r0, c->kpart.p, s);   // r0 = b - A (p + d)
-        copy_convert<T>(n, r0, R.levels[0].r, s);
-        const T *e = smooth_from_zero<T>(R.levels[0], c->warm_smooth_steps, c->cheb_ratio, s);
-        combine<T>(n, 1, e, ld, c->kscal.p, d, s);                      // d += e
+    double *r0 = R.V, *D0 = R.V + ld, *D1 = R.V + 2 * ld, *AD0 = R.V + 3 * ld, *AD1 = R.V + 4 * ld;
+    double *ks = c->kscal.p;
+    const int nd = learned ? 2 : 1;
+    k_history_direction<<<blocks_for(n, 256), 256, 0, s>>>(n, R.p, c->p_hist.p, c->hist_ok.p, D0);
+    MGM_LAUNCHED();
+    if (learned) {
+        warm_direction<double>(c, R.b, R.p, D0, D1, s);
+        if (c->warm_smooth_steps > 0) {
+            double *pd = AD0;
+            copy_out<double>(n, R.p, pd, s);
+            set_scalar(ks, 1.0, s);
+            combine<double>(n, 1, D1, ld, ks, pd, s);                        // pd = p + D1
+            resid64(n, k, L0.idx.p, L0.A64.p, R.b, pd, r0, c->kpart.p, s);    // r0 = b - A (p + D1)
+            copy_convert<T>(n, r0, R.levels[0].r, s);
+            const T *e = smooth_from_zero<T>(R.levels[0], c->warm_smooth_steps, c->cheb_ratio, s);
+            combine<T>(n, 1, e, ld, ks, D1, s);                              // D1 += e
+        }
     }
     resid64(n, k, L0.idx.p, L0.A64.p, R.b, R.p, r0, c->kpart.p, s);
-    apply64<double>(n, k, L0.idx.p, L0.A64.p, d, Ad, s);
-    multidot(n, 1, r0, ld, Ad, c->kpart.p, c->kscal.p, s);
-    multidot(n, 1, Ad, ld, Ad, c->kpart.p, c->kscal.p + 1, s);
-    fg_alpha(R.st, c->kscal.p, s);
-    combine<double>(n, 1, d, ld, c->kscal.p, R.p, s);
+    apply64<double>(n, k, L0.idx.p, L0.A64.p, D0, AD0, s);
+    if (learned) apply64<double>(n, k, L0.idx.p, L0.A64.p, D1, AD1, s);
+    multidot(n, nd, AD0, ld, r0, c->kpart.p, ks, s);             // ks[i] = AD_i . r0
+    multidot(n, nd, AD0, ld, AD0, c->kpart.p, ks + 2, s);        // ks[2 + i] = AD_i . AD0
+    if (learned) multidot(n, nd, AD0, ld, AD1, c->kpart.p, ks + 4, s);  // ks[4 + i] = AD_i . AD1
+    fg_guess_coefficients(R.st, ks, nd, s);                      // ks[6 .. 6 + nd)
+    combine<double>(n, nd, D0, ld, ks + 6, R.p, s);
 }
 
 // Enqueues the solve on c->s.  captured: c->s is capturing a graph and the
 // loops become conditional nodes (kernel counts of the loop bodies into
 // k_outer / k_inner); else host loops, and the result is checked here.
+// guesses: the step's initial guess (mgm_set_initial_guess) is applied first.
 template <class T>
 void fgmres(mgm_ctx *c, const double *b, double *p, bool captured = false, long long *k_outer = nullptr,
-            long long *k_inner = nullptr)
+            long long *k_inner = nullptr, bool guesses = false)
 {
     cudaStream_t s = c->s;
     Level &L0 = c->L[0];
@@ -676,7 +700,10 @@ void fgmres(mgm_ctx *c, const double *b, double *p, bool captured = false, long 
     R.p = p;
     const int m = std::min(c->max_iters, kMaxKrylov);
     fg_init(R.st, m, c->max_iters * (kMaxRestarts + 1), kMaxRestarts, c->tol, s);
-    if (warm_start_enabled(c)) warm_start<T>(R, s);
+    if (guesses) {
+        MGM_REQUIRE(m >= 4, "initial guesses need max_iters >= 4 (their directions are staged in the Krylov basis)");
+        initial_guess<T>(R, warm_start_enabled(c), s);
+    }
     FgHandles hd;
     if (captured) {
         hd.use = 1;
@@ -765,8 +792,10 @@ void ensure_compat(mgm_ctx *c)
 // The Poisson solve of a step on L0.src -> L0.p.  captured: enqueued into a
 // graph being captured on c->s (the loops as conditional nodes, kernel counts
 // of the loop bodies into k_outer / k_inner).
+// step: a fractional step's solve, which applies the initial guess of
+// mgm_set_initial_guess and keeps the pressure history
 void poisson(mgm_ctx *c, int mode, bool timple = false, bool captured = false, long long *k_outer = nullptr,
-             long long *k_inner = nullptr)
+             long long *k_inner = nullptr, bool step = false)
 {
     Level &L0 = c->L[0];
     if (mode == MGM_MODE_REFERENCE) {
@@ -783,8 +812,16 @@ void poisson(mgm_ctx *c, int mode, bool timple = false, bool captured = false, l
     copy_out<double>(L0.n, L0.src.p, c->bvec.p, c->s);
     k_zero_pinned<<<1, 1, 0, c->s>>>(c->bvec.p);
     MGM_LAUNCHED();
-    if (mode == MGM_MODE_FP64) fgmres<double>(c, c->bvec.p, L0.p.p, captured, k_outer, k_inner);
-    else fgmres<float>(c, c->bvec.p, L0.p.p, captured, k_outer, k_inner);
+    const bool guesses = step && c->guess_flags != 0 && !c->warm_suspended;
+    if (step) copy_out<double>(L0.n, L0.p.p, c->p_start.p, c->s);
+    if (mode == MGM_MODE_FP64) fgmres<double>(c, c->bvec.p, L0.p.p, captured, k_outer, k_inner, guesses);
+    else fgmres<float>(c, c->bvec.p, L0.p.p, captured, k_outer, k_inner, guesses);
+    if (step) {
+        // the pressure this solve started from is p_prev2 of the next step
+        copy_out<double>(L0.n, c->p_start.p, c->p_hist.p, c->s);
+        k_set_flag<<<1, 1, 0, c->s>>>(c->hist_ok.p, 1);
+        MGM_LAUNCHED();
+    }
     if (c->compat) {
         k_row0_residual<<<1, 32, 0, c->s>>>(L0.n, L0.k, L0.idx.p, L0.lapP.p, L0.src.p, L0.p.p, c->compat_s.p + 1);
         MGM_LAUNCHED();
@@ -809,7 +846,7 @@ void step_kernels(mgm_ctx *c, int mode, bool captured, long long *k_outer = null
     launch_momentum(a, c->dim, c->s);
     launch_divergence(a, c->dim, c->s);
     fg_time_mark(c->fg.p, 0, c->s);
-    poisson(c, mode, false, captured, k_outer, k_inner);
+    poisson(c, mode, false, captured, k_outer, k_inner, true);
     fg_time_mark(c->fg.p, 1, c->s);
     launch_correct(a, c->dim, c->partial.p, c->scal.p, c->s);
     MGM_CUDA(cudaMemcpyAsync(c->h_pinned, c->scal.p, sizeof(double), cudaMemcpyDeviceToHost, c->s));
@@ -835,8 +872,8 @@ bool step_graph_usable(mgm_ctx *c, int mode)
 mgm_ctx::StepGraph &step_graph(mgm_ctx *c, int mode)
 {
     auto &G = c->sg[mode == MGM_MODE_FP32_IR ? 1 : 0];
-    const bool warm = warm_start_enabled(c);
-    if (G.x && (G.warm != warm || G.compat != c->compat || G.dt != c->dt)) {
+    const int guess = c->guess_flags | (warm_start_enabled(c) ? 0x100 : 0);
+    if (G.x && (G.guess != guess || G.compat != c->compat || G.dt != c->dt)) {
         cudaGraphExecDestroy(G.x);
         cudaGraphDestroy(G.g);
         G = mgm_ctx::StepGraph();
@@ -862,7 +899,7 @@ mgm_ctx::StepGraph &step_graph(mgm_ctx *c, int mode)
     G.k_outer = ko;
     G.k_inner = ki;
     g_launches = before;
-    G.warm = warm;
+    G.guess = guess;
     G.compat = c->compat;
     G.dt = c->dt;
     return G;
@@ -934,6 +971,15 @@ void alloc_solver_buffers(mgm_ctx *c)
     c->Z32.alloc((size_t)m * n);
     c->wv.alloc(n);
     c->wdir.alloc(n);
+    if (c->p_start.n != (size_t)n) {
+        c->p_start.alloc(n);
+        c->p_hist.alloc(n);
+        c->p_hist.zero(c->s);
+    }
+    if (!c->hist_ok.p) {
+        c->hist_ok.alloc(1);
+        c->hist_ok.zero(c->s);
+    }
     c->bvec.alloc(n);
     c->kpart.alloc((size_t)std::max(2 * blocks_for(n, 256), (kMaxKrylov + 1) * dot_blocks(n)) + 16);
     c->kscal.alloc(3 * kMaxKrylov + 16);
@@ -1778,6 +1824,7 @@ int mgm_apply_bc(mgm_ctx *c, int kind)
             c->L[l].src.zero(s);
             c->L[l].res.zero(s);
         }
+        c->hist_ok.zero(s);  // no pressure history from rest
         Level &L = c->L[0];
         k_bc<<<blocks_for(L.n, 256), 256, 0, s>>>(L.n, kind, L.x.p, L.y.p, c->u.p, c->v.p, c->u_new.p, c->v_new.p);
         MGM_LAUNCHED();
@@ -1891,6 +1938,17 @@ int mgm_solve_counters(mgm_ctx *c, long long *vcycles, long long *cycles, long l
         if (vcycles) *vcycles = h.vcycles_total;
         if (cycles) *cycles = h.cycles_total;
         if (solves) *solves = h.solves_total;
+    });
+}
+
+int mgm_set_initial_guess(mgm_ctx *c, int flags)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE((flags & ~(MGM_GUESS_EXTRAPOLATE | MGM_GUESS_LEARNED)) == 0, "mgm_set_initial_guess: unknown flag");
+        MGM_REQUIRE(!(flags & MGM_GUESS_LEARNED) || (c->mpnn != nullptr),
+                    "mgm_set_initial_guess: the learned guess needs a network (mgm_mpnn_init)");
+        c->guess_flags = flags;
     });
 }
 

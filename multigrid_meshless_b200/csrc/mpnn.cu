@@ -2,7 +2,9 @@
 // network on the RBF-FD stencil graph, trained on the GPU by these kernels.
 //
 // Network (fixed shape): per node the inputs x_i = [b_i/rms(b), p_i/rms(p),
-// x_i, y_i, boundary tag]; encoder h0 = relu(x W_e + c_e) (5 -> 64); four
+// dp_i/rms(dp), x_i, y_i, boundary tag] with dp = p_prev - p_prev2 the last
+// pressure increment (0 when there is none); encoder h0 = relu(x W_e + c_e)
+// (6 -> 64); four
 // layers h' = relu([h_i | mean_j h_j | sum_j l_ij h_j] W_l + c_l) + h_i with
 // j over the node's stencil and l_ij = h^2 lap_ij (192 -> 64); decoder
 // y_i = h4_i . w_d + c_d.  Weights and activations are stored in BF16, every
@@ -10,10 +12,10 @@
 // (mma.sync m16n8k16 BF16 -> FP32) fused with the neighbour aggregation.
 //
 // The prediction is the shape of the pressure increment p_new - p_prev.  The
-// solve steps along it with the length that minimises the FP64 residual, then
-// runs the V-cycle-preconditioned FGMRES to the same tolerance as without it:
-// the learned guess can only lower the starting residual, never replace the
-// solver.
+// solve combines it with the extrapolation direction dp by the coefficients
+// that minimise the FP64 residual, then runs the V-cycle-preconditioned FGMRES
+// to the same tolerance as without it: the learned guess can only lower the
+// starting residual, never replace the solver.
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -23,7 +25,7 @@
 
 namespace mgm {
 
-constexpr int kH = 64, kCat = 192, kFin = 5, kLayers = 4;
+constexpr int kH = 64, kCat = 192, kFin = 6, kLayers = 4;
 constexpr int kLayerParams = kCat * kH + kH;
 constexpr int P_WE = 0, P_CE = kFin * kH, P_L0 = P_CE + kH;
 constexpr int P_WD = P_L0 + kLayers * kLayerParams, P_CD = P_WD + kH;
@@ -45,11 +47,10 @@ struct MpnnState {
     DBuf<bf16> cat[kLayers];
     DBuf<float> z[kLayers + 1];
     DBuf<float> y, dy, dH, dHin, dz, dm;
-    DBuf<double> scal;       // device scalars: [0..1] rms^2 of b, p; [2] loss
-    DBuf<float> ds;          // dataset: cap samples x 3 x n (b_hat, p_hat, target)
+    DBuf<double> scal;       // device scalars: [0..1] sum of squares of b, p; [2] loss; [5] of dp
+    DBuf<float> ds;          // dataset: cap samples x kSlot x n (b_hat, p_hat, dp_hat, target)
     int ds_cap = 0, ds_count = 0;
     int adam_t = 0;
-    bool warm = false;
     bool ready = false;
     const int *cloud = nullptr;  // level-0 cloud, row-major [n][k] (owned by the context)
 };
@@ -98,33 +99,39 @@ __device__ __forceinline__ float inv_rms(double sumsq, int n)
     return sumsq > 0 ? (float)(1.0 / sqrt(sumsq / n)) : 0.f;
 }
 
-// inference features from the solver's b and p (double)
-__global__ void k_features(int n, const double *b, const double *p, const double *ss, const double *x,
-                           const double *y, const uint8_t *btag, float *feat)
+// dataset slot: b_hat, p_hat, dp_hat, target, each n floats
+constexpr int kSlot = 4;
+
+// inference features from the solver's b, p and last increment dp (double;
+// dp may be null: no increment yet); ss: sums of squares of b, p, (dp)
+__global__ void k_features(int n, const double *b, const double *p, const double *dp, const double *ss,
+                           const double *x, const double *y, const uint8_t *btag, float *feat)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float sb = inv_rms(ss[0], n), sp = inv_rms(ss[1], n);
+    const float sb = inv_rms(ss[0], n), sp = inv_rms(ss[1], n), sd = dp ? inv_rms(ss[5], n) : 0.f;
     float *f = feat + (long)i * kFin;
     f[0] = (float)b[i] * sb;
     f[1] = (float)p[i] * sp;
-    f[2] = (float)x[i];
-    f[3] = (float)y[i];
-    f[4] = btag[i] ? 1.f : 0.f;
+    f[2] = dp ? (float)dp[i] * sd : 0.f;
+    f[3] = (float)x[i];
+    f[4] = (float)y[i];
+    f[5] = btag[i] ? 1.f : 0.f;
 }
 
 // training features from normalised dataset vectors
-__global__ void k_features_ds(int n, const float *bh, const float *ph, const double *x, const double *y,
-                              const uint8_t *btag, float *feat)
+__global__ void k_features_ds(int n, const float *bh, const float *ph, const float *dh, const double *x,
+                              const double *y, const uint8_t *btag, float *feat)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float *f = feat + (long)i * kFin;
     f[0] = bh[i];
     f[1] = ph[i];
-    f[2] = (float)x[i];
-    f[3] = (float)y[i];
-    f[4] = btag[i] ? 1.f : 0.f;
+    f[2] = dh[i];
+    f[3] = (float)x[i];
+    f[4] = (float)y[i];
+    f[5] = btag[i] ? 1.f : 0.f;
 }
 
 // encoder: warp per node, lane -> features 2l, 2l+1
@@ -543,16 +550,20 @@ __global__ void k_res_bwd(int n, int k, const int *tptr, const int *tpos, const 
     dy[j] += (float)(w_res * (-2.0 * s / Q));
 }
 
-// dataset record: slot <- (b/rms b, p/rms p, (p_new - p_prev)/rms) ; scal[0..2] = sumsq of b, p_prev, dp
-__global__ void k_record(int n, const double *b, const double *pprev, const double *pnew, const double *ss,
-                         float *slot)
+// dataset record: slot <- (b/rms b, p_prev/rms, (p_prev - p_prev2)/rms, (p_new - p_prev)/rms);
+// ss[0..1] sums of squares of b, p_prev; ss[2] of p_new - p_prev; ss[5] of p_prev - p_prev2
+// (pprev2 null: no earlier increment, dp_hat = 0)
+__global__ void k_record(int n, const double *b, const double *pprev, const double *pprev2, const double *pnew,
+                         const double *ss, float *slot)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float sb = inv_rms(ss[0], n), sp = inv_rms(ss[1], n), sd = inv_rms(ss[2], n);
+    const float sq = pprev2 ? inv_rms(ss[5], n) : 0.f;
     slot[i] = (float)b[i] * sb;
     slot[n + i] = (float)pprev[i] * sp;
-    slot[2 * n + i] = (float)(pnew[i] - pprev[i]) * sd;
+    slot[2 * n + i] = pprev2 ? (float)(pprev[i] - pprev2[i]) * sq : 0.f;
+    slot[3 * n + i] = (float)(pnew[i] - pprev[i]) * sd;
 }
 
 __global__ void k_sumsq_diff(int n, const double *a, const double *b, double *out)
@@ -688,8 +699,9 @@ MpnnState &state(mgm_ctx *c)
     return *c->mpnn;
 }
 
-// The learned direction for the current Poisson system: b (device), p (device)
-// -> out (device, precision T).  Called by the FGMRES of mgm_api.cu.
+// The learned direction for the current Poisson system: b, p and the last
+// pressure increment dp (device; dp all zero when there is none) -> out
+// (device, precision T).  Called by the FGMRES of mgm_api.cu.
 template <class T>
 __global__ void k_to_T(int n, const float *y, T *out)
 {
@@ -697,37 +709,51 @@ __global__ void k_to_T(int n, const float *y, T *out)
     if (i < n) out[i] = (T)y[i];
 }
 
-bool warm_start_enabled(mgm_ctx *c) { return c->mpnn && c->mpnn->ready && c->mpnn->warm && !c->warm_suspended; }
+bool warm_start_enabled(mgm_ctx *c)
+{
+    return c->mpnn && c->mpnn->ready && (c->guess_flags & MGM_GUESS_LEARNED) && !c->warm_suspended;
+}
 
 template <class T>
-void warm_direction(mgm_ctx *c, const double *b, const double *p, T *out, cudaStream_t s)
+void warm_direction(mgm_ctx *c, const double *b, const double *p, const double *dp, T *out, cudaStream_t s)
 {
     MpnnState &M = *c->mpnn;
     Level &L = c->L[0];
-    MGM_CUDA(cudaMemsetAsync(M.scal.p, 0, 2 * sizeof(double), s));
+    MGM_CUDA(cudaMemsetAsync(M.scal.p, 0, 6 * sizeof(double), s));
     k_sumsq2<<<red_blocks(M.n), 256, 0, s>>>(M.n, b, p, M.scal.p);
     MGM_LAUNCHED();
-    k_features<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, b, p, M.scal.p, L.x.p, L.y.p, L.btag.p, M.feat.p);
+    k_sumsq2<<<red_blocks(M.n), 256, 0, s>>>(M.n, dp, dp, M.scal.p + 4);  // [5] = |dp|^2
+    MGM_LAUNCHED();
+    k_features<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, b, p, dp, M.scal.p, L.x.p, L.y.p, L.btag.p, M.feat.p);
     MGM_LAUNCHED();
     forward(M, false, s);
     k_to_T<T><<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, M.y.p, out);
     MGM_LAUNCHED();
 }
-template void warm_direction<double>(mgm_ctx *, const double *, const double *, double *, cudaStream_t);
-template void warm_direction<float>(mgm_ctx *, const double *, const double *, float *, cudaStream_t);
+template void warm_direction<double>(mgm_ctx *, const double *, const double *, const double *, double *,
+                                     cudaStream_t);
+template void warm_direction<float>(mgm_ctx *, const double *, const double *, const double *, float *,
+                                    cudaStream_t);
 
-// record one sample (b, p_prev, p_new) into the dataset ring
-void record_sample(mgm_ctx *c, const double *b, const double *pprev, const double *pnew, cudaStream_t s)
+// record one sample (b, p_prev, p_prev - p_prev2, p_new - p_prev) into the
+// dataset ring (pprev2 null: no earlier pressure)
+void record_sample(mgm_ctx *c, const double *b, const double *pprev, const double *pprev2, const double *pnew,
+                   cudaStream_t s)
 {
     MpnnState &M = *c->mpnn;
     if (M.ds_cap == 0) return;
     const int slot = M.ds_count % M.ds_cap;
-    MGM_CUDA(cudaMemsetAsync(M.scal.p, 0, 3 * sizeof(double), s));
+    MGM_CUDA(cudaMemsetAsync(M.scal.p, 0, 6 * sizeof(double), s));
     k_sumsq2<<<red_blocks(M.n), 256, 0, s>>>(M.n, b, pprev, M.scal.p);
     MGM_LAUNCHED();
     k_sumsq_diff<<<red_blocks(M.n), 256, 0, s>>>(M.n, pnew, pprev, M.scal.p + 2);
     MGM_LAUNCHED();
-    k_record<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, b, pprev, pnew, M.scal.p, M.ds.p + (size_t)slot * 3 * M.n);
+    if (pprev2) {
+        k_sumsq_diff<<<red_blocks(M.n), 256, 0, s>>>(M.n, pprev, pprev2, M.scal.p + 5);
+        MGM_LAUNCHED();
+    }
+    k_record<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, b, pprev, pprev2, pnew, M.scal.p,
+                                                  M.ds.p + (size_t)slot * kSlot * M.n);
     MGM_LAUNCHED();
     M.ds_count++;
 }
@@ -792,7 +818,7 @@ int mgm_mpnn_init(mgm_ctx *c, unsigned long long seed, int dataset_capacity)
         M.scal.alloc(8);
         M.ds_cap = dataset_capacity;
         M.ds_count = 0;
-        if (dataset_capacity > 0) M.ds.alloc((size_t)dataset_capacity * 3 * n);
+        if (dataset_capacity > 0) M.ds.alloc((size_t)dataset_capacity * kSlot * n);
         refresh_weights(M, s);
         MGM_CUDA(cudaStreamSynchronize(s));
         M.ready = true;
@@ -823,19 +849,20 @@ int mgm_mpnn_params(mgm_ctx *c, float *get, const float *set)
     }
 }
 
-// loss and gradient for one sample given normalised host vectors (b_hat, p_hat, target)
-int mgm_mpnn_loss_grad(mgm_ctx *c, const float *b_hat, const float *p_hat, const float *target, double *loss,
-                       float *grads, float *prediction)
+// loss and gradient for one sample given normalised host vectors (b_hat, p_hat, dp_hat, target)
+int mgm_mpnn_loss_grad(mgm_ctx *c, const float *b_hat, const float *p_hat, const float *dp_hat, const float *target,
+                       double *loss, float *grads, float *prediction)
 {
     try {
         MpnnState &M = state(c);
         cudaStream_t s = c->s;
         Level &L = c->L[0];
-        DBuf<float> bh, ph, tt;
+        DBuf<float> bh, ph, dh, tt;
         bh.upload(b_hat, M.n, s);
         ph.upload(p_hat, M.n, s);
+        dh.upload(dp_hat, M.n, s);
         tt.upload(target, M.n, s);
-        k_features_ds<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, bh.p, ph.p, L.x.p, L.y.p, L.btag.p, M.feat.p);
+        k_features_ds<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, bh.p, ph.p, dh.p, L.x.p, L.y.p, L.btag.p, M.feat.p);
         MGM_LAUNCHED();
         loss_and_grad(M, tt.p, s);
         double ls = 0;
@@ -860,12 +887,14 @@ int mgm_mpnn_collect(mgm_ctx *c, int mode, int nsteps)
         MpnnState &M = state(c);
         MGM_REQUIRE(M.ds_cap > 0, "mgm_mpnn_collect: dataset capacity is zero");
         MGM_REQUIRE(mode == MGM_MODE_FP64 || mode == MGM_MODE_FP32_IR, "mgm_mpnn_collect: solver mode");
-        DBuf<double> pprev(M.n);
+        DBuf<double> pprev(M.n), pprev2(M.n);
         for (int t = 0; t < nsteps; t++) {
+            if (t > 0)
+                MGM_CUDA(cudaMemcpyAsync(pprev2.p, pprev.p, sizeof(double) * M.n, cudaMemcpyDeviceToDevice, c->s));
             MGM_CUDA(cudaMemcpyAsync(pprev.p, c->L[0].p.p, sizeof(double) * M.n, cudaMemcpyDeviceToDevice, c->s));
             int st = mgm_step(c, mode, nullptr);
             if (st != MGM_OK) return st;
-            record_sample(c, c->bvec.p, pprev.p, c->L[0].p.p, c->s);
+            record_sample(c, c->bvec.p, pprev.p, t > 0 ? pprev2.p : nullptr, c->L[0].p.p, c->s);
         }
         MGM_CUDA(cudaStreamSynchronize(c->s));
         return MGM_OK;
@@ -903,10 +932,11 @@ int mgm_mpnn_train(mgm_ctx *c, int first, int count, int iters, float lr, unsign
         for (int it = 0; it < iters; it++) {
             x ^= x << 13; x ^= x >> 7; x ^= x << 17;
             const int smp = first + (int)(x % (unsigned long long)count);
-            const float *slot = M.ds.p + (size_t)smp * 3 * M.n;
-            k_features_ds<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, slot, slot + M.n, L.x.p, L.y.p, L.btag.p, M.feat.p);
+            const float *slot = M.ds.p + (size_t)smp * kSlot * M.n;
+            k_features_ds<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, slot, slot + M.n, slot + 2 * M.n, L.x.p, L.y.p,
+                                                               L.btag.p, M.feat.p);
             MGM_LAUNCHED();
-            loss_and_grad(M, slot + 2 * M.n, s);
+            loss_and_grad(M, slot + 3 * M.n, s);
             MGM_CUDA(cudaMemcpyAsync(dl.p + it, M.scal.p + 2, sizeof(double), cudaMemcpyDeviceToDevice, s));
             adam_step(M, lr, s);
         }
@@ -931,11 +961,12 @@ int mgm_mpnn_eval(mgm_ctx *c, int first, int count, double *mean_loss)
         DBuf<float> dyv(M.n);
         double tot = 0;
         for (int q = first; q < first + count; q++) {
-            const float *slot = M.ds.p + (size_t)q * 3 * M.n;
-            k_features_ds<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, slot, slot + M.n, L.x.p, L.y.p, L.btag.p, M.feat.p);
+            const float *slot = M.ds.p + (size_t)q * kSlot * M.n;
+            k_features_ds<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, slot, slot + M.n, slot + 2 * M.n, L.x.p, L.y.p,
+                                                               L.btag.p, M.feat.p);
             MGM_LAUNCHED();
             forward(M, false, s);
-            loss_head(M, slot + 2 * M.n, s);
+            loss_head(M, slot + 3 * M.n, s);
             M.scal.download(c->h_pinned, 3, s);
             MGM_CUDA(cudaStreamSynchronize(s));
             tot += c->h_pinned[2];
@@ -966,8 +997,12 @@ int mgm_set_warm_start(mgm_ctx *c, int enable)
 {
     try {
         MGM_REQUIRE(c, "null context");
-        if (enable) state(c).warm = true;
-        else if (c->mpnn) c->mpnn->warm = false;
+        if (enable) {
+            state(c);  // a network must exist
+            c->guess_flags |= MGM_GUESS_LEARNED;
+        } else {
+            c->guess_flags &= ~MGM_GUESS_LEARNED;
+        }
         return MGM_OK;
     } catch (const Error &e) {
         set_error(e.code, e.msg);

@@ -1,7 +1,7 @@
 """CPU restatement of the learned warm-start network (TEST INFRASTRUCTURE ONLY).
 
-Mirrors csrc/mpnn.cu: inputs [b/rms(b), p/rms(p), x, y, tag] -> encoder
-(5 -> 64, relu) -> 4 layers h' = relu([h | mean_j h_j | sum_j l_ij h_j] W + c) + h
+Mirrors csrc/mpnn.cu: inputs [b/rms(b), p/rms(p), dp/rms(dp), x, y, tag]
+(dp the last pressure increment) -> encoder (6 -> 64, relu) -> 4 layers h' = relu([h | mean_j h_j | sum_j l_ij h_j] W + c) + h
 -> decoder (64 -> 1); loss mean (y - t)^2.  With bf16=True the values the GPU
 stores in BF16 (activations, aggregated features, layer weights) are rounded
 to BF16 (round to nearest even) at the same points; the backward pass treats
@@ -12,7 +12,7 @@ from __future__ import annotations
 
 import numpy as np
 
-H, CAT, FIN, LAYERS = 64, 192, 5, 4
+H, CAT, FIN, LAYERS = 64, 192, 6, 4
 LAYER_PARAMS = CAT * H + H
 P_WE, P_CE = 0, FIN * H
 P_L0 = P_CE + H

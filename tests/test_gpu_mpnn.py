@@ -41,6 +41,7 @@ def test_gradients_match_oracle(small, w_mse, w_res):
     rng = np.random.default_rng(3)
     bh = (np.sin(3 * g["x"]) * np.cos(2 * g["y"])).astype(np.float32)
     ph = (np.cos(4 * g["x"] * g["y"])).astype(np.float32)
+    dh = (np.sin(2 * g["x"] + g["y"])).astype(np.float32)
     t = (np.sin(5 * g["x"]) + 0.3 * rng.normal(size=n)).astype(np.float32)
     npar = L.mgm_mpnn_num_params()
     assert npar == MO.NUM_PARAMS
@@ -49,9 +50,9 @@ def test_gradients_match_oracle(small, w_mse, w_res):
     loss = C.c_double()
     grads = np.zeros(npar, np.float32)
     pred = np.zeros(n, np.float32)
-    _lib.check(L.mgm_mpnn_loss_grad(mg.h, bh.ctypes.data, ph.ctypes.data, t.ctypes.data, C.byref(loss),
-                                    grads.ctypes.data, pred.ctypes.data))
-    feat = np.stack([bh, ph, g["x"].astype(np.float32), g["y"].astype(np.float32),
+    _lib.check(L.mgm_mpnn_loss_grad(mg.h, bh.ctypes.data, ph.ctypes.data, dh.ctypes.data, t.ctypes.data,
+                                    C.byref(loss), grads.ctypes.data, pred.ctypes.data))
+    feat = np.stack([bh, ph, dh, g["x"].astype(np.float32), g["y"].astype(np.float32),
                      g["btag"].astype(np.float32)], axis=1)
     ops = mg.operators(0)
     A = ops["lapP"].copy()
