@@ -45,19 +45,25 @@ def parse():
     ap.add_argument("--levels", type=int, default=6)
     ap.add_argument("--k", type=int, default=30)
     ap.add_argument("--poly", type=int, default=4)
-    ap.add_argument("--Re", type=float, default=100.0)
-    ap.add_argument("--courant", type=float, default=0.5)
+    ap.add_argument("--Re", type=float, default=None,
+                    help="Reynolds number of the timed episode (default: the first held-out draw of U[100, 1000])")
+    ap.add_argument("--courant", type=float, default=0.3,
+                    help="Courant number of the learned-warm-start protocol (explicit Euler is stable at 0.3 on "
+                         "the 1M cavity; 0.5 grows within ~12 steps)")
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--cheb-degree", type=int, default=3)
     ap.add_argument("--cheb-ratio", type=float, default=20.0)
     ap.add_argument("--episode", type=int, default=10,
-                    help="steps per episode from rest (the explicit scheme is unstable beyond ~12 steps at 1M nodes)")
+                    help="steps per episode from rest of the other workloads (annulus, cube, TIMPLE)")
     ap.add_argument("--sample-m", type=int, default=128, help="cavity size of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start measurement")
     ap.add_argument("--no-half", action="store_true", help="skip the FP16-operator measurement")
-    ap.add_argument("--learn-episodes", type=int, default=12, help="training episodes (Re ~ U[100, 1000])")
-    ap.add_argument("--learn-iters", type=int, default=400, help="Adam iterations of the GPU training")
+    ap.add_argument("--train-episodes", type=int, default=10, help="training episodes from rest (Re ~ U[100, 1000])")
+    ap.add_argument("--train-steps", type=int, default=200, help="steps per training episode (2000 in all)")
+    ap.add_argument("--eval-episodes", type=int, default=2, help="held-out episodes at unseen Re")
+    ap.add_argument("--eval-steps", type=int, default=100, help="steps per held-out episode (200 in all)")
+    ap.add_argument("--learn-iters", type=int, default=2000, help="Adam iterations of the GPU training")
     ap.add_argument("--workload", choices=["cavity", "annulus", "timple", "cube", "shell-batch"], default="cavity",
                     help="cavity: the headline (1M-node cavity); annulus / cube / shell-batch: the other configs, "
                          "each printing its own line")
@@ -66,8 +72,10 @@ def parse():
 
 def workload(a):
     return {
-        "workload": f"2D lid-driven cavity, {a.m}x{a.m} jittered nodes, {a.levels} levels (/4), PHS3 + poly{a.poly}, "
-                    f"k={a.k}, Re={a.Re:g}, Courant {a.courant:g}, Poisson to {a.tol:g} rel. residual",
+        "workload": (f"2D lid-driven cavity, {a.m}x{a.m} jittered nodes, {a.levels} levels (/4), PHS3 + poly{a.poly}, "
+                     f"k={a.k}, Courant {a.courant:g}, Re ~ U[100, 1000]; learned warm start trained on "
+                     f"{a.train_episodes * a.train_steps} steps, timed on a held-out episode at Re={a.Re:g}; "
+                     f"Poisson to {a.tol:g} rel. residual"),
         "nodes": a.m * a.m - 4,
         "levels": a.levels,
         "k": a.k,
@@ -77,7 +85,8 @@ def workload(a):
         "rel_tol": a.tol,
         "l2": "inputs larger than L2 (operators + hierarchy ~2 GB per step, L2 126 MB)",
         "seed": 1,
-        "episodes": f"steps run in episodes of {a.episode} from rest (lid BC re-applied, p = 0; untimed resets)",
+        "episodes": (f"each arm: one episode from rest at Re={a.Re:g} (lid BC applied, p = 0), {a.warmup} untimed "
+                     f"steps, then the timed steps"),
     }
 
 
@@ -194,6 +203,31 @@ def reference_sample(a, steps, warmup, opt="O2"):
     return {"kind": kind, "sec_per_step": per, "nodes": cl[0].n, "levels": nl, "setup_s": setup_s, "opt": opt}
 
 
+def convergent_cpu_sample(a):
+    """The library's convergent FP64 solve restated on the CPU
+    (oracle/fgmres_oracle.c, OpenMP on every host core) on the sample cavity
+    (a.sample_m^2 nodes, 3 levels, the workload's k and polynomial degree):
+    ms per Poisson solve to a.tol from zero with a smooth source, V-cycles,
+    threads.  The reference's own solver never reaches a tolerance."""
+    import numpy as np
+
+    from multigrid_meshless_b200 import clouds
+    from oracle import oracle as O
+    cl = clouds.cavity_hierarchy(a.sample_m, 3, seed=1)
+    P = O.solver_transfer(O.orc_pipeline(cl, [a.k] * 3, [a.poly] * 3, reference_rows=False))
+    S = O.ConvergentSolver(P)
+    L = P[0]
+    b = np.where(L.btag == 0, np.cos(np.pi * L.x) * np.cos(np.pi * L.y), 0.0)
+    S.solve(b, tol=a.tol)  # warm-up
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        p, it, rr, ok = S.solve(b, tol=a.tol, cheb_degree=a.cheb_degree, cheb_ratio=a.cheb_ratio)
+    sec = (time.perf_counter() - t0) / reps
+    return {"ms_per_solve": sec * 1e3, "vcycles": it, "rel_res": rr, "converged": bool(ok), "nodes": L.n,
+            "threads": os.cpu_count()}
+
+
 def cpu_baseline_entry(a, s, full_nodes):
     """A bounded sample scaled to the metric's unit: the sample's steps/s
     times (sample nodes / workload nodes), the step's work being linear in
@@ -296,7 +330,7 @@ def ncu_traffic():
 # ---------------------------------------------------------------------------
 # step-level roofline: algorithmic bytes of every kernel of a fractional step
 # ---------------------------------------------------------------------------
-def step_bytes(sizes, dim, deg, fp32, vcycles, cycles, solves, steps):
+def step_bytes(sizes, dim, deg, fp32, vcycles, cycles, solves, steps, guesses=0):
     """Compulsory HBM bytes of `steps` fractional steps whose Poisson solves
     took `vcycles` Arnoldi steps (V-cycles) over `cycles` restart-cycle starts
     and `solves` solves: every array a kernel reads or writes counted once per
@@ -311,7 +345,11 @@ def step_bytes(sizes, dim, deg, fp32, vcycles, cycles, solves, steps):
     (re-orthogonalisation passes not counted), the normalisation; per restart
     start the true residual and V_0's scaling, per cycle the update
     p += Z y; per step momentum, divergence, correction and the solve's
-    right-hand-side copy."""
+    right-hand-side copy.  guesses: 1 adds the extrapolated initial guess
+    (history direction, its A-product, the minimal-residual dots, the update,
+    the history copies), 2 also the network's inference (features, encoder,
+    four message-passing layers with their index and weight streams and the
+    64-wide BF16 activations, decoder) and its Chebyshev cleaning."""
     s = 4 if fp32 else 8            # V-cycle vector bytes
     slot = 6 if fp32 else 12        # weight + index per stencil slot (FP32 + int16 / FP64 + int32)
     n0, _, k0 = sizes[0]
@@ -343,6 +381,17 @@ def step_bytes(sizes, dim, deg, fp32, vcycles, cycles, solves, steps):
     krylov += (cycles - solves) * (J * s * n0 + 16 * n0)          # p += Z y
     ops = 3 if dim == 2 else 4
     step = n0 * (ops * k0 * 8 + 4 * k0 + 8 * 8) + 2 * n0 * (2 * k0 * 8 + 4 * k0 + 5 * 8) + 16 * n0
+    if guesses >= 1:
+        resid = n0 * (12 * k0 + 24)
+        apply = n0 * (12 * k0 + 16)
+        step += 24 * n0 + 32 * n0 + resid + apply + 2 * 24 * n0 + 24 * n0
+    if guesses >= 2:
+        n, nb, k = sizes[0]
+        cheb = n * (k * slot + 5 * s + 1 + (s * (deg - 1) / deg))
+        bnd = nb * (k * (s + 4) + 3 * s)
+        infer = 48 * n0 + 32 * n0 + (24 + 128) * n0 + 4 * (128 + 8 * k0 + 128) * n0 + 132 * n0 + 12 * n0
+        clean = 16 * n0 + 24 * n0 + n0 * (12 * k0 + 24) + 12 * n0 + n0 * (3 * s + 1) + deg * (cheb + bnd) + 24 * n0
+        step += infer + clean + n0 * (12 * k0 + 16) + 3 * 24 * n0
     return per_vcycles + krylov + steps * step
 
 
@@ -350,66 +399,81 @@ def step_bytes(sizes, dim, deg, fp32, vcycles, cycles, solves, steps):
 # learned warm start: trained on the GPU on plain-solver episodes, evaluated on
 # held-out episodes with and without it
 # ---------------------------------------------------------------------------
-def learned_arm(a, mg, mgm, n):
+def c5_reynolds(a):
+    """Seeded Reynolds numbers ~ U[100, 1000] of the training and held-out episodes."""
+    from multigrid_meshless_b200.clouds import uniform
+    return 100.0 + 900.0 * uniform(7, 0, a.train_episodes), 100.0 + 900.0 * uniform(7, 1, a.eval_episodes)
+
+
+def c5_protocol(a, mg, mgm, seed):
+    """The learned warm start as the C5 protocol asks: the network is trained
+    on the GPU on a.train_episodes x a.train_steps fractional steps of the
+    plain solver (Re ~ U[100, 1000], every solve to the tolerance), then four
+    arms run the same a.eval_episodes x a.eval_steps held-out steps at unseen
+    Re, each from rest: plain FP64 (the previous step's pressure as the
+    initial guess), FP32-in-FP64, FP32 with the extrapolated guess
+    p_prev + c (p_prev - p_prev2), and learned + FP32 (the minimal-residual
+    combination of that direction and the network's).  Every solve still
+    V-cycles to the tolerance; pressures are compared with the FP64 arm's at
+    the end of each held-out episode."""
     import ctypes as C
 
     import numpy as np
 
     from multigrid_meshless_b200 import _lib
-    from multigrid_meshless_b200.clouds import uniform
     L = _lib.load()
-    ep_len = a.episode
-    n_train, n_eval = a.learn_episodes, 2
-    res_train = 100.0 + 900.0 * uniform(7, 0, n_train)
-    res_eval = 100.0 + 900.0 * uniform(7, 1, n_eval)
+    re_train, re_eval = c5_reynolds(a)
     t0 = time.perf_counter()
-    _lib.check(L.mgm_mpnn_init(mg.h, 1, n_train * ep_len))
-    for Re in res_train:
+    _lib.check(L.mgm_mpnn_init(mg.h, seed, a.train_episodes * a.train_steps))
+    mg.set_initial_guess(mgm.GUESS_EXTRAPOLATE)  # the guess changes no solution beyond the tolerance
+    for Re in re_train:
         mg.set_flow(Re=float(Re), courant=a.courant)
         mg.apply_bc(mgm.BC_LID)
-        _lib.check(L.mgm_mpnn_collect(mg.h, mgm.MODE_FP32_IR, ep_len))
+        _lib.check(L.mgm_mpnn_collect(mg.h, mgm.MODE_FP32_IR, a.train_steps))
     collect_s = time.perf_counter() - t0
     cnt = C.c_int()
     _lib.check(L.mgm_mpnn_dataset_size(mg.h, C.byref(cnt)))
-    n_fit = max(1, cnt.value - ep_len)
     losses = np.zeros(a.learn_iters)
     t0 = time.perf_counter()
-    _lib.check(L.mgm_mpnn_train(mg.h, 0, n_fit, a.learn_iters, 1e-3, 1, losses.ctypes.data))
+    _lib.check(L.mgm_mpnn_train(mg.h, 0, cnt.value, a.learn_iters, 1e-3, seed, losses.ctypes.data))
+    mg.sync()
     train_s = time.perf_counter() - t0
-    held = C.c_double()
-    _lib.check(L.mgm_mpnn_eval(mg.h, n_fit, cnt.value - n_fit, C.byref(held)))
-    out = {"episodes_train": int(n_train), "steps_train": int(cnt.value), "episodes_eval": n_eval,
-           "steps_eval": n_eval * ep_len, "Re_train": "U[100, 1000] (seeded)",
-           "Re_eval": [float(r) for r in res_eval], "adam_iters": a.learn_iters,
-           "loss_first": float(losses[:20].mean()), "loss_last": float(losses[-20:].mean()),
-           "loss_held_out_samples": float(held.value), "collect_s": collect_s, "train_s": train_s}
-    arms = {}
-    pressures = {}
-    for name, mode, warm in (("fp64", mgm.MODE_FP64, 0), ("fp32", mgm.MODE_FP32_IR, 0),
-                             ("learned_fp32", mgm.MODE_FP32_IR, 1)):
-        _lib.check(L.mgm_set_warm_start(mg.h, warm))
+    out = {"steps_train": int(cnt.value), "episodes_train": a.train_episodes, "Re_train": [float(r) for r in re_train],
+           "steps_eval": a.eval_episodes * a.eval_steps, "episodes_eval": a.eval_episodes,
+           "Re_eval": [float(r) for r in re_eval], "courant": a.courant, "adam_iters": a.learn_iters,
+           "loss_first": float(losses[:50].mean()), "loss_last": float(losses[-50:].mean()),
+           "collect_s": collect_s, "train_s": train_s}
+    arms, pressures = {}, {}
+    G = mgm.GUESS_EXTRAPOLATE
+    for name, mode, flags in (("fp64", mgm.MODE_FP64, 0), ("fp32", mgm.MODE_FP32_IR, 0),
+                              ("fp32_extrapolated", mgm.MODE_FP32_IR, G),
+                              ("learned_fp32", mgm.MODE_FP32_IR, G | mgm.GUESS_LEARNED)):
+        mg.set_initial_guess(flags)
         tot = [0.0, 0.0, 0]
         ps = []
-        for Re in res_eval:
+        for Re in re_eval:
             mg.set_flow(Re=float(Re), courant=a.courant)
             mg.apply_bc(mgm.BC_LID)
-            ms_, pms_, vc_, _ = mg.run_steps(mode, ep_len)
+            ms_, pms_, vc_, _ = mg.run_steps(mode, a.eval_steps)
             tot[0] += ms_; tot[1] += pms_; tot[2] += vc_
             ps.append(mg.get_field("p"))
-        steps = n_eval * ep_len
-        arms[name] = {"ms_per_step": tot[0] / steps, "poisson_ms": tot[1] / steps, "vcycles_per_step": tot[2] / steps}
+        steps = a.eval_episodes * a.eval_steps
+        arms[name] = {"ms_per_step": tot[0] / steps, "poisson_ms": tot[1] / steps, "vcycles_per_step": tot[2] / steps,
+                      "steps_per_s": steps / (tot[0] / 1e3)}
         pressures[name] = ps
-    _lib.check(L.mgm_set_warm_start(mg.h, 0))
-    mg.set_flow(Re=a.Re, courant=a.courant)
+    mg.set_initial_guess(0)
     rel = lambda x, y: max(float(np.linalg.norm(u - v) / np.linalg.norm(v)) for u, v in zip(x, y))
     out.update(arms)
-    out["vcycles_saved_per_step"] = arms["fp32"]["vcycles_per_step"] - arms["learned_fp32"]["vcycles_per_step"]
-    out["speedup_learned_fp32_vs_fp64"] = arms["fp64"]["ms_per_step"] / arms["learned_fp32"]["ms_per_step"]
-    out["speedup_fp32_vs_fp64"] = arms["fp64"]["ms_per_step"] / arms["fp32"]["ms_per_step"]
-    out["pressure_rel_l2_learned_fp32_vs_fp64"] = rel(pressures["learned_fp32"], pressures["fp64"])
-    out["pressure_rel_l2_fp32_vs_fp64"] = rel(pressures["fp32"], pressures["fp64"])
-    out["note"] = ("held-out episodes of a.episode steps from rest at unseen Re; the FP64 arm is the plain FP64 "
-                   "V-cycle solve, pressures compared after each episode")
+    lf, f32, ex, f64 = arms["learned_fp32"], arms["fp32"], arms["fp32_extrapolated"], arms["fp64"]
+    out["vcycles_saved_per_step_vs_fp32"] = f32["vcycles_per_step"] - lf["vcycles_per_step"]
+    out["vcycles_saved_per_step_vs_extrapolation"] = ex["vcycles_per_step"] - lf["vcycles_per_step"]
+    out["speedup_learned_fp32_vs_fp64"] = f64["ms_per_step"] / lf["ms_per_step"]
+    out["speedup_learned_fp32_vs_fp32"] = f32["ms_per_step"] / lf["ms_per_step"]
+    out["speedup_fp32_vs_fp64"] = f64["ms_per_step"] / f32["ms_per_step"]
+    for name in ("fp32", "fp32_extrapolated", "learned_fp32"):
+        out[f"pressure_rel_l2_{name}_vs_fp64"] = rel(pressures[name], pressures["fp64"])
+    out["note"] = ("held-out episodes from rest at unseen Re; pressures compared after each episode with the plain "
+                   "FP64 arm's (each solve to the tolerance)")
     return out
 
 
@@ -440,29 +504,34 @@ def run_ours(a, rank, world, local_rank):
     setup_launches = api.kernel_launches()
     print(f"setup_launches={setup_launches}", file=sys.stderr, flush=True)
     n = mg.n()
-    mg.set_flow(Re=a.Re, courant=a.courant)
     mg.set_solver(rel_tol=a.tol, max_iters=100, cheb_degree=a.cheb_degree, cheb_ratio=a.cheb_ratio)
-    mg.apply_bc(mgm.BC_LID)
 
     fast = mgm.MODE_FP32_IR
+    LEARNED = mgm.GUESS_EXTRAPOLATE | mgm.GUESS_LEARNED
+
+    # the learned warm start, trained on the GPU and evaluated on held-out
+    # steps (every rank trains its own network on its own replica)
+    learned = None
+    head_flags = mgm.GUESS_EXTRAPOLATE
+    if not a.no_learned:
+        learned = c5_protocol(a, mg, mgm, replicas.replica_seed(1, rank))
+        head_flags = LEARNED
 
     counts = {}
 
-    def arm(mode, steps):
-        """steps fractional steps in episodes from rest; device time of the steps only"""
-        tot = [0.0, 0.0, 0, 0.0]
-        cnt = [0, 0, 0]
-        done = 0
-        while done < steps:
-            m_ = min(a.episode, steps - done)
-            mg.apply_bc(mgm.BC_LID)
-            ms_, pms_, vc_, err_ = mg.run_steps(mode, m_)
-            tot[0] += ms_; tot[1] += pms_; tot[2] += vc_; tot[3] = err_
-            for i, v in enumerate(mg.solve_counters()):
-                cnt[i] += v
-            done += m_
-        counts[mode] = cnt
-        return tot
+    def arm(mode, flags, steps, warm):
+        """one episode from rest at a.Re: `warm` untimed steps, then `steps`
+        timed steps (device time of the steps only)"""
+        mg.set_flow(Re=a.Re, courant=a.courant)
+        mg.set_initial_guess(flags)
+        mg.apply_bc(mgm.BC_LID)
+        if warm:
+            mg.run_steps(mode, warm)
+        barrier()
+        mg.sync()
+        out = mg.run_steps(mode, steps)
+        counts[(mode, flags)] = list(mg.solve_counters())
+        return out
 
     def smoother_pass(steps):
         """CUDA events around every level-0 smoother launch, recorded inside
@@ -470,42 +539,40 @@ def run_ours(a, rank, world, local_rank):
         nodes cannot sit in the step graph's conditional bodies): total ms,
         launches, algorithmic bytes per launch"""
         mg.profile_smoother(True)
-        arm(fast, 1)  # captures the V-cycle graphs with their event nodes
+        arm(fast, head_flags, 1, 0)  # captures the V-cycle graphs with their event nodes
         mg.sync()
         s0 = mg.profile_read()
-        arm(fast, steps)
+        arm(fast, head_flags, steps, 0)
         s1 = mg.profile_read()
         mg.profile_smoother(False)
         return s1[0] - s0[0], s1[1] - s0[1], s1[2]
 
-    # warm-up (captures the step graphs), then the plain FP64 arm
-    arm(fast, a.warmup)
-    arm(mgm.MODE_FP64, min(a.warmup, 2))
-    barrier()
-    mg.sync()
-    plain_ms, plain_pms, plain_vc, _ = arm(mgm.MODE_FP64, a.steps)
+    # the denominator: plain FP64 V-cycles in FP64 FGMRES, the previous
+    # pressure as the initial guess
+    plain_ms, plain_pms, plain_vc, _ = arm(mgm.MODE_FP64, 0, a.steps, a.warmup)
     plain_ms = max_over_ranks(plain_ms)
 
-    # headline: FP32-in-FP64 refinement, each step one graph launch (the
-    # solve's loops as conditional nodes), device-timed on the library's stream
-    barrier()
-    mg.sync()
+    # headline: learned warm start + FP32 V-cycles in FP64 FGMRES, each step
+    # one graph launch (the solve's loops as conditional nodes), device-timed
+    # on the library's stream
     clocks = ClockSampler(local_rank)
     clocks.start()
     l0 = api.kernel_launches()
-    ms, pms, vc, err = arm(fast, a.steps)
+    ms, pms, vc, err = arm(fast, head_flags, a.steps, a.warmup)
     launches = api.kernel_launches() - l0
     ck = clocks.stop()
     barrier()
     ms = max_over_ranks(ms)
-    head_counts = list(counts[fast])
+    head_counts = counts[(fast, head_flags)]
 
-    # the same steps with the solve's loops driven from the host (one read of
-    # the loop flags per Arnoldi step, V-cycle graphs): what the one-graph step saves
+    # FP32 without any guess beyond the previous pressure, on the same steps
+    f32_ms, f32_pms, f32_vc, _ = arm(fast, 0, a.steps, a.warmup)
+    f32_ms = max_over_ranks(f32_ms)
+
+    # the headline steps with the solve's loops driven from the host (one read
+    # of the loop flags per Arnoldi step, V-cycle graphs): what the one-graph step saves
     mg.use_step_graph(False)
-    arm(fast, min(a.warmup, 2))
-    mg.sync()
-    hd_ms, hd_pms, hd_vc, _ = arm(fast, a.steps)
+    hd_ms, hd_pms, hd_vc, _ = arm(fast, head_flags, a.steps, a.warmup)
     mg.use_step_graph(True)
     hd_ms = max_over_ranks(hd_ms)
 
@@ -517,13 +584,9 @@ def run_ours(a, rank, world, local_rank):
     half = None
     if not a.no_half:
         mg.use_half_operator(True)
-        arm(fast, min(a.warmup, 2))
-        barrier()
-        mg.sync()
-        half_ms, half_pms, half_vc, half_err = arm(fast, a.steps)
-        barrier()
+        half_ms, half_pms, half_vc, half_err = arm(fast, head_flags, a.steps, a.warmup)
         half_ms = max_over_ranks(half_ms)
-        h_ms, h_launch, h_bytes = smoother_pass(min(a.steps, a.episode))
+        h_ms, h_launch, h_bytes = smoother_pass(min(a.steps, 10))
         mg.use_half_operator(False)
         h_avg_s = (h_ms / 1e3) / max(h_launch, 1)
         half = {"steps_per_s": a.steps * world / (half_ms / 1e3), "ms_per_step": half_ms / a.steps,
@@ -538,31 +601,28 @@ def run_ours(a, rank, world, local_rank):
     # end to end through the public API with page-locked host buffers:
     # per step H2D of u, v and D2H of u, v, p (the reference's `update host(field[0])`)
     bufs = [api.PinnedArray(n) for _ in range(5)]
+    mg.set_flow(Re=a.Re, courant=a.courant)
+    mg.set_initial_guess(head_flags)
+    mg.apply_bc(mgm.BC_LID)
+    if a.warmup:
+        mg.run_steps(fast, a.warmup)
+    bufs[0].array[:] = mg.get_field("u")
+    bufs[1].array[:] = mg.get_field("v")
     barrier()
     mg.sync()
-    e2e_s = 0.0
-    done = 0
-    while done < a.steps:
-        m_ = min(a.episode, a.steps - done)
-        mg.apply_bc(mgm.BC_LID)
-        bufs[0].array[:] = mg.get_field("u")
-        bufs[1].array[:] = mg.get_field("v")
-        t0 = time.perf_counter()
-        for _ in range(m_):
-            mg.step_host(fast, bufs[0].ptr, bufs[1].ptr, bufs[2].ptr, bufs[3].ptr, bufs[4].ptr)
-            bufs[0].array, bufs[2].array = bufs[2].array, bufs[0].array
-            bufs[0].ptr, bufs[2].ptr = bufs[2].ptr, bufs[0].ptr
-            bufs[1].array, bufs[3].array = bufs[3].array, bufs[1].array
-            bufs[1].ptr, bufs[3].ptr = bufs[3].ptr, bufs[1].ptr
-        e2e_s += time.perf_counter() - t0
-        done += m_
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        mg.step_host(fast, bufs[0].ptr, bufs[1].ptr, bufs[2].ptr, bufs[3].ptr, bufs[4].ptr)
+        bufs[0].array, bufs[2].array = bufs[2].array, bufs[0].array
+        bufs[0].ptr, bufs[2].ptr = bufs[2].ptr, bufs[0].ptr
+        bufs[1].array, bufs[3].array = bufs[3].array, bufs[1].array
+        bufs[1].ptr, bufs[3].ptr = bufs[3].ptr, bufs[1].ptr
+    e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s)
     finite = bool(np.all(np.isfinite(bufs[0].array)))
     for b in bufs:
         b.free()
-    learned = None
-    if rank == 0 and not a.no_learned:
-        learned = learned_arm(a, mg, mgm, n)
+    mg.set_initial_guess(0)
 
     line = None
     if rank == 0:
@@ -572,7 +632,8 @@ def run_ours(a, rank, world, local_rank):
         avg_launch_s = (sm_ms / 1e3) / max(sm_launch, 1)
         achieved = sm_bytes / avg_launch_s / 1e9 if sm_launch else None
         sizes = [tuple(mg.sizes[l][:3]) for l in range(mg.nl)]
-        sb = step_bytes(sizes, 2, a.cheb_degree, True, *head_counts, a.steps)
+        sb = step_bytes(sizes, 2, a.cheb_degree, True, *head_counts, a.steps,
+                        guesses=2 if head_flags & mgm.GUESS_LEARNED else 1)
         step_roof = {"bytes_per_step": sb / a.steps, "achieved": sb / (ms / 1e3) / 1e9, "unit": "GB/s",
                      "frac": sb / (ms / 1e3) / 1e9 / peak,
                      "vcycles": head_counts[0], "restart_cycle_starts": head_counts[1], "solves": head_counts[2],
@@ -601,7 +662,11 @@ def run_ours(a, rank, world, local_rank):
             "vcycles_per_step": vc / a.steps,
             "steady_err_last": err,
             "plain_fp64": {"steps_per_s": a.steps * world / (plain_ms / 1e3), "ms_per_step": plain_ms / a.steps,
-                           "poisson_ms": plain_pms / a.steps, "vcycles_per_step": plain_vc / a.steps},
+                           "poisson_ms": plain_pms / a.steps, "vcycles_per_step": plain_vc / a.steps,
+                           "note": "FP64 V-cycle in FP64 FGMRES, previous pressure as the initial guess, same steps"},
+            "speedup_vs_plain_fp64": plain_ms / ms,
+            "fp32_no_guess": {"steps_per_s": a.steps * world / (f32_ms / 1e3), "ms_per_step": f32_ms / a.steps,
+                              "poisson_ms": f32_pms / a.steps, "vcycles_per_step": f32_vc / a.steps},
             "host_driven_fp32": {"ms_per_step": hd_ms / a.steps, "poisson_ms": hd_pms / a.steps,
                                  "vcycles_per_step": hd_vc / a.steps,
                                  "note": ("the same steps with the solve's loops driven from the host (one read of "
@@ -609,8 +674,11 @@ def run_ours(a, rank, world, local_rank):
                                           "headline runs each step as one graph launch")},
             "learned_warm_start": learned,
             "half_operator": half,
-            "headline_arm": ("FP32 V-cycle inside FP64 FGMRES without the learned warm start (the faster arm: "
-                             "the measured learned arm is in learned_warm_start)"),
+            "headline_arm": ("learned warm start (minimal-residual combination of the network's increment and "
+                             "the last pressure increment) + FP32 V-cycle inside FP64 FGMRES"
+                             if head_flags & mgm.GUESS_LEARNED else
+                             "FP32 V-cycle inside FP64 FGMRES with the extrapolated initial guess (no network: "
+                             "--no-learned)"),
             "e2e": {"value": steps_total / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": 2 * 8 * n,
                     "d2h_bytes_per_step": 3 * 8 * n, "finite": finite},
             "roofline": {"bound": "hbm", "kernel": ("level-0 FP32 Chebyshev smoother step (k_level_v4<0>: FP32 "
@@ -633,10 +701,16 @@ def run_ours(a, rank, world, local_rank):
             # the same sample through the reference compiled as its README
             # documents (-O0), beside the -O2 figure
             s0 = reference_sample(a, steps=2, warmup=0, opt="O0")
+            cs = convergent_cpu_sample(a)
             cb["variants"] = {"reference_gcc_O2_1core": cb["value"],
                               "reference_gcc_O0_1core": cpu_baseline_entry(a, s0, n)["value"],
                               "note": ("the reference's OpenACC builds (nvc -acc multicore / GPU) are unavailable on "
                                        "this box (no nvc); its C code is serial")}
+            cs["ms_per_solve_scaled_to_workload"] = cs["ms_per_solve"] * n / cs["nodes"]
+            cs["note"] = ("the library's convergent FP64 solve restated in C (oracle/fgmres_oracle.c, OpenMP, "
+                          f"{cs['threads']} threads) on the {a.sample_m}^2 sample, solved to {a.tol:g} from zero; "
+                          "scaled by node count to the workload; the GPU's Poisson ms per step is poisson_ms")
+            cb["convergent_fp64_cpu"] = cs
             line["cpu_baseline"] = cb
     mg.close()
     if dist is not None:
@@ -827,6 +901,7 @@ def run_reference(a, rank):
     workload (reference_full), one JSON line on rank 0; other ranks exit."""
     if rank != 0:
         return None
+    a.episode = a.warmup + max(a.steps, 1)  # one episode from rest, as each arm of ours
     s = reference_full(a, steps=max(a.steps, 1), warmup=a.warmup)
     val = 1.0 / s["sec_per_step"]
     cfg = workload(a)
@@ -862,6 +937,8 @@ def run_reference(a, rank):
 
 def main():
     a = parse()
+    if a.Re is None:
+        a.Re = float(c5_reynolds(a)[1][0])
     from multigrid_meshless_b200.replicas import env_rank
     rank, world, local_rank = env_rank()
     if a.impl == "reference":

@@ -60,6 +60,15 @@ def lib(crpow: bool = False):
             raise RuntimeError(f"{path} missing: run `make -C oracle`")
         L = C.CDLL(path)
         L.orc_knn_cloud.argtypes = [C.c_int, C.c_int, dp, dp, dp, u8p, C.c_int, C.c_int, ip]
+        L.orc_cs_new.argtypes = [C.c_int]
+        L.orc_cs_new.restype = C.c_void_p
+        L.orc_cs_free.argtypes = [C.c_void_p]
+        L.orc_cs_level.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, ip, dp, u8p, C.c_int, C.c_void_p,
+                                   C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.orc_cs_prepare.argtypes = [C.c_void_p]
+        L.orc_cs_solve.argtypes = [C.c_void_p, dp, dp, C.c_double, C.c_int, C.c_int, C.c_double,
+                                   C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.orc_cs_solve.restype = C.c_int
         L.orc_count_ties.argtypes = [C.c_int, C.c_int, dp, dp, dp, C.c_int, ip]
         L.orc_count_ties.restype = C.c_long
         L.orc_nearest.argtypes = [C.c_int, dp, dp, dp, C.c_int, dp, dp, dp, C.c_int, ip]
@@ -498,6 +507,75 @@ def pinned_poisson_direct(lapP, cloud, b):
     bb = np.array(b, dtype=np.float64)
     bb[0] = 0.0
     return spla.spsolve(A.tocsc(), bb)
+
+
+def solver_transfer(levels, crpow=False, phs=3):
+    """The convergent solver's transfer weights on restated levels (set as
+    L.s_restr / L.s_prol): restriction into level l from l-1 with
+    create_restriction_matrix's interpolation on every non-boundary row,
+    prolongation into l from l+1 with create_prolongation_matrix's on every
+    row (mesh_functions.h:533-670)."""
+    O = lib(crpow)
+    nl = len(levels)
+    for l, L in enumerate(levels):
+        dim = L.dim
+        L.s_restr = L.s_prol = None
+        if l > 0:
+            F = levels[l - 1]
+            W = np.zeros(L.n * F.k)
+            O.orc_transfer_weights(L.n, L.x, L.y, L.z, L.btag, L.rpts, 0, 1, F.n, F.k, dim, phs, F.poly, F.x, F.y,
+                                   F.z, np.ascontiguousarray(F.cloud.ravel()), W)
+            L.s_restr = W.reshape(L.n, F.k)
+        if l < nl - 1:
+            Cn = levels[l + 1]
+            W = np.zeros(L.n * Cn.k)
+            O.orc_transfer_weights(L.n, L.x, L.y, L.z, L.btag, L.ppts, 0, 0, Cn.n, Cn.k, dim, phs, Cn.poly, Cn.x,
+                                   Cn.y, Cn.z, np.ascontiguousarray(Cn.cloud.ravel()), W)
+            L.s_prol = W.reshape(L.n, Cn.k)
+    return levels
+
+
+class ConvergentSolver:
+    """The library's convergent FP64 Poisson solve restated on the CPU
+    (oracle/fgmres_oracle.c, OpenMP): FGMRES preconditioned by a V-cycle of
+    Chebyshev smoothing, exact boundary rows, RBF restriction/prolongation and
+    a dense coarsest inverse.  levels need cloud, lapP, btag, rpts, ppts and
+    s_restr / s_prol (solver_transfer)."""
+
+    def __init__(self, levels, crpow=False):
+        self.O = lib(crpow)
+        self.h = self.O.orc_cs_new(len(levels))
+        self.keep = []
+        nl = len(levels)
+        for l, L in enumerate(levels):
+            cl = np.ascontiguousarray(L.cloud, np.int32)
+            lp = np.ascontiguousarray(L.lapP, np.float64)
+            bt = np.ascontiguousarray(L.btag, np.uint8)
+            rp = np.ascontiguousarray(L.rpts, np.int32)
+            pp = np.ascontiguousarray(L.ppts, np.int32)
+            rw = np.ascontiguousarray(L.s_restr, np.float64) if l > 0 else None
+            pw = np.ascontiguousarray(L.s_prol, np.float64) if l < nl - 1 else None
+            self.keep += [cl, lp, bt, rp, pp, rw, pw]
+            kr = levels[l - 1].k if l > 0 else 0
+            kp = levels[l + 1].k if l < nl - 1 else 0
+            self.O.orc_cs_level(self.h, l, L.n, L.k, cl, lp, bt, kr, rp.ctypes.data,
+                                rw.ctypes.data if rw is not None else None, kp, pp.ctypes.data,
+                                pw.ctypes.data if pw is not None else None)
+        self.O.orc_cs_prepare(self.h)
+
+    def solve(self, b, p0=None, tol=1e-8, max_iters=100, cheb_degree=3, cheb_ratio=20.0):
+        """(p, V-cycles, relative residual, converged) of the pinned system (b[0] taken as 0)."""
+        p = np.zeros(len(b)) if p0 is None else np.array(p0, np.float64)
+        it, rr = C.c_int(), C.c_double()
+        st = self.O.orc_cs_solve(self.h, np.ascontiguousarray(b, np.float64), p, tol, max_iters, cheb_degree,
+                                 cheb_ratio, C.byref(it), C.byref(rr))
+        return p, it.value, rr.value, st == 0
+
+    def __del__(self):
+        try:
+            self.O.orc_cs_free(self.h)
+        except Exception:
+            pass
 
 
 def pinned_lu(lapP, cloud):

@@ -307,3 +307,25 @@ def test_step_graph_reports_unconverged_solve(cavity):
             mg.run_steps(mgm.MODE_FP32_IR, 1)
     finally:
         mg.set_solver(rel_tol=1e-8, max_iters=80)
+
+
+def test_fp64_solve_matches_cpu_restatement(cavity):
+    """The GPU's convergent FP64 solve and its CPU restatement
+    (oracle/fgmres_oracle.c, the same algorithm on the same operators and
+    transfer weights) take the same number of V-cycles (at most one apart:
+    their dot products are summed in different orders) and give the same
+    pressure to the tolerance's precision."""
+    mg = cavity
+    mg.set_solver(rel_tol=1e-9, max_iters=80, cheb_degree=3, cheb_ratio=20.0)
+    levels = O.levels_from_device(mg)
+    for l, L in enumerate(levels):
+        st = mg.solver_transfer(l)
+        L.s_restr, L.s_prol = st["restr"], st["prol"]
+    S = O.ConvergentSolver(levels)
+    g = mg.geometry(0)
+    b = _smooth_rhs(g, 11)
+    p_gpu, it_gpu, rr_gpu = mg.solve_poisson(b, mode=mgm.MODE_FP64)
+    p_cpu, it_cpu, rr_cpu, ok = S.solve(b, tol=1e-9, max_iters=80, cheb_degree=3, cheb_ratio=20.0)
+    assert ok and rr_gpu < 1e-9
+    assert abs(it_gpu - it_cpu) <= 1, (it_gpu, it_cpu)
+    assert np.linalg.norm(p_gpu - p_cpu) / np.linalg.norm(p_cpu) < 1e-7
