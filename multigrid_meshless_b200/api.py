@@ -529,11 +529,16 @@ class Batch:
     def set_solver(self, rel_tol=1e-8, restart=24, cheb_degree=3, cheb_ratio=20.0):
         check(self.L.mgm_batch_set_solver(self.h, rel_tol, restart, cheb_degree, cheb_ratio))
 
-    def solve(self, rhs, mode=_lib.MODE_FP32_IR):
-        """rhs [nrhs][n0] -> (solutions [nrhs][n0], V-cycles, rel. residuals [nrhs], device ms)."""
+    def solve(self, rhs, mode=_lib.MODE_FP32_IR, out=None):
+        """rhs [nrhs][n0] -> (solutions [nrhs][n0], V-cycles, rel. residuals [nrhs], device ms).
+        rhs and out (the solutions' array, allocated when None) may be views
+        of PinnedArray buffers: the copies to and from the device then run
+        from page-locked memory."""
         rhs = _f(np.atleast_2d(rhs))
         nrhs = rhs.shape[0]
-        sol = np.zeros_like(rhs)
+        sol = np.zeros_like(rhs) if out is None else out
+        if sol.shape != rhs.shape or sol.dtype != np.float64 or not sol.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a C-contiguous float64 array shaped like rhs")
         vc = C.c_int()
         rr = np.zeros(nrhs)
         ms = C.c_double()

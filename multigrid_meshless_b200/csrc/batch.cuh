@@ -83,6 +83,7 @@ struct mgm_batch {
     mgm::BVecs<double> v64[mgm::kBatchMaxLevels];
     mgm::BVecs<float> v32[mgm::kBatchMaxLevels];
     mgm::DBuf<double> X, Bv, V, part, hsc;
+    mgm::DBuf<double> stage;  // right-hand sides / solutions in the caller's [nrhs][n] order, kept across solves
     mgm::DBuf<float> Z32;
     mgm::DBuf<double> Z64;
     int V_cols = 0, Z_cols32 = 0, Z_cols64 = 0;

@@ -570,7 +570,7 @@ void batch_free_solver(mgm_batch *b)
         b->v64[l] = BVecs<double>();
         b->v32[l] = BVecs<float>();
     }
-    b->X.release(); b->Bv.release(); b->V.release(); b->part.release(); b->hsc.release();
+    b->X.release(); b->Bv.release(); b->V.release(); b->part.release(); b->hsc.release(); b->stage.release();
     b->Z32.release(); b->Z64.release();
     b->V_cols = b->Z_cols32 = b->Z_cols64 = 0;
     b->B = 0;
@@ -862,8 +862,11 @@ void batch_solve(mgm_batch *b, int mode, int nrhs, const double *rhs_host, doubl
     const int m = std::min(b->restart, kBatchMaxRestart);
     if (mode == MGM_MODE_FP64) ensure_vecs<double>(b, B, m); else ensure_vecs<float>(b, B, m);
     const int n = b->L[0].n;
-    DBuf<double> hbuf((size_t)n * nrhs);
-    hbuf.upload(rhs_host, (size_t)n * nrhs, s);
+    // staging buffer kept across solves (no allocation per solve); the copies
+    // run at page-locked speed when the caller's buffers are page-locked
+    if (b->stage.n < (size_t)n * nrhs) b->stage.alloc((size_t)n * nrhs);
+    DBuf<double> &hbuf = b->stage;
+    MGM_CUDA(cudaMemcpyAsync(hbuf.p, rhs_host, sizeof(double) * (size_t)n * nrhs, cudaMemcpyHostToDevice, s));
     for (int q = 0; q < 4; q++) if (!b->ev[q]) MGM_CUDA(cudaEventCreate(&b->ev[q]));
     k_b_to_nodemajor<<<blocks_for((long)n * B, 256), 256, 0, s>>>(n, nrhs, B, hbuf.p, b->Bv.p);
     MGM_LAUNCHED();
@@ -877,7 +880,7 @@ void batch_solve(mgm_batch *b, int mode, int nrhs, const double *rhs_host, doubl
     MGM_CUDA(cudaEventRecord(b->ev[1], s));
     k_b_to_rhsmajor<<<blocks_for((long)n * nrhs, 256), 256, 0, s>>>(n, nrhs, B, b->X.p, hbuf.p);
     MGM_LAUNCHED();
-    hbuf.download(sol_host, (size_t)n * nrhs, s);
+    MGM_CUDA(cudaMemcpyAsync(sol_host, hbuf.p, sizeof(double) * (size_t)n * nrhs, cudaMemcpyDeviceToHost, s));
     MGM_CUDA(cudaStreamSynchronize(s));
     float ms = 0;
     MGM_CUDA(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
