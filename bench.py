@@ -834,6 +834,18 @@ def run_other(a):
     }
 
 
+def weights_flops(rep):
+    """FP64 throughput of the one-launch weight assembly: per system of order
+    N the Gauss-Jordan elimination on [A | I] (N pivots, each updating N - 1
+    rows of 2N entries with a multiply and a subtract: 4 N^2 (N - 1) flops;
+    the operator rows' products are not counted) over the launch's time."""
+    flops = sum(c["systems"] * 4.0 * c["order"] ** 2 * (c["order"] - 1) for c in rep["classes"])
+    sec = rep["weights_ms"] / 1e3
+    return {"gj_flops": flops, "achieved_fp64_tflops": flops / sec / 1e12 if sec > 0 else None,
+            "flops_note": ("Gauss-Jordan flops only (4 N^2 (N - 1) per system); no measured FP64 peak is available "
+                           "on this pool to divide by")}
+
+
 def run_batch(a):
     import numpy as np
 
@@ -895,7 +907,7 @@ def run_batch(a):
                                f"k 40/60 (poly 3) on the fine level and 25/35 (poly 2) below by boundary proximity",
                    "nodes_total": n_tot, "nodes_fine": cl[0].n, "levels": nl,
                    "nrhs": nrhs, "rel_tol": a.tol},
-        "weights": {k_: v for k_, v in rep.items()},
+        "weights": dict(rep, **weights_flops(rep)),
         "fp32": arms["fp32"], "fp64": arms["fp64"],
         "solution_rel_l2_fp32_vs_fp64": rel,
         "e2e": {"value": nrhs / (arms["fp32"]["wall_ms_per_solve"] / 1e3), "unit": "RHS solved/s",
