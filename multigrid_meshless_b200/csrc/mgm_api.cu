@@ -598,6 +598,8 @@ void arnoldi_step(FgRun<T> &R, cudaStream_t s, FgHandles hd, bool captured)
     fg_scale_w(R.n, R.V, R.ld, R.st, s);
     fg_arnoldi_end(R.st, hd, s);
     if (!captured && c->prof.on) {
+        // the events of this V-cycle must have completed before they are read
+        MGM_CUDA(cudaStreamSynchronize(c->s));
         auto &G = c->vg[sizeof(T) == 4 ? 1 : 0];
         if (c->use_graphs && G.x && G.prof) c->prof.harvest_graph(G.ev_first, G.ev_pairs);
         else c->prof.harvest();
