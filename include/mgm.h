@@ -483,16 +483,18 @@ MGM_API int mgm_profile_read(mgm_ctx *ctx, double *ms_total, long long *launches
 MGM_API int mgm_set_initial_guess(mgm_ctx *ctx, int flags);
 /* A 4-layer message-passing network (hidden width 64, BF16 weights and
  * activations, FP32 accumulation) on the level-0 stencil graph predicts the
- * pressure increment of a Poisson solve from (b, previous p, the last
- * increment p_prev - p_prev2, coordinates).  With the warm start on
+ * part of a Poisson solve's pressure increment that extrapolating the last
+ * increment misses, from (b, previous p, the last increment p_prev - p_prev2,
+ * coordinates).  With the warm start on
  * (mgm_set_warm_start: the MGM_GUESS_LEARNED bit of mgm_set_initial_guess)
  * each step's solve starts from the minimal-residual combination of the
  * prediction (and, with MGM_GUESS_EXTRAPOLATE, the last increment); the
  * V-cycle-preconditioned FGMRES then runs to the same tolerance as without
  * it.  mgm_mpnn_init allocates it (seeded weights) and a dataset ring of
  * dataset_capacity samples (4 n floats each); mgm_mpnn_collect runs time
- * steps with a solver mode and records (b, p_prev, p_prev - p_prev2,
- * p_new - p_prev), each normalised by its RMS; mgm_mpnn_train runs Adam on a
+ * steps with a solver mode and records (b, p_prev, dp = p_prev - p_prev2,
+ * (p_new - p_prev) - dp: the part of the new increment the extrapolation
+ * misses, which the network learns), each normalised by its RMS; mgm_mpnn_train runs Adam on a
  * range of samples (losses[it] per iteration, may be NULL); mgm_mpnn_eval
  * returns the mean loss on a range.  Params: mgm_mpnn_num_params() floats. */
 MGM_API int mgm_mpnn_init(mgm_ctx *ctx, unsigned long long seed, int dataset_capacity);

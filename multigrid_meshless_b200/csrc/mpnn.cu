@@ -11,11 +11,12 @@
 // product is accumulated in FP32; the layer GEMM runs on the tensor cores
 // (mma.sync m16n8k16 BF16 -> FP32) fused with the neighbour aggregation.
 //
-// The prediction is the shape of the pressure increment p_new - p_prev.  The
-// solve combines it with the extrapolation direction dp by the coefficients
-// that minimise the FP64 residual, then runs the V-cycle-preconditioned FGMRES
-// to the same tolerance as without it: the learned guess can only lower the
-// starting residual, never replace the solver.
+// The prediction is the shape of what the extrapolation misses,
+// (p_new - p_prev) - dp.  The solve combines it with the extrapolation
+// direction dp by the coefficients that minimise the FP64 residual, then runs
+// the V-cycle-preconditioned FGMRES to the same tolerance as without it: the
+// learned guess can only lower the starting residual, never replace the
+// solver.
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -49,6 +50,7 @@ struct MpnnState {
     DBuf<float> y, dy, dH, dHin, dz, dm;
     DBuf<double> scal;       // device scalars: [0..1] sum of squares of b, p; [2] loss; [5] of dp
     DBuf<float> ds;          // dataset: cap samples x kSlot x n (b_hat, p_hat, dp_hat, target)
+    DBuf<double> dp;         // p_prev - p_prev2 of the sample being recorded
     int ds_cap = 0, ds_count = 0;
     int adam_t = 0;
     bool ready = false;
@@ -550,9 +552,11 @@ __global__ void k_res_bwd(int n, int k, const int *tptr, const int *tpos, const 
     dy[j] += (float)(w_res * (-2.0 * s / Q));
 }
 
-// dataset record: slot <- (b/rms b, p_prev/rms, (p_prev - p_prev2)/rms, (p_new - p_prev)/rms);
-// ss[0..1] sums of squares of b, p_prev; ss[2] of p_new - p_prev; ss[5] of p_prev - p_prev2
-// (pprev2 null: no earlier increment, dp_hat = 0)
+// dataset record: slot <- (b/rms b, p_prev/rms, dp/rms, target/rms) with
+// dp = p_prev - p_prev2 and target = (p_new - p_prev) - dp, the part of the
+// new increment the extrapolation misses (p_new - p_prev when there is no
+// p_prev2: pprev2 null, dp_hat = 0); ss[0..1] sums of squares of b, p_prev,
+// ss[2] of the target, ss[5] of dp
 __global__ void k_record(int n, const double *b, const double *pprev, const double *pprev2, const double *pnew,
                          const double *ss, float *slot)
 {
@@ -560,10 +564,30 @@ __global__ void k_record(int n, const double *b, const double *pprev, const doub
     if (i >= n) return;
     const float sb = inv_rms(ss[0], n), sp = inv_rms(ss[1], n), sd = inv_rms(ss[2], n);
     const float sq = pprev2 ? inv_rms(ss[5], n) : 0.f;
+    const double dp = pprev2 ? pprev[i] - pprev2[i] : 0.0;
     slot[i] = (float)b[i] * sb;
     slot[n + i] = (float)pprev[i] * sp;
-    slot[2 * n + i] = pprev2 ? (float)(pprev[i] - pprev2[i]) * sq : 0.f;
-    slot[3 * n + i] = (float)(pnew[i] - pprev[i]) * sd;
+    slot[2 * n + i] = (float)dp * sq;
+    slot[3 * n + i] = (float)((pnew[i] - pprev[i]) - dp) * sd;
+}
+
+// sum of (a - b - c)^2 (c may be null) -> atomically into out[0]
+__global__ void k_sumsq_diff2(int n, const double *a, const double *b, const double *c, double *out)
+{
+    __shared__ double sm[32];
+    double s = 0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double d = a[i] - b[i] - (c ? c[i] : 0.0);
+        s += d * d;
+    }
+    s = bsum_d<256>(s, sm);
+    if (threadIdx.x == 0) atomicAdd(out, s);
+}
+
+__global__ void k_diff(int n, const double *a, const double *b, double *out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = a[i] - b[i];
 }
 
 __global__ void k_sumsq_diff(int n, const double *a, const double *b, double *out)
@@ -746,12 +770,14 @@ void record_sample(mgm_ctx *c, const double *b, const double *pprev, const doubl
     MGM_CUDA(cudaMemsetAsync(M.scal.p, 0, 6 * sizeof(double), s));
     k_sumsq2<<<red_blocks(M.n), 256, 0, s>>>(M.n, b, pprev, M.scal.p);
     MGM_LAUNCHED();
-    k_sumsq_diff<<<red_blocks(M.n), 256, 0, s>>>(M.n, pnew, pprev, M.scal.p + 2);
-    MGM_LAUNCHED();
     if (pprev2) {
         k_sumsq_diff<<<red_blocks(M.n), 256, 0, s>>>(M.n, pprev, pprev2, M.scal.p + 5);
         MGM_LAUNCHED();
+        k_diff<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, pprev, pprev2, M.dp.p);
+        MGM_LAUNCHED();
     }
+    k_sumsq_diff2<<<red_blocks(M.n), 256, 0, s>>>(M.n, pnew, pprev, pprev2 ? M.dp.p : nullptr, M.scal.p + 2);
+    MGM_LAUNCHED();
     k_record<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, b, pprev, pprev2, pnew, M.scal.p,
                                                   M.ds.p + (size_t)slot * kSlot * M.n);
     MGM_LAUNCHED();
@@ -816,6 +842,7 @@ int mgm_mpnn_init(mgm_ctx *c, unsigned long long seed, int dataset_capacity)
         M.y.alloc(n); M.dy.alloc(n); M.dH.alloc(n * kH); M.dHin.alloc(n * kH); M.dz.alloc(n * kH);
         M.dm.alloc(n * 128);
         M.scal.alloc(8);
+        M.dp.alloc(n);
         M.ds_cap = dataset_capacity;
         M.ds_count = 0;
         if (dataset_capacity > 0) M.ds.alloc((size_t)dataset_capacity * kSlot * n);
