@@ -328,7 +328,10 @@ MGM_API int mgm_heat_step(mgm_ctx *ctx, double *steady_err);
  * and a checksum; a context loads only a checkpoint of matching levels
  * (MGM_ERR_ARG otherwise), after mgm_setup (and after mgm_heat_init for the
  * heat-conduction program).  A run continued from a checkpoint repeats the
- * uninterrupted run bit for bit.  No counterpart in the reference. */
+ * uninterrupted run bit for bit (with the default initial guess: the
+ * pressure history of mgm_set_initial_guess is not saved, so the first step
+ * after a load starts from the previous pressure alone).  No counterpart in
+ * the reference. */
 MGM_API int mgm_write_solution(mgm_ctx *ctx, const char *path, int pressure_field);
 MGM_API int mgm_checkpoint_save(mgm_ctx *ctx, const char *path);
 MGM_API int mgm_checkpoint_load(mgm_ctx *ctx, const char *path);

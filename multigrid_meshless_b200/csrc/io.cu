@@ -225,6 +225,12 @@ int mgm_checkpoint_load(mgm_ctx *c, const char *path)
         MGM_REQUIRE(c->setup_done, "mgm_checkpoint_load: call mgm_setup first");
         MGM_CUDA(cudaStreamSynchronize(c->s));
         load(c, path);
+        // the pressure history of the initial guesses belongs to the run
+        // that was interrupted, not to the loaded state
+        if (c->hist_ok.p) {
+            c->hist_ok.zero(c->s);
+            MGM_CUDA(cudaStreamSynchronize(c->s));
+        }
     });
 }
 

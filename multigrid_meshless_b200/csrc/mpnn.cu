@@ -169,8 +169,32 @@ struct bf4 { __nv_bfloat162 a, b; };
 // One message-passing layer for 64 nodes: gather [h_i | mean h_j | sum l_ij h_j]
 // into shared memory (BF16), multiply by W (tensor cores, FP32 accumulate),
 // bias + relu + residual, store h' (BF16); in training also z and the row.
-// Aggregation: a half-warp per node (4 features per lane, one 128-byte row
-// per neighbour), 8 neighbour rows in flight.  W (24 KB) is read through L1.
+// Aggregation: eight lanes per node (8 features, one 16-byte load per lane
+// and neighbour row), four nodes per warp at a time; each lane holds the
+// node's stencil slots l, l+8, ... and the group shares them by shuffles;
+// the neighbour rows of kGather slots are in flight at once.  Each feature's
+// sums run over the slots in order.  W (24 KB) is read through L1.
+constexpr int kGather = 10;
+
+__device__ __forceinline__ void unpack8(const uint4 &u, float *f)
+{
+    const __nv_bfloat162 *b = reinterpret_cast<const __nv_bfloat162 *>(&u);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const float2 v = __bfloat1622float2(b[q]);
+        f[2 * q] = v.x;
+        f[2 * q + 1] = v.y;
+    }
+}
+__device__ __forceinline__ uint4 pack8(const float *f)
+{
+    uint4 u;
+    __nv_bfloat162 *b = reinterpret_cast<__nv_bfloat162 *>(&u);
+#pragma unroll
+    for (int q = 0; q < 4; q++) b[q] = __floats2bfloat162_rn(f[2 * q], f[2 * q + 1]);
+    return u;
+}
+
 __global__ void __launch_bounds__(128) k_mp_layer(int n, int k, const int *__restrict__ cloud,
                                                   const float *__restrict__ lapS, float inv_k,
                                                   const bf16 *__restrict__ h_in, const bf16 *__restrict__ WT,
@@ -179,60 +203,60 @@ __global__ void __launch_bounds__(128) k_mp_layer(int n, int k, const int *__res
 {
     __shared__ __align__(16) bf16 Xs[kTile][kPad];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int half = lane >> 4, hl = lane & 15;
-    const unsigned hmask = 0xffffffffu;  // rows past n are clamped, so all lanes stay converged
+    const int grp = lane >> 3, gl = lane & 7;
+    const unsigned full = 0xffffffffu;  // rows past n are clamped, so all lanes stay converged
     const long base = (long)blockIdx.x * kTile;
-    for (int rr = 0; rr < kTile / 8; rr++) {
-        const int row = warp * (kTile / 4) + 2 * rr + half;
+    for (int rr = 0; rr < kTile / 16; rr++) {
+        const int row = warp * 16 + rr * 4 + grp;
         const bool valid = base + row < n;
         const long i = valid ? base + row : (long)n - 1;
-        float sf[4] = {0, 0, 0, 0}, mn[4] = {0, 0, 0, 0}, lp[4] = {0, 0, 0, 0};
-        {
-            const bf4 sv = *reinterpret_cast<const bf4 *>(h_in + i * kH + 4 * hl);
-            const float2 s0 = __bfloat1622float2(sv.a), s1 = __bfloat1622float2(sv.b);
-            sf[0] = s0.x; sf[1] = s0.y; sf[2] = s1.x; sf[3] = s1.y;
-            const int c0 = hl < k ? cloud[i * k + hl] : 0;
-            const float w0 = hl < k ? lapS[i * k + hl] : 0.f;
-            const int c1 = hl + 16 < k ? cloud[i * k + hl + 16] : 0;
-            const float w1 = hl + 16 < k ? lapS[i * k + hl + 16] : 0.f;
-            const int c2 = hl + 32 < k ? cloud[i * k + hl + 32] : 0;
-            const float w2 = hl + 32 < k ? lapS[i * k + hl + 32] : 0.f;
-            const int c3 = hl + 48 < k ? cloud[i * k + hl + 48] : 0;
-            const float w3 = hl + 48 < k ? lapS[i * k + hl + 48] : 0.f;
-            for (int j0 = 0; j0 < k; j0 += 8) {
-                bf4 v[8];
-                float wj[8];
+        float sf[8], mn[8], lp[8];
 #pragma unroll
-                for (int q = 0; q < 8; q++) {
-                    const int j = j0 + q;
-                    const int src = j & 15, sel = j >> 4;
-                    const int cs = __shfl_sync(hmask, sel == 0 ? c0 : sel == 1 ? c1 : sel == 2 ? c2 : c3, src, 16);
-                    wj[q] = __shfl_sync(hmask, sel == 0 ? w0 : sel == 1 ? w1 : sel == 2 ? w2 : w3, src, 16);
-                    if (j < k) v[q] = *reinterpret_cast<const bf4 *>(h_in + (long)cs * kH + 4 * hl);
-                    else { wj[q] = 0.f; v[q].a = v[q].b = __floats2bfloat162_rn(0.f, 0.f); }
-                }
+        for (int q = 0; q < 8; q++) mn[q] = lp[q] = 0.f;
+        unpack8(__ldg(reinterpret_cast<const uint4 *>(h_in + i * kH + 8 * gl)), sf);
+        // the node's slots gl, gl + 8, ... (k <= 64)
+        int cl[8];
+        float wl[8];
 #pragma unroll
-                for (int q = 0; q < 8; q++) {
-                    if (j0 + q >= k) break;
-                    const float2 a = __bfloat1622float2(v[q].a), b = __bfloat1622float2(v[q].b);
-                    mn[0] += a.x; mn[1] += a.y; mn[2] += b.x; mn[3] += b.y;
-                    lp[0] += wj[q] * a.x; lp[1] += wj[q] * a.y; lp[2] += wj[q] * b.x; lp[3] += wj[q] * b.y;
-                }
+        for (int q = 0; q < 8; q++) {
+            const int j = gl + 8 * q;
+            cl[q] = j < k ? __ldg(cloud + i * k + j) : 0;
+            wl[q] = j < k ? __ldg(lapS + i * k + j) : 0.f;
+        }
+#pragma unroll
+        for (int j0 = 0; j0 < 64; j0 += kGather) {
+            if (j0 >= k) break;
+            uint4 v[kGather];
+            float wj[kGather];
+#pragma unroll
+            for (int q = 0; q < kGather; q++) {
+                const int j = j0 + q;
+                if (j >= 64) { wj[q] = 0.f; v[q] = make_uint4(0, 0, 0, 0); continue; }
+                const int cs = __shfl_sync(full, cl[j >> 3], j & 7, 8);
+                wj[q] = __shfl_sync(full, wl[j >> 3], j & 7, 8);
+                v[q] = j < k ? __ldg(reinterpret_cast<const uint4 *>(h_in + (long)cs * kH + 8 * gl))
+                             : make_uint4(0, 0, 0, 0);
             }
 #pragma unroll
-            for (int q = 0; q < 4; q++) mn[q] *= inv_k;
-            if (!valid) {
+            for (int q = 0; q < kGather; q++) {
+                if (j0 + q >= k) break;
+                float f[8];
+                unpack8(v[q], f);
 #pragma unroll
-                for (int q = 0; q < 4; q++) sf[q] = mn[q] = lp[q] = 0.f;
+                for (int e = 0; e < 8; e++) {
+                    mn[e] += f[e];
+                    lp[e] += wj[q] * f[e];
+                }
             }
         }
-        bf4 o;
-        o.a = __floats2bfloat162_rn(sf[0], sf[1]); o.b = __floats2bfloat162_rn(sf[2], sf[3]);
-        *reinterpret_cast<bf4 *>(&Xs[row][4 * hl]) = o;
-        o.a = __floats2bfloat162_rn(mn[0], mn[1]); o.b = __floats2bfloat162_rn(mn[2], mn[3]);
-        *reinterpret_cast<bf4 *>(&Xs[row][kH + 4 * hl]) = o;
-        o.a = __floats2bfloat162_rn(lp[0], lp[1]); o.b = __floats2bfloat162_rn(lp[2], lp[3]);
-        *reinterpret_cast<bf4 *>(&Xs[row][2 * kH + 4 * hl]) = o;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            mn[q] *= inv_k;
+            if (!valid) sf[q] = mn[q] = lp[q] = 0.f;
+        }
+        *reinterpret_cast<uint4 *>(&Xs[row][8 * gl]) = pack8(sf);
+        *reinterpret_cast<uint4 *>(&Xs[row][kH + 8 * gl]) = pack8(mn);
+        *reinterpret_cast<uint4 *>(&Xs[row][2 * kH + 8 * gl]) = pack8(lp);
     }
     __syncthreads();
     const int g = lane >> 2, t = lane & 3, r0 = warp * 16;

@@ -16,7 +16,7 @@
   weights and the solver's transfer weights on a seeded sample of at least
   20,000 rows per level (every row of smaller levels), boundary rows and the
   rows with the widest 16-bit neighbour offsets included, bit for bit against
-  the correctly-rounded-power build and within 5e-10 against the libm build
+  the correctly-rounded-power build and within 2e-9 against the libm build
   (see W_TOL_LARGE); the FP32 V-cycle's compact copies decoded back to the
   neighbours and weights they stand for, on every row.
 * Ten fractional steps on a 250k-node cavity with the FP32-in-FP64 solve
@@ -42,8 +42,9 @@ W_TOL = 1e-10      # weights against the libm build, relative to each row's larg
 # conditioned (unscaled monomials of offsets ~h about the seed), and libm's
 # one-ulp pow errors -- the only difference between the libm build and the
 # correctly rounded one, which the GPU matches bit for bit -- reach ~1.2e-10
-# of a row's largest weight; the large configurations allow 5e-10 there.
-W_TOL_LARGE = 5e-10
+# of a row's largest weight in 2D and ~1e-9 on the 3D cube's coarse levels;
+# the large configurations allow 2e-9 there.
+W_TOL_LARGE = 2e-9
 P_TOL = 1e-6       # pressure and velocity, relative L2
 SAMPLE = 20000     # rows per level checked against the per-row weight solves
 
