@@ -5,8 +5,10 @@ relative residual: FP32-in-FP64 refinement vs plain FP64 on the GPU.
 Workload (the 1M-node 2D lid-driven cavity): unit square, 1000 x 1000 jittered
 Cartesian nodes (999,996 after the corner nodes are removed), 6 levels each
 coarser by 4x, PHS degree 3, polynomial degree 4 (15 terms), 30-node stencils,
-Re = 100, Courant 0.5.  A step is one fractional step (momentum, divergence,
-Poisson solve to 1e-8, velocity correction) through the C ABI.
+Courant 0.3, Re drawn from U[100, 1000] (the timed episode at the first
+held-out draw), timed past the start-up transient (--eval-start steps from
+rest).  A step is one fractional step (momentum, divergence, Poisson solve to
+1e-8, velocity correction) through the C ABI.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -22,6 +24,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -64,6 +67,15 @@ def parse():
     ap.add_argument("--eval-episodes", type=int, default=2, help="held-out episodes at unseen Re")
     ap.add_argument("--eval-steps", type=int, default=100, help="steps per held-out episode (200 in all)")
     ap.add_argument("--learn-iters", type=int, default=2000, help="Adam iterations of the GPU training")
+    ap.add_argument("--eval-start", type=int, default=300,
+                    help="untimed steps from rest before an episode's collected or timed steps (the cavity's "
+                         "start-up transient; 0 times the steps right after rest)")
+    ap.add_argument("--w-mse", type=float, default=1.0, help="weight of the increment MSE in the training loss")
+    ap.add_argument("--w-res", type=float, default=0.0,
+                    help="weight of the smoothed-residual term in the training loss (mgm_mpnn_set_loss)")
+    ap.add_argument("--host-driven", action="store_true",
+                    help="run every arm with the solve's loops driven from the host (V-cycle graphs without "
+                         "conditional nodes, so that a profiler sees each kernel launch)")
     ap.add_argument("--workload", choices=["cavity", "annulus", "timple", "cube", "shell-batch"], default="cavity",
                     help="cavity: the headline (1M-node cavity); annulus / cube / shell-batch: the other configs, "
                          "each printing its own line")
@@ -85,8 +97,11 @@ def workload(a):
         "rel_tol": a.tol,
         "l2": "inputs larger than L2 (operators + hierarchy ~2 GB per step, L2 126 MB)",
         "seed": 1,
-        "episodes": (f"each arm: one episode from rest at Re={a.Re:g} (lid BC applied, p = 0), {a.warmup} untimed "
-                     f"steps, then the timed steps"),
+        "step": ("host-driven solve loops (--host-driven)" if a.host_driven else
+                 "one CUDA graph launch per step (solve loops as conditional nodes)"),
+        "episodes": (f"each arm starts from the same saved state of an episode at Re={a.Re:g}: the lid BC applied "
+                     f"at rest (p = 0), {a.eval_start} untimed steps (FP32 V-cycles, extrapolated guess), then per "
+                     f"arm {a.warmup} untimed and the timed steps"),
     }
 
 
@@ -405,15 +420,31 @@ def c5_reynolds(a):
     return 100.0 + 900.0 * uniform(7, 0, a.train_episodes), 100.0 + 900.0 * uniform(7, 1, a.eval_episodes)
 
 
-def c5_protocol(a, mg, mgm, seed):
+def develop(a, mg, mgm, Re, path=None):
+    """An episode at Re brought past the cavity's start-up transient: the lid
+    BC applied at rest (p = 0), then a.eval_start untimed steps with FP32
+    V-cycles and the extrapolated guess (any mode gives the same flow to the
+    tolerance).  With `path`, the state is saved there (mgm_checkpoint_save)."""
+    mg.set_flow(Re=float(Re), courant=a.courant)
+    mg.set_initial_guess(mgm.GUESS_EXTRAPOLATE)
+    mg.apply_bc(mgm.BC_LID)
+    if a.eval_start:
+        mg.run_steps(mgm.MODE_FP32_IR, a.eval_start)
+    if path:
+        mg.checkpoint_save(path)
+
+
+def c5_protocol(a, mg, mgm, seed, tmpdir):
     """The learned warm start as the C5 protocol asks: the network is trained
     on the GPU on a.train_episodes x a.train_steps fractional steps of the
     plain solver (Re ~ U[100, 1000], every solve to the tolerance), then four
     arms run the same a.eval_episodes x a.eval_steps held-out steps at unseen
-    Re, each from rest: plain FP64 (the previous step's pressure as the
-    initial guess), FP32-in-FP64, FP32 with the extrapolated guess
-    p_prev + c (p_prev - p_prev2), and learned + FP32 (the minimal-residual
-    combination of that direction and the network's).  Every solve still
+    Re: plain FP64 (the previous step's pressure as the initial guess),
+    FP32-in-FP64, FP32 with the extrapolated guess p_prev + c (p_prev -
+    p_prev2), and learned + FP32 (the minimal-residual combination of that
+    direction and the network's).  Every episode, training and held-out, is
+    first brought a.eval_start steps past rest (develop); the held-out arms
+    all start from the same saved state of their episode.  Every solve still
     V-cycles to the tolerance; pressures are compared with the FP64 arm's at
     the end of each held-out episode."""
     import ctypes as C
@@ -425,10 +456,9 @@ def c5_protocol(a, mg, mgm, seed):
     re_train, re_eval = c5_reynolds(a)
     t0 = time.perf_counter()
     _lib.check(L.mgm_mpnn_init(mg.h, seed, a.train_episodes * a.train_steps))
-    mg.set_initial_guess(mgm.GUESS_EXTRAPOLATE)  # the guess changes no solution beyond the tolerance
+    _lib.check(L.mgm_mpnn_set_loss(mg.h, C.c_float(a.w_mse), C.c_float(a.w_res)))
     for Re in re_train:
-        mg.set_flow(Re=float(Re), courant=a.courant)
-        mg.apply_bc(mgm.BC_LID)
+        develop(a, mg, mgm, Re)
         _lib.check(L.mgm_mpnn_collect(mg.h, mgm.MODE_FP32_IR, a.train_steps))
     collect_s = time.perf_counter() - t0
     cnt = C.c_int()
@@ -441,19 +471,25 @@ def c5_protocol(a, mg, mgm, seed):
     out = {"steps_train": int(cnt.value), "episodes_train": a.train_episodes, "Re_train": [float(r) for r in re_train],
            "steps_eval": a.eval_episodes * a.eval_steps, "episodes_eval": a.eval_episodes,
            "Re_eval": [float(r) for r in re_eval], "courant": a.courant, "adam_iters": a.learn_iters,
+           "episode_start_step": a.eval_start, "loss_weights": {"mse": a.w_mse, "residual": a.w_res},
            "loss_first": float(losses[:50].mean()), "loss_last": float(losses[-50:].mean()),
            "collect_s": collect_s, "train_s": train_s}
+    starts = []
+    for i, Re in enumerate(re_eval):
+        path = os.path.join(tmpdir, f"heldout{i}.ckpt")
+        develop(a, mg, mgm, Re, path)
+        starts.append((Re, path))
     arms, pressures = {}, {}
     G = mgm.GUESS_EXTRAPOLATE
     for name, mode, flags in (("fp64", mgm.MODE_FP64, 0), ("fp32", mgm.MODE_FP32_IR, 0),
                               ("fp32_extrapolated", mgm.MODE_FP32_IR, G),
                               ("learned_fp32", mgm.MODE_FP32_IR, G | mgm.GUESS_LEARNED)):
-        mg.set_initial_guess(flags)
         tot = [0.0, 0.0, 0]
         ps = []
-        for Re in re_eval:
+        for Re, path in starts:
             mg.set_flow(Re=float(Re), courant=a.courant)
-            mg.apply_bc(mgm.BC_LID)
+            mg.checkpoint_load(path)
+            mg.set_initial_guess(flags)
             ms_, pms_, vc_, _ = mg.run_steps(mode, a.eval_steps)
             tot[0] += ms_; tot[1] += pms_; tot[2] += vc_
             ps.append(mg.get_field("p"))
@@ -472,8 +508,9 @@ def c5_protocol(a, mg, mgm, seed):
     out["speedup_fp32_vs_fp64"] = f64["ms_per_step"] / f32["ms_per_step"]
     for name in ("fp32", "fp32_extrapolated", "learned_fp32"):
         out[f"pressure_rel_l2_{name}_vs_fp64"] = rel(pressures[name], pressures["fp64"])
-    out["note"] = ("held-out episodes from rest at unseen Re; pressures compared after each episode with the plain "
-                   "FP64 arm's (each solve to the tolerance)")
+    out["note"] = (f"held-out episodes at unseen Re, each arm from the same saved state {a.eval_start} steps past "
+                   "rest; pressures compared after each episode with the plain FP64 arm's (each solve to the "
+                   "tolerance)")
     return out
 
 
@@ -505,26 +542,33 @@ def run_ours(a, rank, world, local_rank):
     print(f"setup_launches={setup_launches}", file=sys.stderr, flush=True)
     n = mg.n()
     mg.set_solver(rel_tol=a.tol, max_iters=100, cheb_degree=a.cheb_degree, cheb_ratio=a.cheb_ratio)
+    mg.use_step_graph(not a.host_driven)
 
     fast = mgm.MODE_FP32_IR
     LEARNED = mgm.GUESS_EXTRAPOLATE | mgm.GUESS_LEARNED
 
     # the learned warm start, trained on the GPU and evaluated on held-out
     # steps (every rank trains its own network on its own replica)
+    tmpdir = tempfile.mkdtemp(prefix="mgm_bench_")
     learned = None
     head_flags = mgm.GUESS_EXTRAPOLATE
     if not a.no_learned:
-        learned = c5_protocol(a, mg, mgm, replicas.replica_seed(1, rank))
+        learned = c5_protocol(a, mg, mgm, replicas.replica_seed(1, rank), tmpdir)
         head_flags = LEARNED
+
+    # the timed episode at a.Re, brought past the start-up transient once;
+    # every arm below starts from this saved state
+    start = os.path.join(tmpdir, "timed.ckpt")
+    develop(a, mg, mgm, a.Re, start)
 
     counts = {}
 
     def arm(mode, flags, steps, warm):
-        """one episode from rest at a.Re: `warm` untimed steps, then `steps`
-        timed steps (device time of the steps only)"""
+        """the timed episode from its saved state: `warm` untimed steps, then
+        `steps` timed steps (device time of the steps only)"""
         mg.set_flow(Re=a.Re, courant=a.courant)
+        mg.checkpoint_load(start)
         mg.set_initial_guess(flags)
-        mg.apply_bc(mgm.BC_LID)
         if warm:
             mg.run_steps(mode, warm)
         barrier()
@@ -573,8 +617,15 @@ def run_ours(a, rank, world, local_rank):
     # of the loop flags per Arnoldi step, V-cycle graphs): what the one-graph step saves
     mg.use_step_graph(False)
     hd_ms, hd_pms, hd_vc, _ = arm(fast, head_flags, a.steps, a.warmup)
-    mg.use_step_graph(True)
+    mg.use_step_graph(not a.host_driven)
     hd_ms = max_over_ranks(hd_ms)
+
+    # the headline steps with the V-cycle's kernels launched the ordinary way
+    # (no programmatic dependent launch): what chaining them saves
+    mg.use_launch_chaining(False)
+    uc_ms, uc_pms, uc_vc, _ = arm(fast, head_flags, a.steps, a.warmup)
+    mg.use_launch_chaining(True)
+    uc_ms = max_over_ranks(uc_ms)
 
     # the dominant kernel's launches, timed by events (roofline)
     sm_ms, sm_launch, sm_bytes = smoother_pass(a.steps)
@@ -602,8 +653,8 @@ def run_ours(a, rank, world, local_rank):
     # per step H2D of u, v and D2H of u, v, p (the reference's `update host(field[0])`)
     bufs = [api.PinnedArray(n) for _ in range(5)]
     mg.set_flow(Re=a.Re, courant=a.courant)
+    mg.checkpoint_load(start)
     mg.set_initial_guess(head_flags)
-    mg.apply_bc(mgm.BC_LID)
     if a.warmup:
         mg.run_steps(fast, a.warmup)
     bufs[0].array[:] = mg.get_field("u")
@@ -672,6 +723,10 @@ def run_ours(a, rank, world, local_rank):
                                  "note": ("the same steps with the solve's loops driven from the host (one read of "
                                           "the loop flags per Arnoldi step, each V-cycle a graph replay); the "
                                           "headline runs each step as one graph launch")},
+            "unchained_fp32": {"ms_per_step": uc_ms / a.steps, "poisson_ms": uc_pms / a.steps,
+                               "vcycles_per_step": uc_vc / a.steps,
+                               "note": ("the headline steps with the V-cycle's kernels launched without "
+                                        "programmatic dependent launch (mgm_use_launch_chaining(0))")},
             "learned_warm_start": learned,
             "half_operator": half,
             "headline_arm": ("learned warm start (minimal-residual combination of the network's increment and "
@@ -713,6 +768,7 @@ def run_ours(a, rank, world, local_rank):
             cb["convergent_fp64_cpu"] = cs
             line["cpu_baseline"] = cb
     mg.close()
+    shutil.rmtree(tmpdir, ignore_errors=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -372,6 +372,13 @@ MGM_API int mgm_ref_routine(mgm_ctx *ctx, int level, int routine);
  * solves replay each V-cycle from a captured graph.  Results are identical
  * either way. */
 MGM_API int mgm_use_graphs(mgm_ctx *ctx, int enable);
+/* V-cycle kernels after the first of a cycle or smoothing pass launched
+ * with programmatic stream serialisation (enable = 1, default): a kernel's
+ * CTAs may be scheduled while its predecessor's last CTAs finish, and wait
+ * on the device for the predecessor's completion before touching memory, so
+ * the launch latency between the ~100 kernels of a V-cycle overlaps.
+ * enable = 0 launches them the ordinary way.  Results are identical. */
+MGM_API int mgm_use_launch_chaining(mgm_ctx *ctx, int enable);
 /* With graphs on: the whole fractional step as one captured graph (enable =
  * 1, default) -- momentum, divergence, the Poisson solve with its restart and
  * Arnoldi loops as conditional WHILE nodes whose conditions device kernels
@@ -505,6 +512,10 @@ MGM_API int mgm_mpnn_num_params(void);
 MGM_API int mgm_mpnn_params(mgm_ctx *ctx, float *get, const float *set);
 MGM_API int mgm_mpnn_loss_grad(mgm_ctx *ctx, const float *b_hat, const float *p_hat, const float *dp_hat,
                                const float *target, double *loss, float *grads, float *prediction);
+/* The inference pass a step runs (the decoder fused into the last layer,
+ * no activations kept) on normalised host inputs; prediction: n floats. */
+MGM_API int mgm_mpnn_predict(mgm_ctx *ctx, const float *b_hat, const float *p_hat, const float *dp_hat,
+                             float *prediction);
 MGM_API int mgm_mpnn_collect(mgm_ctx *ctx, int mode, int nsteps);
 MGM_API int mgm_mpnn_dataset_size(mgm_ctx *ctx, int *count);
 MGM_API int mgm_mpnn_train(mgm_ctx *ctx, int first, int count, int iters, float lr, unsigned long long seed,

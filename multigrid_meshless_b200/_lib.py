@@ -88,6 +88,7 @@ SIGNATURES = {
     "mgm_step": ([vp, C.c_int, C.POINTER(C.c_double)], C.c_int),
     "mgm_set_solver": ([vp, C.c_double, C.c_int, C.c_int, C.c_double], C.c_int),
     "mgm_use_graphs": ([vp, C.c_int], C.c_int),
+    "mgm_use_launch_chaining": ([vp, C.c_int], C.c_int),
     "mgm_use_step_graph": ([vp, C.c_int], C.c_int),
     "mgm_solve_counters": ([vp, vp, vp, vp], C.c_int),
     "mgm_set_initial_guess": ([vp, C.c_int], C.c_int),
@@ -112,6 +113,7 @@ SIGNATURES = {
     "mgm_mpnn_num_params": ([], C.c_int),
     "mgm_mpnn_params": ([vp, vp, vp], C.c_int),
     "mgm_mpnn_loss_grad": ([vp, vp, vp, vp, vp, C.POINTER(C.c_double), vp, vp], C.c_int),
+    "mgm_mpnn_predict": ([vp, vp, vp, vp, vp], C.c_int),
     "mgm_mpnn_collect": ([vp, C.c_int, C.c_int], C.c_int),
     "mgm_mpnn_dataset_size": ([vp, C.POINTER(C.c_int)], C.c_int),
     "mgm_mpnn_train": ([vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_ulonglong, vp], C.c_int),

@@ -348,6 +348,10 @@ class Multigrid:
     def use_graphs(self, enable=True):
         check(self.L.mgm_use_graphs(self.h, 1 if enable else 0))
 
+    def use_launch_chaining(self, enable=True):
+        """Programmatic dependent launch between the V-cycle's kernels (default on)."""
+        check(self.L.mgm_use_launch_chaining(self.h, 1 if enable else 0))
+
     def solve_counters(self):
         """(V-cycles, restart-cycle starts, solves) of the last run_steps / step."""
         v, c, n = C.c_longlong(), C.c_longlong(), C.c_longlong()

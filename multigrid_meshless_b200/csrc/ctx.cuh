@@ -106,6 +106,7 @@ struct mgm_ctx {
     DBuf<int> hist_ok;
     bool use_tma = false;             // tile-streamed level kernels where a level has them (else 4 rows per thread)
     bool half_operator = false;       // FP32 V-cycle reads the FP16 operator where built
+    bool chain_launches = true;       // V-cycle kernels after the first use programmatic dependent launch
     // compatible right-hand sides (mgm_set_compatible_rhs): the pinned solution
     // for the interior indicator and {rho0(w), rho0(b)} on the device
     bool compat = false, compat_ready = false;

@@ -446,7 +446,7 @@ const T *run_vcycle(mgm_ctx *c, std::vector<SolveLevel<T>> &levels, const Coarse
 {
     cudaStream_t s = c->s;
     if (!c->use_graphs) {
-        vcycle<T>(levels, cs, c->cheb_deg, c->cheb_ratio, s, &c->prof);
+        vcycle<T>(levels, cs, c->cheb_deg, c->cheb_ratio, s, &c->prof, c->chain_launches);
         return levels[0].e;
     }
     auto &G = c->vg[sizeof(T) == 4 ? 1 : 0];
@@ -465,7 +465,7 @@ const T *run_vcycle(mgm_ctx *c, std::vector<SolveLevel<T>> &levels, const Coarse
         const long long launches_before = g_launches;
         MGM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         try {
-            vcycle<T>(cap, cs, c->cheb_deg, c->cheb_ratio, s, c->prof.on ? &c->prof : nullptr);
+            vcycle<T>(cap, cs, c->cheb_deg, c->cheb_ratio, s, c->prof.on ? &c->prof : nullptr, c->chain_launches);
         } catch (...) {
             cudaGraph_t junk = nullptr;
             cudaStreamEndCapture(s, &junk);
@@ -585,7 +585,7 @@ void arnoldi_step(FgRun<T> &R, cudaStream_t s, FgHandles hd, bool captured)
     fg_load<T>(R.n, R.V, R.ld, R.st, R.levels[0].r, s);
     const T *z;
     if (captured) {
-        vcycle<T>(R.levels, R.cs, c->cheb_deg, c->cheb_ratio, s, nullptr);
+        vcycle<T>(R.levels, R.cs, c->cheb_deg, c->cheb_ratio, s, nullptr, c->chain_launches);
         z = R.levels[0].e;
     } else {
         z = run_vcycle<T>(c, R.levels, R.cs);
@@ -662,7 +662,7 @@ void initial_guess(FgRun<T> &R, bool learned, cudaStream_t s)
             combine<double>(n, 1, D1, ld, ks, pd, s);                        // pd = p + D1
             resid64(n, k, L0.idx.p, L0.A64.p, R.b, pd, r0, c->kpart.p, s);    // r0 = b - A (p + D1)
             copy_convert<T>(n, r0, R.levels[0].r, s);
-            const T *e = smooth_from_zero<T>(R.levels[0], c->warm_smooth_steps, c->cheb_ratio, s);
+            const T *e = smooth_from_zero<T>(R.levels[0], c->warm_smooth_steps, c->cheb_ratio, s, c->chain_launches);
             combine<T>(n, 1, e, ld, ks, D1, s);                              // D1 += e
         }
     }
@@ -1908,6 +1908,16 @@ int mgm_use_half_operator(mgm_ctx *c, int enable)
         MGM_CUDA(cudaStreamSynchronize(c->s));
         drop_graphs(c);
         c->half_operator = enable != 0;
+    });
+}
+
+int mgm_use_launch_chaining(mgm_ctx *c, int enable)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+        drop_graphs(c);
+        c->chain_launches = enable != 0;
     });
 }
 

@@ -176,4 +176,60 @@ inline void launch_k(void (*kern)(P...), dim3 grid, dim3 block, size_t smem, cud
     MGM_LAUNCHED();
 }
 
+// Programmatic dependent launch (griddepcontrol, sm_90 and later).  A kernel
+// launched by launch_pdl may have its CTAs scheduled while its predecessor on
+// the stream is still finishing; pdl_enter, its first statement, waits until
+// the predecessor grid has completed and its memory operations are visible,
+// then allows the kernel's own successor to be scheduled early.  Launched
+// the ordinary way, pdl_enter returns at once.  Every kernel launched by
+// launch_pdl calls pdl_enter before it reads or writes any buffer.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <class... P, class... A>
+inline void launch_pdl(void (*kern)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A... args)
+{
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, static_cast<P>(args)...);
+    if (e != cudaSuccess) throw Error{1, std::string("kernel launch (programmatic): ") + cudaGetErrorString(e)};
+    MGM_LAUNCHED();
+}
+
+// The launches of one V-cycle or smoothing pass.  With chaining enabled,
+// a kernel whose predecessor on the stream is a kernel of the same chain is
+// launched by launch_pdl (such kernels begin with pdl_enter); the first
+// launch of a chain, and a launch after an event record (broken()), is an
+// ordinary launch.
+struct Chain {
+    bool enabled = false;
+    bool after_kernel = false;
+    template <class... P, class... A>
+    void operator()(void (*kern)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A... args)
+    {
+        if (enabled && after_kernel) launch_pdl(kern, grid, block, smem, s, args...);
+        else launch_k(kern, grid, block, smem, s, args...);
+        after_kernel = true;
+    }
+    // an ordinary launch of a kernel without pdl_enter inside the chain
+    template <class... P, class... A>
+    void plain(void (*kern)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A... args)
+    {
+        launch_k(kern, grid, block, smem, s, args...);
+        after_kernel = true;
+    }
+    void broken() { after_kernel = false; }
+};
+
 }  // namespace mgm

@@ -136,21 +136,42 @@ __global__ void k_features_ds(int n, const float *bh, const float *ph, const flo
     f[5] = btag[i] ? 1.f : 0.f;
 }
 
-// encoder: warp per node, lane -> features 2l, 2l+1
-__global__ void __launch_bounds__(256) k_encode(int n, const float *feat, const float *P, bf16 *h0, float *z0)
+// encoder: eight lanes per node (hidden features 8l..8l+7, one 16-byte store
+// of h0), four nodes per warp; W_e and c_e (contiguous in P) staged in
+// shared memory.  Each feature's sum is c_e then the inputs in order.
+__global__ void __launch_bounds__(256) k_encode(int n, const float *__restrict__ feat, const float *__restrict__ P,
+                                                bf16 *__restrict__ h0, float *__restrict__ z0)
 {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (w >= n) return;
-    const float *f = feat + (long)w * kFin;
-    const int c = 2 * lane;
-    float a0 = P[P_CE + c], a1 = P[P_CE + c + 1];
+    __shared__ __align__(16) float We[kFin * kH + kH];
+    for (int q = threadIdx.x; q < kFin * kH + kH; q += blockDim.x) We[q] = P[P_WE + q];
+    __syncthreads();
+    const long node = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+    const int c = 8 * (threadIdx.x & 7);
+    if (node >= n) return;
+    float f[kFin], a[8];
+#pragma unroll
+    for (int q = 0; q < kFin; q++) f[q] = __ldg(feat + node * kFin + q);
+#pragma unroll
+    for (int e = 0; e < 8; e++) a[e] = We[P_CE - P_WE + c + e];
 #pragma unroll
     for (int q = 0; q < kFin; q++) {
-        a0 += f[q] * P[P_WE + q * kH + c];
-        a1 += f[q] * P[P_WE + q * kH + c + 1];
+        const float4 w0 = *reinterpret_cast<const float4 *>(&We[q * kH + c]);
+        const float4 w1 = *reinterpret_cast<const float4 *>(&We[q * kH + c + 4]);
+        a[0] += f[q] * w0.x; a[1] += f[q] * w0.y; a[2] += f[q] * w0.z; a[3] += f[q] * w0.w;
+        a[4] += f[q] * w1.x; a[5] += f[q] * w1.y; a[6] += f[q] * w1.z; a[7] += f[q] * w1.w;
     }
-    st_bf2(h0 + (long)w * kH + c, fmaxf(a0, 0.f), fmaxf(a1, 0.f));
-    if (z0) { z0[(long)w * kH + c] = a0; z0[(long)w * kH + c + 1] = a1; }
+    float r[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) r[e] = fmaxf(a[e], 0.f);
+    uint4 u;
+    __nv_bfloat162 *b = reinterpret_cast<__nv_bfloat162 *>(&u);
+#pragma unroll
+    for (int q = 0; q < 4; q++) b[q] = __floats2bfloat162_rn(r[2 * q], r[2 * q + 1]);
+    *reinterpret_cast<uint4 *>(h0 + node * kH + c) = u;
+    if (z0) {
+        *reinterpret_cast<float4 *>(z0 + node * kH + c) = make_float4(a[0], a[1], a[2], a[3]);
+        *reinterpret_cast<float4 *>(z0 + node * kH + c + 4) = make_float4(a[4], a[5], a[6], a[7]);
+    }
 }
 
 __device__ __forceinline__ void mma_bf16(float *c, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
@@ -195,111 +216,170 @@ __device__ __forceinline__ uint4 pack8(const float *f)
     return u;
 }
 
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+
+// shared memory of k_mp_layer: the layer's W^T [64][kPad] and the node tile
+// [kTile][kPad] (BF16; rows padded to 400 bytes so that the eight rows an
+// ldmatrix phase reads fall in distinct 16-byte bank groups)
+constexpr size_t kMpSmem = 2 * (size_t)kTile * kPad * sizeof(bf16);
+
+// Persistent: each CTA stages W^T once, then loops over 64-node tiles.
 __global__ void __launch_bounds__(128) k_mp_layer(int n, int k, const int *__restrict__ cloud,
                                                   const float *__restrict__ lapS, float inv_k,
                                                   const bf16 *__restrict__ h_in, const bf16 *__restrict__ WT,
                                                   const float *__restrict__ bias, bf16 *__restrict__ h_out,
-                                                  float *__restrict__ z_out, bf16 *__restrict__ cat_out)
+                                                  float *__restrict__ z_out, bf16 *__restrict__ cat_out,
+                                                  const float *__restrict__ dec, float *__restrict__ y_out)
 {
-    __shared__ __align__(16) bf16 Xs[kTile][kPad];
+    extern __shared__ __align__(16) unsigned char mp_smem[];
+    bf16(*Ws)[kPad] = reinterpret_cast<bf16(*)[kPad]>(mp_smem);
+    bf16(*Xs)[kPad] = reinterpret_cast<bf16(*)[kPad]>(mp_smem + (size_t)kTile * kPad * sizeof(bf16));
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int grp = lane >> 3, gl = lane & 7;
     const unsigned full = 0xffffffffu;  // rows past n are clamped, so all lanes stay converged
-    const long base = (long)blockIdx.x * kTile;
-    for (int rr = 0; rr < kTile / 16; rr++) {
-        const int row = warp * 16 + rr * 4 + grp;
-        const bool valid = base + row < n;
-        const long i = valid ? base + row : (long)n - 1;
-        float sf[8], mn[8], lp[8];
+    for (int w = tid; w < kH * (kCat / 8); w += blockDim.x) {
+        const int r = w / (kCat / 8), c = w % (kCat / 8);
+        *reinterpret_cast<uint4 *>(&Ws[r][8 * c]) = __ldg(reinterpret_cast<const uint4 *>(WT + r * kCat) + c);
+    }
+    // ldmatrix source rows of this lane: A (tile rows) and B (W^T rows)
+    const int g = lane >> 2, t = lane & 3, r0 = warp * 16;
+    const int q = lane >> 3, rq = lane & 7;
+    const uint32_t a_addr = (uint32_t)__cvta_generic_to_shared(&Xs[r0 + rq + 8 * (q & 1)][8 * (q >> 1)]);
+    // B: matrices (n-tile 2p + (q >> 1), k-half q & 1)
+    const uint32_t b_addr = (uint32_t)__cvta_generic_to_shared(&Ws[8 * (q >> 1) + rq][8 * (q & 1)]);
+    constexpr uint32_t kRowB = kPad * sizeof(bf16);
+    const int ntiles = (n + kTile - 1) / kTile;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long base = (long)tile * kTile;
+        __syncthreads();  // W staged; the previous tile's reads of Xs are done
+        for (int rr = 0; rr < kTile / 16; rr++) {
+            const int row = warp * 16 + rr * 4 + grp;
+            const bool valid = base + row < n;
+            const long i = valid ? base + row : (long)n - 1;
+            float sf[8], mn[8], lp[8];
 #pragma unroll
-        for (int q = 0; q < 8; q++) mn[q] = lp[q] = 0.f;
-        unpack8(__ldg(reinterpret_cast<const uint4 *>(h_in + i * kH + 8 * gl)), sf);
-        // the node's slots gl, gl + 8, ... (k <= 64)
-        int cl[8];
-        float wl[8];
+            for (int e = 0; e < 8; e++) mn[e] = lp[e] = 0.f;
+            unpack8(__ldg(reinterpret_cast<const uint4 *>(h_in + i * kH + 8 * gl)), sf);
+            // the node's slots gl, gl + 8, ... (k <= 64)
+            int cl[8];
+            float wl[8];
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-            const int j = gl + 8 * q;
-            cl[q] = j < k ? __ldg(cloud + i * k + j) : 0;
-            wl[q] = j < k ? __ldg(lapS + i * k + j) : 0.f;
-        }
-#pragma unroll
-        for (int j0 = 0; j0 < 64; j0 += kGather) {
-            if (j0 >= k) break;
-            uint4 v[kGather];
-            float wj[kGather];
-#pragma unroll
-            for (int q = 0; q < kGather; q++) {
-                const int j = j0 + q;
-                if (j >= 64) { wj[q] = 0.f; v[q] = make_uint4(0, 0, 0, 0); continue; }
-                const int cs = __shfl_sync(full, cl[j >> 3], j & 7, 8);
-                wj[q] = __shfl_sync(full, wl[j >> 3], j & 7, 8);
-                v[q] = j < k ? __ldg(reinterpret_cast<const uint4 *>(h_in + (long)cs * kH + 8 * gl))
-                             : make_uint4(0, 0, 0, 0);
+            for (int e = 0; e < 8; e++) {
+                const int j = gl + 8 * e;
+                cl[e] = j < k ? __ldg(cloud + i * k + j) : 0;
+                wl[e] = j < k ? __ldg(lapS + i * k + j) : 0.f;
             }
 #pragma unroll
-            for (int q = 0; q < kGather; q++) {
-                if (j0 + q >= k) break;
-                float f[8];
-                unpack8(v[q], f);
+            for (int j0 = 0; j0 < 64; j0 += kGather) {
+                if (j0 >= k) break;
+                uint4 v[kGather];
+                float wj[kGather];
 #pragma unroll
-                for (int e = 0; e < 8; e++) {
-                    mn[e] += f[e];
-                    lp[e] += wj[q] * f[e];
+                for (int e = 0; e < kGather; e++) {
+                    const int j = j0 + e;
+                    if (j >= 64) { wj[e] = 0.f; v[e] = make_uint4(0, 0, 0, 0); continue; }
+                    const int cs = __shfl_sync(full, cl[j >> 3], j & 7, 8);
+                    wj[e] = __shfl_sync(full, wl[j >> 3], j & 7, 8);
+                    v[e] = j < k ? __ldg(reinterpret_cast<const uint4 *>(h_in + (long)cs * kH + 8 * gl))
+                                 : make_uint4(0, 0, 0, 0);
+                }
+#pragma unroll
+                for (int e = 0; e < kGather; e++) {
+                    if (j0 + e >= k) break;
+                    float f[8];
+                    unpack8(v[e], f);
+#pragma unroll
+                    for (int c = 0; c < 8; c++) {
+                        mn[c] += f[c];
+                        lp[c] += wj[e] * f[c];
+                    }
+                }
+            }
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+                mn[e] *= inv_k;
+                if (!valid) sf[e] = mn[e] = lp[e] = 0.f;
+            }
+            *reinterpret_cast<uint4 *>(&Xs[row][8 * gl]) = pack8(sf);
+            *reinterpret_cast<uint4 *>(&Xs[row][kH + 8 * gl]) = pack8(mn);
+            *reinterpret_cast<uint4 *>(&Xs[row][2 * kH + 8 * gl]) = pack8(lp);
+        }
+        __syncthreads();
+        float acc[8][4];
+#pragma unroll
+        for (int e = 0; e < 8; e++) acc[e][0] = acc[e][1] = acc[e][2] = acc[e][3] = 0.f;
+#pragma unroll
+        for (int ks = 0; ks < kCat / 16; ks++) {
+            const uint32_t kb = ks * 16 * sizeof(bf16);
+            uint32_t a0, a1, a2, a3;
+            ldsm_x4(a_addr + kb, a0, a1, a2, a3);
+#pragma unroll
+            for (int p = 0; p < 4; p++) {
+                uint32_t b0, b1, b2, b3;  // n-tile 2p: (b0, b1); n-tile 2p + 1: (b2, b3)
+                ldsm_x4(b_addr + 16 * p * kRowB + kb, b0, b1, b2, b3);
+                mma_bf16(acc[2 * p], a0, a1, a2, a3, b0, b1);
+                mma_bf16(acc[2 * p + 1], a0, a1, a2, a3, b2, b3);
+            }
+        }
+        float yp[2] = {0.f, 0.f};
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const int col = nt * 8 + 2 * t;
+#pragma unroll
+            for (int hh = 0; hh < 2; hh++) {
+                const int row = r0 + g + 8 * hh;
+                const long i = base + row;
+                if (i >= n) continue;
+                const float z0 = acc[nt][2 * hh] + bias[col], z1 = acc[nt][2 * hh + 1] + bias[col + 1];
+                const float2 res = ld_bf2(&Xs[row][col]);
+                const __nv_bfloat162 o = __floats2bfloat162_rn(fmaxf(z0, 0.f) + res.x, fmaxf(z1, 0.f) + res.y);
+                if (h_out) *reinterpret_cast<__nv_bfloat162 *>(h_out + i * kH + col) = o;
+                if (z_out) { z_out[i * kH + col] = z0; z_out[i * kH + col + 1] = z1; }
+                if (y_out) {
+                    const float2 of = __bfloat1622float2(o);
+                    yp[hh] += of.x * __ldg(dec + P_WD + col) + of.y * __ldg(dec + P_WD + col + 1);
                 }
             }
         }
+        if (y_out) {
+            // decoder: the four lanes of a row hold its 64 features in 16-column
+            // parts; the row's output is their sum plus c_d
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-            mn[q] *= inv_k;
-            if (!valid) sf[q] = mn[q] = lp[q] = 0.f;
+            for (int hh = 0; hh < 2; hh++) {
+                float v = yp[hh];
+                v += __shfl_xor_sync(0xffffffffu, v, 1);
+                v += __shfl_xor_sync(0xffffffffu, v, 2);
+                const long i = base + r0 + g + 8 * hh;
+                if (t == 0 && i < n) y_out[i] = v + __ldg(dec + P_CD);
+            }
         }
-        *reinterpret_cast<uint4 *>(&Xs[row][8 * gl]) = pack8(sf);
-        *reinterpret_cast<uint4 *>(&Xs[row][kH + 8 * gl]) = pack8(mn);
-        *reinterpret_cast<uint4 *>(&Xs[row][2 * kH + 8 * gl]) = pack8(lp);
-    }
-    __syncthreads();
-    const int g = lane >> 2, t = lane & 3, r0 = warp * 16;
-    const uint32_t *W32 = reinterpret_cast<const uint32_t *>(WT);  // [64][96] words
-    float acc[8][4];
-#pragma unroll
-    for (int q = 0; q < 8; q++) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = 0.f;
-#pragma unroll
-    for (int ks = 0; ks < kCat / 16; ks++) {
-        const int k0 = ks * 16;
-        const uint32_t a0 = *reinterpret_cast<const uint32_t *>(&Xs[r0 + g][k0 + 2 * t]);
-        const uint32_t a1 = *reinterpret_cast<const uint32_t *>(&Xs[r0 + g + 8][k0 + 2 * t]);
-        const uint32_t a2 = *reinterpret_cast<const uint32_t *>(&Xs[r0 + g][k0 + 2 * t + 8]);
-        const uint32_t a3 = *reinterpret_cast<const uint32_t *>(&Xs[r0 + g + 8][k0 + 2 * t + 8]);
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++) {
-            const uint32_t b0 = __ldg(W32 + (nt * 8 + g) * (kCat / 2) + (k0 >> 1) + t);
-            const uint32_t b1 = __ldg(W32 + (nt * 8 + g) * (kCat / 2) + (k0 >> 1) + t + 4);
-            mma_bf16(acc[nt], a0, a1, a2, a3, b0, b1);
+        if (cat_out) {
+            for (int w = tid; w < kTile * (kCat / 2); w += blockDim.x) {
+                const int r = w / (kCat / 2), cw = w % (kCat / 2);
+                if (base + r < n)
+                    reinterpret_cast<uint32_t *>(cat_out + (base + r) * kCat)[cw] =
+                        reinterpret_cast<const uint32_t *>(&Xs[r][0])[cw];
+            }
         }
     }
-#pragma unroll
-    for (int nt = 0; nt < 8; nt++) {
-        const int col = nt * 8 + 2 * t;
-#pragma unroll
-        for (int hh = 0; hh < 2; hh++) {
-            const int row = r0 + g + 8 * hh;
-            const long i = base + row;
-            if (i >= n) continue;
-            const float z0 = acc[nt][2 * hh] + bias[col], z1 = acc[nt][2 * hh + 1] + bias[col + 1];
-            const float2 res = ld_bf2(&Xs[row][col]);
-            st_bf2(h_out + i * kH + col, fmaxf(z0, 0.f) + res.x, fmaxf(z1, 0.f) + res.y);
-            if (z_out) { z_out[i * kH + col] = z0; z_out[i * kH + col + 1] = z1; }
-        }
-    }
-    if (cat_out) {
-        for (int w = tid; w < kTile * (kCat / 2); w += blockDim.x) {
-            const int r = w / (kCat / 2), cw = w % (kCat / 2);
-            if (base + r < n)
-                reinterpret_cast<uint32_t *>(cat_out + (base + r) * kCat)[cw] =
-                    reinterpret_cast<const uint32_t *>(&Xs[r][0])[cw];
-        }
-    }
+}
+
+// grid of k_mp_layer: resident CTAs on every SM, at most one per tile
+int mp_layer_grid(int n)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    MGM_CUDA(cudaGetDevice(&dev));
+    MGM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MGM_CUDA(cudaFuncSetAttribute(k_mp_layer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMpSmem));
+    MGM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mp_layer, 128, kMpSmem));
+    per_sm = std::max(per_sm, 1);
+    const int tiles = (n + kTile - 1) / kTile;
+    return std::max(1, std::min(tiles, sms * per_sm));
 }
 
 // decoder: warp per node
@@ -644,16 +724,22 @@ static void forward(MpnnState &M, bool train, cudaStream_t s)
 {
     const int n = M.n;
     const float *P = M.params.p;
-    k_encode<<<warp_blocks(n), 256, 0, s>>>(n, M.feat.p, P, M.h[0].p, train ? M.z[0].p : nullptr);
+    k_encode<<<blocks_for((long)n * 8, 256), 256, 0, s>>>(n, M.feat.p, P, M.h[0].p, train ? M.z[0].p : nullptr);
     MGM_LAUNCHED();
     for (int l = 0; l < kLayers; l++) {
-        k_mp_layer<<<blocks_for(n, kTile), 128, 0, s>>>(n, M.k, M.cloud, M.lapS.p, 1.f / M.k, M.h[l].p, M.WT[l].p,
-                                                       P + P_L0 + l * kLayerParams + kCat * kH, M.h[l + 1].p,
-                                                       train ? M.z[l + 1].p : nullptr, train ? M.cat[l].p : nullptr);
+        // inference: the last layer decodes in its epilogue and stores no h4
+        const bool dec = !train && l == kLayers - 1;
+        k_mp_layer<<<mp_layer_grid(n), 128, kMpSmem, s>>>(n, M.k, M.cloud, M.lapS.p, 1.f / M.k, M.h[l].p, M.WT[l].p,
+                                                       P + P_L0 + l * kLayerParams + kCat * kH,
+                                                       dec ? nullptr : M.h[l + 1].p, train ? M.z[l + 1].p : nullptr,
+                                                       train ? M.cat[l].p : nullptr, dec ? P : nullptr,
+                                                       dec ? M.y.p : nullptr);
         MGM_LAUNCHED();
     }
-    k_decode<<<warp_blocks(n), 256, 0, s>>>(n, M.h[kLayers].p, P, M.y.p);
-    MGM_LAUNCHED();
+    if (train) {
+        k_decode<<<warp_blocks(n), 256, 0, s>>>(n, M.h[kLayers].p, P, M.y.p);
+        MGM_LAUNCHED();
+    }
 }
 
 // loss w_mse * mean (y - t)^2 + w_res * |A (t - y)|^2 / |A t|^2 and dL/dy; loss -> M.scal[2]
@@ -923,6 +1009,30 @@ int mgm_mpnn_loss_grad(mgm_ctx *c, const float *b_hat, const float *p_hat, const
         if (loss) *loss = ls;
         if (grads) M.grads.download(grads, kNumParams, s);
         if (prediction) M.y.download(prediction, M.n, s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+        return MGM_OK;
+    } catch (const Error &e) {
+        set_error(e.code, e.msg);
+        return e.code;
+    }
+}
+
+// the network's inference pass (the one a step runs) on normalised inputs
+int mgm_mpnn_predict(mgm_ctx *c, const float *b_hat, const float *p_hat, const float *dp_hat, float *prediction)
+{
+    try {
+        MpnnState &M = state(c);
+        MGM_REQUIRE(b_hat && p_hat && dp_hat && prediction, "mgm_mpnn_predict: null argument");
+        cudaStream_t s = c->s;
+        Level &L = c->L[0];
+        DBuf<float> bh, ph, dh;
+        bh.upload(b_hat, M.n, s);
+        ph.upload(p_hat, M.n, s);
+        dh.upload(dp_hat, M.n, s);
+        k_features_ds<<<blocks_for(M.n, 256), 256, 0, s>>>(M.n, bh.p, ph.p, dh.p, L.x.p, L.y.p, L.btag.p, M.feat.p);
+        MGM_LAUNCHED();
+        forward(M, false, s);
+        M.y.download(prediction, M.n, s);
         MGM_CUDA(cudaStreamSynchronize(s));
         return MGM_OK;
     } catch (const Error &e) {

@@ -43,6 +43,7 @@ template <class T>
 __global__ void __launch_bounds__(256) k_start_e(int n, const uint8_t *__restrict__ btag, const T *__restrict__ dinv,
                                                  const T *__restrict__ r, T *__restrict__ e)
 {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) e[i] = btag[i] ? r[i] * dinv[i] : T(0);
 }
@@ -57,6 +58,7 @@ __global__ void __launch_bounds__(256) k_bnd_exact(int nbl, const int *__restric
                                                    const T *__restrict__ dinv, const T *__restrict__ r,
                                                    T *__restrict__ e)
 {
+    pdl_enter();
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (w >= nbl) return;
     const int i = list[w];
@@ -74,6 +76,7 @@ __global__ void __launch_bounds__(256) k_cheb(int n, int ld, int k, const int *_
                                               const T *__restrict__ r, const T *__restrict__ e, T *__restrict__ eout,
                                               T *__restrict__ d, T c1, T c2, int first)
 {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const T ei = e[i];
@@ -90,6 +93,7 @@ __global__ void __launch_bounds__(256) k_residual(int n, int ld, int k, const in
                                                   const T *__restrict__ A, const uint8_t *__restrict__ btag,
                                                   const T *__restrict__ r, const T *__restrict__ e, T *__restrict__ q)
 {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (btag[i]) { q[i] = T(0); return; }
@@ -102,6 +106,7 @@ __global__ void __launch_bounds__(256) k_restrict(int n, int k, const int *__res
                                                   const uint8_t *__restrict__ btag, const T *__restrict__ qf,
                                                   T *__restrict__ rc)
 {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (btag[i] || i == 0) { rc[i] = T(0); return; }
@@ -113,6 +118,7 @@ template <class T>
 __global__ void __launch_bounds__(256) k_prolong(int n, int k, const int *__restrict__ pidx, const T *__restrict__ pw,
                                                  const T *__restrict__ ec, T *__restrict__ ef)
 {
+    pdl_enter();
     __shared__ T shift;
     if (threadIdx.x == 0) {
         T s = T(0);
@@ -194,6 +200,7 @@ __global__ void __launch_bounds__(256) k_level_c1(int n, int ld, int k, const sh
                                                   const T *__restrict__ e, T *__restrict__ out,
                                                   T *__restrict__ d, T c1, T c2, int first)
 {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (btag[i]) {
@@ -223,6 +230,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) k_level_v4(
     const uint8_t *__restrict__ btag, const T *__restrict__ r, const T *__restrict__ e, T *__restrict__ out,
     T *__restrict__ d, T c1, T c2, int first)
 {
+    pdl_enter();
     const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
     if (i0 >= n) return;
     T s[4] = {T(0), T(0), T(0), T(0)};
@@ -299,6 +307,7 @@ __global__ void __launch_bounds__(256, 4) k_level_h4(int n, int ld, int k, const
                                                   float *__restrict__ out, float *__restrict__ d, float c1, float c2,
                                                   int first)
 {
+    pdl_enter();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int ib = (t >> 5) * 128 + (t & 31);   // rows ib + 32 v, v = 0..3
     if (ib >= n) return;
@@ -349,21 +358,22 @@ __global__ void __launch_bounds__(256, 4) k_level_h4(int n, int ld, int k, const
 }
 
 template <int MODE, class T>
-static void launch_compact(const SolveLevel<T> &L, const T *e, T *out, T c1, T c2, int first, cudaStream_t s)
+static void launch_compact(const SolveLevel<T> &L, const T *e, T *out, T c1, T c2, int first, cudaStream_t s,
+                           Chain &launch)
 {
     if constexpr (sizeof(T) == 4) {
         if (L.W16) {
-            launch_k(k_level_h4<MODE>, blocks_for(L.ldi / 4, 256), 256, 0, s, L.n, L.ldi, L.k, L.W16, L.dinv, L.btag,
+            launch(k_level_h4<MODE>, blocks_for(L.ldi / 4, 256), 256, 0, s, L.n, L.ldi, L.k, L.W16, L.dinv, L.btag,
                      L.r, e, out, L.d, c1, c2, first);
             return;
         }
     }
     if (L.n >= kVecMinRows)
-        launch_k(k_level_v4<MODE, T>, blocks_for((L.n + 3) / 4, 256), 256, 0, s, L.n, L.ld, L.k, L.off, L.A, L.dinv,
-                 L.btag, L.r, e, out, L.d, c1, c2, first);
+        launch(k_level_v4<MODE, T>, blocks_for((L.n + 3) / 4, 256), 256, 0, s, L.n, L.ld, L.k, L.off, L.A, L.dinv,
+               L.btag, L.r, e, out, L.d, c1, c2, first);
     else
-        launch_k(k_level_c1<MODE, T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.ld, L.k, L.off, L.A, L.dinv, L.btag,
-                 L.r, e, out, L.d, c1, c2, first);
+        launch(k_level_c1<MODE, T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.ld, L.k, L.off, L.A, L.dinv, L.btag,
+               L.r, e, out, L.d, c1, c2, first);
 }
 
 template <class T>
@@ -372,6 +382,7 @@ __global__ void __launch_bounds__(256) k_restrict_o(int n, int k, const short *_
                                                     const uint8_t *__restrict__ btag, const T *__restrict__ qf,
                                                     T *__restrict__ rc)
 {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (btag[i] || i == 0) { rc[i] = T(0); return; }
@@ -383,6 +394,7 @@ __global__ void __launch_bounds__(256) k_prolong_o(int n, int k, const short *__
                                                    const int *__restrict__ base, const T *__restrict__ pw,
                                                    const T *__restrict__ ec, T *__restrict__ ef)
 {
+    pdl_enter();
     __shared__ T shift;
     if (threadIdx.x == 0) shift = ell_row_dot_o(off, pw, ec, n, k, 0, base[0]);
     __syncthreads();
@@ -672,19 +684,19 @@ static int tiled_grid(K kernel, int n, size_t smem)
 
 template <int MODE>
 static void launch_tiled(const SolveLevel<float> &L, const float *e, float *out, float c1, float c2, int first,
-                         cudaStream_t s)
+                         cudaStream_t s, Chain &launch)
 {
     const size_t smem = 2 * tile_stage_bytes(L.k);
     if (L.k <= 32) {
         MGM_CUDA(cudaFuncSetAttribute(k_level_tiled_r<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(2 * tile_stage_bytes(32))));
-        launch_k(k_level_tiled_r<MODE>, tiled_grid(k_level_tiled_r<MODE>, L.n, smem), kTileRows, smem, s, L.n, L.k,
-                 L.offt, L.At, L.dinv, L.btag, L.r, e, out, L.d, c1, c2, first, L.tma_err);
+        launch.plain(k_level_tiled_r<MODE>, tiled_grid(k_level_tiled_r<MODE>, L.n, smem), kTileRows, smem, s, L.n,
+                     L.k, L.offt, L.At, L.dinv, L.btag, L.r, e, out, L.d, c1, c2, first, L.tma_err);
     } else {
         MGM_CUDA(cudaFuncSetAttribute(k_level_tiled<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(2 * tile_stage_bytes(kTileMaxK))));
-        launch_k(k_level_tiled<MODE>, tiled_grid(k_level_tiled<MODE>, L.n, smem), kTileRows, smem, s, L.n, L.k,
-                 L.offt, L.At, L.dinv, L.btag, L.r, e, out, L.d, c1, c2, first, L.tma_err);
+        launch.plain(k_level_tiled<MODE>, tiled_grid(k_level_tiled<MODE>, L.n, smem), kTileRows, smem, s, L.n, L.k,
+                     L.offt, L.At, L.dinv, L.btag, L.r, e, out, L.d, c1, c2, first, L.tma_err);
     }
 }
 
@@ -693,6 +705,7 @@ template <class T>
 __global__ void __launch_bounds__(256) k_dense_solve(int n, const T *__restrict__ inv, const T *__restrict__ r,
                                                      T *__restrict__ e)
 {
+    pdl_enter();
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= n) return;
     const T *row = inv + (long)warp * n;
@@ -744,16 +757,16 @@ SmootherProfile::~SmootherProfile()
 
 template <class T>
 static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, cudaStream_t s,
-                   SmootherProfile *prof)
+                   SmootherProfile *prof, Chain &launch)
 {
     const double lM = 1.05 * L.lmax, lm = L.lmax / ratio;
     const double th = 0.5 * (lM + lm), de = 0.5 * (lM - lm), sig = th / de;
     double rho = 1.0 / sig;
     const int nb = blocks_for(L.n, 256), nbb = blocks_for((long)L.nb_list * 32, 256);
     if (zero_start)
-        launch_k(k_start_e<T>, nb, 256, 0, s, L.n, L.btag, L.dinv, L.r, L.e);
+        launch(k_start_e<T>, nb, 256, 0, s, L.n, L.btag, L.dinv, L.r, L.e);
     else
-        launch_k(k_bnd_exact<T>, nbb, 256, 0, s, L.nb_list, L.bnd_list, L.k, L.bnd_idx, L.bnd_A, L.dinv, L.r, L.e);
+        launch(k_bnd_exact<T>, nbb, 256, 0, s, L.nb_list, L.bnd_list, L.k, L.bnd_idx, L.bnd_A, L.dinv, L.r, L.e);
     for (int step = 0; step < degree; step++) {
         double c1 = 0, c2;
         if (step == 0) c2 = 1.0 / th;
@@ -763,90 +776,100 @@ static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, 
             c2 = 2.0 * rn / de;
             rho = rn;
         }
-        if (prof) prof->mark(s);
+        if (prof) {
+            prof->mark(s);
+            launch.broken();
+        }
         bool done = false;
         if constexpr (sizeof(T) == 4) {
             if (L.At) {
-                launch_tiled<0>(L, L.e, L.e2, (float)c1, (float)c2, step == 0 ? 1 : 0, s);
+                launch_tiled<0>(L, L.e, L.e2, (float)c1, (float)c2, step == 0 ? 1 : 0, s, launch);
                 done = true;
             }
         }
         if (done) {
         } else if (L.off) {
-            launch_compact<0, T>(L, L.e, L.e2, (T)c1, (T)c2, step == 0 ? 1 : 0, s);
+            launch_compact<0, T>(L, L.e, L.e2, (T)c1, (T)c2, step == 0 ? 1 : 0, s, launch);
         } else {
-            launch_k(k_cheb<T>, nb, 256, 0, s, L.n, L.ld, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d,
-                     (T)c1, (T)c2, step == 0 ? 1 : 0);
+            launch(k_cheb<T>, nb, 256, 0, s, L.n, L.ld, L.k, L.idx, L.A, L.dinv, L.btag, L.r, L.e, L.e2, L.d, (T)c1,
+                   (T)c2, step == 0 ? 1 : 0);
         }
-        if (prof) prof->mark(s);
+        if (prof) {
+            prof->mark(s);
+            launch.broken();
+        }
         std::swap(L.e, L.e2);
-        launch_k(k_bnd_exact<T>, nbb, 256, 0, s, L.nb_list, L.bnd_list, L.k, L.bnd_idx, L.bnd_A, L.dinv, L.r, L.e);
+        launch(k_bnd_exact<T>, nbb, 256, 0, s, L.nb_list, L.bnd_list, L.k, L.bnd_idx, L.bnd_A, L.dinv, L.r, L.e);
     }
 }
 
 template <class T>
 static void vcycle_rec(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int l, int deg, double ratio,
-                       cudaStream_t s, SmootherProfile *prof)
+                       cudaStream_t s, SmootherProfile *prof, Chain &launch)
 {
     SmootherProfile *lp = (l == 0 && prof && prof->on) ? prof : nullptr;
     SolveLevel<T> &L = Ls[l];
     const int nl = (int)Ls.size();
     if (l == nl - 1) {
-        launch_k(k_dense_solve<T>, blocks_for((long)L.n * 32, 256), 256, 0, s, cs.n, cs.inv, L.r, L.e);
+        launch(k_dense_solve<T>, blocks_for((long)L.n * 32, 256), 256, 0, s, cs.n, cs.inv, L.r, L.e);
         return;
     }
-    smooth(L, deg, ratio, true, s, lp);  // from e = 0
+    smooth(L, deg, ratio, true, s, lp, launch);  // from e = 0
     SolveLevel<T> &C = Ls[l + 1];
     bool tiled = false;
     if constexpr (sizeof(T) == 4) {
         if (L.At) {
-            launch_tiled<1>(L, L.e, L.q, 0.f, 0.f, 0, s);
+            launch_tiled<1>(L, L.e, L.q, 0.f, 0.f, 0, s, launch);
             tiled = true;
         }
     }
     if (tiled) {
     } else if (L.off) {
-        launch_compact<1, T>(L, L.e, L.q, T(0), T(0), 0, s);
+        launch_compact<1, T>(L, L.e, L.q, T(0), T(0), 0, s, launch);
     } else {
-        launch_k(k_residual<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.ld, L.k, L.idx, L.A, L.btag, L.r, L.e, L.q);
+        launch(k_residual<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.ld, L.k, L.idx, L.A, L.btag, L.r, L.e, L.q);
     }
     if (C.r_off)
-        launch_k(k_restrict_o<T>, blocks_for(C.n, 256), 256, 0, s, C.n, C.kr, C.r_off, C.r_base, C.r_w, C.btag, L.q,
-                 C.r);
+        launch(k_restrict_o<T>, blocks_for(C.n, 256), 256, 0, s, C.n, C.kr, C.r_off, C.r_base, C.r_w, C.btag, L.q,
+               C.r);
     else
-        launch_k(k_restrict<T>, blocks_for(C.n, 256), 256, 0, s, C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
-    vcycle_rec(Ls, cs, l + 1, deg, ratio, s, prof);
+        launch(k_restrict<T>, blocks_for(C.n, 256), 256, 0, s, C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
+    vcycle_rec(Ls, cs, l + 1, deg, ratio, s, prof, launch);
     if (L.p_off) {
-        launch_k(k_prolong_o<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.kp, L.p_off, L.p_base, L.p_w,
-                 (const T *)C.e, L.e);
+        launch(k_prolong_o<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.kp, L.p_off, L.p_base, L.p_w, (const T *)C.e,
+               L.e);
     } else {
-        launch_k(k_prolong<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.kp, L.p_idx, L.p_w, (const T *)C.e, L.e);
+        launch(k_prolong<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.kp, L.p_idx, L.p_w, (const T *)C.e, L.e);
     }
-    smooth(L, deg, ratio, false, s, lp);
+    smooth(L, deg, ratio, false, s, lp, launch);
 }
 
 template <class T>
 void vcycle(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int cheb_degree, double cheb_ratio,
-            cudaStream_t s, SmootherProfile *prof)
+            cudaStream_t s, SmootherProfile *prof, bool chain)
 {
-    vcycle_rec(Ls, cs, 0, cheb_degree, cheb_ratio, s, prof);
+    Chain launch;
+    launch.enabled = chain;
+    vcycle_rec(Ls, cs, 0, cheb_degree, cheb_ratio, s, prof, launch);
 }
 
 // Chebyshev smoothing of A e = r on one level from e = 0 (r already in L.r);
 // returns the buffer holding e.
 template <class T>
-const T *smooth_from_zero(SolveLevel<T> &L, int degree, double ratio, cudaStream_t s)
+const T *smooth_from_zero(SolveLevel<T> &L, int degree, double ratio, cudaStream_t s, bool chain)
 {
-    smooth(L, degree, ratio, true, s, nullptr);  // from e = 0
+    Chain launch;
+    launch.enabled = chain;
+    smooth(L, degree, ratio, true, s, nullptr, launch);  // from e = 0
     return L.e;
 }
-template const double *smooth_from_zero<double>(SolveLevel<double> &, int, double, cudaStream_t);
-template const float *smooth_from_zero<float>(SolveLevel<float> &, int, double, cudaStream_t);
+template const double *smooth_from_zero<double>(SolveLevel<double> &, int, double, cudaStream_t, bool);
+template const float *smooth_from_zero<float>(SolveLevel<float> &, int, double, cudaStream_t, bool);
 
 template void vcycle<double>(std::vector<SolveLevel<double>> &, const CoarseSolve<double> &, int, double, cudaStream_t,
-                             SmootherProfile *);
+                             SmootherProfile *, bool);
 template void vcycle<float>(std::vector<SolveLevel<float>> &, const CoarseSolve<float> &, int, double, cudaStream_t,
-                            SmootherProfile *);
+                            SmootherProfile *, bool);
 
 // ---------------------------------------------------------------------------
 // spectral radius of D^-1 A restricted to interior rows (power iteration)

@@ -132,11 +132,13 @@ struct SmootherProfile {
 };
 
 template <class T>
+// chain: launch the kernels after the first with programmatic stream
+// serialisation (Chain in mgm_internal.cuh)
 void vcycle(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int cheb_degree, double cheb_ratio,
-            cudaStream_t s, SmootherProfile *prof = nullptr);
+            cudaStream_t s, SmootherProfile *prof = nullptr, bool chain = false);
 template <class T>
 void estimate_lmax(SolveLevel<T> &L, cudaStream_t s);
 template <class T>
-const T *smooth_from_zero(SolveLevel<T> &L, int degree, double ratio, cudaStream_t s);
+const T *smooth_from_zero(SolveLevel<T> &L, int degree, double ratio, cudaStream_t s, bool chain = false);
 
 }  // namespace mgm

@@ -263,17 +263,21 @@ def test_step_graph_matches_host_driven_steps(cavity):
     """A fractional step as ONE graph launch (the solve's restart and Arnoldi
     loops as conditional WHILE nodes set by device kernels) gives the bits of
     the host-driven solve (host reads the loop flags, V-cycle graphs) and of
-    fully eager launches: fields after every step, V-cycle counts, steady
-    error; through mgm_run_steps and mgm_step."""
+    fully eager launches, with the V-cycle's kernels chained by programmatic
+    dependent launch (default) or launched the ordinary way: fields after
+    every step, V-cycle counts, steady error; through mgm_run_steps and
+    mgm_step."""
     mg = cavity
     mg.set_flow(Re=100.0, courant=0.5)
     mg.set_solver(rel_tol=1e-8, max_iters=80)
     try:
         for mode in (mgm.MODE_FP64, mgm.MODE_FP32_IR):
             runs = []
-            for graphs, step_graph in ((True, True), (True, False), (False, False)):
+            for graphs, step_graph, chain in ((True, True, True), (True, True, False), (True, False, True),
+                                              (True, False, False), (False, False, True)):
                 mg.use_graphs(graphs)
                 mg.use_step_graph(step_graph)
+                mg.use_launch_chaining(chain)
                 mg.apply_bc(mgm.BC_LID)
                 out = []
                 for rep in range(2):  # second replay of the same step graph
@@ -292,6 +296,7 @@ def test_step_graph_matches_host_driven_steps(cavity):
     finally:
         mg.use_graphs(True)
         mg.use_step_graph(True)
+        mg.use_launch_chaining(True)
 
 
 def test_step_graph_reports_unconverged_solve(cavity):
