@@ -379,6 +379,18 @@ MGM_API int mgm_use_graphs(mgm_ctx *ctx, int enable);
  * the launch latency between the ~100 kernels of a V-cycle overlaps.
  * enable = 0 launches them the ordinary way.  Results are identical. */
 MGM_API int mgm_use_launch_chaining(mgm_ctx *ctx, int enable);
+/* The levels below 65,536 rows (latency-bound: about 17 short kernels per
+ * level per V-cycle) run as ONE cooperative launch per V-cycle, one CTA per
+ * SM, a grid barrier between dependent passes (enable = 1, default);
+ * enable = 0 launches every operation of those levels as its own kernel.
+ * Results are identical.  The barrier's wait is bounded: when it runs out
+ * the solve returns MGM_ERR_TIMEOUT. */
+MGM_API int mgm_use_fused_coarse(mgm_ctx *ctx, int enable);
+/* 1 when the fused coarse V-cycle can run here (after mgm_setup: a CTA fits
+ * on an SM and the driver accepts a cooperative kernel inside a conditional
+ * graph node); 0: every level runs per-operation kernels whatever
+ * mgm_use_fused_coarse says. */
+MGM_API int mgm_fused_coarse_available(mgm_ctx *ctx, int *available);
 /* With graphs on: the whole fractional step as one captured graph (enable =
  * 1, default) -- momentum, divergence, the Poisson solve with its restart and
  * Arnoldi loops as conditional WHILE nodes whose conditions device kernels

@@ -352,6 +352,15 @@ class Multigrid:
         """Programmatic dependent launch between the V-cycle's kernels (default on)."""
         check(self.L.mgm_use_launch_chaining(self.h, 1 if enable else 0))
 
+    def use_fused_coarse(self, enable=True):
+        """The small levels' V-cycle as one cooperative launch (default on)."""
+        check(self.L.mgm_use_fused_coarse(self.h, 1 if enable else 0))
+
+    def fused_coarse_available(self):
+        v = C.c_int()
+        check(self.L.mgm_fused_coarse_available(self.h, C.byref(v)))
+        return bool(v.value)
+
     def solve_counters(self):
         """(V-cycles, restart-cycle starts, solves) of the last run_steps / step."""
         v, c, n = C.c_longlong(), C.c_longlong(), C.c_longlong()

@@ -428,6 +428,81 @@ namespace {
 
 void drop_step_graphs(mgm_ctx *c);
 
+// Whether a cooperative kernel may sit in a conditional node's body graph
+// (the step graph puts the fused coarse V-cycle there): one is captured into
+// a WHILE body (condition 0) and the graph instantiated, never launched.
+bool cooperative_in_conditional_ok(mgm_ctx *c)
+{
+    cudaStream_t s = c->s, bs = c->s_body[0];
+    bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        return false;
+    }
+    cudaGraph_t g = nullptr, body = nullptr;
+    cudaStreamCaptureStatus cst;
+    unsigned long long id = 0;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraphConditionalHandle h;
+    ok = cudaStreamGetCaptureInfo(s, &cst, &id, &g, &deps, &ndeps) == cudaSuccess && g &&
+         cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        ok = cudaGraphAddNode(&node, g, deps, ndeps, &np) == cudaSuccess &&
+             cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies) == cudaSuccess;
+        if (ok) body = np.conditional.phGraph_out[0];
+    }
+    if (ok && cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+                  cudaSuccess) {
+        const bool launched = launch_coop_probe(bs) == cudaSuccess;
+        cudaGraph_t out = nullptr;
+        ok = cudaStreamEndCapture(bs, &out) == cudaSuccess && launched;
+    } else {
+        ok = false;
+    }
+    cudaGraph_t whole = nullptr;
+    const bool ended = cudaStreamEndCapture(s, &whole) == cudaSuccess;
+    cudaGraphExec_t x = nullptr;
+    ok = ok && ended && whole && cudaGraphInstantiate(&x, whole, 0) == cudaSuccess;
+    if (x) cudaGraphExecDestroy(x);
+    if (whole) cudaGraphDestroy(whole);
+    cudaGetLastError();  // a refused capture leaves no sticky error; clear the last one
+    return ok;
+}
+
+FusedCtl fused_ctl(mgm_ctx *c)
+{
+    FusedCtl f;
+    f.on = c->fused_coarse && c->fused_blocks > 0;
+    f.blocks = c->fused_blocks;
+    f.bar = c->fused_bar.p;
+    f.err = c->tma_err.p;
+    return f;
+}
+
+// a level kernel's bounded wait ran out (tile-streamed copies, the fused
+// coarse V-cycle's grid barrier): clear the flags and report
+void check_wait_flags(mgm_ctx *c, cudaStream_t s)
+{
+    if (!c->tma_err.p) return;
+    int h_err = 0;
+    c->tma_err.download(&h_err, 1, s);
+    MGM_CUDA(cudaStreamSynchronize(s));
+    if (h_err) {
+        c->tma_err.zero(s);
+        c->fused_bar.zero(s);
+        MGM_CUDA(cudaStreamSynchronize(s));
+        throw Error{MGM_ERR_TIMEOUT, "Poisson solve: a level kernel's bounded wait ran out (tile copies or the "
+                                     "fused coarse V-cycle's grid barrier)"};
+    }
+}
+
 void drop_graphs(mgm_ctx *c)
 {
     drop_step_graphs(c);
@@ -446,7 +521,8 @@ const T *run_vcycle(mgm_ctx *c, std::vector<SolveLevel<T>> &levels, const Coarse
 {
     cudaStream_t s = c->s;
     if (!c->use_graphs) {
-        vcycle<T>(levels, cs, c->cheb_deg, c->cheb_ratio, s, &c->prof, c->chain_launches);
+        const FusedCtl fc = fused_ctl(c);
+        vcycle<T>(levels, cs, c->cheb_deg, c->cheb_ratio, s, &c->prof, c->chain_launches, &fc);
         return levels[0].e;
     }
     auto &G = c->vg[sizeof(T) == 4 ? 1 : 0];
@@ -465,7 +541,8 @@ const T *run_vcycle(mgm_ctx *c, std::vector<SolveLevel<T>> &levels, const Coarse
         const long long launches_before = g_launches;
         MGM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         try {
-            vcycle<T>(cap, cs, c->cheb_deg, c->cheb_ratio, s, c->prof.on ? &c->prof : nullptr, c->chain_launches);
+            const FusedCtl fc = fused_ctl(c);
+            vcycle<T>(cap, cs, c->cheb_deg, c->cheb_ratio, s, c->prof.on ? &c->prof : nullptr, c->chain_launches, &fc);
         } catch (...) {
             cudaGraph_t junk = nullptr;
             cudaStreamEndCapture(s, &junk);
@@ -585,7 +662,8 @@ void arnoldi_step(FgRun<T> &R, cudaStream_t s, FgHandles hd, bool captured)
     fg_load<T>(R.n, R.V, R.ld, R.st, R.levels[0].r, s);
     const T *z;
     if (captured) {
-        vcycle<T>(R.levels, R.cs, c->cheb_deg, c->cheb_ratio, s, nullptr, c->chain_launches);
+        const FusedCtl fc = fused_ctl(c);
+        vcycle<T>(R.levels, R.cs, c->cheb_deg, c->cheb_ratio, s, nullptr, c->chain_launches, &fc);
         z = R.levels[0].e;
     } else {
         z = run_vcycle<T>(c, R.levels, R.cs);
@@ -727,17 +805,7 @@ void fgmres(mgm_ctx *c, const double *b, double *p, bool captured = false, long 
     } while (read_fg_head(c).go_outer);
     fg_final(R.st, s);
     const FgState &h = read_fg_head(c);
-    if constexpr (sizeof(T) == 4) {
-        if (c->tma_err.p) {
-            int h_err = 0;
-            c->tma_err.download(&h_err, 1, s);
-            MGM_CUDA(cudaStreamSynchronize(s));
-            if (h_err) {
-                c->tma_err.zero(s);
-                throw Error{MGM_ERR_TIMEOUT, "Poisson solve: a tile-streamed level kernel timed out waiting for its copies"};
-            }
-        }
-    }
+    check_wait_flags(c, s);
     c->last_iters = h.vcycles;  // V-cycles (learned directions are not V-cycles)
     c->last_relres = h.relres;
     c->last_learned_alpha = h.alpha;
@@ -920,15 +988,7 @@ double run_steps_device(mgm_ctx *c, int mode, int nsteps)
         MGM_CUDA(cudaStreamSynchronize(c->s));
         const FgState &h = read_fg_head(c);
         g_launches += (long long)nsteps * G.k_top + h.cycles_total * G.k_outer + h.vcycles_total * G.k_inner;
-        if (c->tma_err.p) {
-            int h_err = 0;
-            c->tma_err.download(&h_err, 1, c->s);
-            MGM_CUDA(cudaStreamSynchronize(c->s));
-            if (h_err) {
-                c->tma_err.zero(c->s);
-                throw Error{MGM_ERR_TIMEOUT, "Poisson solve: a tile-streamed level kernel timed out waiting for its copies"};
-            }
-        }
+        check_wait_flags(c, c->s);
         if (h.err_any & 1) throw Error{MGM_ERR_DIVERGED, "Poisson solve: non-finite residual"};
         if (h.err_any & 2) throw Error{MGM_ERR_DIVERGED, "Poisson solve did not reach the tolerance"};
         c->last_iters = h.vcycles;
@@ -1476,6 +1536,11 @@ void prepare_solver(mgm_ctx *c)
     c->scal.alloc(8);
     c->tma_err.alloc(1);
     c->tma_err.zero(s);
+    c->fused_bar.alloc(2);
+    c->fused_bar.zero(s);
+    c->fused_blocks = fused_vcycle_blocks();
+    MGM_CUDA(cudaStreamSynchronize(s));
+    if (!cooperative_in_conditional_ok(c)) c->fused_blocks = 0;  // the per-operation kernels then
     alloc_solver_buffers(c);
     MGM_CUDA(cudaStreamSynchronize(s));
     c->setup_done = true;
@@ -1908,6 +1973,25 @@ int mgm_use_half_operator(mgm_ctx *c, int enable)
         MGM_CUDA(cudaStreamSynchronize(c->s));
         drop_graphs(c);
         c->half_operator = enable != 0;
+    });
+}
+
+int mgm_use_fused_coarse(mgm_ctx *c, int enable)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_CUDA(cudaStreamSynchronize(c->s));
+        drop_graphs(c);
+        c->fused_coarse = enable != 0;
+    });
+}
+
+int mgm_fused_coarse_available(mgm_ctx *c, int *available)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(available, "mgm_fused_coarse_available: null argument");
+        *available = c->fused_blocks > 0 ? 1 : 0;
     });
 }
 

@@ -47,6 +47,11 @@ constexpr int kMaxN = 192;     // k + num_poly_terms capacity of the batched sol
 
 inline int blocks_for(long n, int bs) { return (int)((n + bs - 1) / bs); }
 
+// fused multiply-add a * b + c, rounded once (the contraction the compiler
+// applies to s += a * b), spelled out where two kernels must agree bit for bit
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 // sum_j A[j][i] * x[idx[j][i]] over an ELL row (column-major by stencil slot).
 // Slots are fetched in chunks of 8 (16 independent loads in flight per
 // thread, then 8 gathers) to hide DRAM latency; the products are summed in
@@ -66,11 +71,11 @@ __device__ __forceinline__ T ell_row_dot(const int *__restrict__ idx, const T *_
             a[q] = __ldg(A + (long)(j + q) * n + i);
         }
 #pragma unroll
-        for (int q = 0; q < 8; q++) s += a[q] * (T)__ldg(x + c[q]);
+        for (int q = 0; q < 8; q++) s = fma_rn(a[q], (T)__ldg(x + c[q]), s);
     }
     for (; j < k; j++) {
         const long o = (long)j * n + i;
-        s += A[o] * (T)x[idx[o]];
+        s = fma_rn(A[o], (T)x[idx[o]], s);
     }
     return s;
 }

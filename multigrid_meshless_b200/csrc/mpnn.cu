@@ -39,6 +39,7 @@ struct MpnnState {
     double d2 = 1;  // d_avg^2, scales lap weights to O(1)
     DBuf<float> params, grads, am, av;
     DBuf<bf16> WT[kLayers];  // [64][192]
+    DBuf<bf16> WF[kLayers];  // the same in the forward GEMM's B-fragment order
     DBuf<float> lapS;        // row-major [n][k]
     DBuf<int> tptr, tpos;    // transpose adjacency: in-edges of node j as positions i*k+s, sorted
     DBuf<float> Arm;         // pinned Poisson operator, row-major [n][k] (FP32), for the residual loss
@@ -223,163 +224,141 @@ __device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t &r0, uint32_t &r
                  : "r"(addr));
 }
 
-// shared memory of k_mp_layer: the layer's W^T [64][kPad] and the node tile
-// [kTile][kPad] (BF16; rows padded to 400 bytes so that the eight rows an
-// ldmatrix phase reads fall in distinct 16-byte bank groups)
-constexpr size_t kMpSmem = 2 * (size_t)kTile * kPad * sizeof(bf16);
+// W^T in the order of the mma.sync B fragments: for k-step ks (16 of the 192
+// inputs), n-tile pair p (16 of the 64 outputs) and lane l, one 16-byte word
+// {b0, b1 of n-tile 2p, b0, b1 of n-tile 2p + 1}; a warp reads a pair's
+// fragments as 512 contiguous bytes (kept in L1 for every CTA of the SM)
+__host__ __device__ constexpr int frag_pos(int f, int c)
+{
+    // f: output (n) 0..63, c: input (k) 0..191 -> position in the fragment-ordered copy (bf16 units)
+    return (((c / 16) * 4 + (f / 16)) * 32 + (f % 8) * 4 + (c % 8) / 2) * 8 + (((f / 8) % 2) * 2 + (c % 16) / 8) * 2 +
+           (c % 2);
+}
 
-// Persistent: each CTA stages W^T once, then loops over 64-node tiles.
 __global__ void __launch_bounds__(128) k_mp_layer(int n, int k, const int *__restrict__ cloud,
                                                   const float *__restrict__ lapS, float inv_k,
-                                                  const bf16 *__restrict__ h_in, const bf16 *__restrict__ WT,
+                                                  const bf16 *__restrict__ h_in, const bf16 *__restrict__ WF,
                                                   const float *__restrict__ bias, bf16 *__restrict__ h_out,
                                                   float *__restrict__ z_out, bf16 *__restrict__ cat_out,
                                                   const float *__restrict__ dec, float *__restrict__ y_out)
 {
-    extern __shared__ __align__(16) unsigned char mp_smem[];
-    bf16(*Ws)[kPad] = reinterpret_cast<bf16(*)[kPad]>(mp_smem);
-    bf16(*Xs)[kPad] = reinterpret_cast<bf16(*)[kPad]>(mp_smem + (size_t)kTile * kPad * sizeof(bf16));
+    __shared__ __align__(16) bf16 Xs[kTile][kPad];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int grp = lane >> 3, gl = lane & 7;
     const unsigned full = 0xffffffffu;  // rows past n are clamped, so all lanes stay converged
-    for (int w = tid; w < kH * (kCat / 8); w += blockDim.x) {
-        const int r = w / (kCat / 8), c = w % (kCat / 8);
-        *reinterpret_cast<uint4 *>(&Ws[r][8 * c]) = __ldg(reinterpret_cast<const uint4 *>(WT + r * kCat) + c);
+    const long base = (long)blockIdx.x * kTile;
+    for (int rr = 0; rr < kTile / 16; rr++) {
+        const int row = warp * 16 + rr * 4 + grp;
+        const bool valid = base + row < n;
+        const long i = valid ? base + row : (long)n - 1;
+        float sf[8], mn[8], lp[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) mn[e] = lp[e] = 0.f;
+        unpack8(__ldg(reinterpret_cast<const uint4 *>(h_in + i * kH + 8 * gl)), sf);
+        // the node's slots gl, gl + 8, ... (k <= 64)
+        int cl[8];
+        float wl[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const int j = gl + 8 * e;
+            cl[e] = j < k ? __ldg(cloud + i * k + j) : 0;
+            wl[e] = j < k ? __ldg(lapS + i * k + j) : 0.f;
+        }
+#pragma unroll
+        for (int j0 = 0; j0 < 64; j0 += kGather) {
+            if (j0 >= k) break;
+            uint4 v[kGather];
+            float wj[kGather];
+#pragma unroll
+            for (int e = 0; e < kGather; e++) {
+                const int j = j0 + e;
+                if (j >= 64) { wj[e] = 0.f; v[e] = make_uint4(0, 0, 0, 0); continue; }
+                const int cs = __shfl_sync(full, cl[j >> 3], j & 7, 8);
+                wj[e] = __shfl_sync(full, wl[j >> 3], j & 7, 8);
+                v[e] = j < k ? __ldg(reinterpret_cast<const uint4 *>(h_in + (long)cs * kH + 8 * gl))
+                             : make_uint4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int e = 0; e < kGather; e++) {
+                if (j0 + e >= k) break;
+                float f[8];
+                unpack8(v[e], f);
+#pragma unroll
+                for (int c = 0; c < 8; c++) {
+                    mn[c] += f[c];
+                    lp[c] += wj[e] * f[c];
+                }
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            mn[e] *= inv_k;
+            if (!valid) sf[e] = mn[e] = lp[e] = 0.f;
+        }
+        *reinterpret_cast<uint4 *>(&Xs[row][8 * gl]) = pack8(sf);
+        *reinterpret_cast<uint4 *>(&Xs[row][kH + 8 * gl]) = pack8(mn);
+        *reinterpret_cast<uint4 *>(&Xs[row][2 * kH + 8 * gl]) = pack8(lp);
     }
-    // ldmatrix source rows of this lane: A (tile rows) and B (W^T rows)
+    __syncthreads();
     const int g = lane >> 2, t = lane & 3, r0 = warp * 16;
+    // A fragments by ldmatrix: lanes 8q..8q+7 address rows r0 + (q & 1) * 8 + 0..7 at column (q >> 1) * 8
     const int q = lane >> 3, rq = lane & 7;
     const uint32_t a_addr = (uint32_t)__cvta_generic_to_shared(&Xs[r0 + rq + 8 * (q & 1)][8 * (q >> 1)]);
-    // B: matrices (n-tile 2p + (q >> 1), k-half q & 1)
-    const uint32_t b_addr = (uint32_t)__cvta_generic_to_shared(&Ws[8 * (q >> 1) + rq][8 * (q & 1)]);
-    constexpr uint32_t kRowB = kPad * sizeof(bf16);
-    const int ntiles = (n + kTile - 1) / kTile;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long base = (long)tile * kTile;
-        __syncthreads();  // W staged; the previous tile's reads of Xs are done
-        for (int rr = 0; rr < kTile / 16; rr++) {
-            const int row = warp * 16 + rr * 4 + grp;
-            const bool valid = base + row < n;
-            const long i = valid ? base + row : (long)n - 1;
-            float sf[8], mn[8], lp[8];
+    const uint4 *Wq = reinterpret_cast<const uint4 *>(WF) + lane;
+    float acc[8][4];
 #pragma unroll
-            for (int e = 0; e < 8; e++) mn[e] = lp[e] = 0.f;
-            unpack8(__ldg(reinterpret_cast<const uint4 *>(h_in + i * kH + 8 * gl)), sf);
-            // the node's slots gl, gl + 8, ... (k <= 64)
-            int cl[8];
-            float wl[8];
+    for (int e = 0; e < 8; e++) acc[e][0] = acc[e][1] = acc[e][2] = acc[e][3] = 0.f;
 #pragma unroll
-            for (int e = 0; e < 8; e++) {
-                const int j = gl + 8 * e;
-                cl[e] = j < k ? __ldg(cloud + i * k + j) : 0;
-                wl[e] = j < k ? __ldg(lapS + i * k + j) : 0.f;
-            }
+    for (int ks = 0; ks < kCat / 16; ks++) {
+        uint32_t a0, a1, a2, a3;
+        ldsm_x4(a_addr + ks * 16 * (uint32_t)sizeof(bf16), a0, a1, a2, a3);
 #pragma unroll
-            for (int j0 = 0; j0 < 64; j0 += kGather) {
-                if (j0 >= k) break;
-                uint4 v[kGather];
-                float wj[kGather];
-#pragma unroll
-                for (int e = 0; e < kGather; e++) {
-                    const int j = j0 + e;
-                    if (j >= 64) { wj[e] = 0.f; v[e] = make_uint4(0, 0, 0, 0); continue; }
-                    const int cs = __shfl_sync(full, cl[j >> 3], j & 7, 8);
-                    wj[e] = __shfl_sync(full, wl[j >> 3], j & 7, 8);
-                    v[e] = j < k ? __ldg(reinterpret_cast<const uint4 *>(h_in + (long)cs * kH + 8 * gl))
-                                 : make_uint4(0, 0, 0, 0);
-                }
-#pragma unroll
-                for (int e = 0; e < kGather; e++) {
-                    if (j0 + e >= k) break;
-                    float f[8];
-                    unpack8(v[e], f);
-#pragma unroll
-                    for (int c = 0; c < 8; c++) {
-                        mn[c] += f[c];
-                        lp[c] += wj[e] * f[c];
-                    }
-                }
-            }
-#pragma unroll
-            for (int e = 0; e < 8; e++) {
-                mn[e] *= inv_k;
-                if (!valid) sf[e] = mn[e] = lp[e] = 0.f;
-            }
-            *reinterpret_cast<uint4 *>(&Xs[row][8 * gl]) = pack8(sf);
-            *reinterpret_cast<uint4 *>(&Xs[row][kH + 8 * gl]) = pack8(mn);
-            *reinterpret_cast<uint4 *>(&Xs[row][2 * kH + 8 * gl]) = pack8(lp);
+        for (int p = 0; p < 4; p++) {
+            const uint4 b = __ldg(Wq + (ks * 4 + p) * 32);
+            mma_bf16(acc[2 * p], a0, a1, a2, a3, b.x, b.y);
+            mma_bf16(acc[2 * p + 1], a0, a1, a2, a3, b.z, b.w);
         }
-        __syncthreads();
-        float acc[8][4];
+    }
+    float yp[2] = {0.f, 0.f};
 #pragma unroll
-        for (int e = 0; e < 8; e++) acc[e][0] = acc[e][1] = acc[e][2] = acc[e][3] = 0.f;
+    for (int nt = 0; nt < 8; nt++) {
+        const int col = nt * 8 + 2 * t;
 #pragma unroll
-        for (int ks = 0; ks < kCat / 16; ks++) {
-            const uint32_t kb = ks * 16 * sizeof(bf16);
-            uint32_t a0, a1, a2, a3;
-            ldsm_x4(a_addr + kb, a0, a1, a2, a3);
-#pragma unroll
-            for (int p = 0; p < 4; p++) {
-                uint32_t b0, b1, b2, b3;  // n-tile 2p: (b0, b1); n-tile 2p + 1: (b2, b3)
-                ldsm_x4(b_addr + 16 * p * kRowB + kb, b0, b1, b2, b3);
-                mma_bf16(acc[2 * p], a0, a1, a2, a3, b0, b1);
-                mma_bf16(acc[2 * p + 1], a0, a1, a2, a3, b2, b3);
-            }
-        }
-        float yp[2] = {0.f, 0.f};
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++) {
-            const int col = nt * 8 + 2 * t;
-#pragma unroll
-            for (int hh = 0; hh < 2; hh++) {
-                const int row = r0 + g + 8 * hh;
-                const long i = base + row;
-                if (i >= n) continue;
-                const float z0 = acc[nt][2 * hh] + bias[col], z1 = acc[nt][2 * hh + 1] + bias[col + 1];
-                const float2 res = ld_bf2(&Xs[row][col]);
-                const __nv_bfloat162 o = __floats2bfloat162_rn(fmaxf(z0, 0.f) + res.x, fmaxf(z1, 0.f) + res.y);
-                if (h_out) *reinterpret_cast<__nv_bfloat162 *>(h_out + i * kH + col) = o;
-                if (z_out) { z_out[i * kH + col] = z0; z_out[i * kH + col + 1] = z1; }
-                if (y_out) {
-                    const float2 of = __bfloat1622float2(o);
-                    yp[hh] += of.x * __ldg(dec + P_WD + col) + of.y * __ldg(dec + P_WD + col + 1);
-                }
-            }
-        }
-        if (y_out) {
-            // decoder: the four lanes of a row hold its 64 features in 16-column
-            // parts; the row's output is their sum plus c_d
-#pragma unroll
-            for (int hh = 0; hh < 2; hh++) {
-                float v = yp[hh];
-                v += __shfl_xor_sync(0xffffffffu, v, 1);
-                v += __shfl_xor_sync(0xffffffffu, v, 2);
-                const long i = base + r0 + g + 8 * hh;
-                if (t == 0 && i < n) y_out[i] = v + __ldg(dec + P_CD);
-            }
-        }
-        if (cat_out) {
-            for (int w = tid; w < kTile * (kCat / 2); w += blockDim.x) {
-                const int r = w / (kCat / 2), cw = w % (kCat / 2);
-                if (base + r < n)
-                    reinterpret_cast<uint32_t *>(cat_out + (base + r) * kCat)[cw] =
-                        reinterpret_cast<const uint32_t *>(&Xs[r][0])[cw];
+        for (int hh = 0; hh < 2; hh++) {
+            const int row = r0 + g + 8 * hh;
+            const long i = base + row;
+            if (i >= n) continue;
+            const float z0 = acc[nt][2 * hh] + bias[col], z1 = acc[nt][2 * hh + 1] + bias[col + 1];
+            const float2 res = ld_bf2(&Xs[row][col]);
+            const __nv_bfloat162 o = __floats2bfloat162_rn(fmaxf(z0, 0.f) + res.x, fmaxf(z1, 0.f) + res.y);
+            if (h_out) *reinterpret_cast<__nv_bfloat162 *>(h_out + i * kH + col) = o;
+            if (z_out) { z_out[i * kH + col] = z0; z_out[i * kH + col + 1] = z1; }
+            if (y_out) {
+                const float2 of = __bfloat1622float2(o);
+                yp[hh] += of.x * __ldg(dec + P_WD + col) + of.y * __ldg(dec + P_WD + col + 1);
             }
         }
     }
-}
-
-// grid of k_mp_layer: resident CTAs on every SM, at most one per tile
-int mp_layer_grid(int n)
-{
-    int dev = 0, sms = 0, per_sm = 0;
-    MGM_CUDA(cudaGetDevice(&dev));
-    MGM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    MGM_CUDA(cudaFuncSetAttribute(k_mp_layer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMpSmem));
-    MGM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mp_layer, 128, kMpSmem));
-    per_sm = std::max(per_sm, 1);
-    const int tiles = (n + kTile - 1) / kTile;
-    return std::max(1, std::min(tiles, sms * per_sm));
+    if (y_out) {
+        // decoder: the four lanes of a row hold its 64 features in 16-column
+        // parts; the row's output is their sum plus c_d
+#pragma unroll
+        for (int hh = 0; hh < 2; hh++) {
+            float v = yp[hh];
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            v += __shfl_xor_sync(0xffffffffu, v, 2);
+            const long i = base + r0 + g + 8 * hh;
+            if (t == 0 && i < n) y_out[i] = v + __ldg(dec + P_CD);
+        }
+    }
+    if (cat_out) {
+        for (int w = tid; w < kTile * (kCat / 2); w += blockDim.x) {
+            const int r = w / (kCat / 2), cw = w % (kCat / 2);
+            if (base + r < n)
+                reinterpret_cast<uint32_t *>(cat_out + (base + r) * kCat)[cw] =
+                    reinterpret_cast<const uint32_t *>(&Xs[r][0])[cw];
+        }
+    }
 }
 
 // decoder: warp per node
@@ -563,14 +542,18 @@ __global__ void k_adam(int np, float *P, const float *G, float *m, float *v, flo
     P[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
-// BF16 copies of the layer weights, transposed to [64][192] for the GEMM B operand
-__global__ void k_refresh_WT(const float *P, bf16 *W0, bf16 *W1, bf16 *W2, bf16 *W3)
+// BF16 copies of the layer weights: transposed to [64][192] (the backward
+// pass) and in the forward GEMM's B-fragment order (frag_pos)
+__global__ void k_refresh_WT(const float *P, bf16 *W0, bf16 *W1, bf16 *W2, bf16 *W3, bf16 *F0, bf16 *F1, bf16 *F2,
+                             bf16 *F3)
 {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= kLayers * kH * kCat) return;
     const int l = e / (kH * kCat), r = e % (kH * kCat), f = r / kCat, c = r % kCat;
-    bf16 *dst[4] = {W0, W1, W2, W3};
-    dst[l][f * kCat + c] = __float2bfloat16(P[P_L0 + l * kLayerParams + c * kH + f]);
+    bf16 *dst[4] = {W0, W1, W2, W3}, *frg[4] = {F0, F1, F2, F3};
+    const bf16 w = __float2bfloat16(P[P_L0 + l * kLayerParams + c * kH + f]);
+    dst[l][f * kCat + c] = w;
+    frg[l][frag_pos(f, c)] = w;
 }
 
 // scaled lap weights row-major from the ELL operator
@@ -715,7 +698,8 @@ static int warp_blocks(long n) { return blocks_for(n * 32, 256); }
 static void refresh_weights(MpnnState &M, cudaStream_t s)
 {
     k_refresh_WT<<<blocks_for(kLayers * kH * kCat, 256), 256, 0, s>>>(M.params.p, M.WT[0].p, M.WT[1].p, M.WT[2].p,
-                                                                      M.WT[3].p);
+                                                                      M.WT[3].p, M.WF[0].p, M.WF[1].p, M.WF[2].p,
+                                                                      M.WF[3].p);
     MGM_LAUNCHED();
 }
 
@@ -729,7 +713,7 @@ static void forward(MpnnState &M, bool train, cudaStream_t s)
     for (int l = 0; l < kLayers; l++) {
         // inference: the last layer decodes in its epilogue and stores no h4
         const bool dec = !train && l == kLayers - 1;
-        k_mp_layer<<<mp_layer_grid(n), 128, kMpSmem, s>>>(n, M.k, M.cloud, M.lapS.p, 1.f / M.k, M.h[l].p, M.WT[l].p,
+        k_mp_layer<<<blocks_for(n, kTile), 128, 0, s>>>(n, M.k, M.cloud, M.lapS.p, 1.f / M.k, M.h[l].p, M.WF[l].p,
                                                        P + P_L0 + l * kLayerParams + kCat * kH,
                                                        dec ? nullptr : M.h[l + 1].p, train ? M.z[l + 1].p : nullptr,
                                                        train ? M.cat[l].p : nullptr, dec ? P : nullptr,
@@ -926,6 +910,7 @@ int mgm_mpnn_init(mgm_ctx *c, unsigned long long seed, int dataset_capacity)
         init_params(hp, seed);
         M.params.upload(hp.data(), kNumParams, s);
         for (auto &w : M.WT) w.alloc((size_t)kH * kCat);
+        for (auto &w : M.WF) w.alloc((size_t)kH * kCat);
         M.lapS.alloc(nk);
         k_lapS<<<blocks_for((long)nk, 256), 256, 0, s>>>(L.n, L.k, L.lap.p, M.d2, M.lapS.p);
         MGM_LAUNCHED();

@@ -37,6 +37,37 @@ __device__ __forceinline__ double block_sum_d(double v, double *sm)
 // ---------------------------------------------------------------------------
 // smoother
 // ---------------------------------------------------------------------------
+// Row work of the V-cycle kernels, shared by the one-operation kernels and
+// the fused coarse-level V-cycle (k_coarse_vcycle), which therefore give the
+// same bits.  COH: the vectors (r, e, d, q) are loaded from L2, past the
+// SM's L1 and the read-only path -- in the fused kernel other CTAs rewrite
+// them between passes; the operators are read-only throughout.
+template <bool COH, class T>
+__device__ __forceinline__ T ldv(const T *p)
+{
+    if constexpr (COH) return __ldcg(p);
+    else return *p;
+}
+
+template <class T, bool COH = false>
+__device__ __forceinline__ void start_row(int i, const uint8_t *__restrict__ btag, const T *__restrict__ dinv,
+                                          const T *r, T *e)
+{
+    e[i] = btag[i] ? ldv<COH>(r + i) * dinv[i] : T(0);
+}
+// boundary row w of the list, by the 32 lanes of a warp
+template <class T, bool COH = false>
+__device__ __forceinline__ void bnd_row_warp(int w, int lane, const int *__restrict__ list, int k,
+                                             const int *__restrict__ bidx, const T *__restrict__ bA,
+                                             const T *__restrict__ dinv, const T *r, T *e)
+{
+    const int i = list[w];
+    T s = T(0);
+    for (int j = lane; j < k; j += 32) s += bA[(long)w * k + j] * ldv<COH>(e + bidx[(long)w * k + j]);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) e[i] = ldv<COH>(e + i) + (ldv<COH>(r + i) - s) * dinv[i];
+}
+
 // Start of a smoothing pass from e = 0: interior rows 0, boundary rows their
 // exact solve r_i / a_ii (they couple only to interior nodes).
 template <class T>
@@ -45,7 +76,7 @@ __global__ void __launch_bounds__(256) k_start_e(int n, const uint8_t *__restric
 {
     pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) e[i] = btag[i] ? r[i] * dinv[i] : T(0);
+    if (i < n) start_row(i, btag, dinv, r, e);
 }
 
 // Exact solve of the boundary rows, one warp per row.  A boundary row couples
@@ -61,11 +92,7 @@ __global__ void __launch_bounds__(256) k_bnd_exact(int nbl, const int *__restric
     pdl_enter();
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (w >= nbl) return;
-    const int i = list[w];
-    T s = T(0);
-    for (int j = lane; j < k; j += 32) s += bA[(long)w * k + j] * e[bidx[(long)w * k + j]];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) e[i] = e[i] + (r[i] - s) * dinv[i];
+    bnd_row_warp(w, lane, list, k, bidx, bA, dinv, r, e);
 }
 
 // One Chebyshev step on interior rows: q = r - A e, d = c1*d + c2*D^-1 q, e' = e + d.
@@ -113,6 +140,26 @@ __global__ void __launch_bounds__(256) k_restrict(int n, int k, const int *__res
     rc[i] = ell_row_dot(ridx, rw, qf, n, k, i);
 }
 
+// (P e_c)[0], the prolongated correction at the pinned node, by the 32 lanes
+// of warp 0: the lanes fetch the operands of 32 slots at once (operand(j, a,
+// x): weight and gathered value of slot j), then every lane sums the
+// products in slot order, one fused multiply-add per slot -- the rounding of
+// the row dots (ell_row_dot, ell_row_dot_o), so the shift has the bits a
+// serial row-0 dot would give.
+template <class T, class Op>
+__device__ __forceinline__ T row0_dot_warp(int k, Op operand)
+{
+    const int lane = threadIdx.x & 31;
+    T s = T(0);
+    for (int j0 = 0; j0 < k; j0 += 32) {
+        T a = T(0), x = T(0);
+        if (j0 + lane < k) operand(j0 + lane, a, x);
+        const int m = min(32, k - j0);
+        for (int q = 0; q < m; q++) s = fma_rn(__shfl_sync(0xffffffffu, a, q), __shfl_sync(0xffffffffu, x, q), s);
+    }
+    return s;
+}
+
 // e_f[i] += (P e_c)[i] - (P e_c)[0]  (the shift keeps the pinned node uncorrected)
 template <class T>
 __global__ void __launch_bounds__(256) k_prolong(int n, int k, const int *__restrict__ pidx, const T *__restrict__ pw,
@@ -120,10 +167,12 @@ __global__ void __launch_bounds__(256) k_prolong(int n, int k, const int *__rest
 {
     pdl_enter();
     __shared__ T shift;
-    if (threadIdx.x == 0) {
-        T s = T(0);
-        for (int j = 0; j < k; j++) s += pw[(long)j * n] * ec[pidx[(long)j * n]];
-        shift = s;
+    if (threadIdx.x < 32) {
+        const T s = row0_dot_warp<T>(k, [&](int j, T &a, T &x) {
+            a = pw[(long)j * n];
+            x = ec[pidx[(long)j * n]];
+        });
+        if (threadIdx.x == 0) shift = s;
     }
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -135,7 +184,9 @@ __global__ void __launch_bounds__(256) k_prolong(int n, int k, const int *__rest
 // compact FP32 path: FP32 weights, neighbours stored as int16 offsets c - base
 // (6 bytes per stencil slot instead of 8)
 // ---------------------------------------------------------------------------
-template <class T, class X>
+// The gathered vector x is read through the read-only path unless COHERENT
+// (the fused coarse V-cycle, where other CTAs rewrite x between passes).
+template <class T, class X, bool COHERENT = false>
 __device__ __forceinline__ T ell_row_dot_o(const short *__restrict__ off, const T *__restrict__ A,
                                            const X *__restrict__ x, long n, int k, long i, int base)
 {
@@ -151,11 +202,11 @@ __device__ __forceinline__ T ell_row_dot_o(const short *__restrict__ off, const 
             a[q] = __ldg(A + o);
         }
 #pragma unroll
-        for (int q = 0; q < 8; q++) s += a[q] * (T)__ldg(x + c[q]);
+        for (int q = 0; q < 8; q++) s = fma_rn(a[q], (T)(COHERENT ? __ldcg(x + c[q]) : __ldg(x + c[q])), s);
     }
     for (; j < k; j++) {
         const long o = (long)j * n + i;
-        s += A[o] * (T)x[base + (int)off[o]];
+        s = fma_rn(A[o], (T)ldv<COHERENT>(x + base + (int)off[o]), s);
     }
     return s;
 }
@@ -175,22 +226,35 @@ __device__ __forceinline__ T ell_row_dot_o(const short *__restrict__ off, const 
 // Chebyshev step q = r - A e, d = c1 d + c2 D^-1 q, e' = e + d on interior
 // rows (boundary rows copy e); MODE 1: residual q = r - A e on interior rows,
 // 0 on boundary rows.
-template <int MODE, class T>
+template <int MODE, class T, bool COH = false>
 __device__ __forceinline__ void level_row_out(int i, T s, const T *__restrict__ dinv,
-                                              const uint8_t *__restrict__ btag, const T *__restrict__ r,
-                                              const T *__restrict__ e, T *__restrict__ out,
-                                              T *__restrict__ d, T c1, T c2, int first)
+                                              const uint8_t *__restrict__ btag, const T *r, const T *e, T *out, T *d,
+                                              T c1, T c2, int first)
 {
     if (MODE == 0) {
-        const T ei = e[i];
+        const T ei = ldv<COH>(e + i);
         if (btag[i]) { out[i] = ei; return; }
-        const T q = r[i] - s;
-        const T di = first ? c2 * dinv[i] * q : c1 * d[i] + c2 * dinv[i] * q;
+        const T q = ldv<COH>(r + i) - s;
+        const T di = first ? c2 * dinv[i] * q : c1 * ldv<COH>(d + i) + c2 * dinv[i] * q;
         d[i] = di;
         out[i] = ei + di;
     } else {
-        out[i] = btag[i] ? T(0) : r[i] - s;
+        out[i] = btag[i] ? T(0) : ldv<COH>(r + i) - s;
     }
+}
+
+template <int MODE, class T, bool COHERENT = false>
+__device__ __forceinline__ void c1_row(int i, int ld, int k, const short *__restrict__ off, const T *__restrict__ A,
+                                       const T *__restrict__ dinv, const uint8_t *__restrict__ btag,
+                                       const T *__restrict__ r, const T *__restrict__ e, T *__restrict__ out,
+                                       T *__restrict__ d, T c1, T c2, int first)
+{
+    if (btag[i]) {
+        out[i] = MODE == 0 ? ldv<COHERENT>(e + i) : T(0);
+        return;
+    }
+    level_row_out<MODE, T, COHERENT>(i, ell_row_dot_o<T, T, COHERENT>(off, A, e, ld, k, i, i), dinv, btag, r, e, out,
+                                     d, c1, c2, first);
 }
 
 template <int MODE, class T>
@@ -203,11 +267,7 @@ __global__ void __launch_bounds__(256) k_level_c1(int n, int ld, int k, const sh
     pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    if (btag[i]) {
-        out[i] = MODE == 0 ? e[i] : T(0);
-        return;
-    }
-    level_row_out<MODE, T>(i, ell_row_dot_o(off, A, e, ld, k, i, i), dinv, btag, r, e, out, d, c1, c2, first);
+    c1_row<MODE, T>(i, ld, k, off, A, dinv, btag, r, e, out, d, c1, c2, first);
 }
 
 // the four weights of rows i0..i0+3 in slot o (evict-first)
@@ -376,6 +436,34 @@ static void launch_compact(const SolveLevel<T> &L, const T *e, T *out, T c1, T c
                L.r, e, out, L.d, c1, c2, first);
 }
 
+template <class T, bool COHERENT = false>
+__device__ __forceinline__ void restrict_row(int i, int n, int k, const short *__restrict__ off,
+                                             const int *__restrict__ base, const T *__restrict__ rw,
+                                             const uint8_t *__restrict__ btag, const T *__restrict__ qf,
+                                             T *__restrict__ rc)
+{
+    if (btag[i] || i == 0) { rc[i] = T(0); return; }
+    rc[i] = ell_row_dot_o<T, T, COHERENT>(off, rw, qf, n, k, i, base[i]);
+}
+// (P e_c)[0] of the compact prolongation, by warp 0 of a CTA (row0_dot_warp)
+template <class T, bool COH = false>
+__device__ __forceinline__ T prolong_shift_warp(int n, int k, const short *__restrict__ off,
+                                                const int *__restrict__ base, const T *__restrict__ pw, const T *ec)
+{
+    const int b0 = base[0];
+    return row0_dot_warp<T>(k, [&](int j, T &a, T &x) {
+        a = pw[(long)j * n];
+        x = ldv<COH>(ec + b0 + (int)off[(long)j * n]);
+    });
+}
+template <class T, bool COHERENT = false>
+__device__ __forceinline__ void prolong_row(int i, int n, int k, const short *__restrict__ off,
+                                            const int *__restrict__ base, const T *__restrict__ pw, const T *ec, T *ef,
+                                            T shift)
+{
+    ef[i] = ldv<COHERENT>(ef + i) + (ell_row_dot_o<T, T, COHERENT>(off, pw, ec, n, k, i, base[i]) - shift);
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) k_restrict_o(int n, int k, const short *__restrict__ off,
                                                     const int *__restrict__ base, const T *__restrict__ rw,
@@ -385,8 +473,7 @@ __global__ void __launch_bounds__(256) k_restrict_o(int n, int k, const short *_
     pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    if (btag[i] || i == 0) { rc[i] = T(0); return; }
-    rc[i] = ell_row_dot_o(off, rw, qf, n, k, i, base[i]);
+    restrict_row(i, n, k, off, base, rw, btag, qf, rc);
 }
 
 template <class T>
@@ -396,11 +483,14 @@ __global__ void __launch_bounds__(256) k_prolong_o(int n, int k, const short *__
 {
     pdl_enter();
     __shared__ T shift;
-    if (threadIdx.x == 0) shift = ell_row_dot_o(off, pw, ec, n, k, 0, base[0]);
+    if (threadIdx.x < 32) {
+        const T s = prolong_shift_warp(n, k, off, base, pw, ec);
+        if (threadIdx.x == 0) shift = s;
+    }
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    ef[i] += ell_row_dot_o(off, pw, ec, n, k, i, base[i]) - shift;
+    prolong_row(i, n, k, off, base, pw, ec, ef, shift);
 }
 
 // ---------------------------------------------------------------------------
@@ -701,6 +791,16 @@ static void launch_tiled(const SolveLevel<float> &L, const float *e, float *out,
 }
 
 // e = inv * r, one warp per row of the dense coarsest inverse
+template <class T, bool COH = false>
+__device__ __forceinline__ void dense_row_warp(int w, int lane, int n, const T *__restrict__ inv, const T *r, T *e)
+{
+    const T *row = inv + (long)w * n;
+    T s = T(0);
+    for (int j = lane; j < n; j += 32) s += row[j] * ldv<COH>(r + j);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) e[w] = s;
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) k_dense_solve(int n, const T *__restrict__ inv, const T *__restrict__ r,
                                                      T *__restrict__ e)
@@ -708,11 +808,245 @@ __global__ void __launch_bounds__(256) k_dense_solve(int n, const T *__restrict_
     pdl_enter();
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= n) return;
-    const T *row = inv + (long)warp * n;
-    T s = T(0);
-    for (int j = lane; j < n; j += 32) s += row[j] * r[j];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) e[warp] = s;
+    dense_row_warp(warp, lane, n, inv, r, e);
+}
+
+// ---------------------------------------------------------------------------
+// fused coarse-level V-cycle
+//
+// The levels below kVecMinRows rows are latency-bound: each operation of the
+// V-cycle on them (about 17 per level) is a short kernel whose launch and
+// ramp cost as much as its work.  k_coarse_vcycle runs the whole V-cycle from
+// level `first` down to the coarsest and back as ONE cooperative launch: one
+// CTA per SM, every operation a grid-stride pass over the level's rows with
+// the row work of the one-operation kernels (so the same bits), and a grid
+// barrier between dependent passes.
+// ---------------------------------------------------------------------------
+constexpr int kFusedMaxLevels = 8, kFusedMaxCheb = 8, kFusedThreads = 512;
+
+template <class T>
+struct FusedLevel {
+    int n, ld, k, nb_list, kr, kp;
+    const short *off;
+    const T *A, *dinv;
+    const uint8_t *btag;
+    const int *bnd_list, *bnd_idx;
+    const T *bnd_A;
+    T *r, *e, *e2, *d, *q;
+    const short *r_off;   // restriction into this level (compact)
+    const int *r_base;
+    const T *r_w;
+    const short *p_off;   // prolongation from the next coarser level into this one (compact)
+    const int *p_base;
+    const T *p_w;
+    T c1[kFusedMaxCheb], c2[kFusedMaxCheb];  // Chebyshev coefficients of each step
+};
+
+template <class T>
+struct FusedArgs {
+    int first, nl, deg;
+    int cn;        // coarsest rows
+    const T *cinv; // its dense inverse
+    unsigned *bar; // grid barrier: {arrivals, generation}
+    int *err;      // set when a barrier wait runs out
+    FusedLevel<T> L[kFusedMaxLevels];
+};
+
+// Grid barrier of a cooperative launch (all CTAs resident): thread 0 of each
+// CTA arrives on a counter; the last arrival resets it and advances the
+// generation the others wait on.  The wait is bounded (about 0.5 s); when it
+// runs out the CTA records the error and the kernel's CTAs return at their
+// next barrier.  Returns false once any CTA has given up.
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err, unsigned &gen)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int good = 1;
+        __threadfence();
+        const unsigned arrived = atomicAdd(&bar[0], 1u) + 1u;
+        if (arrived == gridDim.x) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicAdd(&bar[1], 1u);
+        } else {
+            long spins = 0;
+            while (*(volatile unsigned *)&bar[1] == gen) {
+                if (++spins > (1L << 22) || *(volatile int *)err) {
+                    atomicExch(err, 1);
+                    good = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        gen++;
+        ok = good && *(volatile int *)err == 0;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kFusedThreads) k_coarse_vcycle(const __grid_constant__ FusedArgs<T> a)
+{
+    const int nth = gridDim.x * blockDim.x, tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, nwarp = nth >> 5, wid = tid >> 5;
+    __shared__ T shift;
+    unsigned gen = 0;
+    if (threadIdx.x == 0) gen = *(volatile unsigned *)&a.bar[1];
+#define MGM_SYNC() \
+    if (!grid_barrier(a.bar, a.err, gen)) return
+    T *cur[kFusedMaxLevels], *nxt[kFusedMaxLevels];
+    // one smoothing pass on level l: deg Chebyshev steps, each followed by
+    // the boundary rows' exact solve; from e = 0 or from the current e
+    auto smooth = [&](int l, bool zero_start) -> bool {
+        const FusedLevel<T> &L = a.L[l];
+        if (zero_start) {
+            for (int i = tid; i < L.n; i += nth) start_row<T, true>(i, L.btag, L.dinv, L.r, cur[l]);
+        } else {
+            for (int w = wid; w < L.nb_list; w += nwarp)
+                bnd_row_warp<T, true>(w, lane, L.bnd_list, L.k, L.bnd_idx, L.bnd_A, L.dinv, L.r, cur[l]);
+        }
+        if (!grid_barrier(a.bar, a.err, gen)) return false;
+        for (int st = 0; st < a.deg; st++) {
+            for (int i = tid; i < L.n; i += nth)
+                c1_row<0, T, true>(i, L.ld, L.k, L.off, L.A, L.dinv, L.btag, L.r, cur[l], nxt[l], L.d, L.c1[st],
+                                   L.c2[st], st == 0 ? 1 : 0);
+            if (!grid_barrier(a.bar, a.err, gen)) return false;
+            T *t = cur[l]; cur[l] = nxt[l]; nxt[l] = t;
+            for (int w = wid; w < L.nb_list; w += nwarp)
+                bnd_row_warp<T, true>(w, lane, L.bnd_list, L.k, L.bnd_idx, L.bnd_A, L.dinv, L.r, cur[l]);
+            if (!grid_barrier(a.bar, a.err, gen)) return false;
+        }
+        return true;
+    };
+    for (int l = a.first; l < a.nl; l++) { cur[l] = a.L[l].e; nxt[l] = a.L[l].e2; }
+    for (int l = a.first; l < a.nl - 1; l++) {
+        const FusedLevel<T> &L = a.L[l], &C = a.L[l + 1];
+        if (!smooth(l, true)) return;
+        for (int i = tid; i < L.n; i += nth)
+            c1_row<1, T, true>(i, L.ld, L.k, L.off, L.A, L.dinv, L.btag, L.r, cur[l], L.q, L.d, T(0), T(0), 0);
+        MGM_SYNC();
+        for (int i = tid; i < C.n; i += nth)
+            restrict_row<T, true>(i, C.n, C.kr, C.r_off, C.r_base, C.r_w, C.btag, L.q, C.r);
+        MGM_SYNC();
+    }
+    {
+        const FusedLevel<T> &L = a.L[a.nl - 1];
+        for (int w = wid; w < a.cn; w += nwarp) dense_row_warp<T, true>(w, lane, a.cn, a.cinv, L.r, cur[a.nl - 1]);
+        MGM_SYNC();
+    }
+    for (int l = a.nl - 2; l >= a.first; l--) {
+        const FusedLevel<T> &L = a.L[l];
+        if (threadIdx.x < 32) {
+            const T s = prolong_shift_warp<T, true>(L.n, L.kp, L.p_off, L.p_base, L.p_w, (const T *)cur[l + 1]);
+            if (threadIdx.x == 0) shift = s;
+        }
+        __syncthreads();
+        for (int i = tid; i < L.n; i += nth)
+            prolong_row<T, true>(i, L.n, L.kp, L.p_off, L.p_base, L.p_w, (const T *)cur[l + 1], cur[l], shift);
+        MGM_SYNC();
+        if (!smooth(l, false)) return;
+    }
+#undef MGM_SYNC
+}
+
+// Whether levels first..nl-1 can run fused: small (one-row-per-thread)
+// compact levels without the tile-streamed or FP16 operator.
+template <class T>
+static bool fusable(const std::vector<SolveLevel<T>> &Ls, int first, int deg)
+{
+    const int nl = (int)Ls.size();
+    if (first >= nl - 1 || nl > kFusedMaxLevels || deg > kFusedMaxCheb || deg < 1) return false;
+    for (int l = first; l < nl; l++) {
+        const SolveLevel<T> &L = Ls[l];
+        if (l < nl - 1) {
+            if (L.n >= kVecMinRows || !L.off || L.At || L.W16 || !L.p_off) return false;
+        }
+        if (l > first && !L.r_off) return false;
+    }
+    return true;
+}
+
+template <class T>
+static void launch_fused(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int first, int deg, double ratio,
+                         cudaStream_t s, const FusedCtl &fc)
+{
+    FusedArgs<T> a{};
+    a.first = first;
+    a.nl = (int)Ls.size();
+    a.deg = deg;
+    a.cn = cs.n;
+    a.cinv = cs.inv;
+    a.bar = fc.bar;
+    a.err = fc.err;
+    for (int l = first; l < a.nl; l++) {
+        const SolveLevel<T> &S = Ls[l];
+        FusedLevel<T> &F = a.L[l];
+        F.n = S.n; F.ld = S.ld; F.k = S.k; F.nb_list = S.nb_list; F.kr = S.kr; F.kp = S.kp;
+        F.off = S.off; F.A = S.A; F.dinv = S.dinv; F.btag = S.btag;
+        F.bnd_list = S.bnd_list; F.bnd_idx = S.bnd_idx; F.bnd_A = S.bnd_A;
+        F.r = S.r; F.e = S.e; F.e2 = S.e2; F.d = S.d; F.q = S.q;
+        F.r_off = S.r_off; F.r_base = S.r_base; F.r_w = S.r_w;
+        F.p_off = S.p_off; F.p_base = S.p_base; F.p_w = S.p_w;
+        // the coefficients smooth() passes to the level kernels, step by step
+        const double lM = 1.05 * S.lmax, lm = S.lmax / ratio;
+        const double th = 0.5 * (lM + lm), de = 0.5 * (lM - lm), sig = th / de;
+        double rho = 1.0 / sig;
+        for (int st = 0; st < deg; st++) {
+            double c1 = 0, c2;
+            if (st == 0) c2 = 1.0 / th;
+            else {
+                const double rn = 1.0 / (2.0 * sig - rho);
+                c1 = rn * rho;
+                c2 = 2.0 * rn / de;
+                rho = rn;
+            }
+            F.c1[st] = (T)c1;
+            F.c2[st] = (T)c2;
+        }
+    }
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(fc.blocks);
+    cfg.blockDim = dim3(kFusedThreads);
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_coarse_vcycle<T>, a);
+    if (e != cudaSuccess) throw Error{1, std::string("kernel launch (cooperative): ") + cudaGetErrorString(e)};
+    MGM_LAUNCHED();
+}
+
+// a cooperative launch of one CTA that does nothing (capture probe)
+__global__ void k_coop_probe(int) {}
+cudaError_t launch_coop_probe(cudaStream_t s)
+{
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(32);
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_coop_probe, 0);
+}
+
+int fused_vcycle_blocks()
+{
+    int dev = 0, sms = 0, per32 = 0, per64 = 0;
+    MGM_CUDA(cudaGetDevice(&dev));
+    MGM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MGM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_coarse_vcycle<float>, kFusedThreads, 0));
+    MGM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per64, k_coarse_vcycle<double>, kFusedThreads, 0));
+    MGM_REQUIRE(per32 >= 1 && per64 >= 1, "fused coarse V-cycle: a CTA does not fit on an SM");
+    return sms;  // one CTA per SM
 }
 
 void SmootherProfile::mark(cudaStream_t s)
@@ -805,11 +1139,18 @@ static void smooth(SolveLevel<T> &L, int degree, double ratio, bool zero_start, 
 
 template <class T>
 static void vcycle_rec(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int l, int deg, double ratio,
-                       cudaStream_t s, SmootherProfile *prof, Chain &launch)
+                       cudaStream_t s, SmootherProfile *prof, Chain &launch, const FusedCtl *fused)
 {
     SmootherProfile *lp = (l == 0 && prof && prof->on) ? prof : nullptr;
     SolveLevel<T> &L = Ls[l];
     const int nl = (int)Ls.size();
+    if (fused && fused->on && fusable(Ls, l, deg)) {
+        // levels l..nl-1 in one cooperative launch; each level's correction
+        // ends in its e buffer, as after the 2 deg swaps of the per-level path
+        launch_fused(Ls, cs, l, deg, ratio, s, *fused);
+        launch.after_kernel = true;
+        return;
+    }
     if (l == nl - 1) {
         launch(k_dense_solve<T>, blocks_for((long)L.n * 32, 256), 256, 0, s, cs.n, cs.inv, L.r, L.e);
         return;
@@ -834,7 +1175,7 @@ static void vcycle_rec(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs,
                C.r);
     else
         launch(k_restrict<T>, blocks_for(C.n, 256), 256, 0, s, C.n, C.kr, C.r_idx, C.r_w, C.btag, L.q, C.r);
-    vcycle_rec(Ls, cs, l + 1, deg, ratio, s, prof, launch);
+    vcycle_rec(Ls, cs, l + 1, deg, ratio, s, prof, launch, fused);
     if (L.p_off) {
         launch(k_prolong_o<T>, blocks_for(L.n, 256), 256, 0, s, L.n, L.kp, L.p_off, L.p_base, L.p_w, (const T *)C.e,
                L.e);
@@ -846,11 +1187,11 @@ static void vcycle_rec(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs,
 
 template <class T>
 void vcycle(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int cheb_degree, double cheb_ratio,
-            cudaStream_t s, SmootherProfile *prof, bool chain)
+            cudaStream_t s, SmootherProfile *prof, bool chain, const FusedCtl *fused)
 {
     Chain launch;
     launch.enabled = chain;
-    vcycle_rec(Ls, cs, 0, cheb_degree, cheb_ratio, s, prof, launch);
+    vcycle_rec(Ls, cs, 0, cheb_degree, cheb_ratio, s, prof, launch, fused);
 }
 
 // Chebyshev smoothing of A e = r on one level from e = 0 (r already in L.r);
@@ -867,9 +1208,9 @@ template const double *smooth_from_zero<double>(SolveLevel<double> &, int, doubl
 template const float *smooth_from_zero<float>(SolveLevel<float> &, int, double, cudaStream_t, bool);
 
 template void vcycle<double>(std::vector<SolveLevel<double>> &, const CoarseSolve<double> &, int, double, cudaStream_t,
-                             SmootherProfile *, bool);
+                             SmootherProfile *, bool, const FusedCtl *);
 template void vcycle<float>(std::vector<SolveLevel<float>> &, const CoarseSolve<float> &, int, double, cudaStream_t,
-                            SmootherProfile *, bool);
+                            SmootherProfile *, bool, const FusedCtl *);
 
 // ---------------------------------------------------------------------------
 // spectral radius of D^-1 A restricted to interior rows (power iteration)

@@ -49,150 +49,99 @@ void spmv_parity(int n, int k, const double *W, const int *idx, const double *f,
 // ---------------------------------------------------------------------------
 // calculate_intermediate_velocity (fractional_step_solver.h:73-114), fused:
 // Dx, Dy, (Dz), lap read once and applied to every velocity component.
-// Each thread updates R rows 256 apart (coalesced loads, R independent gather
-// chains in flight); every row's sums run over the stencil slots in order.
-template <int DIM>
-__host__ __device__ constexpr int rows_per_thread() { return DIM == 2 ? 4 : 2; }
-
 template <int DIM>
 __global__ void __launch_bounds__(256) k_momentum(StepArgs a)
 {
-    constexpr int R = rows_per_thread<DIM>();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = a.n;
-    const long i0 = (long)blockIdx.x * (256 * R) + threadIdx.x;
-    double gx[R][DIM], gy[R][DIM], gz[R][DIM], gl[R][DIM];
-    long ii[R];
+    if (i >= n) return;
+    double gx[DIM], gy[DIM], gz[DIM], gl[DIM];
 #pragma unroll
-    for (int r = 0; r < R; r++) {
-        ii[r] = i0 + 256 * r < n ? i0 + 256 * r : (long)n - 1;  // rows past n are computed on row n-1, not stored
-#pragma unroll
-        for (int c = 0; c < DIM; c++) { gx[r][c] = 0.0; gy[r][c] = 0.0; gz[r][c] = 0.0; gl[r][c] = 0.0; }
-    }
+    for (int c = 0; c < DIM; c++) { gx[c] = 0.0; gy[c] = 0.0; gz[c] = 0.0; gl[c] = 0.0; }
     const double *vel[3] = {a.u, a.v, a.w};
-#pragma unroll 2
     for (int j = 0; j < a.k; j++) {
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-            const long o = (long)j * n + ii[r];
-            const int c = a.idx[o];
-            const double wx = a.Dx[o], wy = a.Dy[o], wl = a.lap[o];
-            const double wz = DIM == 3 ? a.Dz[o] : 0.0;
-#pragma unroll
-            for (int q = 0; q < DIM; q++) {
-                const double f = vel[q][c];
-                gx[r][q] = MGM_ADD(gx[r][q], MGM_MUL(wx, f));
-                gy[r][q] = MGM_ADD(gy[r][q], MGM_MUL(wy, f));
-                if (DIM == 3) gz[r][q] = MGM_ADD(gz[r][q], MGM_MUL(wz, f));
-                gl[r][q] = MGM_ADD(gl[r][q], MGM_MUL(wl, f));
-            }
-        }
-    }
-    double *outs[3] = {a.u_new, a.v_new, a.w_new};
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-        const long i = i0 + 256 * r;
-        if (i >= n) break;
-        const double ui = a.u[i], vi = a.v[i], wi = a.w[i];
+        const long o = (long)j * n + i;
+        const int c = a.idx[o];
+        const double wx = a.Dx[o], wy = a.Dy[o], wl = a.lap[o];
+        const double wz = DIM == 3 ? a.Dz[o] : 0.0;
 #pragma unroll
         for (int q = 0; q < DIM; q++) {
-            // in 2D the reference's dpdz array is never written and stays 0
-            const double adv =
-                MGM_ADD(MGM_ADD(MGM_MUL(ui, gx[r][q]), MGM_MUL(vi, gy[r][q])), MGM_MUL(wi, DIM == 3 ? gz[r][q] : 0.0));
-            const double rhs = MGM_SUB(adv, MGM_MUL(a.nu, gl[r][q]));
-            outs[q][i] = MGM_SUB(vel[q][i], MGM_MUL(a.dt, rhs));
+            const double f = vel[q][c];
+            gx[q] = MGM_ADD(gx[q], MGM_MUL(wx, f));
+            gy[q] = MGM_ADD(gy[q], MGM_MUL(wy, f));
+            if (DIM == 3) gz[q] = MGM_ADD(gz[q], MGM_MUL(wz, f));
+            gl[q] = MGM_ADD(gl[q], MGM_MUL(wl, f));
         }
-        if (a.dpdn) a.dpdn[i] = gl[r][DIM - 1];  // the reference leaves lap(last component) in dpdn
     }
+    const double ui = a.u[i], vi = a.v[i], wi = a.w[i];
+    double *outs[3] = {a.u_new, a.v_new, a.w_new};
+#pragma unroll
+    for (int q = 0; q < DIM; q++) {
+        // in 2D the reference's dpdz array is never written and stays 0
+        const double adv = MGM_ADD(MGM_ADD(MGM_MUL(ui, gx[q]), MGM_MUL(vi, gy[q])), MGM_MUL(wi, DIM == 3 ? gz[q] : 0.0));
+        const double rhs = MGM_SUB(adv, MGM_MUL(a.nu, gl[q]));
+        outs[q][i] = MGM_SUB(vel[q][i], MGM_MUL(a.dt, rhs));
+    }
+    if (a.dpdn) a.dpdn[i] = gl[DIM - 1];  // the reference leaves lap(last component) in dpdn
 }
 
-// calculate_mass_residual + calculate_boundary_dpdn (fractional_step_solver.h:116-148);
-// R rows per thread as in k_momentum
+// calculate_mass_residual + calculate_boundary_dpdn (fractional_step_solver.h:116-148)
 template <int DIM>
 __global__ void __launch_bounds__(256) k_divergence(StepArgs a)
 {
-    constexpr int R = rows_per_thread<DIM>();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = a.n;
-    const long i0 = (long)blockIdx.x * (256 * R) + threadIdx.x;
-    double sx[R], sy[R], sz[R];
-    long ii[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-        ii[r] = i0 + 256 * r < n ? i0 + 256 * r : (long)n - 1;
-        sx[r] = sy[r] = sz[r] = 0.0;
+    if (i >= n) return;
+    const bool bnd = a.btag[i] != 0;
+    if (bnd) {
+        const double dx = MGM_DIV(MGM_MUL(MGM_SUB(a.u_new[i], a.u[i]), a.rho), a.dt);
+        const double dy = MGM_DIV(MGM_MUL(MGM_SUB(a.v_new[i], a.v[i]), a.rho), a.dt);
+        double dn = MGM_ADD(MGM_MUL(dx, a.nx[i]), MGM_MUL(dy, a.ny[i]));
+        if (DIM == 3) {
+            const double dz = MGM_DIV(MGM_MUL(MGM_SUB(a.w_new[i], a.w[i]), a.rho), a.dt);
+            dn = MGM_ADD(dn, MGM_MUL(dz, a.nz[i]));
+        }
+        if (a.dpdn) a.dpdn[i] = dn;
+        return;  // the boundary source keeps its value (zero): homogeneous Neumann rows
     }
-#pragma unroll 2
+    double sx = 0.0, sy = 0.0, sz = 0.0;
     for (int j = 0; j < a.k; j++) {
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-            const long o = (long)j * n + ii[r];
-            const int c = a.idx[o];
-            sx[r] = MGM_ADD(sx[r], MGM_MUL(a.Dx[o], a.u_new[c]));
-            sy[r] = MGM_ADD(sy[r], MGM_MUL(a.Dy[o], a.v_new[c]));
-            if (DIM == 3) sz[r] = MGM_ADD(sz[r], MGM_MUL(a.Dz[o], a.w_new[c]));
-        }
+        const long o = (long)j * n + i;
+        const int c = a.idx[o];
+        sx = MGM_ADD(sx, MGM_MUL(a.Dx[o], a.u_new[c]));
+        sy = MGM_ADD(sy, MGM_MUL(a.Dy[o], a.v_new[c]));
+        if (DIM == 3) sz = MGM_ADD(sz, MGM_MUL(a.Dz[o], a.w_new[c]));
     }
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-        const long i = i0 + 256 * r;
-        if (i >= n) break;
-        if (a.btag[i]) {
-            const double dx = MGM_DIV(MGM_MUL(MGM_SUB(a.u_new[i], a.u[i]), a.rho), a.dt);
-            const double dy = MGM_DIV(MGM_MUL(MGM_SUB(a.v_new[i], a.v[i]), a.rho), a.dt);
-            double dn = MGM_ADD(MGM_MUL(dx, a.nx[i]), MGM_MUL(dy, a.ny[i]));
-            if (DIM == 3) {
-                const double dz = MGM_DIV(MGM_MUL(MGM_SUB(a.w_new[i], a.w[i]), a.rho), a.dt);
-                dn = MGM_ADD(dn, MGM_MUL(dz, a.nz[i]));
-            }
-            if (a.dpdn) a.dpdn[i] = dn;
-            continue;  // the boundary source keeps its value (zero): homogeneous Neumann rows
-        }
-        a.source[i] = MGM_DIV(MGM_MUL(a.rho, MGM_ADD(MGM_ADD(sx[r], sy[r]), sz[r])), a.dt);
-    }
+    a.source[i] = MGM_DIV(MGM_MUL(a.rho, MGM_ADD(MGM_ADD(sx, sy), sz)), a.dt);
 }
 
 // update_velocity (fractional_step_solver.h:248-265) fused with the steady
 // error partial sums of fractional_step_explicit (:63-69); u_old is the
 // velocity at the start of the step (the update leaves boundary rows alone).
-// R rows per thread as in k_momentum.
 template <int DIM>
 __global__ void __launch_bounds__(256) k_correct(StepArgs a, double *__restrict__ partial)
 {
-    constexpr int R = rows_per_thread<DIM>();
     __shared__ double sm[32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = a.n;
-    const long i0 = (long)blockIdx.x * (256 * R) + threadIdx.x;
-    double sx[R], sy[R], sz[R];
-    long ii[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-        ii[r] = i0 + 256 * r < n ? i0 + 256 * r : (long)n - 1;
-        sx[r] = sy[r] = sz[r] = 0.0;
-    }
-#pragma unroll 2
-    for (int j = 0; j < a.k; j++) {
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-            const long o = (long)j * n + ii[r];
-            const double pc = a.p[a.idx[o]];
-            sx[r] = MGM_ADD(sx[r], MGM_MUL(a.Dx[o], pc));
-            sy[r] = MGM_ADD(sy[r], MGM_MUL(a.Dy[o], pc));
-            if (DIM == 3) sz[r] = MGM_ADD(sz[r], MGM_MUL(a.Dz[o], pc));
-        }
-    }
     double e = 0.0;
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-        const long i = i0 + 256 * r;
-        if (i >= n) break;
-        if (a.btag[i]) continue;
-        const double un = MGM_SUB(a.u_new[i], MGM_DIV(MGM_MUL(a.dt, sx[r]), a.rho));
-        const double vn = MGM_SUB(a.v_new[i], MGM_DIV(MGM_MUL(a.dt, sy[r]), a.rho));
+    if (i < n && !a.btag[i]) {
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int j = 0; j < a.k; j++) {
+            const long o = (long)j * n + i;
+            const double pc = a.p[a.idx[o]];
+            sx = MGM_ADD(sx, MGM_MUL(a.Dx[o], pc));
+            sy = MGM_ADD(sy, MGM_MUL(a.Dy[o], pc));
+            if (DIM == 3) sz = MGM_ADD(sz, MGM_MUL(a.Dz[o], pc));
+        }
+        const double un = MGM_SUB(a.u_new[i], MGM_DIV(MGM_MUL(a.dt, sx), a.rho));
+        const double vn = MGM_SUB(a.v_new[i], MGM_DIV(MGM_MUL(a.dt, sy), a.rho));
         const double du = un - a.u[i], dv = vn - a.v[i];
-        e += du * du + dv * dv;
+        e = du * du + dv * dv;
         a.u[i] = un;
         a.v[i] = vn;
         if (DIM == 3) {
-            const double wn = MGM_SUB(a.w_new[i], MGM_DIV(MGM_MUL(a.dt, sz[r]), a.rho));
+            const double wn = MGM_SUB(a.w_new[i], MGM_DIV(MGM_MUL(a.dt, sz), a.rho));
             const double dw = wn - a.w[i];
             e += dw * dw;
             a.w[i] = wn;
@@ -243,19 +192,19 @@ __global__ void k_finish_mean(const double *partial, int nparts, int n, double *
 
 void launch_momentum(const StepArgs &a, int dim, cudaStream_t s)
 {
-    if (dim == 3) k_momentum<3><<<blocks_for(a.n, 256 * rows_per_thread<3>()), 256, 0, s>>>(a);
-    else k_momentum<2><<<blocks_for(a.n, 256 * rows_per_thread<2>()), 256, 0, s>>>(a);
+    if (dim == 3) k_momentum<3><<<blocks_for(a.n, 256), 256, 0, s>>>(a);
+    else k_momentum<2><<<blocks_for(a.n, 256), 256, 0, s>>>(a);
     MGM_LAUNCHED();
 }
 void launch_divergence(const StepArgs &a, int dim, cudaStream_t s)
 {
-    if (dim == 3) k_divergence<3><<<blocks_for(a.n, 256 * rows_per_thread<3>()), 256, 0, s>>>(a);
-    else k_divergence<2><<<blocks_for(a.n, 256 * rows_per_thread<2>()), 256, 0, s>>>(a);
+    if (dim == 3) k_divergence<3><<<blocks_for(a.n, 256), 256, 0, s>>>(a);
+    else k_divergence<2><<<blocks_for(a.n, 256), 256, 0, s>>>(a);
     MGM_LAUNCHED();
 }
 void launch_correct(const StepArgs &a, int dim, double *partial, double *d_err, cudaStream_t s)
 {
-    const int nb = blocks_for(a.n, 256 * (dim == 3 ? rows_per_thread<3>() : rows_per_thread<2>()));
+    const int nb = blocks_for(a.n, 256);
     if (dim == 3) k_correct<3><<<nb, 256, 0, s>>>(a, partial);
     else k_correct<2><<<nb, 256, 0, s>>>(a, partial);
     MGM_LAUNCHED();

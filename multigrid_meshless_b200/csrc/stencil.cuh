@@ -131,11 +131,23 @@ struct SmootherProfile {
     ~SmootherProfile();
 };
 
-template <class T>
+// the fused coarse-level V-cycle's launch: CTAs (one per SM), its grid
+// barrier {arrivals, generation} and the flag a timed-out barrier sets
+struct FusedCtl {
+    bool on = false;
+    int blocks = 0;
+    unsigned *bar = nullptr;
+    int *err = nullptr;
+};
+int fused_vcycle_blocks();
+cudaError_t launch_coop_probe(cudaStream_t s);
+
 // chain: launch the kernels after the first with programmatic stream
-// serialisation (Chain in mgm_internal.cuh)
+// serialisation (Chain in mgm_internal.cuh); fused (when on): the levels
+// below kVecMinRows rows run as one cooperative launch (k_coarse_vcycle)
+template <class T>
 void vcycle(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &cs, int cheb_degree, double cheb_ratio,
-            cudaStream_t s, SmootherProfile *prof = nullptr, bool chain = false);
+            cudaStream_t s, SmootherProfile *prof = nullptr, bool chain = false, const FusedCtl *fused = nullptr);
 template <class T>
 void estimate_lmax(SolveLevel<T> &L, cudaStream_t s);
 template <class T>

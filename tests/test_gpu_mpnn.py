@@ -16,10 +16,22 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def small(require_gpu):
-    # the benchmark's stencils (k = 30, poly 4): with k = 20, poly 3 the
-    # explicit step on this small cloud grows from the first steps whatever
-    # the time step (the restated step with a direct solve: |u| ~ 1e3 after
-    # 5 steps at Courant 0.1), while k = 30, poly 4 stays bounded for 150
+    # kernels against the oracle: 20-node stencils keep the BF16 rounding
+    # points' disagreement small (an FP32 restatement with the GPU's
+    # summation order differs from the oracle by 0.3% in y here, 1.9% with
+    # 30-node stencils)
+    cl = clouds.cavity_hierarchy(40, 3, seed=5)
+    mg = api.Multigrid(cl, [20, 20, 20], [3, 3, 3])
+    yield mg
+    mg.close()
+
+
+@pytest.fixture(scope="module")
+def stable(require_gpu):
+    # time steps: the benchmark's stencils (k = 30, poly 4).  With k = 20,
+    # poly 3 the explicit step on this small cloud grows from the first steps
+    # whatever the time step (the restated step with a direct solve: |u| ~ 1e3
+    # after 5 steps at Courant 0.1), while k = 30, poly 4 stays bounded for 150
     # steps at Re 180 and 900, Courant 0.3
     cl = clouds.cavity_hierarchy(48, 3, seed=5)
     mg = api.Multigrid(cl, [30, 30, 30], [4, 4, 4])
@@ -83,7 +95,7 @@ def test_gradients_match_oracle(small, w_mse, w_res):
         assert err < 2e-2, (a, b, err)
 
 
-def test_training_and_warm_start(small):
+def test_training_and_warm_start(stable):
     """The C5 protocol in small: the network is trained on the GPU on steps of
     the plain solver at Re drawn from [100, 1000] (Courant 0.3, where the
     explicit scheme is stable for long runs), then the same held-out episode
@@ -93,7 +105,7 @@ def test_training_and_warm_start(small):
     the last pressure increment and the network's prediction).  The learned
     guess must save V-cycles over the method without it, strictly, and cost
     no more than the extrapolation alone; pressures agree to 1e-6."""
-    mg = small
+    mg = stable
     L = _lib.load()
     steps_ep = 30
     _lib.check(L.mgm_mpnn_init(mg.h, 11, 4 * steps_ep))

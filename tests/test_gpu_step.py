@@ -264,20 +264,25 @@ def test_step_graph_matches_host_driven_steps(cavity):
     loops as conditional WHILE nodes set by device kernels) gives the bits of
     the host-driven solve (host reads the loop flags, V-cycle graphs) and of
     fully eager launches, with the V-cycle's kernels chained by programmatic
-    dependent launch (default) or launched the ordinary way: fields after
-    every step, V-cycle counts, steady error; through mgm_run_steps and
-    mgm_step."""
+    dependent launch (default) or launched the ordinary way, and with the
+    small levels' V-cycle as one cooperative launch (default; every level of
+    this cloud is small) or one kernel per operation: fields after every
+    step, V-cycle counts, steady error; through mgm_run_steps and mgm_step."""
     mg = cavity
+    assert mg.fused_coarse_available()
     mg.set_flow(Re=100.0, courant=0.5)
     mg.set_solver(rel_tol=1e-8, max_iters=80)
     try:
         for mode in (mgm.MODE_FP64, mgm.MODE_FP32_IR):
             runs = []
-            for graphs, step_graph, chain in ((True, True, True), (True, True, False), (True, False, True),
-                                              (True, False, False), (False, False, True)):
+            for graphs, step_graph, chain, fused in ((True, True, True, True), (True, True, False, True),
+                                                     (True, True, True, False), (True, False, True, True),
+                                                     (True, False, False, False), (False, False, True, True),
+                                                     (False, False, True, False)):
                 mg.use_graphs(graphs)
                 mg.use_step_graph(step_graph)
                 mg.use_launch_chaining(chain)
+                mg.use_fused_coarse(fused)
                 mg.apply_bc(mgm.BC_LID)
                 out = []
                 for rep in range(2):  # second replay of the same step graph
@@ -297,6 +302,7 @@ def test_step_graph_matches_host_driven_steps(cavity):
         mg.use_graphs(True)
         mg.use_step_graph(True)
         mg.use_launch_chaining(True)
+        mg.use_fused_coarse(True)
 
 
 def test_step_graph_reports_unconverged_solve(cavity):
