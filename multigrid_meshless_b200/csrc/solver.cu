@@ -854,9 +854,10 @@ struct FusedArgs {
 
 // Grid barrier of a cooperative launch (all CTAs resident): thread 0 of each
 // CTA arrives on a counter; the last arrival resets it and advances the
-// generation the others wait on.  The wait is bounded (about 0.5 s); when it
-// runs out the CTA records the error and the kernel's CTAs return at their
-// next barrier.  Returns false once any CTA has given up.
+// generation the others wait on (polled without sleeping: the wait is a few
+// microseconds).  The wait is bounded (2^20 polls of L2, under a second);
+// when it runs out the CTA records the error and the kernel's CTAs
+// return at their next barrier.  Returns false once any CTA has given up.
 __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err, unsigned &gen)
 {
     __shared__ int ok;
@@ -872,12 +873,11 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err, unsigned &
         } else {
             long spins = 0;
             while (*(volatile unsigned *)&bar[1] == gen) {
-                if (++spins > (1L << 22) || *(volatile int *)err) {
+                if (++spins > (1L << 20) || ((spins & 255) == 0 && *(volatile int *)err)) {
                     atomicExch(err, 1);
                     good = 0;
                     break;
                 }
-                __nanosleep(64);
             }
         }
         __threadfence();
