@@ -334,7 +334,7 @@ def measured_peak():
 # one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, one launch) of
 # level 0 of the 1M-node cavity; the summary with its command is committed
 # under profiles/.  Scaled by node count in the bench line's `traffic`.
-NCU_L0_SMOOTHER_DRAM_BYTES = 200_700_000
+NCU_L0_SMOOTHER_DRAM_BYTES = 200_900_000
 NCU_L0_SMOOTHER_NODES = 999_996
 
 
