@@ -381,10 +381,12 @@ MGM_API int mgm_use_graphs(mgm_ctx *ctx, int enable);
 MGM_API int mgm_use_launch_chaining(mgm_ctx *ctx, int enable);
 /* The levels below 65,536 rows (latency-bound: about 17 short kernels per
  * level per V-cycle) run as ONE cooperative launch per V-cycle, one CTA per
- * SM, a grid barrier between dependent passes (enable = 1, default);
- * enable = 0 launches every operation of those levels as its own kernel.
- * Results are identical.  The barrier's wait is bounded: when it runs out
- * the solve returns MGM_ERR_TIMEOUT. */
+ * SM, a grid barrier between dependent passes (enable = 1, opt-in);
+ * enable = 0 (default) launches every operation of those levels as its own
+ * kernel, which measured faster on the 1M cavity (52 grid barriers per
+ * V-cycle cost more than the launches they replace).  Results are
+ * identical.  The barrier's wait is bounded: when it runs out the solve
+ * returns MGM_ERR_TIMEOUT. */
 MGM_API int mgm_use_fused_coarse(mgm_ctx *ctx, int enable);
 /* 1 when the fused coarse V-cycle can run here (after mgm_setup: a CTA fits
  * on an SM and the driver accepts a cooperative kernel inside a conditional

@@ -353,7 +353,7 @@ class Multigrid:
         check(self.L.mgm_use_launch_chaining(self.h, 1 if enable else 0))
 
     def use_fused_coarse(self, enable=True):
-        """The small levels' V-cycle as one cooperative launch (default on)."""
+        """The small levels' V-cycle as one cooperative launch (opt-in; default off)."""
         check(self.L.mgm_use_fused_coarse(self.h, 1 if enable else 0))
 
     def fused_coarse_available(self):

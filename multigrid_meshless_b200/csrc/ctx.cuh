@@ -107,7 +107,7 @@ struct mgm_ctx {
     bool use_tma = false;             // tile-streamed level kernels where a level has them (else 4 rows per thread)
     bool half_operator = false;       // FP32 V-cycle reads the FP16 operator where built
     bool chain_launches = true;       // V-cycle kernels after the first use programmatic dependent launch
-    bool fused_coarse = true;         // levels below kVecMinRows rows in one cooperative V-cycle launch
+    bool fused_coarse = false;        // levels below kVecMinRows rows in one cooperative V-cycle launch (opt-in: slower here)
     int fused_blocks = 0;             // its CTAs (one per SM)
     DBuf<unsigned> fused_bar;         // its grid barrier {arrivals, generation}
     // compatible right-hand sides (mgm_set_compatible_rhs): the pinned solution

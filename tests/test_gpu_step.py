@@ -265,8 +265,8 @@ def test_step_graph_matches_host_driven_steps(cavity):
     the host-driven solve (host reads the loop flags, V-cycle graphs) and of
     fully eager launches, with the V-cycle's kernels chained by programmatic
     dependent launch (default) or launched the ordinary way, and with the
-    small levels' V-cycle as one cooperative launch (default; every level of
-    this cloud is small) or one kernel per operation: fields after every
+    small levels' V-cycle as one cooperative launch (opt-in; every level of
+    this cloud is small) or one kernel per operation (default): fields after every
     step, V-cycle counts, steady error; through mgm_run_steps and mgm_step."""
     mg = cavity
     assert mg.fused_coarse_available()
@@ -302,7 +302,7 @@ def test_step_graph_matches_host_driven_steps(cavity):
         mg.use_graphs(True)
         mg.use_step_graph(True)
         mg.use_launch_chaining(True)
-        mg.use_fused_coarse(True)
+        mg.use_fused_coarse(False)
 
 
 def test_step_graph_reports_unconverged_solve(cavity):
