@@ -990,12 +990,14 @@ def run_reference(a, rank):
     workload (reference_full), one JSON line on rank 0; other ranks exit."""
     if rank != 0:
         return None
-    a.episode = a.warmup + max(a.steps, 1)  # one episode from rest, as each arm of ours
+    a.episode = a.warmup + max(a.steps, 1)  # one episode from rest
     s = reference_full(a, steps=max(a.steps, 1), warmup=a.warmup)
     val = 1.0 / s["sec_per_step"]
     cfg = workload(a)
     cfg["reference_solver"] = ("the reference's own multigrid_Poisson_solver: a fixed 10 V-cycles of 3 SOR sweeps "
                                "(omega 1.0) per step; it has no tolerance test and never reaches 1e-8")
+    cfg["episodes"] = (f"one episode from rest at Re={a.Re:g}: {a.warmup} warm-up and {max(a.steps, 1)} timed steps "
+                       "(the reference's work per step does not depend on the flow: a fixed V-cycle count)")
     return {
         "impl": "reference",
         "metric": METRIC,
