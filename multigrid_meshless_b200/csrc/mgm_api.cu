@@ -1532,7 +1532,7 @@ void prepare_solver(mgm_ctx *c)
         b->alloc(n0);
         b->zero(s);
     }
-    c->partial.alloc(blocks_for(n0, 256) + 8);
+    c->partial.alloc(blocks_for(n0, 32) + 8);  // per-warp partial sums (k_correct)
     c->scal.alloc(8);
     c->tma_err.alloc(1);
     c->tma_err.zero(s);

@@ -59,7 +59,37 @@ __global__ void __launch_bounds__(256) k_momentum(StepArgs a)
 #pragma unroll
     for (int c = 0; c < DIM; c++) { gx[c] = 0.0; gy[c] = 0.0; gz[c] = 0.0; gl[c] = 0.0; }
     const double *vel[3] = {a.u, a.v, a.w};
-    for (int j = 0; j < a.k; j++) {
+    // slots in chunks of C: the chunk's indices and weights, then its
+    // gathers, are in flight together; each sum still runs in slot order
+    constexpr int C = DIM == 2 ? 6 : 3;
+    int j = 0;
+    for (; j + C <= a.k; j += C) {
+        int c[C];
+        double wx[C], wy[C], wz[C], wl[C], f[DIM][C];
+#pragma unroll
+        for (int q = 0; q < C; q++) {
+            const long o = (long)(j + q) * n + i;
+            c[q] = __ldg(a.idx + o);
+            wx[q] = __ldg(a.Dx + o);
+            wy[q] = __ldg(a.Dy + o);
+            wz[q] = DIM == 3 ? __ldg(a.Dz + o) : 0.0;
+            wl[q] = __ldg(a.lap + o);
+        }
+#pragma unroll
+        for (int q = 0; q < C; q++)
+#pragma unroll
+            for (int d = 0; d < DIM; d++) f[d][q] = __ldg(vel[d] + c[q]);
+#pragma unroll
+        for (int q = 0; q < C; q++)
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+                gx[d] = MGM_ADD(gx[d], MGM_MUL(wx[q], f[d][q]));
+                gy[d] = MGM_ADD(gy[d], MGM_MUL(wy[q], f[d][q]));
+                if (DIM == 3) gz[d] = MGM_ADD(gz[d], MGM_MUL(wz[q], f[d][q]));
+                gl[d] = MGM_ADD(gl[d], MGM_MUL(wl[q], f[d][q]));
+            }
+    }
+    for (; j < a.k; j++) {
         const long o = (long)j * n + i;
         const int c = a.idx[o];
         const double wx = a.Dx[o], wy = a.Dy[o], wl = a.lap[o];
@@ -105,7 +135,34 @@ __global__ void __launch_bounds__(256) k_divergence(StepArgs a)
         return;  // the boundary source keeps its value (zero): homogeneous Neumann rows
     }
     double sx = 0.0, sy = 0.0, sz = 0.0;
-    for (int j = 0; j < a.k; j++) {
+    // slots in chunks of C (as k_momentum); each sum in slot order
+    constexpr int C = DIM == 2 ? 6 : 3;
+    int j = 0;
+    for (; j + C <= a.k; j += C) {
+        int c[C];
+        double wx[C], wy[C], wz[C], fu[C], fv[C], fw[C];
+#pragma unroll
+        for (int q = 0; q < C; q++) {
+            const long o = (long)(j + q) * n + i;
+            c[q] = __ldg(a.idx + o);
+            wx[q] = __ldg(a.Dx + o);
+            wy[q] = __ldg(a.Dy + o);
+            wz[q] = DIM == 3 ? __ldg(a.Dz + o) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < C; q++) {
+            fu[q] = __ldg(a.u_new + c[q]);
+            fv[q] = __ldg(a.v_new + c[q]);
+            fw[q] = DIM == 3 ? __ldg(a.w_new + c[q]) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < C; q++) {
+            sx = MGM_ADD(sx, MGM_MUL(wx[q], fu[q]));
+            sy = MGM_ADD(sy, MGM_MUL(wy[q], fv[q]));
+            if (DIM == 3) sz = MGM_ADD(sz, MGM_MUL(wz[q], fw[q]));
+        }
+    }
+    for (; j < a.k; j++) {
         const long o = (long)j * n + i;
         const int c = a.idx[o];
         sx = MGM_ADD(sx, MGM_MUL(a.Dx[o], a.u_new[c]));
@@ -118,22 +175,47 @@ __global__ void __launch_bounds__(256) k_divergence(StepArgs a)
 // update_velocity (fractional_step_solver.h:248-265) fused with the steady
 // error partial sums of fractional_step_explicit (:63-69); u_old is the
 // velocity at the start of the step (the update leaves boundary rows alone).
+// Slots in chunks of C (each sum in slot order); the steady-error sums are
+// reduced per warp (partial[global warp], summed by k_finish_steady) with no
+// CTA barrier, which let warps that finish early hold the CTA's slot.
 template <int DIM>
 __global__ void __launch_bounds__(256) k_correct(StepArgs a, double *__restrict__ partial)
 {
-    __shared__ double sm[32];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = a.n;
-    double e = 0.0;
-    if (i < n && !a.btag[i]) {
-        double sx = 0.0, sy = 0.0, sz = 0.0;
-        for (int j = 0; j < a.k; j++) {
-            const long o = (long)j * n + i;
-            const double pc = a.p[a.idx[o]];
-            sx = MGM_ADD(sx, MGM_MUL(a.Dx[o], pc));
-            sy = MGM_ADD(sy, MGM_MUL(a.Dy[o], pc));
-            if (DIM == 3) sz = MGM_ADD(sz, MGM_MUL(a.Dz[o], pc));
+    const int i = i0 < n ? i0 : n - 1;  // rows past n compute row n-1 and store nothing
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    constexpr int C = DIM == 2 ? 10 : 5;
+    int j = 0;
+    for (; j + C <= a.k; j += C) {
+        int c[C];
+        double wx[C], wy[C], wz[C], pc[C];
+#pragma unroll
+        for (int q = 0; q < C; q++) {
+            const long o = (long)(j + q) * n + i;
+            c[q] = __ldg(a.idx + o);
+            wx[q] = __ldg(a.Dx + o);
+            wy[q] = __ldg(a.Dy + o);
+            wz[q] = DIM == 3 ? __ldg(a.Dz + o) : 0.0;
         }
+#pragma unroll
+        for (int q = 0; q < C; q++) pc[q] = __ldg(a.p + c[q]);
+#pragma unroll
+        for (int q = 0; q < C; q++) {
+            sx = MGM_ADD(sx, MGM_MUL(wx[q], pc[q]));
+            sy = MGM_ADD(sy, MGM_MUL(wy[q], pc[q]));
+            if (DIM == 3) sz = MGM_ADD(sz, MGM_MUL(wz[q], pc[q]));
+        }
+    }
+    for (; j < a.k; j++) {
+        const long o = (long)j * n + i;
+        const double pc = a.p[a.idx[o]];
+        sx = MGM_ADD(sx, MGM_MUL(a.Dx[o], pc));
+        sy = MGM_ADD(sy, MGM_MUL(a.Dy[o], pc));
+        if (DIM == 3) sz = MGM_ADD(sz, MGM_MUL(a.Dz[o], pc));
+    }
+    double e = 0.0;
+    if (i0 < n && !a.btag[i]) {
         const double un = MGM_SUB(a.u_new[i], MGM_DIV(MGM_MUL(a.dt, sx), a.rho));
         const double vn = MGM_SUB(a.v_new[i], MGM_DIV(MGM_MUL(a.dt, sy), a.rho));
         const double du = un - a.u[i], dv = vn - a.v[i];
@@ -147,8 +229,8 @@ __global__ void __launch_bounds__(256) k_correct(StepArgs a, double *__restrict_
             a.w[i] = wn;
         }
     }
-    e = block_sum<256>(e, sm);
-    if (threadIdx.x == 0) partial[blockIdx.x] = e;
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+    if ((threadIdx.x & 31) == 0) partial[i0 >> 5] = e;
 }
 
 __global__ void k_finish_steady(const double *partial, int nparts, int n, double *out)
@@ -208,7 +290,7 @@ void launch_correct(const StepArgs &a, int dim, double *partial, double *d_err, 
     if (dim == 3) k_correct<3><<<nb, 256, 0, s>>>(a, partial);
     else k_correct<2><<<nb, 256, 0, s>>>(a, partial);
     MGM_LAUNCHED();
-    k_finish_steady<<<1, 256, 0, s>>>(partial, nb, a.n, d_err);
+    k_finish_steady<<<1, 256, 0, s>>>(partial, nb * 8, a.n, d_err);  // one partial per warp
     MGM_LAUNCHED();
 }
 void launch_mass_diag(const StepArgs &a, int dim, double *partial, double *d_out, cudaStream_t s)
