@@ -393,6 +393,12 @@ MGM_API int mgm_use_fused_coarse(mgm_ctx *ctx, int enable);
  * graph node); 0: every level runs per-operation kernels whatever
  * mgm_use_fused_coarse says. */
 MGM_API int mgm_fused_coarse_available(mgm_ctx *ctx, int *available);
+/* Self-test of the bounded wait in the fused V-cycle's grid barrier: a
+ * two-CTA cooperative launch in which one CTA never arrives, so the other's
+ * wait runs out (under a second), records the timeout and returns; the
+ * flags and the barrier are cleared after.  *status = MGM_ERR_TIMEOUT when
+ * the bound worked (the context stays usable).  No reference counterpart. */
+MGM_API int mgm_selftest_barrier_timeout(mgm_ctx *ctx, int *status);
 /* With graphs on: the whole fractional step as one captured graph (enable =
  * 1, default) -- momentum, divergence, the Poisson solve with its restart and
  * Arnoldi loops as conditional WHILE nodes whose conditions device kernels

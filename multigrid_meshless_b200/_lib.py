@@ -91,6 +91,7 @@ SIGNATURES = {
     "mgm_use_launch_chaining": ([vp, C.c_int], C.c_int),
     "mgm_use_fused_coarse": ([vp, C.c_int], C.c_int),
     "mgm_fused_coarse_available": ([vp, C.POINTER(C.c_int)], C.c_int),
+    "mgm_selftest_barrier_timeout": ([vp, C.POINTER(C.c_int)], C.c_int),
     "mgm_use_step_graph": ([vp, C.c_int], C.c_int),
     "mgm_solve_counters": ([vp, vp, vp, vp], C.c_int),
     "mgm_set_initial_guess": ([vp, C.c_int], C.c_int),

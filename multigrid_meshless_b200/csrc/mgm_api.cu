@@ -1986,6 +1986,27 @@ int mgm_use_fused_coarse(mgm_ctx *c, int enable)
     });
 }
 
+int mgm_selftest_barrier_timeout(mgm_ctx *c, int *status)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(status, "mgm_selftest_barrier_timeout: null argument");
+        MGM_CUDA(cudaSetDevice(c->device));
+        cudaStream_t s = c->s;
+        MGM_CUDA(cudaStreamSynchronize(s));
+        c->tma_err.zero(s);
+        c->fused_bar.zero(s);
+        MGM_CUDA(launch_barrier_selftest(s, c->fused_bar.p, c->tma_err.p));
+        MGM_LAUNCHED();
+        *status = MGM_OK;
+        try {
+            check_wait_flags(c, s);  // clears the flags and the barrier when the wait ran out
+        } catch (const Error &e) {
+            *status = e.code;
+        }
+    });
+}
+
 int mgm_fused_coarse_available(mgm_ctx *c, int *available)
 {
     return guard([&] {

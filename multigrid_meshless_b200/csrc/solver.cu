@@ -1022,6 +1022,29 @@ static void launch_fused(std::vector<SolveLevel<T>> &Ls, const CoarseSolve<T> &c
     MGM_LAUNCHED();
 }
 
+// Self-test of the grid barrier's bounded wait: CTA 1 returns without
+// arriving, so CTA 0's wait runs out, sets *err and returns.
+__global__ void k_barrier_selftest(unsigned *bar, int *err)
+{
+    unsigned gen = 0;
+    if (threadIdx.x == 0) gen = *(volatile unsigned *)&bar[1];
+    if (blockIdx.x == 1) return;
+    grid_barrier(bar, err, gen);
+}
+cudaError_t launch_barrier_selftest(cudaStream_t s, unsigned *bar, int *err)
+{
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2);
+    cfg.blockDim = dim3(32);
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_barrier_selftest, bar, err);
+}
+
 // a cooperative launch of one CTA that does nothing (capture probe)
 __global__ void k_coop_probe(int) {}
 cudaError_t launch_coop_probe(cudaStream_t s)

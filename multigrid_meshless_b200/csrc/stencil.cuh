@@ -141,6 +141,7 @@ struct FusedCtl {
 };
 int fused_vcycle_blocks();
 cudaError_t launch_coop_probe(cudaStream_t s);
+cudaError_t launch_barrier_selftest(cudaStream_t s, unsigned *bar, int *err);
 
 // chain: launch the kernels after the first with programmatic stream
 // serialisation (Chain in mgm_internal.cuh); fused (when on): the levels

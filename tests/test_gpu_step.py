@@ -340,3 +340,31 @@ def test_fp64_solve_matches_cpu_restatement(cavity):
     assert ok and rr_gpu < 1e-9
     assert abs(it_gpu - it_cpu) <= 1, (it_gpu, it_cpu)
     assert np.linalg.norm(p_gpu - p_cpu) / np.linalg.norm(p_cpu) < 1e-7
+
+
+def test_fused_barrier_wait_runs_out_and_context_stays_usable(cavity):
+    """The fused coarse V-cycle's grid barrier bounds its wait: in a two-CTA
+    self-test one CTA never arrives, the other's wait runs out, the kernel
+    returns and the host reads MGM_ERR_TIMEOUT (no trap, no hang).  After it
+    the context still solves, with the fused V-cycle giving the bits of the
+    per-operation kernels."""
+    import ctypes as C
+    from multigrid_meshless_b200 import _lib
+    mg = cavity
+    L = _lib.load()
+    st = C.c_int(-1)
+    _lib.check(L.mgm_selftest_barrier_timeout(mg.h, C.byref(st)))
+    assert st.value == _lib.MGM_ERR_TIMEOUT
+    mg.set_flow(Re=100.0, courant=0.5)
+    mg.set_solver(rel_tol=1e-8, max_iters=80)
+    out = []
+    try:
+        for fused in (True, False):
+            mg.use_fused_coarse(fused)
+            mg.apply_bc(mgm.BC_LID)
+            _, _, vc, err = mg.run_steps(mgm.MODE_FP32_IR, 2)
+            out.append((vc, err, mg.get_field("p")))
+    finally:
+        mg.use_fused_coarse(False)
+    assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2], out[1][2])
