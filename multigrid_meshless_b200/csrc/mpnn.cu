@@ -138,40 +138,43 @@ __global__ void k_features_ds(int n, const float *bh, const float *ph, const flo
 }
 
 // encoder: eight lanes per node (hidden features 8l..8l+7, one 16-byte store
-// of h0), four nodes per warp; W_e and c_e (contiguous in P) staged in
-// shared memory.  Each feature's sum is c_e then the inputs in order.
+// of h0), four nodes per warp, grid-stride over nodes; each lane keeps its 8
+// columns of W_e and c_e in registers (loaded once), so the node loop reads
+// only the 6 inputs.  Each feature's sum is c_e then the inputs in order.
 __global__ void __launch_bounds__(256) k_encode(int n, const float *__restrict__ feat, const float *__restrict__ P,
                                                 bf16 *__restrict__ h0, float *__restrict__ z0)
 {
-    __shared__ __align__(16) float We[kFin * kH + kH];
-    for (int q = threadIdx.x; q < kFin * kH + kH; q += blockDim.x) We[q] = P[P_WE + q];
-    __syncthreads();
-    const long node = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 3;
     const int c = 8 * (threadIdx.x & 7);
-    if (node >= n) return;
-    float f[kFin], a[8];
+    float w[kFin][8], cb[8];
 #pragma unroll
-    for (int q = 0; q < kFin; q++) f[q] = __ldg(feat + node * kFin + q);
+    for (int e = 0; e < 8; e++) cb[e] = __ldg(P + P_CE + c + e);
 #pragma unroll
-    for (int e = 0; e < 8; e++) a[e] = We[P_CE - P_WE + c + e];
+    for (int q = 0; q < kFin; q++)
 #pragma unroll
-    for (int q = 0; q < kFin; q++) {
-        const float4 w0 = *reinterpret_cast<const float4 *>(&We[q * kH + c]);
-        const float4 w1 = *reinterpret_cast<const float4 *>(&We[q * kH + c + 4]);
-        a[0] += f[q] * w0.x; a[1] += f[q] * w0.y; a[2] += f[q] * w0.z; a[3] += f[q] * w0.w;
-        a[4] += f[q] * w1.x; a[5] += f[q] * w1.y; a[6] += f[q] * w1.z; a[7] += f[q] * w1.w;
-    }
-    float r[8];
+        for (int e = 0; e < 8; e++) w[q][e] = __ldg(P + P_WE + q * kH + c + e);
+    const long stride = (long)gridDim.x * (blockDim.x >> 3);
+    for (long node = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 3; node < n; node += stride) {
+        float f[kFin], a[8];
 #pragma unroll
-    for (int e = 0; e < 8; e++) r[e] = fmaxf(a[e], 0.f);
-    uint4 u;
-    __nv_bfloat162 *b = reinterpret_cast<__nv_bfloat162 *>(&u);
+        for (int q = 0; q < kFin; q++) f[q] = __ldg(feat + node * kFin + q);
 #pragma unroll
-    for (int q = 0; q < 4; q++) b[q] = __floats2bfloat162_rn(r[2 * q], r[2 * q + 1]);
-    *reinterpret_cast<uint4 *>(h0 + node * kH + c) = u;
-    if (z0) {
-        *reinterpret_cast<float4 *>(z0 + node * kH + c) = make_float4(a[0], a[1], a[2], a[3]);
-        *reinterpret_cast<float4 *>(z0 + node * kH + c + 4) = make_float4(a[4], a[5], a[6], a[7]);
+        for (int e = 0; e < 8; e++) a[e] = cb[e];
+#pragma unroll
+        for (int q = 0; q < kFin; q++)
+#pragma unroll
+            for (int e = 0; e < 8; e++) a[e] += f[q] * w[q][e];
+        float r[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) r[e] = fmaxf(a[e], 0.f);
+        uint4 u;
+        __nv_bfloat162 *b = reinterpret_cast<__nv_bfloat162 *>(&u);
+#pragma unroll
+        for (int q = 0; q < 4; q++) b[q] = __floats2bfloat162_rn(r[2 * q], r[2 * q + 1]);
+        *reinterpret_cast<uint4 *>(h0 + node * kH + c) = u;
+        if (z0) {
+            *reinterpret_cast<float4 *>(z0 + node * kH + c) = make_float4(a[0], a[1], a[2], a[3]);
+            *reinterpret_cast<float4 *>(z0 + node * kH + c + 4) = make_float4(a[4], a[5], a[6], a[7]);
+        }
     }
 }
 
@@ -710,7 +713,8 @@ static void forward(MpnnState &M, bool train, cudaStream_t s)
 {
     const int n = M.n;
     const float *P = M.params.p;
-    k_encode<<<blocks_for((long)n * 8, 256), 256, 0, s>>>(n, M.feat.p, P, M.h[0].p, train ? M.z[0].p : nullptr);
+    k_encode<<<std::min(blocks_for((long)n * 8, 256), 148 * 8), 256, 0, s>>>(n, M.feat.p, P, M.h[0].p,
+                                                                             train ? M.z[0].p : nullptr);
     MGM_LAUNCHED();
     for (int l = 0; l < kLayers; l++) {
         // inference: the last layer decodes in its epilogue and stores no h4
