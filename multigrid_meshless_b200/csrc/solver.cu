@@ -62,12 +62,10 @@ __device__ __forceinline__ void bnd_row_warp(int w, int lane, const int *__restr
                                              const T *__restrict__ dinv, const T *r, T *e)
 {
     const int i = list[w];
-    // the row's own values first (every lane: no divergence), overlapping the dot
-    const T ei = ldv<COH>(e + i), ri = ldv<COH>(r + i), di = dinv[i];
     T s = T(0);
     for (int j = lane; j < k; j += 32) s += bA[(long)w * k + j] * ldv<COH>(e + bidx[(long)w * k + j]);
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) e[i] = ei + (ri - s) * di;
+    if (lane == 0) e[i] = ldv<COH>(e + i) + (ldv<COH>(r + i) - s) * dinv[i];
 }
 
 // Start of a smoothing pass from e = 0: interior rows 0, boundary rows their
@@ -228,23 +226,6 @@ __device__ __forceinline__ T ell_row_dot_o(const short *__restrict__ off, const 
 // Chebyshev step q = r - A e, d = c1 d + c2 D^-1 q, e' = e + d on interior
 // rows (boundary rows copy e); MODE 1: residual q = r - A e on interior rows,
 // 0 on boundary rows.
-// level_row_out on values loaded beforehand (ei = e[i], ri = r[i], dinvi =
-// dinv[i], dold = d[i] when not first, bt = btag[i]): the same arithmetic
-template <int MODE, class T>
-__device__ __forceinline__ void level_row_vals(int i, T s, T ei, T ri, T dinvi, T dold, uint8_t bt, T *out, T *d, T c1,
-                                               T c2, int first)
-{
-    if (MODE == 0) {
-        if (bt) { out[i] = ei; return; }
-        const T q = ri - s;
-        const T di = first ? c2 * dinvi * q : c1 * dold + c2 * dinvi * q;
-        d[i] = di;
-        out[i] = ei + di;
-    } else {
-        out[i] = bt ? T(0) : ri - s;
-    }
-}
-
 template <int MODE, class T, bool COH = false>
 __device__ __forceinline__ void level_row_out(int i, T s, const T *__restrict__ dinv,
                                               const uint8_t *__restrict__ btag, const T *r, const T *e, T *out, T *d,
@@ -286,15 +267,7 @@ __global__ void __launch_bounds__(256) k_level_c1(int n, int ld, int k, const sh
     pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    // the row's own values first, so that their latency overlaps the dot
-    const uint8_t bt = btag[i];
-    const T ri = r[i], ei = MODE == 0 ? e[i] : T(0);
-    const T dvi = MODE == 0 ? dinv[i] : T(0), dold = (MODE == 0 && !first) ? d[i] : T(0);
-    if (bt) {
-        out[i] = MODE == 0 ? ei : T(0);
-        return;
-    }
-    level_row_vals<MODE, T>(i, ell_row_dot_o(off, A, e, ld, k, i, i), ei, ri, dvi, dold, bt, out, d, c1, c2, first);
+    c1_row<MODE, T>(i, ld, k, off, A, dinv, btag, r, e, out, d, c1, c2, first);
 }
 
 // the four weights of rows i0..i0+3 in slot o (evict-first)
@@ -320,19 +293,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) k_level_v4(
     pdl_enter();
     const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
     if (i0 >= n) return;
-    // the rows' own values, loaded before the slot loop so that their
-    // latency overlaps it rather than adding a round trip after it
-    T ev[4], rv[4], dv[4], dd[4];
-    uint8_t bt[4];
-#pragma unroll
-    for (int v = 0; v < 4; v++) {
-        const int i = min(i0 + v, n - 1);
-        bt[v] = btag[i];
-        rv[v] = r[i];
-        ev[v] = MODE == 0 ? e[i] : T(0);
-        dv[v] = MODE == 0 ? dinv[i] : T(0);
-        dd[v] = (MODE == 0 && !first) ? d[i] : T(0);
-    }
     T s[4] = {T(0), T(0), T(0), T(0)};
     int j = 0;
     for (; j + 4 <= k; j += 4) {
@@ -363,7 +323,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) k_level_v4(
     }
 #pragma unroll
     for (int v = 0; v < 4; v++)
-        if (i0 + v < n) level_row_vals<MODE, T>(i0 + v, s[v], ev[v], rv[v], dv[v], dd[v], bt[v], out, d, c1, c2, first);
+        if (i0 + v < n) level_row_out<MODE, T>(i0 + v, s[v], dinv, btag, r, e, out, d, c1, c2, first);
 }
 
 // k_level_h4: k_level_v4 on the FP16 operator W ~ D^-1 A, four rows per
@@ -501,8 +461,7 @@ __device__ __forceinline__ void prolong_row(int i, int n, int k, const short *__
                                             const int *__restrict__ base, const T *__restrict__ pw, const T *ec, T *ef,
                                             T shift)
 {
-    const T old = ldv<COHERENT>(ef + i);  // loaded first: its latency overlaps the dot
-    ef[i] = old + (ell_row_dot_o<T, T, COHERENT>(off, pw, ec, n, k, i, base[i]) - shift);
+    ef[i] = ldv<COHERENT>(ef + i) + (ell_row_dot_o<T, T, COHERENT>(off, pw, ec, n, k, i, base[i]) - shift);
 }
 
 template <class T>
