@@ -418,6 +418,11 @@ MGM_API int mgm_use_step_graph(mgm_ctx *ctx, int enable);
  * restart-cycle starts (each computes a true residual), solves.  Any pointer
  * may be NULL.  No counterpart in the reference. */
 MGM_API int mgm_solve_counters(mgm_ctx *ctx, long long *vcycles, long long *cycles, long long *solves);
+/* Geometric mean, over the solves of the last run, of the relative residual
+ * |b - A p0| / |b| each solve started from (p0 its initial guess,
+ * mgm_set_initial_guess): what the guesses achieve before the first
+ * V-cycle.  No reference counterpart. */
+MGM_API int mgm_solve_start_residual(mgm_ctx *ctx, double *geo_mean);
 /* FP32 compact path: on levels of at least 65,536 rows, stream the operator
  * tile by tile into shared memory with bulk asynchronous copies (enable = 1),
  * or read it with plain vector loads, four rows per thread (enable = 0, the

@@ -94,6 +94,7 @@ SIGNATURES = {
     "mgm_selftest_barrier_timeout": ([vp, C.POINTER(C.c_int)], C.c_int),
     "mgm_use_step_graph": ([vp, C.c_int], C.c_int),
     "mgm_solve_counters": ([vp, vp, vp, vp], C.c_int),
+    "mgm_solve_start_residual": ([vp, C.POINTER(C.c_double)], C.c_int),
     "mgm_set_initial_guess": ([vp, C.c_int], C.c_int),
     "mgm_use_compact": ([vp, C.c_int], C.c_int),
     "mgm_use_tiled": ([vp, C.c_int], C.c_int),

@@ -367,6 +367,12 @@ class Multigrid:
         check(self.L.mgm_solve_counters(self.h, C.byref(v), C.byref(c), C.byref(n)))
         return v.value, c.value, n.value
 
+    def solve_start_residual(self):
+        """Geometric mean of the relative residual each solve of the last run started from."""
+        v = C.c_double()
+        check(self.L.mgm_solve_start_residual(self.h, C.byref(v)))
+        return v.value
+
     def set_initial_guess(self, flags):
         """MGM_GUESS_* flags of the steps' Poisson solves (0: previous pressure)."""
         check(self.L.mgm_set_initial_guess(self.h, int(flags)))

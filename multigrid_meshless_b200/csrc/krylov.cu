@@ -261,6 +261,7 @@ __global__ void k_fg_clear_totals(FgState *st)
     st->cycles_total = 0;
     st->solves_total = 0;
     st->t_ns = 0;
+    st->start_log_relres = 0.0;
 }
 
 __global__ void k_fg_time_mark(FgState *st, int end)
@@ -290,6 +291,9 @@ __global__ void __launch_bounds__(256) k_fg_begin(FgState *st, const double *__r
     st->bnorm = bnorm;
     st->beta = beta;
     st->relres = relres;
+    // the solve's first cycle: the residual its initial guess left
+    if (st->restarts == 0 && st->total_it == 0 && relres > 0 && isfinite(relres))
+        st->start_log_relres += log10(relres);
     st->j = 0;
     st->j_done = 0;
     int go = 0;

@@ -59,6 +59,7 @@ struct FgState {
     long long solves_total;
     unsigned long long t_mark;  // %globaltimer at the last start mark
     unsigned long long t_ns;    // summed ns between start and end marks
+    double start_log_relres;    // summed log10 of each solve's starting relative residual (after its guess)
     double head_end_;
     // arrays
     double H[(kMaxKrylov + 1) * kMaxKrylov];  // column j at H[j * (m + 1)]

@@ -2058,6 +2058,16 @@ int mgm_solve_counters(mgm_ctx *c, long long *vcycles, long long *cycles, long l
     });
 }
 
+int mgm_solve_start_residual(mgm_ctx *c, double *geo_mean)
+{
+    return guard([&] {
+        check_ctx(c);
+        MGM_REQUIRE(c->setup_done && c->fg.p && geo_mean, "mgm_solve_start_residual: not set up");
+        const FgState &h = read_fg_head(c);
+        *geo_mean = h.solves_total > 0 ? std::pow(10.0, h.start_log_relres / (double)h.solves_total) : 0.0;
+    });
+}
+
 int mgm_set_initial_guess(mgm_ctx *c, int flags)
 {
     return guard([&] {

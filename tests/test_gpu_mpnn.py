@@ -125,7 +125,7 @@ def test_training_and_warm_start(stable):
     held = C.c_double()
     _lib.check(L.mgm_mpnn_eval(mg.h, cnt.value - steps_ep, steps_ep, C.byref(held)))
     assert np.isfinite(held.value)
-    res, ps = {}, {}
+    res, ps, start = {}, {}, {}
     for name, flags in (("previous", 0), ("extrapolated", mgm.GUESS_EXTRAPOLATE),
                         ("learned", mgm.GUESS_EXTRAPOLATE | mgm.GUESS_LEARNED)):
         mg.set_initial_guess(flags)
@@ -135,9 +135,15 @@ def test_training_and_warm_start(stable):
         it, rr = mg.last_solve()
         assert rr < 1e-8
         res[name] = vc
+        start[name] = mg.solve_start_residual()
         ps[name] = mg.get_field("p")
     mg.set_initial_guess(0)
-    print("V-cycles over 25 held-out steps:", res)
+    print("V-cycles over 25 held-out steps:", res, "starting residuals:", start)
+    # the minimal-residual combination never starts further from the answer
+    # than its directions' span without the network (up to the trajectories'
+    # 1e-8-level differences between the arms)
+    assert start["extrapolated"] < start["previous"], start
+    assert start["learned"] <= 1.05 * start["extrapolated"], start
     assert res["learned"] < res["previous"], res
     assert res["learned"] <= res["extrapolated"] + 1, res
     for name in ("extrapolated", "learned"):
